@@ -1,0 +1,171 @@
+/*
+ * pdac_gpu.h -- C ABI of the B200 (sm_100a) PDAC time-step engine.
+ *
+ * The engine replaces the argument-less Fortran module procedures that
+ * PDAC's time loop calls (prog.f:162-331 of the reference) with calls on an
+ * opaque context that owns one device-resident domain.  Every entry point
+ * returns an int status (PDAC_OK = 0, see the codes below); nothing in these
+ * signatures is a torch or CUDA type, so a Fortran (ISO_C_BINDING), C, C++
+ * or Python ctypes caller binds them directly.
+ *
+ * Layout of every host array exchanged through this header is the
+ * reference's: one flat index ijk = i + nx*(j + ny*k) (0-based, i fastest;
+ * j absent in 2D), per-solid arrays (ncell, nsolid) column-major -- i.e.
+ * solid class slowest -- and per-gas arrays (ncell, ngas) likewise
+ * (press.f:2-28, velocity.f:2-38, dens.f:2-29, temp.f:2-30, eosg.f:11-17).
+ * All cells, including the one-cell boundary frame, are stored.
+ */
+#ifndef PDAC_GPU_H
+#define PDAC_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (comm/error.F:1-59 aborts; here they are returned) --- */
+#define PDAC_OK                 0
+#define PDAC_ERR_CONFIG         1   /* unsupported or inconsistent cfg        */
+#define PDAC_ERR_CUDA           2   /* CUDA runtime error                     */
+#define PDAC_ERR_MAXOUT         3   /* iter.f:428-450: maxout sweeps reached  */
+#define PDAC_ERR_EOS            4   /* ftem.f:191-193: caloric EOS failures   */
+#define PDAC_ERR_NONFINITE      5   /* non-finite value detected              */
+#define PDAC_ERR_ARG            6   /* bad argument (NULL, size, name)        */
+#define PDAC_ERR_BOUNDARY       7   /* inoutflow.f:99,143: rls >= 1 on a BC   */
+#define PDAC_ERR_TIMEOUT        8   /* a bounded device wait gave up          */
+
+/* ---- cell flags, grid.f:45-58 ----------------------------------------- */
+#define PDAC_FLUID        1
+#define PDAC_SLIP_WALL    2
+#define PDAC_NOSLIP_WALL  4
+#define PDAC_FREE_IO      8
+#define PDAC_INLET_CELL   16
+#define PDAC_ZERO_GRAD    32
+#define PDAC_VENT_CELL    64
+
+#define PDAC_MAX_NSOLID   8
+#define PDAC_MAX_NGAS     7
+
+/* precision modes */
+#define PDAC_PREC_FP64    0   /* every kernel in FP64                         */
+#define PDAC_PREC_MIXED   1   /* FP32 fluxes/tilde/drag/EOS, FP64 corrector   */
+
+/*
+ * Run configuration: the subset of the reference namelists (input.f:159-209,
+ * defaults input.f:219-468, derived values check_input input.f:912-1013)
+ * that the per-step path reads, plus the mesh metric and cell flags.  The
+ * pointer members are read during pdac_gpu_create only.
+ */
+typedef struct pdac_cfg {
+    int    job_type;            /* 2 = 2D (x|r, z), 3 = 3D (x, y, z)         */
+    int    nx, ny, nz;          /* cells including the boundary frame        */
+    int    itc;                 /* 1 = cylindrical (2D only)                 */
+    int    nsolid, ngas;
+    int    gas_type[PDAC_MAX_NGAS]; /* 1..7: O2 N2 CO2 H2 H2O Air SO2 (setup.f:563-571) */
+
+    /* &numeric */
+    double dt;
+    int    rungekut;
+    double alpha, alphagrav;
+    double omega, delg;
+    int    inmax, maxout;
+    int    muscl, lv, lm;       /* limiter types (limiters.f:14-56)          */
+    double beta;                /* beta-limiter parameter                    */
+    double flim;                /* invdm decoupling threshold (ftem.f:221)   */
+    int    update_eosg;
+
+    /* &model */
+    int    pmodel, drag_model, icpc;
+    double tref;
+    int    gas_viscosity, part_viscosity, repulsive_model;
+    double gravx, gravy, gravz;
+
+    /* &particles */
+    double dk[PDAC_MAX_NSOLID];     /* diameter [m]                          */
+    double rl[PDAC_MAX_NSOLID];     /* density [kg/m3]                       */
+    double phis[PDAC_MAX_NSOLID];   /* sphericity                            */
+    double cmus[PDAC_MAX_NSOLID];   /* particle viscosity [Pa s]             */
+    double cps[PDAC_MAX_NSOLID];    /* specific heat                         */
+    double kap[PDAC_MAX_NSOLID];    /* thermal conductivity                  */
+    double plim[PDAC_MAX_NSOLID];   /* twophase_limit (matrix.f:355)         */
+
+    /* &atmosphere: inflow state for free in/out boundaries */
+    double void_fraction;
+    double atm_ygc[PDAC_MAX_NGAS];  /* indexed by reference gas type - 1     */
+
+    /* &inlet: vent velocity fluctuations (vent.f:902-936) */
+    int    irand;
+
+    int    precision;               /* PDAC_PREC_FP64 / PDAC_PREC_MIXED      */
+
+    /* mesh metric and flags (read at create) */
+    const double *dx, *dy, *dz;     /* nx, ny, nz cell sizes                 */
+    const int    *flag;             /* ncell flags                           */
+    const double *p_atm, *t_atm;    /* nz hydrostatic profile (atmosphere.f:160-230) */
+    int           nvent;            /* number of vent cells                  */
+    const int    *vent_ijk;         /* nvent flat indices of vent cells      */
+} pdac_cfg;
+
+/*
+ * Prognostic state, host pointers in the reference layout.  Members may be
+ * NULL in a download call to skip that field; upload requires all fields
+ * except the 3D-only ones in 2D (vg, vs).
+ */
+typedef struct pdac_state_view {
+    double *p, *ep, *rog, *rgp, *tg, *sieg, *cg;   /* ncell                  */
+    double *ug, *vg, *wg;                          /* ncell (face E, N, T)   */
+    double *rlk, *ts, *sies;                       /* ncell * nsolid         */
+    double *us, *vs, *ws;                          /* ncell * nsolid         */
+    double *ygc, *xgc;                             /* ncell * ngas           */
+} pdac_state_view;
+
+typedef struct pdac_ctx pdac_ctx;
+
+/* ---- lifecycle -------------------------------------------------------- */
+/* replaces the allocate_* calls of pdac.f:126-131,249-261 */
+int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out);
+int pdac_gpu_destroy(pdac_ctx *ctx);
+/* human-readable text of the last error on this context */
+const char *pdac_gpu_last_error(const pdac_ctx *ctx);
+
+/* ---- state transfer ---------------------------------------------------- */
+int pdac_gpu_upload_state(pdac_ctx *ctx, const pdac_state_view *s);
+int pdac_gpu_download_state(pdac_ctx *ctx, pdac_state_view *s);
+
+/* ---- per-call mirrors of the time loop (prog.f:143-417) --------------- */
+/* boundary (bdry.f:22-726) at time-step number 'sweep' (1-based)          */
+int pdac_gpu_boundary(pdac_ctx *ctx, int sweep);
+/* fieldn (tilde.f:125-274) incl. viscon (visc.f:37-148)                   */
+int pdac_gpu_fieldn(pdac_ctx *ctx);
+/* tilde (tilde.f:276-848): fluxes, stresses, drag, interphase matrix      */
+int pdac_gpu_tilde(pdac_ctx *ctx, double dt);
+/* iter (iter.f:38-477); *nit receives the number of outer sweeps          */
+int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit);
+/* ygas (ygas.f:27-156)                                                    */
+int pdac_gpu_ygas(pdac_ctx *ctx, double dt);
+/* htilde (htilde.f:25-178)                                                */
+int pdac_gpu_htilde(pdac_ctx *ctx, double dt);
+/* ftem (ftem.f:19-199)                                                    */
+int pdac_gpu_ftem(pdac_ctx *ctx, double dt);
+/* one whole time step: boundary, fieldn, RK loop of tilde/iter/ygas/htilde/ftem */
+int pdac_gpu_step(pdac_ctx *ctx, int sweep, int *nit);
+
+/* vent fluctuation factors for the next boundary call, one per vent cell in
+ * cfg->vent_ijk order (vent.f:824-873 random_switch draws them in 3D).     */
+int pdac_gpu_set_vent_factors(pdac_ctx *ctx, const double *fact, int nvent);
+
+/* ---- diagnostics ------------------------------------------------------- */
+/* Copy one named device array (state or intermediate, e.g. "rug", "appu",
+ * "rgfe") into host memory; *n_inout holds the capacity in doubles on entry
+ * and the element count on return.  Test and debugging aid.               */
+int pdac_gpu_get_array(pdac_ctx *ctx, const char *name, double *out, long *n_inout);
+/* Mass totals over fluid cells (residuals.f:14-130): out[0] = gas mass,
+ * out[1..nsolid] = per-class solid mass, out[1+nsolid ..] = per-gas mass.  */
+int pdac_gpu_mass_totals(pdac_ctx *ctx, double *out, int nout);
+/* device time (ms) of the kernels of the last call, by phase:
+ * [boundary, fieldn, tilde, iter, ygas, htilde, ftem]                    */
+int pdac_gpu_phase_times(pdac_ctx *ctx, double *ms7);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PDAC_GPU_H */

@@ -1,0 +1,63 @@
+// common.cuh -- shared definitions of the B200 PDAC engine (sm_100a).
+//
+// Data layout in HBM: one flat index c = i0 + nx*(j0 + ny*k0) over all
+// cells including the one-cell boundary frame (the reference's ijk order,
+// i fastest), structure-of-arrays, one contiguous array per field; per-solid
+// and per-gas fields are (ncell, n) column-major, i.e. class-major blocks of
+// ncell values.  Mesh metric arrays are 1-based with padding so that device
+// formulas use the reference's indices (dx(i-1), dx(i+2) ...) unchanged.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define PDAC_MAXS 8          // max solid classes
+#define PDAC_MAXP (PDAC_MAXS + 1)
+#define PDAC_MAXG 7
+
+namespace pdac {
+
+// cell flags, grid.f:45-58
+enum : int { FLUID = 1, SLIP = 2, NOSLIP = 4, BL_CELL = 5, FREE_IO = 8, INLET = 16, ZERO_GRAD = 32,
+             VENT = 64, DOME = 129, IMMB = 257, FILLED1 = 512, FILLED2 = 1024 };
+
+// Scalar run parameters, passed by value to every kernel.
+struct Prm {
+    int nx, ny, nz, ncell, ns, ng, nph, nap;
+    int itc, muscl, lv, lm, pmodel, drag_model, icpc;
+    int gas_viscosity, part_viscosity, repulsive_model, inmax;
+    int gas_type[PDAC_MAXG];
+    double alpha, alphagrav, omega, delg, beta, flim, tref;
+    double gravx, gravy, gravz, void_fraction;
+    double atm_ygc[PDAC_MAXG];
+    double gmw[8], mmugs[8], mmugek[8];
+    double rgas, gammaair;
+    double dk[PDAC_MAXP], rl[PDAC_MAXP], inrl[PDAC_MAXP], phis[PDAC_MAXP], cmus[PDAC_MAXP];
+    double cps[PDAC_MAXP], kap[PDAC_MAXP], plim[PDAC_MAXP], phi[PDAC_MAXP];
+    double philim[PDAC_MAXP][PDAC_MAXP], epsl[PDAC_MAXP][PDAC_MAXP], epsu[PDAC_MAXP][PDAC_MAXP];
+    double dkf[PDAC_MAXP][PDAC_MAXP];
+    // device metric, 1-based padded
+    const double *dx, *dy, *dz, *indx, *indy, *indz, *r, *rb, *inr, *inrb;
+    const double *p_atm, *t_atm;
+    const int *flag;
+};
+
+// Device pointers of every field (state, n-level, tilde, fluxes, solver).
+struct Fld {
+    double *p, *ep, *rog, *rgp, *tg, *sieg, *cg, *ug, *vg, *wg;
+    double *rlk, *ts, *sies, *us, *vs, *ws, *ygc, *xgc;
+    double *pn, *epn, *rgpn, *siegn, *rlkn, *siesn, *rgpgcn, *mug, *kapg;
+    double *rugn, *rwgn, *rusn, *rwsn;
+    double *rug, *rwg, *rus, *rws, *appu, *appw;
+    double *ugfe, *ugft, *wgfe, *wgft, *usfe, *usft, *wsfe, *wsft;
+    double *rgfe, *rgft, *rsfe, *rsft, *conv, *abeta;
+    double *egfe, *egft, *esfe, *esft, *rhg, *rhs;
+    double *yfe, *yft;
+    double *sink;
+    int *counters;  // [0] non-converged cells this sweep, [1] eos failures, [2] rls>1 cells, [3] boundary errors
+};
+
+__host__ __device__ inline bool is_wall(int f) { return f == SLIP || f == NOSLIP; }
+__host__ __device__ inline bool is_wallf(int f) { return f == SLIP || f == NOSLIP || f == FILLED1; }
+__host__ __device__ inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+}  // namespace pdac

@@ -1,0 +1,497 @@
+// engine.cu -- host side of the B200 PDAC engine: context, device memory,
+// kernel orchestration and the C ABI of include/pdac_gpu.h.
+//
+// One context owns one device-resident domain on the current CUDA device and
+// one stream; every entry point enqueues work on that stream and returns a
+// status.  The outer corrector sweeps of iter run as three colour-phase
+// launches; the host reads the non-converged count after each sweep (the
+// reference's parallel_sum_integer(mustit), iter.f:388).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+#include "../../include/pdac_gpu.h"
+#include "kernels2d.cuh"
+
+using namespace pdac;
+
+struct pdac_ctx {
+    pdac_cfg cfg;
+    Prm P;
+    Fld F;
+    int nx = 0, ny = 1, nz = 0, ncell = 0, ns = 0, ng = 0, nph = 0, nap = 0;
+    bool d3 = false;
+    cudaStream_t stream = nullptr;
+    double *arena = nullptr;
+    size_t arena_doubles = 0;
+    double *metric = nullptr;
+    int *d_flag = nullptr, *d_vent = nullptr, *d_counters = nullptr, *h_counters = nullptr;
+    double *d_vfact = nullptr, *d_vfact0 = nullptr;
+    double *d_app0u = nullptr, *d_app0w = nullptr;
+    double *d_partial = nullptr;
+    int nvent = 0;
+    std::string err;
+    cudaEvent_t ev[16];
+    float phase_ms[7] = {0};
+    std::vector<std::pair<std::string, std::pair<double *, size_t>>> names;
+};
+
+namespace {
+
+const int TPB = 128;
+
+int fail(pdac_ctx *c, int code, const std::string &msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+#define CK(x)                                                                                  \
+    do {                                                                                       \
+        cudaError_t e_ = (x);                                                                  \
+        if (e_ != cudaSuccess) return fail(ctx, PDAC_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+inline int blocks(long n) { return (int)((n + TPB - 1) / TPB); }
+
+// setup.f:551-616 and particles.f:35-79: gas and particle constants
+void set_constants(pdac_ctx *ctx) {
+    Prm &P = ctx->P;
+    const pdac_cfg &c = ctx->cfg;
+    double g[8] = {0, 32.0, 28.0, 44.0, 2.0, 18.0, 28.96442, 64.0};
+    double s[8] = {0, 3.467, 3.798, 3.941, 2.827, 2.641, 3.711, 4.112};
+    double e[8] = {0, 106.7, 71.4, 195.2, 59.7, 809.1, 78.6, 335.4};
+    for (int q = 0; q < 8; ++q) { P.gmw[q] = g[q] * 1.0e-3; P.mmugs[q] = s[q]; P.mmugek[q] = e[q]; }
+    P.rgas = 8.31432;
+    P.gammaair = 1.4;
+    for (int is = 1; is <= ctx->ns; ++is) {
+        P.dk[is] = c.dk[is - 1];
+        P.rl[is] = c.rl[is - 1];
+        P.inrl[is] = 1.0 / P.rl[is];
+        P.phis[is] = c.phis[is - 1];
+        P.cmus[is] = c.cmus[is - 1];
+        P.cps[is] = c.cps[is - 1];
+        P.kap[is] = c.kap[is - 1];
+        P.plim[is] = c.plim[is - 1];
+        P.phi[is] = (double)0.63f;
+    }
+    for (int k = 1; k <= ctx->ns; ++k)
+        for (int kk = 1; kk <= ctx->ns; ++kk) {
+            int k1, k2;
+            if (P.dk[k] >= P.dk[kk]) { k1 = k; k2 = kk; }
+            else { k1 = kk; k2 = k; }
+            double a = std::sqrt(P.dk[k2] / P.dk[k1]);
+            P.philim[k][kk] = P.phi[k1] / (P.phi[k1] + (1.0 - P.phi[k1]) * P.phi[k2]);
+            P.epsl[k][kk] = (P.phi[k1] - P.phi[k2]) + ((1.0 - a) * (1.0 - P.phi[k1]) * P.phi[k2]);
+            double fact = (P.phi[k1] + (1.0 - P.phi[k2]) * P.phi[k1]) / P.phi[k1];
+            P.epsl[k][kk] = P.epsl[k][kk] * fact;
+            P.epsu[k][kk] = (1.0 - a) * (P.phi[k1] + (1.0 - P.phi[k1]) * P.phi[k2]);
+            double s2 = P.dk[k] + P.dk[kk];
+            P.dkf[k][kk] = s2 * s2 / (P.rl[k] * P.dk[k] * P.dk[k] * P.dk[k] + P.rl[kk] * P.dk[kk] * P.dk[kk] * P.dk[kk]);
+            P.dkf[kk][k] = P.dkf[k][kk];
+        }
+}
+
+int validate(const pdac_cfg *c, std::string &why) {
+    if (c->job_type != 2) { why = "only job_type 2 (2D) is built in this engine"; return 1; }
+    if (c->nx < 5 || c->nz < 5) { why = "nx and nz must be >= 5"; return 1; }
+    if (c->nsolid < 1 || c->nsolid > PDAC_MAX_NSOLID) { why = "nsolid out of range"; return 1; }
+    if (c->ngas < 1 || c->ngas > PDAC_MAX_NGAS) { why = "ngas out of range"; return 1; }
+    for (int ig = 0; ig < c->ngas; ++ig)
+        if (c->gas_type[ig] < 1 || c->gas_type[ig] > 7) { why = "gas_type out of range"; return 1; }
+    if (c->inmax < 1 || c->maxout < 1) { why = "inmax and maxout must be >= 1"; return 1; }
+    if (c->rungekut < 1) { why = "rungekut must be >= 1"; return 1; }
+    if (!c->dx || !c->dz || !c->flag || !c->p_atm || !c->t_atm) { why = "metric, flag or atmosphere pointer is NULL"; return 1; }
+    if (c->nvent > 0 && !c->vent_ijk) { why = "vent_ijk is NULL"; return 1; }
+    if (c->precision != PDAC_PREC_FP64) { why = "only PDAC_PREC_FP64 is built"; return 1; }
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *pdac_gpu_last_error(const pdac_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
+    if (!cfg || !out) return PDAC_ERR_ARG;
+    *out = nullptr;
+    std::string why;
+    if (validate(cfg, why)) {
+        fprintf(stderr, "pdac_gpu_create: %s\n", why.c_str());
+        return PDAC_ERR_CONFIG;
+    }
+    pdac_ctx *ctx = new pdac_ctx();
+    ctx->cfg = *cfg;
+    ctx->d3 = false;
+    ctx->nx = cfg->nx; ctx->ny = 1; ctx->nz = cfg->nz;
+    ctx->ncell = ctx->nx * ctx->ny * ctx->nz;
+    ctx->ns = cfg->nsolid; ctx->ng = cfg->ngas; ctx->nph = ctx->ns + 1; ctx->nap = ctx->nph * (ctx->nph + 1) / 2;
+    int n = ctx->ncell, ns = ctx->ns, ng = ctx->ng, nap = ctx->nap;
+    Prm &P = ctx->P;
+    std::memset(&P, 0, sizeof(P));
+    P.nx = ctx->nx; P.ny = 1; P.nz = ctx->nz; P.ncell = n; P.ns = ns; P.ng = ng; P.nph = ctx->nph; P.nap = nap;
+    P.itc = cfg->itc; P.muscl = cfg->muscl; P.lv = cfg->lv; P.lm = cfg->lm; P.pmodel = cfg->pmodel;
+    P.drag_model = cfg->drag_model; P.icpc = cfg->icpc; P.gas_viscosity = cfg->gas_viscosity;
+    P.part_viscosity = cfg->part_viscosity; P.repulsive_model = cfg->repulsive_model; P.inmax = cfg->inmax;
+    for (int ig = 0; ig < ng; ++ig) P.gas_type[ig] = cfg->gas_type[ig];
+    P.alpha = cfg->alpha; P.alphagrav = cfg->alphagrav; P.omega = cfg->omega; P.delg = cfg->delg;
+    P.beta = cfg->beta; P.flim = cfg->flim; P.tref = cfg->tref;
+    P.gravx = cfg->gravx; P.gravy = cfg->gravy; P.gravz = cfg->gravz; P.void_fraction = cfg->void_fraction;
+    for (int g = 0; g < PDAC_MAX_NGAS; ++g) P.atm_ygc[g] = cfg->atm_ygc[g];
+    set_constants(ctx);
+
+    // host metric, 1-based padded, grid.f:306-345
+    int nx = ctx->nx, nz = ctx->nz;
+    std::vector<double> dx(nx + 4), dz(nz + 4), indx(nx + 4), indz(nz + 4), r(nx + 4, 1.0), rb(nx + 4, 1.0),
+        inr(nx + 4, 1.0), inrb(nx + 4, 1.0), patm(nz + 2, 0.0), tatm(nz + 2, 0.0), dy(4, 0.0), indy(4, 0.0);
+    for (int i = 1; i <= nx; ++i) dx[i] = cfg->dx[i - 1];
+    dx[0] = dx[1]; dx[nx + 1] = dx[nx + 2] = dx[nx + 3] = dx[nx];
+    for (int k = 1; k <= nz; ++k) dz[k] = cfg->dz[k - 1];
+    dz[0] = dz[1]; dz[nz + 1] = dz[nz + 2] = dz[nz + 3] = dz[nz];
+    for (int i = 0; i < nx + 4; ++i) indx[i] = 1.0 / dx[i];
+    for (int k = 0; k < nz + 4; ++k) indz[k] = 1.0 / dz[k];
+    if (cfg->itc == 1) {
+        std::vector<double> xb(nx + 4, 0.0), x(nx + 4, 0.0);
+        xb[1] = 0.0; x[1] = -0.5 * dx[1] + xb[1];
+        for (int i = 2; i <= nx; ++i) { xb[i] = (xb[i - 1] + dx[i]); x[i] = (xb[i] - 0.5 * dx[i]); }
+        for (int i = 1; i <= nx; ++i) { r[i] = x[i]; rb[i] = xb[i]; }
+        rb[0] = rb[1] - dx[1];
+        inrb[1] = (rb[1] == 0.0) ? 1.0e10 : 1.0 / rb[1];
+        for (int i = 2; i <= nx; ++i) inrb[i] = 1.0 / rb[i];
+        for (int i = 1; i <= nx; ++i) inr[i] = 1.0 / r[i];
+    }
+    for (int k = 1; k <= nz; ++k) { patm[k] = cfg->p_atm[k - 1]; tatm[k] = cfg->t_atm[k - 1]; }
+
+    CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    for (auto &e : ctx->ev) CK(cudaEventCreate(&e));
+    std::vector<std::vector<double> *> mets = {&dx, &dy, &dz, &indx, &indy, &indz, &r, &rb, &inr, &inrb, &patm, &tatm};
+    size_t mtot = 0;
+    for (auto *v : mets) mtot += v->size();
+    CK(cudaMalloc(&ctx->metric, mtot * sizeof(double)));
+    size_t off = 0;
+    std::vector<const double *> mp;
+    for (auto *v : mets) {
+        CK(cudaMemcpy(ctx->metric + off, v->data(), v->size() * sizeof(double), cudaMemcpyHostToDevice));
+        mp.push_back(ctx->metric + off);
+        off += v->size();
+    }
+    P.dx = mp[0]; P.dy = mp[1]; P.dz = mp[2]; P.indx = mp[3]; P.indy = mp[4]; P.indz = mp[5];
+    P.r = mp[6]; P.rb = mp[7]; P.inr = mp[8]; P.inrb = mp[9]; P.p_atm = mp[10]; P.t_atm = mp[11];
+    CK(cudaMalloc(&ctx->d_flag, n * sizeof(int)));
+    CK(cudaMemcpy(ctx->d_flag, cfg->flag, n * sizeof(int), cudaMemcpyHostToDevice));
+    P.flag = ctx->d_flag;
+    ctx->nvent = cfg->nvent;
+    int nv = std::max(1, cfg->nvent);
+    CK(cudaMalloc(&ctx->d_vent, nv * sizeof(int)));
+    CK(cudaMalloc(&ctx->d_vfact, nv * sizeof(double)));
+    CK(cudaMalloc(&ctx->d_vfact0, nv * sizeof(double)));
+    if (cfg->nvent > 0) {
+        CK(cudaMemcpy(ctx->d_vent, cfg->vent_ijk, cfg->nvent * sizeof(int), cudaMemcpyHostToDevice));
+        // vent.f:176-178 initialises fact = 1 and fact0 = 0; random_switch
+        // (vent.f:824-873) redraws fact only in 3D
+        std::vector<double> one(cfg->nvent, 1.0), zero(cfg->nvent, 0.0);
+        CK(cudaMemcpy(ctx->d_vfact, one.data(), cfg->nvent * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(ctx->d_vfact0, zero.data(), cfg->nvent * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    CK(cudaMalloc(&ctx->d_counters, 8 * sizeof(int)));
+    CK(cudaMemset(ctx->d_counters, 0, 8 * sizeof(int)));
+    CK(cudaMallocHost(&ctx->h_counters, 8 * sizeof(int)));
+
+    // field arena: (name, number of ncell blocks)
+    Fld &F = ctx->F;
+    struct Slot { const char *name; double **ptr; int blocks; };
+    std::vector<Slot> slots = {
+        {"p", &F.p, 1}, {"ep", &F.ep, 1}, {"rog", &F.rog, 1}, {"rgp", &F.rgp, 1}, {"tg", &F.tg, 1},
+        {"sieg", &F.sieg, 1}, {"cg", &F.cg, 1}, {"ug", &F.ug, 1}, {"vg", &F.vg, 1}, {"wg", &F.wg, 1},
+        {"rlk", &F.rlk, ns}, {"ts", &F.ts, ns}, {"sies", &F.sies, ns}, {"us", &F.us, ns}, {"vs", &F.vs, ns},
+        {"ws", &F.ws, ns}, {"ygc", &F.ygc, ng}, {"xgc", &F.xgc, ng},
+        {"pn", &F.pn, 1}, {"epn", &F.epn, 1}, {"rgpn", &F.rgpn, 1}, {"siegn", &F.siegn, 1},
+        {"rlkn", &F.rlkn, ns}, {"siesn", &F.siesn, ns}, {"rgpgcn", &F.rgpgcn, ng}, {"mug", &F.mug, 1},
+        {"kapg", &F.kapg, 1}, {"rugn", &F.rugn, 1}, {"rwgn", &F.rwgn, 1}, {"rusn", &F.rusn, ns},
+        {"rwsn", &F.rwsn, ns}, {"rug", &F.rug, 1}, {"rwg", &F.rwg, 1}, {"rus", &F.rus, ns},
+        {"rws", &F.rws, ns}, {"appu", &F.appu, nap}, {"appw", &F.appw, nap},
+        {"ugfe", &F.ugfe, 1}, {"ugft", &F.ugft, 1}, {"wgfe", &F.wgfe, 1}, {"wgft", &F.wgft, 1},
+        {"usfe", &F.usfe, ns}, {"usft", &F.usft, ns}, {"wsfe", &F.wsfe, ns}, {"wsft", &F.wsft, ns},
+        {"rgfe", &F.rgfe, 1}, {"rgft", &F.rgft, 1}, {"rsfe", &F.rsfe, ns}, {"rsft", &F.rsft, ns},
+        {"conv", &F.conv, 1}, {"abeta", &F.abeta, 1}, {"egfe", &F.egfe, 1}, {"egft", &F.egft, 1},
+        {"esfe", &F.esfe, ns}, {"esft", &F.esft, ns}, {"rhg", &F.rhg, 1}, {"rhs", &F.rhs, ns},
+        {"yfe", &F.yfe, ng}, {"yft", &F.yft, ng}, {"sink", &F.sink, ns},
+        {"app0u", &ctx->d_app0u, nap}, {"app0w", &ctx->d_app0w, nap}};
+    // each field starts on a 256-byte boundary
+    size_t stride = ((size_t)n + 31) / 32 * 32;
+    size_t total = 0;
+    for (auto &s : slots) total += stride * s.blocks;
+    ctx->arena_doubles = total;
+    CK(cudaMalloc(&ctx->arena, total * sizeof(double)));
+    CK(cudaMemset(ctx->arena, 0, total * sizeof(double)));
+    size_t o2 = 0;
+    for (auto &s : slots) {
+        *s.ptr = ctx->arena + o2;
+        ctx->names.push_back({s.name, {*s.ptr, (size_t)n * s.blocks}});
+        o2 += stride * s.blocks;
+    }
+    // per-class blocks inside a slot are exactly ncell apart, as the
+    // reference's (ncell, n) column-major arrays; the stride pads slot ends
+    F.counters = ctx->d_counters;
+    int nq = 1 + ns + ng;
+    CK(cudaMalloc(&ctx->d_partial, (size_t)nq * 1024 * sizeof(double)));
+    *out = ctx;
+    return PDAC_OK;
+}
+
+int pdac_gpu_destroy(pdac_ctx *ctx) {
+    if (!ctx) return PDAC_ERR_ARG;
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(ctx->arena);
+    cudaFree(ctx->metric);
+    cudaFree(ctx->d_flag);
+    cudaFree(ctx->d_vent);
+    cudaFree(ctx->d_vfact);
+    cudaFree(ctx->d_vfact0);
+    cudaFree(ctx->d_counters);
+    cudaFree(ctx->d_partial);
+    cudaFreeHost(ctx->h_counters);
+    for (auto &e : ctx->ev) cudaEventDestroy(e);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return PDAC_OK;
+}
+
+static int xfer_state(pdac_ctx *ctx, pdac_state_view *s, bool up) {
+    if (!ctx || !s) return PDAC_ERR_ARG;
+    size_t n = ctx->ncell, ns = ctx->ns, ng = ctx->ng;
+    Fld &F = ctx->F;
+    struct X { double *h; double *d; size_t cnt; bool need; };
+    X xs[] = {{s->p, F.p, n, true}, {s->ep, F.ep, n, true}, {s->rog, F.rog, n, true}, {s->rgp, F.rgp, n, true},
+              {s->tg, F.tg, n, true}, {s->sieg, F.sieg, n, true}, {s->cg, F.cg, n, true},
+              {s->ug, F.ug, n, true}, {s->vg, F.vg, n, false}, {s->wg, F.wg, n, true},
+              {s->rlk, F.rlk, n * ns, true}, {s->ts, F.ts, n * ns, true}, {s->sies, F.sies, n * ns, true},
+              {s->us, F.us, n * ns, true}, {s->vs, F.vs, n * ns, false}, {s->ws, F.ws, n * ns, true},
+              {s->ygc, F.ygc, n * ng, true}, {s->xgc, F.xgc, n * ng, true}};
+    for (auto &x : xs) {
+        if (!x.h) {
+            if (up && x.need) return fail(ctx, PDAC_ERR_ARG, "upload: a required state field is NULL");
+            continue;
+        }
+        if (up) CK(cudaMemcpyAsync(x.d, x.h, x.cnt * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        else CK(cudaMemcpyAsync(x.h, x.d, x.cnt * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return PDAC_OK;
+}
+
+int pdac_gpu_upload_state(pdac_ctx *ctx, const pdac_state_view *s) { return xfer_state(ctx, const_cast<pdac_state_view *>(s), true); }
+int pdac_gpu_download_state(pdac_ctx *ctx, pdac_state_view *s) { return xfer_state(ctx, s, false); }
+
+int pdac_gpu_boundary(pdac_ctx *ctx, int sweep) {
+    if (!ctx) return PDAC_ERR_ARG;
+    (void)sweep;
+    cudaStream_t st = ctx->stream;
+    CK(cudaEventRecord(ctx->ev[0], st));
+    if (ctx->nvent > 0 && ctx->cfg.irand >= 1)
+        pdac::k_vent<<<blocks(ctx->nvent), TPB, 0, st>>>(ctx->P, ctx->F, ctx->d_vent, ctx->nvent, ctx->d_vfact, ctx->d_vfact0);
+    pdac::k_boundary2d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev[1], st));
+    return PDAC_OK;
+}
+
+int pdac_gpu_fieldn(pdac_ctx *ctx) {
+    if (!ctx) return PDAC_ERR_ARG;
+    cudaStream_t st = ctx->stream;
+    CK(cudaEventRecord(ctx->ev[2], st));
+    pdac::k_fieldn2d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F);
+    // allocate_fluxes (tilde.f:56-102): tilde and interphase terms start from
+    // zero in every step
+    size_t n = ctx->ncell;
+    Fld &F = ctx->F;
+    CK(cudaMemsetAsync(F.rug, 0, n * sizeof(double), st));
+    CK(cudaMemsetAsync(F.rwg, 0, n * sizeof(double), st));
+    CK(cudaMemsetAsync(F.rus, 0, n * ctx->ns * sizeof(double), st));
+    CK(cudaMemsetAsync(F.rws, 0, n * ctx->ns * sizeof(double), st));
+    CK(cudaMemsetAsync(F.appu, 0, n * ctx->nap * sizeof(double), st));
+    CK(cudaMemsetAsync(F.appw, 0, n * ctx->nap * sizeof(double), st));
+    CK(cudaMemsetAsync(ctx->d_app0u, 0, n * ctx->nap * sizeof(double), st));
+    CK(cudaMemsetAsync(ctx->d_app0w, 0, n * ctx->nap * sizeof(double), st));
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev[3], st));
+    return PDAC_OK;
+}
+
+int pdac_gpu_tilde(pdac_ctx *ctx, double dt) {
+    if (!ctx) return PDAC_ERR_ARG;
+    cudaStream_t st = ctx->stream;
+    size_t n = ctx->ncell, ns = ctx->ns;
+    Fld &F = ctx->F;
+    CK(cudaEventRecord(ctx->ev[4], st));
+    for (double *a : {F.ugfe, F.ugft, F.wgfe, F.wgft}) CK(cudaMemsetAsync(a, 0, n * sizeof(double), st));
+    for (double *a : {F.usfe, F.usft, F.wsfe, F.wsft}) CK(cudaMemsetAsync(a, 0, n * ns * sizeof(double), st));
+    pdac::k_tilde_flux2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F);
+    pdac::k_tilde2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt, ctx->d_app0u, ctx->d_app0w);
+    if (ctx->P.alpha != 1.0 && ctx->cfg.rungekut > 1) {
+        CK(cudaMemcpyAsync(ctx->d_app0u, F.appu, n * ctx->nap * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(ctx->d_app0w, F.appw, n * ctx->nap * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev[5], st));
+    return PDAC_OK;
+}
+
+int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
+    if (!ctx) return PDAC_ERR_ARG;
+    cudaStream_t st = ctx->stream;
+    size_t n = ctx->ncell, ns = ctx->ns;
+    Fld &F = ctx->F;
+    CK(cudaEventRecord(ctx->ev[6], st));
+    for (double *a : {F.rgfe, F.rgft, F.conv, F.abeta}) CK(cudaMemsetAsync(a, 0, n * sizeof(double), st));
+    for (double *a : {F.rsfe, F.rsft}) CK(cudaMemsetAsync(a, 0, n * ns * sizeof(double), st));
+    pdac::k_predictor2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt);
+    pdac::k_mflux_init2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt);
+    CK(cudaGetLastError());
+    int m = (ctx->nx + 2) / 3;
+    long nthr = (long)m * ctx->nz;
+    int nit;
+    for (nit = 1; nit <= ctx->cfg.maxout; ++nit) {
+        CK(cudaMemsetAsync(ctx->d_counters, 0, sizeof(int), st));
+        for (int col = 0; col < 3; ++col)
+            pdac::k_corrector2d<<<blocks(nthr), TPB, 0, st>>>(ctx->P, F, dt, col, nit);
+        CK(cudaMemcpyAsync(ctx->h_counters, ctx->d_counters, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (ctx->h_counters[0] == 0) break;
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev[7], st));
+    if (nit_out) *nit_out = nit;
+    return PDAC_OK;
+}
+
+int pdac_gpu_ygas(pdac_ctx *ctx, double dt) {
+    if (!ctx) return PDAC_ERR_ARG;
+    cudaStream_t st = ctx->stream;
+    size_t n = ctx->ncell;
+    CK(cudaEventRecord(ctx->ev[8], st));
+    if (ctx->ng == 1) {
+        std::vector<double> one(n, 1.0);
+        CK(cudaMemcpyAsync(ctx->F.ygc, one.data(), n * sizeof(double), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->F.xgc, one.data(), n * sizeof(double), cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+    } else {
+        CK(cudaMemsetAsync(ctx->F.yfe, 0, n * ctx->ng * sizeof(double), st));
+        CK(cudaMemsetAsync(ctx->F.yft, 0, n * ctx->ng * sizeof(double), st));
+        pdac::k_ygas_flux2d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F);
+        pdac::k_ygas2d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F, dt);
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev[9], st));
+    return PDAC_OK;
+}
+
+int pdac_gpu_htilde(pdac_ctx *ctx, double dt) {
+    if (!ctx) return PDAC_ERR_ARG;
+    cudaStream_t st = ctx->stream;
+    size_t n = ctx->ncell, ns = ctx->ns;
+    Fld &F = ctx->F;
+    CK(cudaEventRecord(ctx->ev[10], st));
+    CK(cudaMemsetAsync(F.egfe, 0, n * sizeof(double), st));
+    CK(cudaMemsetAsync(F.egft, 0, n * sizeof(double), st));
+    CK(cudaMemsetAsync(F.esfe, 0, n * ns * sizeof(double), st));
+    CK(cudaMemsetAsync(F.esft, 0, n * ns * sizeof(double), st));
+    pdac::k_htilde_flux2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F);
+    pdac::k_htilde2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev[11], st));
+    return PDAC_OK;
+}
+
+int pdac_gpu_ftem(pdac_ctx *ctx, double dt) {
+    if (!ctx) return PDAC_ERR_ARG;
+    cudaStream_t st = ctx->stream;
+    CK(cudaEventRecord(ctx->ev[12], st));
+    CK(cudaMemsetAsync(ctx->d_counters + 1, 0, sizeof(int), st));
+    pdac::k_ftem2d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F, dt);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev[13], st));
+    CK(cudaMemcpyAsync(ctx->h_counters + 1, ctx->d_counters + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (ctx->h_counters[1] > 1) return fail(ctx, PDAC_ERR_EOS, "ftem: caloric equation of state failed");
+    return PDAC_OK;
+}
+
+int pdac_gpu_step(pdac_ctx *ctx, int sweep, int *nit) {
+    if (!ctx) return PDAC_ERR_ARG;
+    int s;
+    if ((s = pdac_gpu_boundary(ctx, sweep))) return s;
+    if (ctx->cfg.update_eosg) return fail(ctx, PDAC_ERR_CONFIG, "update_eosg is not built");
+    if ((s = pdac_gpu_fieldn(ctx))) return s;
+    double dt0 = ctx->cfg.dt;
+    int status = PDAC_OK;
+    for (int rk = 1; rk <= ctx->cfg.rungekut; ++rk) {
+        double dt = dt0 / (ctx->cfg.rungekut + 1 - rk);
+        if ((s = pdac_gpu_tilde(ctx, dt))) return s;
+        if ((s = pdac_gpu_iter(ctx, dt, nit))) return s;
+        if ((s = pdac_gpu_ygas(ctx, dt))) return s;
+        if ((s = pdac_gpu_htilde(ctx, dt))) return s;
+        s = pdac_gpu_ftem(ctx, dt);
+        if (s == PDAC_ERR_EOS) status = s;
+        else if (s) return s;
+    }
+    return status;
+}
+
+int pdac_gpu_get_array(pdac_ctx *ctx, const char *name, double *out, long *n_inout) {
+    if (!ctx || !name || !n_inout) return PDAC_ERR_ARG;
+    for (auto &e : ctx->names) {
+        if (e.first == name) {
+            long need = (long)e.second.second;
+            if (!out || *n_inout < need) { *n_inout = need; return PDAC_ERR_ARG; }
+            CK(cudaMemcpyAsync(out, e.second.first, need * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            *n_inout = need;
+            return PDAC_OK;
+        }
+    }
+    return fail(ctx, PDAC_ERR_ARG, std::string("unknown array ") + name);
+}
+
+int pdac_gpu_mass_totals(pdac_ctx *ctx, double *out, int nout) {
+    if (!ctx || !out) return PDAC_ERR_ARG;
+    int nq = 1 + ctx->ns + ctx->ng;
+    if (nout < nq) return PDAC_ERR_ARG;
+    int nb = 148;
+    pdac::k_mass_partial<<<nb, 256, nq * 256 * sizeof(double), ctx->stream>>>(ctx->P, ctx->F, ctx->d_partial, nq);
+    CK(cudaGetLastError());
+    std::vector<double> h((size_t)nq * nb);
+    CK(cudaMemcpyAsync(h.data(), ctx->d_partial, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int q = 0; q < nq; ++q) {
+        double s = 0;
+        for (int b = 0; b < nb; ++b) s += h[(size_t)q * nb + b];
+        out[q] = s;
+    }
+    return PDAC_OK;
+}
+
+int pdac_gpu_phase_times(pdac_ctx *ctx, double *ms7) {
+    if (!ctx || !ms7) return PDAC_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int q = 0; q < 7; ++q) {
+        float t = 0;
+        if (cudaEventElapsedTime(&t, ctx->ev[2 * q], ctx->ev[2 * q + 1]) != cudaSuccess) t = 0;
+        ms7[q] = t;
+    }
+    cudaGetLastError();
+    return PDAC_OK;
+}
+
+// vent fluctuation factors for the next boundary call (random_switch, vent.f:824-873)
+int pdac_gpu_set_vent_factors(pdac_ctx *ctx, const double *fact, int nvent) {
+    if (!ctx || !fact || nvent != ctx->nvent) return PDAC_ERR_ARG;
+    CK(cudaMemcpyAsync(ctx->d_vfact, fact, nvent * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return PDAC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,161 @@
+"""Python binding of the CUDA engine (ctypes over include/pdac_gpu.h).
+
+:class:`Engine` mirrors the reference's time-loop calls (prog.f:143-417):
+``boundary``, ``fieldn``, ``tilde``, ``iter``, ``ygas``, ``htilde``,
+``ftem`` and the fused ``step``.  There is no CPU fallback: if the CUDA
+library is missing or no GPU is visible, construction raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libpdac_b200.so")
+
+_lib = None
+
+
+class PdacError(RuntimeError):
+    def __init__(self, status, where, detail=""):
+        self.status = status
+        name = abi.STATUS_NAMES.get(status, str(status))
+        super().__init__(f"{where}: {name}" + (f" ({detail})" if detail else ""))
+
+
+def lib():
+    """Load libpdac_b200.so (built in-tree by pdac_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"CUDA engine library not built: {LIB_PATH} (run python -m pdac_b200.build)")
+        L = C.CDLL(LIB_PATH)
+        P = C.c_void_p
+        L.pdac_gpu_create.argtypes = [C.POINTER(abi.PdacCfg), C.POINTER(P)]
+        L.pdac_gpu_create.restype = C.c_int
+        L.pdac_gpu_destroy.argtypes = [P]
+        L.pdac_gpu_destroy.restype = C.c_int
+        L.pdac_gpu_last_error.argtypes = [P]
+        L.pdac_gpu_last_error.restype = C.c_char_p
+        L.pdac_gpu_upload_state.argtypes = [P, C.POINTER(abi.PdacStateView)]
+        L.pdac_gpu_upload_state.restype = C.c_int
+        L.pdac_gpu_download_state.argtypes = [P, C.POINTER(abi.PdacStateView)]
+        L.pdac_gpu_download_state.restype = C.c_int
+        L.pdac_gpu_phase_times.argtypes = [P, C.POINTER(C.c_double)]
+        L.pdac_gpu_phase_times.restype = C.c_int
+        L.pdac_gpu_set_vent_factors.argtypes = [P, C.POINTER(C.c_double), C.c_int]
+        L.pdac_gpu_set_vent_factors.restype = C.c_int
+        abi.declare(L, "pdac_gpu", P)
+        _lib = L
+    return _lib
+
+
+EXPORTED = (
+    "pdac_gpu_create", "pdac_gpu_destroy", "pdac_gpu_last_error", "pdac_gpu_upload_state",
+    "pdac_gpu_download_state", "pdac_gpu_boundary", "pdac_gpu_fieldn", "pdac_gpu_tilde", "pdac_gpu_iter",
+    "pdac_gpu_ygas", "pdac_gpu_htilde", "pdac_gpu_ftem", "pdac_gpu_step", "pdac_gpu_set_vent_factors",
+    "pdac_gpu_get_array", "pdac_gpu_mass_totals", "pdac_gpu_phase_times",
+)
+
+
+class Engine:
+    """One device-resident domain set up from a :class:`~pdac_b200.setup_state.Case`."""
+
+    def __init__(self, case, upload=True):
+        self.case = case
+        self.L = lib()
+        self._cfg = case.cfg()
+        self.h = C.c_void_p()
+        st = self.L.pdac_gpu_create(C.byref(self._cfg), C.byref(self.h))
+        if st != 0:
+            raise PdacError(st, "pdac_gpu_create")
+        self.sweep = 0
+        if upload:
+            self.upload(case.state)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pdac_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, st, where):
+        if st != 0:
+            raise PdacError(st, where, (self.L.pdac_gpu_last_error(self.h) or b"").decode())
+
+    # ---- state -----------------------------------------------------------
+    def upload(self, state):
+        self._up = {k: np.ascontiguousarray(v, dtype=np.float64) for k, v in state.items()}
+        view = abi.make_state_view(self._up)
+        self._chk(self.L.pdac_gpu_upload_state(self.h, C.byref(view)), "upload_state")
+
+    def download(self):
+        out = {k: np.zeros_like(v) for k, v in self.case.state.items()}
+        view = abi.make_state_view(out)
+        self._chk(self.L.pdac_gpu_download_state(self.h, C.byref(view)), "download_state")
+        return out
+
+    def get(self, name):
+        n = C.c_long(0)
+        self.L.pdac_gpu_get_array(self.h, name.encode(), abi.dptr(None), C.byref(n))
+        if n.value <= 0:
+            raise KeyError(name)
+        buf = np.zeros(n.value)
+        self._chk(self.L.pdac_gpu_get_array(self.h, name.encode(), abi.dptr(buf), C.byref(n)), f"get_array({name})")
+        return buf
+
+    # ---- time-loop calls ---------------------------------------------------
+    def boundary(self, sweep):
+        self._chk(self.L.pdac_gpu_boundary(self.h, sweep), "boundary")
+
+    def fieldn(self):
+        self._chk(self.L.pdac_gpu_fieldn(self.h), "fieldn")
+
+    def tilde(self, dt):
+        self._chk(self.L.pdac_gpu_tilde(self.h, dt), "tilde")
+
+    def iter(self, dt):
+        nit = C.c_int(0)
+        self._chk(self.L.pdac_gpu_iter(self.h, dt, C.byref(nit)), "iter")
+        return nit.value
+
+    def ygas(self, dt):
+        self._chk(self.L.pdac_gpu_ygas(self.h, dt), "ygas")
+
+    def htilde(self, dt):
+        self._chk(self.L.pdac_gpu_htilde(self.h, dt), "htilde")
+
+    def ftem(self, dt):
+        self._chk(self.L.pdac_gpu_ftem(self.h, dt), "ftem")
+
+    def step(self, sweep=None):
+        if sweep is None:
+            sweep = self.sweep + 1
+        self.sweep = sweep
+        nit = C.c_int(0)
+        self._chk(self.L.pdac_gpu_step(self.h, sweep, C.byref(nit)), "step")
+        return nit.value
+
+    def set_vent_factors(self, fact):
+        fact = np.ascontiguousarray(fact, dtype=np.float64)
+        self._chk(self.L.pdac_gpu_set_vent_factors(self.h, abi.dptr(fact), len(fact)), "set_vent_factors")
+
+    def mass_totals(self):
+        n = 1 + self.case.nsolid + self.case.ngas
+        out = np.zeros(n)
+        self._chk(self.L.pdac_gpu_mass_totals(self.h, abi.dptr(out), n), "mass_totals")
+        return out
+
+    def phase_times(self):
+        out = (C.c_double * 7)()
+        self._chk(self.L.pdac_gpu_phase_times(self.h, out), "phase_times")
+        return dict(zip(("boundary", "fieldn", "tilde", "iter", "ygas", "htilde", "ftem"), list(out)))

@@ -1,0 +1,439 @@
+"""Host-side run set-up: mesh, cell flags, atmosphere, vent and initial state.
+
+This is the once-per-run part of PDAC that precedes the time loop
+(pdac.f:108-281).  It is host logic, restated in numpy from:
+  grid_setup / flic        grid.f:206-483
+  set_atmosphere           atmosphere.f:81-142, compute_profile :150-230,
+                           hydrostatic :240-264
+  locate_vent_2D           vent.f:130-246
+  set_atmc / specified_flow / cnvert / set_ventc
+                           setup.f:204-275, 397-498, 280-390; vent.f:443-581
+The result is a :class:`Case` holding the metric, flags, hydrostatic
+profile, vent cell list and an initial :class:`State` in the reference
+layout, plus the ``pdac_cfg`` structure for the C ABI.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import abi
+from .deck import Deck, MAX_NGAS
+
+# cell flags, grid.f:45-58
+FLUID, SLIP, NOSLIP, FREE_IO, INLET, ZERO_GRAD, VENT = 1, 2, 4, 8, 16, 32, 64
+
+# setup.f:563-571 (g/mol) and 608
+GMW = np.array([32.0, 28.0, 44.0, 2.0, 18.0, 28.96442, 64.0]) * 1.0e-3
+RGAS = 8.31432
+
+
+def hcapg(tg, icpc=2, tref=298.0):
+    """Per-species specific heats [J/(kg K)], hcapgs.f:33-85 (vectorised)."""
+    t1 = np.full_like(np.asarray(tg, dtype=np.float64), tref) if icpc <= 1 else np.asarray(tg, dtype=np.float64)
+    t2 = t1 * t1
+    t3 = t1 * t2
+    cp = np.stack([
+        (2.811e1 - 3.68e-6 * t1 + 1.746e-5 * t2 - 1.065e-8 * t3),
+        (3.115e1 - 1.357e-2 * t1 + 2.680e-5 * t2 - 1.168e-8 * t3),
+        (1.980e1 + 7.344e-2 * t1 - 5.602e-5 * t2 + 1.715e-8 * t3),
+        (2.714e1 + 9.274e-3 * t1 - 1.381e-5 * t2 + 7.645e-9 * t3),
+        (3.224e1 + 1.924e-3 * t1 + 1.055e-5 * t2 - 3.596e-9 * t3),
+        (3.0413e1 - 1.059e-2 * t1 + 2.458e-5 * t2 - 1.135e-8 * t3),
+        (2.385e1 + 6.699e-2 * t1 - 4.961e-5 * t2 + 1.328e-8 * t3)])
+    cp = cp / GMW.reshape((7,) + (1,) * t1.ndim)
+    if icpc == 0:
+        cp[4] = 1810.0
+        cp[5] = 1004.0
+    return cp
+
+
+def mole(ygc, gas_type):
+    """Mass to molar fractions, eosg.f:38-68; ygc has shape (ngas, ...)."""
+    g = GMW[np.asarray(gas_type) - 1].reshape((-1,) + (1,) * (ygc.ndim - 1))
+    mol = np.zeros(ygc.shape[1:])
+    for ig in range(ygc.shape[0]):
+        mol = mol + ygc[ig] / g[ig]
+    molinv = np.where(np.abs(mol) <= 1e-10, 0.0, 1.0 / np.where(mol == 0, 1.0, mol))
+    return np.stack([ygc[ig] / g[ig] * molinv for ig in range(ygc.shape[0])])
+
+
+def thermal_eosg(tg, p, xgc, gas_type):
+    """Ideal-gas density, eosg.f:114-137."""
+    mg = np.zeros_like(np.asarray(tg, dtype=np.float64))
+    for ig, gt in enumerate(gas_type):
+        mg = mg + xgc[ig] * GMW[gt - 1]
+    return p / (RGAS * tg) * mg
+
+
+def hydrostatic(zb, z, grad, tb, pb, gravz):
+    """atmosphere.f:240-264."""
+    erreair = RGAS / GMW[5]
+    if grad != 0.0:
+        cost = gravz / (erreair * grad)
+        t = tb + grad * (z - zb)
+        p = pb * (t / tb) ** cost
+    else:
+        cost = gravz / (erreair * tb)
+        t = tb
+        p = pb * math.exp(cost * (z - zb))
+    return t, p
+
+
+def atmosphere_profile(deck, z):
+    """set_atmosphere + compute_profile, atmosphere.f:81-230."""
+    names = ("troposphere", "tropopause", "lower_stratosphere", "upper_stratosphere", "ozone_layer",
+             "lower_mesosphere", "upper_mesosphere")
+    layers = []
+    ptop, ttop = deck["p_ground"], deck["t_ground"]
+    gz = deck["gravz"]
+    for li, nm in enumerate(names):
+        zbot = layers[li - 1]["ztop"] if li > 0 else 0.0
+        ztop = deck[f"{nm}_z"]
+        gradt = deck[f"{nm}_grad"]
+        pbot, tbot = ptop, ttop
+        ttop, ptop = hydrostatic(zbot, ztop, gradt, tbot, pbot, gz)
+        layers.append(dict(ztop=ztop, gradt=gradt, ptop=ptop, ttop=ttop))
+    nz = len(z)
+    p_atm = np.zeros(nz)
+    t_atm = np.zeros(nz)
+    if z[0] <= layers[0]["ztop"]:
+        lidx = 1
+    else:
+        lidx = 2
+        while lidx <= len(layers) and not (z[0] > layers[lidx - 2]["ztop"]):
+            lidx += 1
+    for k in range(nz):
+        za = z[k]
+        if za > 0.0:
+            if not deck["stratification"]:
+                zbot, pbot, tbot, gradt = 0.0, deck["p_ground"], deck["t_ground"], 0.0
+            else:
+                if za > layers[lidx - 1]["ztop"]:
+                    lidx += 1
+                if lidx == 1:
+                    zbot, pbot, tbot = 0.0, deck["p_ground"], deck["t_ground"]
+                else:
+                    zbot = layers[lidx - 2]["ztop"]
+                    pbot = layers[lidx - 2]["ptop"]
+                    tbot = layers[lidx - 2]["ttop"]
+                gradt = layers[lidx - 1]["gradt"]
+            ta, pa = hydrostatic(zbot, za, gradt, tbot, pbot, gz)
+        else:
+            ta, pa = deck["t_ground"], deck["p_ground"]
+        t_atm[k] = ta
+        p_atm[k] = pa
+    return p_atm, t_atm
+
+
+class State(dict):
+    """Prognostic fields in the reference layout (flat numpy float64 arrays)."""
+
+    def copy(self):
+        return State({k: v.copy() for k, v in self.items()})
+
+
+class Case:
+    """A fully set-up run: metric, flags, atmosphere, vent, state, cfg."""
+
+    def __init__(self, deck: Deck, precision=abi.PREC_FP64):
+        self.deck = deck
+        bad = deck.check()
+        if bad:
+            raise ValueError("unsupported options: " + ", ".join(bad))
+        self.is3d = deck.is3d
+        self.nx = int(deck["nx"])
+        self.ny = int(deck["ny"]) if self.is3d else 1
+        self.nz = int(deck["nz"])
+        self.ncell = self.nx * self.ny * self.nz
+        self.nsolid = int(deck["nsolid"])
+        self.ngas = int(deck["ngas"])
+        self.precision = precision
+        self.gas_type = deck.gas_types()
+        self._grid()
+        self._flags()
+        self.p_atm, self.t_atm = atmosphere_profile(deck, self.z)
+        self._vent()
+        self.state = self._initial_state()
+
+    # grid.f:206-345
+    def _grid(self):
+        d = self.deck
+        if d["iuni"] == 1:
+            self.dx = np.full(self.nx, float(d["dx0"]))
+            self.dy = np.full(self.ny, float(d["dy0"])) if self.is3d else np.zeros(1)
+            self.dz = np.full(self.nz, float(d["dz0"]))
+        elif d["grigen"] == 0:
+            self.dx = np.asarray(d.delta_x, dtype=np.float64)
+            self.dy = np.asarray(d.delta_y, dtype=np.float64) if self.is3d else np.zeros(1)
+            self.dz = np.asarray(d.delta_z, dtype=np.float64)
+        else:
+            raise ValueError("grigen>0 (generated non-uniform mesh) is not supported")
+        nx, nz = self.nx, self.nz
+        self.xb = np.zeros(nx)
+        self.x = np.zeros(nx)
+        self.x[0] = -0.5 * self.dx[0] + self.xb[0]
+        for i in range(1, nx):
+            self.xb[i] = self.xb[i - 1] + self.dx[i]
+            self.x[i] = self.xb[i] - 0.5 * self.dx[i]
+        ny = self.ny
+        self.yb = np.zeros(ny)
+        self.y = np.zeros(ny)
+        if self.is3d:
+            self.y[0] = -0.5 * self.dy[0]
+            for j in range(1, ny):
+                self.yb[j] = self.yb[j - 1] + self.dy[j]
+                self.y[j] = self.yb[j] - 0.5 * self.dy[j]
+        self.zb = np.zeros(nz)
+        self.z = np.zeros(nz)
+        self.zb[0] = float(d["zzero"])
+        self.z[0] = -0.5 * self.dz[0] + self.zb[0]
+        for k in range(1, nz):
+            self.zb[k] = self.zb[k - 1] + self.dz[k]
+            self.z[k] = self.zb[k] - 0.5 * self.dz[k]
+        self.itc = int(d["itc"]) if not self.is3d else 0
+
+    def idx(self, i, j, k):
+        """1-based (i, j, k) -> flat 0-based index."""
+        return (i - 1) + self.nx * ((j - 1) + self.ny * (k - 1))
+
+    # flic, grid.f:375-483
+    def _flags(self):
+        d = self.deck
+        nx, ny, nz = self.nx, self.ny, self.nz
+        fl = np.full((nz, ny, nx), FLUID, dtype=np.int32)
+        if not self.is3d:
+            fl[0, 0, 1:nx - 1] = 2 ** (d["bottom"] - 1)
+            fl[nz - 1, 0, 1:nx - 1] = 2 ** (d["top"] - 1)
+            fl[:, 0, 0] = 2 ** (d["west"] - 1)
+            fl[:, 0, nx - 1] = 2 ** (d["east"] - 1)
+        else:
+            fl[0, 1:ny - 1, 1:nx - 1] = 2 ** (d["bottom"] - 1)
+            fl[nz - 1, 1:ny - 1, 1:nx - 1] = 2 ** (d["top"] - 1)
+            fl[:, :, 0] = 2 ** (d["west"] - 1)
+            fl[:, :, nx - 1] = 2 ** (d["east"] - 1)
+            fl[:, 0, :] = 2 ** (d["south"] - 1)
+            fl[:, ny - 1, :] = 2 ** (d["north"] - 1)
+        for b in d.blocks:
+            ys = slice(b["ylo"] - 1, b["yhi"]) if self.is3d else slice(0, 1)
+            fl[b["zlo"] - 1:b["zhi"], ys, b["xlo"] - 1:b["xhi"]] = 2 ** (b["typ"] - 1)
+            if self.is3d and b["typ"] == 8:
+                fl[b["zlo"] - 1:b["zhi"], ys, b["xlo"] - 1:b["xhi"]] = 129
+        self.flag3 = fl
+
+    # locate_vent_2D, vent.f:130-246 (3D square vents are given as type-5 blocks)
+    def _vent(self):
+        d = self.deck
+        self.vent = []  # dicts: ijk (0-based), frac, dist
+        if d["ivent"] < 1:
+            self.flag = self.flag3.reshape(-1).copy()
+            return
+        if self.is3d:
+            raise ValueError("circular vents in 3D (locate_vent_3D) are not supported; use a FIXED_FLOWS block")
+        nx, nz = self.nx, self.nz
+        fl = self.flag3[:, 0, :]
+        xvent = d["xvent"]
+        iv = int(round(nx / 2.0))
+        if xvent == -99999.0:
+            xvent = self.x[iv - 1] if d["vent_in_center"] else self.xb[iv - 1]
+        iiv = 1
+        for i in range(1, nx + 1):
+            if self.x[i - 1] <= xvent:
+                iiv = i
+        if iiv == 1 or self.itc == 1:
+            iiv = 2
+        xvent = self.xb[iiv - 2]
+        kkv = 1
+        for k in range(1, nz):
+            if fl[k - 1, iiv - 1] in (SLIP, NOSLIP):
+                kkv = k
+        quota = kkv
+        vr = d["vent_radius"]
+        iwest, ieast = 2, 2
+        for i in range(2, nx + 1):
+            if self.xb[i - 2] <= (xvent - vr):
+                iwest = i
+            if self.xb[i - 2] < (xvent + vr):
+                ieast = i
+        nvt = ieast - iwest + 1
+        for nv, i in enumerate(range(iwest, ieast + 1), start=1):
+            for k in range(1, quota):
+                fl[k - 1, i - 1] = NOSLIP
+            k = quota
+            frac = 1.0
+            if nv == nvt:
+                if self.itc == 1:
+                    frac = 1.0 - (self.xb[ieast - 1] - self.xb[iwest - 2] - vr) / self.dx[ieast - 1]
+                else:
+                    frac = 1.0 - (self.xb[ieast - 1] - self.xb[iwest - 2] - 2.0 * vr) / self.dx[ieast - 1]
+            fl[k - 1, i - 1] = VENT
+            self.vent.append(dict(ijk=self.idx(i, 1, k), i=i, k=k, frac=frac, dist=self.x[i - 1] - xvent))
+            for kk in range(quota + 1, nz):
+                fl[kk - 1, i - 1] = FLUID
+        self.flag3[:, 0, :] = fl
+        self.flag = self.flag3.reshape(-1).copy()
+
+    def _initial_state(self):
+        d = self.deck
+        n, ns, ng = self.ncell, self.nsolid, self.ngas
+        kk = np.repeat(np.arange(self.nz), self.nx * self.ny)
+        st = State()
+        for name in abi.STATE_CELL:
+            st[name] = np.zeros(n)
+        for name in abi.STATE_SOLID:
+            st[name] = np.zeros(n * ns)
+        for name in abi.STATE_GAS:
+            st[name] = np.zeros(n * ng)
+        rl = np.array(d["density"][:ns], dtype=np.float64)
+        # set_atmc, setup.f:204-275
+        st["p"][:] = self.p_atm[kk]
+        st["tg"][:] = self.t_atm[kk]
+        st["ep"][:] = d["void_fraction"]
+        atm = d.atm_ygc()
+        Y = st["ygc"].reshape(ng, n)
+        for ig, gt in enumerate(self.gas_type):
+            Y[ig, :] = atm[gt - 1]
+        RL = st["rlk"].reshape(ns, n)
+        TS = st["ts"].reshape(ns, n)
+        for s in range(ns):
+            RL[s] = rl[s] * (1.0 - st["ep"]) / ns
+            TS[s] = st["tg"]
+        moving = np.isin(self.flag, (FLUID, FREE_IO, ZERO_GRAD))
+        st["ug"][moving] = d["wind_x"]
+        st["wg"][moving] = d["wind_z"]
+        if self.is3d:
+            st["vg"][moving] = d["wind_y"]
+        for name, src in (("us", "ug"), ("ws", "wg"), ("vs", "vg")):
+            A = st[name].reshape(ns, n)
+            for s in range(ns):
+                A[s, moving] = st[src][moving]
+        # specified_flow, setup.f:397-498
+        for b in d.blocks:
+            if b["typ"] not in (1, 5):
+                continue
+            for k in range(b["zlo"], b["zhi"] + 1):
+                for j in (range(b["ylo"], b["yhi"] + 1) if self.is3d else (1,)):
+                    for i in range(b["xlo"], b["xhi"] + 1):
+                        c = self.idx(i, j, k)
+                        st["ug"][c] = b["ug"]
+                        if self.is3d:
+                            st["vg"][c] = b["vg"]
+                        st["wg"][c] = b["wg"]
+                        st["tg"][c] = b["tg"]
+                        st["p"][c] = b["p"]
+                        st["ep"][c] = 1.0 - sum(s_["eps"] for s_ in b["solids"])
+                        for ig, gt in enumerate(self.gas_type):
+                            Y[ig, c] = b["ygc"][gt - 1]
+                        for s, sd in enumerate(b["solids"]):
+                            TS[s, c] = sd["t"]
+                            st["us"][s * n + c] = sd["u"]
+                            if self.is3d:
+                                st["vs"][s * n + c] = sd["v"]
+                            st["ws"][s * n + c] = sd["w"]
+                            RL[s, c] = sd["eps"] * rl[s]
+                        if Y[:, c].sum() != 1.0:
+                            Y[ng - 1, c] = 1.0 - Y[:ng - 1, c].sum()
+        # set_ventc, vent.f:443-581 (uniform inlet; iali 4 = velocity profile)
+        if d["ivent"] >= 1:
+            vy = d.vent_ygc()
+            for v in self.vent:
+                c = v["ijk"]
+                st["ug"][c] = d["u_gas"]
+                st["wg"][c] = d["w_gas"]
+                st["tg"][c] = d["t_gas"]
+                st["ep"][c] = 1.0 - sum(d["ep_solid"][:ns])
+                st["p"][c] = d["p_gas"]
+                for ig, gt in enumerate(self.gas_type):
+                    Y[ig, c] = vy[gt - 1]
+                for s in range(ns):
+                    st["us"][s * n + c] = d["u_solid"][s]
+                    st["ws"][s * n + c] = d["w_solid"][s]
+                    TS[s, c] = d["t_solid"][s]
+                    RL[s, c] = d["ep_solid"][s] * rl[s]
+                if Y[:, c].sum() != 1.0:
+                    Y[ng - 1, c] = 1.0 - Y[:ng - 1, c].sum()
+                if d["iali"] == 4:
+                    ra = min(v["dist"] / d["vent_radius"], 1.0)
+                    if d["inlet_profile"] == 1:
+                        bet = (1.0 if (not self.is3d and self.itc == 0) else 2.0) / (d["wrat"] - 1.0)
+                        fac = d["wrat"] * (1.0 - ra ** bet)
+                    else:
+                        fac = 0.5 * (1.0 - math.tanh(0.25 * d["rbyb"] * (ra - 1.0 / ra))) if ra > 0 else 1.0
+                    st["ug"][c] = d["u_gas"] * fac
+                    st["wg"][c] = d["w_gas"] * fac
+                    for s in range(ns):
+                        st["us"][s * n + c] = d["u_solid"][s] * fac
+                        st["ws"][s * n + c] = d["w_solid"][s] * fac
+                elif d["iali"] in (1, 2, 3) and v["frac"] != 1.0:
+                    raise ValueError("vent antialiasing iali=1..3 on partial cells is not supported")
+        # cnvert, setup.f:280-390 (itd <= 1)
+        X = mole(Y, self.gas_type)
+        st["xgc"][:] = X.reshape(-1)
+        st["rog"][:] = thermal_eosg(st["tg"], st["p"], X, self.gas_type)
+        st["rgp"][:] = st["rog"] * st["ep"]
+        cp = hcapg(st["tg"], d["icpc"], d["tref"])
+        hc = np.zeros(n)
+        for ig, gt in enumerate(self.gas_type):
+            hc = hc + cp[gt - 1] * Y[ig]
+        st["cg"][:] = hc
+        st["sieg"][:] = (st["tg"] - 0.0) * st["cg"] + 0.0
+        cps = np.array(d["specific_heat"][:ns], dtype=np.float64)
+        SI = st["sies"].reshape(ns, n)
+        for s in range(ns):
+            SI[s] = (TS[s] - 0.0) * cps[s] + 0.0
+        return st
+
+    # ---- C ABI configuration ---------------------------------------------
+    def cfg(self):
+        """Build a ``pdac_cfg``; the returned object keeps its arrays alive."""
+        d = self.deck
+        c = abi.PdacCfg()
+        c.job_type = 3 if self.is3d else 2
+        c.nx, c.ny, c.nz = self.nx, self.ny, self.nz
+        c.itc = self.itc
+        c.nsolid, c.ngas = self.nsolid, self.ngas
+        for ig, gt in enumerate(self.gas_type):
+            c.gas_type[ig] = gt
+        c.dt = d["dt"]
+        c.rungekut = d["rungekut"]
+        c.alpha, c.alphagrav = d["alpha"], d["alphagrav"]
+        c.omega, c.delg = d["omega"], d["delg"]
+        c.inmax, c.maxout = d["inmax"], d["maxout"]
+        c.muscl, c.lv, c.lm = d["muscl"], d["vel_limiter"], d["mass_limiter"]
+        c.beta, c.flim = d["beta"], d["flim"]
+        c.update_eosg = int(bool(d["update_eosg"]))
+        c.pmodel, c.drag_model, c.icpc = d["pmodel"], d["drag_model"], d["icpc"]
+        c.tref = d["tref"]
+        c.gas_viscosity = int(bool(d["gas_viscosity"]))
+        c.part_viscosity = int(bool(d["part_viscosity"]))
+        c.repulsive_model = d["repulsive_model"]
+        c.gravx, c.gravy, c.gravz = d["gravx"], d["gravy"], d["gravz"]
+        for s in range(self.nsolid):
+            c.dk[s] = d["diameter"][s] * 1.0e-6
+            c.rl[s] = d["density"][s]
+            c.phis[s] = d["sphericity"][s]
+            c.cmus[s] = d["viscosity"][s]
+            c.cps[s] = d["specific_heat"][s]
+            c.kap[s] = d["thermal_conductivity"][s]
+            c.plim[s] = d["twophase_limit"][s]
+        c.void_fraction = d["void_fraction"]
+        for g, v in enumerate(d.atm_ygc()):
+            c.atm_ygc[g] = v
+        c.irand = d["irand"]
+        c.precision = self.precision
+        keep = dict(dx=np.ascontiguousarray(self.dx), dy=np.ascontiguousarray(self.dy),
+                    dz=np.ascontiguousarray(self.dz), flag=np.ascontiguousarray(self.flag, dtype=np.int32),
+                    p_atm=np.ascontiguousarray(self.p_atm), t_atm=np.ascontiguousarray(self.t_atm),
+                    vent=np.array([v["ijk"] for v in self.vent] or [0], dtype=np.int32))
+        c.dx, c.dy, c.dz = abi.dptr(keep["dx"]), abi.dptr(keep["dy"]), abi.dptr(keep["dz"])
+        c.flag = abi.iptr(keep["flag"])
+        c.p_atm, c.t_atm = abi.dptr(keep["p_atm"]), abi.dptr(keep["t_atm"])
+        c.nvent = len(self.vent)
+        c.vent_ijk = abi.iptr(keep["vent"])
+        c._keep = keep
+        return c
+
+    def fluid_count(self):
+        return int(np.count_nonzero(self.flag & 1))

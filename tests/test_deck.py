@@ -1,0 +1,95 @@
+"""Input deck reader: namelist defaults, parsing and the MESH/FIXED_FLOWS cards."""
+import numpy as np
+import pytest
+
+from pdac_b200 import configs
+from pdac_b200.deck import Deck, f32
+from pdac_b200.setup_state import Case, FLUID, SLIP, NOSLIP, FREE_IO, VENT
+
+
+def test_single_precision_defaults():
+    d = Deck()
+    assert d["omega"] == float(np.float32(1.1)) != 1.1
+    assert d["maxout"] == 500 and d["inmax"] == 8 and d["delg"] == 1e-8
+    assert d["alpha"] == 1.0 and d["pmodel"] == 2 and d["icpc"] == 2
+
+
+def test_round_trip_text():
+    d = configs.plume_2d(nx=10, nz=12)
+    d.set("mesh", iuni=0)
+    d.delta_x = np.full(10, 10.0)
+    d.delta_z = np.full(12, 12.5)
+    d.blocks = [dict(typ=5, xlo=2, xhi=3, ylo=0, yhi=0, zlo=1, zhi=1, ug=0.0, vg=0.0, wg=50.0, p=1.01e5,
+                     ep=0.99, tg=900.0, solids=[dict(u=0.0, v=0.0, w=50.0, eps=0.005, t=900.0)] * 2,
+                     ygc=[0.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0])]
+    d2 = Deck.parse(d.to_text())
+    for g in d.nml:
+        for k, v in d.nml[g].items():
+            assert d2.nml[g][k] == v, (g, k)
+    np.testing.assert_array_equal(d2.delta_z, d.delta_z)
+    assert d2.blocks[0]["typ"] == 5 and d2.blocks[0]["wg"] == 50.0
+
+
+HAND_DECK = """
+ &control
+   run_name = 'tube', job_type = '2D', dt = 0.005D0, tstop = 1.0
+ /
+ &model
+   iturb = 0, ngas = 1
+ /
+ &mesh
+   nx = 8, nz = 10, itc = 0, iuni = 1, dx0 = 5.0, dz0 = 5.0
+ /
+ &boundaries
+   west = 3, east = 3, bottom = 3, top = 3
+ /
+ &topography
+ /
+ &inlet
+ /
+ &dome
+ /
+ &atmosphere
+   stratification = .FALSE.
+ /
+ &particles
+   nsolid = 1, diameter = 200, density = 2500.
+ /
+ &numeric
+   muscl = 1, maxout = 300
+ /
+MESH
+FIXED_FLOWS
+0
+"""
+
+
+def test_parse_hand_written_deck_and_set_up_a_closed_box():
+    d = Deck.parse(HAND_DECK)
+    assert d["dt"] == 0.005 and d["nx"] == 8 and d["diameter"][0] == 200.0
+    case = Case(d)
+    f = case.flag.reshape(case.nz, case.nx)
+    assert (f[0, 1:-1] == NOSLIP).all() and (f[-1, 1:-1] == NOSLIP).all()
+    assert (f[:, 0] == NOSLIP).all() and (f[1:-1, 1:-1] == FLUID).all()
+    assert case.gas_type == [6]
+
+
+def test_plume_vent_and_flags():
+    case = Case(configs.plume_2d())
+    f = case.flag.reshape(case.nz, case.nx)
+    assert (f[:, 0] == SLIP).all()                    # axis
+    assert (f[1:, -1] == FREE_IO).all() and (f[-1, 1:-1] == FREE_IO).all()
+    vent_i = [v["i"] for v in case.vent]
+    assert vent_i == [2, 3, 4, 5, 6]                   # r in [0, 50] m with 10 m cells
+    assert all(f[0, i - 1] == VENT for i in vent_i)
+    assert case.gas_type == [5, 6]                     # H2O, Air (gas_check order)
+    st = case.state
+    c = case.vent[0]["ijk"]
+    assert st["tg"][c] == 1100.0 and st["wg"][c] == 100.0 and st["ygc"][c] == 1.0
+
+
+def test_unsupported_options_are_rejected():
+    d = configs.plume_2d()
+    d.set("model", iturb=1)
+    with pytest.raises(ValueError, match="iturb"):
+        Case(d)
