@@ -164,6 +164,14 @@ int pdac_gpu_mass_totals(pdac_ctx *ctx, double *out, int nout);
 /* device time (ms) of the kernels of the last call, by phase:
  * [boundary, fieldn, tilde, iter, ygas, htilde, ftem]                    */
 int pdac_gpu_phase_times(pdac_ctx *ctx, double *ms7);
+/* statistics since the last reset: out[0] kernel launches, out[1] outer
+ * sweeps of iter, out[2] timed corrector launches, out[3] their device time
+ * in ms (timed only when the reset enabled profiling); nout >= 4          */
+int pdac_gpu_stats(pdac_ctx *ctx, double *out, int nout);
+int pdac_gpu_reset_stats(pdac_ctx *ctx, int profile_corrector);
+/* stream-ordered timing marks (slots 0..31) and the device time between two */
+int pdac_gpu_mark(pdac_ctx *ctx, int slot);
+int pdac_gpu_elapsed(pdac_ctx *ctx, int a, int b, double *ms);
 
 #ifdef __cplusplus
 }

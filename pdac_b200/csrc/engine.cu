@@ -36,12 +36,19 @@ struct pdac_ctx {
     std::string err;
     cudaEvent_t ev[16];
     float phase_ms[7] = {0};
+    // statistics: kernel launches, corrector launch timing (when profiling)
+    long long launches = 0, sweeps = 0, corr_launches = 0;
+    double corr_ms = 0.0;
+    bool prof = false;
+    cudaEvent_t cev[6];
+    cudaEvent_t user_ev[32];
     std::vector<std::pair<std::string, std::pair<double *, size_t>>> names;
 };
 
 namespace {
 
 const int TPB = 128;
+const int TPB_CORR = 64;
 
 int fail(pdac_ctx *c, int code, const std::string &msg) {
     if (c) c->err = msg;
@@ -54,7 +61,7 @@ int fail(pdac_ctx *c, int code, const std::string &msg) {
         if (e_ != cudaSuccess) return fail(ctx, PDAC_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-inline int blocks(long n) { return (int)((n + TPB - 1) / TPB); }
+inline int blocks(long n, int tpb = TPB) { return (int)((n + tpb - 1) / tpb); }
 
 // setup.f:551-616 and particles.f:35-79: gas and particle constants
 void set_constants(pdac_ctx *ctx) {
@@ -167,6 +174,8 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
 
     CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     for (auto &e : ctx->ev) CK(cudaEventCreate(&e));
+    for (auto &e : ctx->cev) CK(cudaEventCreate(&e));
+    for (auto &e : ctx->user_ev) CK(cudaEventCreate(&e));
     std::vector<std::vector<double> *> mets = {&dx, &dy, &dz, &indx, &indy, &indz, &r, &rb, &inr, &inrb, &patm, &tatm};
     size_t mtot = 0;
     for (auto *v : mets) mtot += v->size();
@@ -255,6 +264,8 @@ int pdac_gpu_destroy(pdac_ctx *ctx) {
     cudaFree(ctx->d_partial);
     cudaFreeHost(ctx->h_counters);
     for (auto &e : ctx->ev) cudaEventDestroy(e);
+    for (auto &e : ctx->cev) cudaEventDestroy(e);
+    for (auto &e : ctx->user_ev) cudaEventDestroy(e);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return PDAC_OK;
@@ -292,8 +303,8 @@ int pdac_gpu_boundary(pdac_ctx *ctx, int sweep) {
     cudaStream_t st = ctx->stream;
     CK(cudaEventRecord(ctx->ev[0], st));
     if (ctx->nvent > 0 && ctx->cfg.irand >= 1)
-        pdac::k_vent<<<blocks(ctx->nvent), TPB, 0, st>>>(ctx->P, ctx->F, ctx->d_vent, ctx->nvent, ctx->d_vfact, ctx->d_vfact0);
-    pdac::k_boundary2d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F);
+        pdac::k_vent<<<blocks(ctx->nvent), TPB, 0, st>>>(ctx->P, ctx->F, ctx->d_vent, ctx->nvent, ctx->d_vfact, ctx->d_vfact0), ctx->launches++;
+    pdac::k_boundary2d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F), ctx->launches++;
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[1], st));
     return PDAC_OK;
@@ -303,7 +314,7 @@ int pdac_gpu_fieldn(pdac_ctx *ctx) {
     if (!ctx) return PDAC_ERR_ARG;
     cudaStream_t st = ctx->stream;
     CK(cudaEventRecord(ctx->ev[2], st));
-    pdac::k_fieldn2d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F);
+    pdac::k_fieldn2d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F), ctx->launches++;
     // allocate_fluxes (tilde.f:56-102): tilde and interphase terms start from
     // zero in every step
     size_t n = ctx->ncell;
@@ -329,8 +340,8 @@ int pdac_gpu_tilde(pdac_ctx *ctx, double dt) {
     CK(cudaEventRecord(ctx->ev[4], st));
     for (double *a : {F.ugfe, F.ugft, F.wgfe, F.wgft}) CK(cudaMemsetAsync(a, 0, n * sizeof(double), st));
     for (double *a : {F.usfe, F.usft, F.wsfe, F.wsft}) CK(cudaMemsetAsync(a, 0, n * ns * sizeof(double), st));
-    pdac::k_tilde_flux2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F);
-    pdac::k_tilde2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt, ctx->d_app0u, ctx->d_app0w);
+    pdac::k_tilde_flux2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F), ctx->launches++;
+    pdac::k_tilde2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt, ctx->d_app0u, ctx->d_app0w), ctx->launches++;
     if (ctx->P.alpha != 1.0 && ctx->cfg.rungekut > 1) {
         CK(cudaMemcpyAsync(ctx->d_app0u, F.appu, n * ctx->nap * sizeof(double), cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(ctx->d_app0w, F.appw, n * ctx->nap * sizeof(double), cudaMemcpyDeviceToDevice, st));
@@ -348,18 +359,31 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
     CK(cudaEventRecord(ctx->ev[6], st));
     for (double *a : {F.rgfe, F.rgft, F.conv, F.abeta}) CK(cudaMemsetAsync(a, 0, n * sizeof(double), st));
     for (double *a : {F.rsfe, F.rsft}) CK(cudaMemsetAsync(a, 0, n * ns * sizeof(double), st));
-    pdac::k_predictor2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt);
-    pdac::k_mflux_init2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt);
+    pdac::k_predictor2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt), ctx->launches++;
+    pdac::k_mflux_init2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt), ctx->launches++;
     CK(cudaGetLastError());
     int m = (ctx->nx + 2) / 3;
     long nthr = (long)m * ctx->nz;
     int nit;
     for (nit = 1; nit <= ctx->cfg.maxout; ++nit) {
         CK(cudaMemsetAsync(ctx->d_counters, 0, sizeof(int), st));
-        for (int col = 0; col < 3; ++col)
-            pdac::k_corrector2d<<<blocks(nthr), TPB, 0, st>>>(ctx->P, F, dt, col, nit);
+        for (int col = 0; col < 3; ++col) {
+            if (ctx->prof) CK(cudaEventRecord(ctx->cev[2 * col], st));
+            pdac::k_corrector2d<<<blocks(nthr, TPB_CORR), TPB_CORR, 0, st>>>(ctx->P, F, dt, col, nit);
+            ctx->launches++;
+            if (ctx->prof) CK(cudaEventRecord(ctx->cev[2 * col + 1], st));
+        }
         CK(cudaMemcpyAsync(ctx->h_counters, ctx->d_counters, sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        ctx->sweeps++;
+        if (ctx->prof) {
+            for (int col = 0; col < 3; ++col) {
+                float t = 0;
+                CK(cudaEventElapsedTime(&t, ctx->cev[2 * col], ctx->cev[2 * col + 1]));
+                ctx->corr_ms += t;
+                ctx->corr_launches++;
+            }
+        }
         if (ctx->h_counters[0] == 0) break;
     }
     CK(cudaGetLastError());
@@ -381,8 +405,8 @@ int pdac_gpu_ygas(pdac_ctx *ctx, double dt) {
     } else {
         CK(cudaMemsetAsync(ctx->F.yfe, 0, n * ctx->ng * sizeof(double), st));
         CK(cudaMemsetAsync(ctx->F.yft, 0, n * ctx->ng * sizeof(double), st));
-        pdac::k_ygas_flux2d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F);
-        pdac::k_ygas2d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F, dt);
+        pdac::k_ygas_flux2d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F), ctx->launches++;
+        pdac::k_ygas2d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F, dt), ctx->launches++;
     }
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[9], st));
@@ -399,8 +423,8 @@ int pdac_gpu_htilde(pdac_ctx *ctx, double dt) {
     CK(cudaMemsetAsync(F.egft, 0, n * sizeof(double), st));
     CK(cudaMemsetAsync(F.esfe, 0, n * ns * sizeof(double), st));
     CK(cudaMemsetAsync(F.esft, 0, n * ns * sizeof(double), st));
-    pdac::k_htilde_flux2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F);
-    pdac::k_htilde2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt);
+    pdac::k_htilde_flux2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F), ctx->launches++;
+    pdac::k_htilde2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt), ctx->launches++;
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[11], st));
     return PDAC_OK;
@@ -411,7 +435,7 @@ int pdac_gpu_ftem(pdac_ctx *ctx, double dt) {
     cudaStream_t st = ctx->stream;
     CK(cudaEventRecord(ctx->ev[12], st));
     CK(cudaMemsetAsync(ctx->d_counters + 1, 0, sizeof(int), st));
-    pdac::k_ftem2d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F, dt);
+    pdac::k_ftem2d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F, dt), ctx->launches++;
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[13], st));
     CK(cudaMemcpyAsync(ctx->h_counters + 1, ctx->d_counters + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -462,6 +486,7 @@ int pdac_gpu_mass_totals(pdac_ctx *ctx, double *out, int nout) {
     if (nout < nq) return PDAC_ERR_ARG;
     int nb = 148;
     pdac::k_mass_partial<<<nb, 256, nq * 256 * sizeof(double), ctx->stream>>>(ctx->P, ctx->F, ctx->d_partial, nq);
+    ctx->launches++;
     CK(cudaGetLastError());
     std::vector<double> h((size_t)nq * nb);
     CK(cudaMemcpyAsync(h.data(), ctx->d_partial, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -491,6 +516,43 @@ int pdac_gpu_set_vent_factors(pdac_ctx *ctx, const double *fact, int nvent) {
     if (!ctx || !fact || nvent != ctx->nvent) return PDAC_ERR_ARG;
     CK(cudaMemcpyAsync(ctx->d_vfact, fact, nvent * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    return PDAC_OK;
+}
+
+
+// statistics: out[0] kernel launches, out[1] outer sweeps, out[2] timed
+// corrector launches, out[3] their total device time in ms
+int pdac_gpu_stats(pdac_ctx *ctx, double *out, int nout) {
+    if (!ctx || !out || nout < 4) return PDAC_ERR_ARG;
+    out[0] = (double)ctx->launches;
+    out[1] = (double)ctx->sweeps;
+    out[2] = (double)ctx->corr_launches;
+    out[3] = ctx->corr_ms;
+    return PDAC_OK;
+}
+
+int pdac_gpu_reset_stats(pdac_ctx *ctx, int profile_corrector) {
+    if (!ctx) return PDAC_ERR_ARG;
+    ctx->launches = ctx->sweeps = ctx->corr_launches = 0;
+    ctx->corr_ms = 0.0;
+    ctx->prof = profile_corrector != 0;
+    return PDAC_OK;
+}
+
+// record a timing mark (0..31) on the context's stream
+int pdac_gpu_mark(pdac_ctx *ctx, int slot) {
+    if (!ctx || slot < 0 || slot >= 32) return PDAC_ERR_ARG;
+    CK(cudaEventRecord(ctx->user_ev[slot], ctx->stream));
+    return PDAC_OK;
+}
+
+// device time between two marks, after synchronising the stream
+int pdac_gpu_elapsed(pdac_ctx *ctx, int a, int b, double *ms) {
+    if (!ctx || !ms || a < 0 || b < 0 || a >= 32 || b >= 32) return PDAC_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream));
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, ctx->user_ev[a], ctx->user_ev[b]));
+    *ms = t;
     return PDAC_OK;
 }
 

@@ -49,6 +49,14 @@ def lib():
         L.pdac_gpu_phase_times.restype = C.c_int
         L.pdac_gpu_set_vent_factors.argtypes = [P, C.POINTER(C.c_double), C.c_int]
         L.pdac_gpu_set_vent_factors.restype = C.c_int
+        L.pdac_gpu_stats.argtypes = [P, C.POINTER(C.c_double), C.c_int]
+        L.pdac_gpu_stats.restype = C.c_int
+        L.pdac_gpu_reset_stats.argtypes = [P, C.c_int]
+        L.pdac_gpu_reset_stats.restype = C.c_int
+        L.pdac_gpu_mark.argtypes = [P, C.c_int]
+        L.pdac_gpu_mark.restype = C.c_int
+        L.pdac_gpu_elapsed.argtypes = [P, C.c_int, C.c_int, C.POINTER(C.c_double)]
+        L.pdac_gpu_elapsed.restype = C.c_int
         abi.declare(L, "pdac_gpu", P)
         _lib = L
     return _lib
@@ -58,7 +66,8 @@ EXPORTED = (
     "pdac_gpu_create", "pdac_gpu_destroy", "pdac_gpu_last_error", "pdac_gpu_upload_state",
     "pdac_gpu_download_state", "pdac_gpu_boundary", "pdac_gpu_fieldn", "pdac_gpu_tilde", "pdac_gpu_iter",
     "pdac_gpu_ygas", "pdac_gpu_htilde", "pdac_gpu_ftem", "pdac_gpu_step", "pdac_gpu_set_vent_factors",
-    "pdac_gpu_get_array", "pdac_gpu_mass_totals", "pdac_gpu_phase_times",
+    "pdac_gpu_get_array", "pdac_gpu_mass_totals", "pdac_gpu_phase_times", "pdac_gpu_stats",
+    "pdac_gpu_reset_stats", "pdac_gpu_mark", "pdac_gpu_elapsed",
 )
 
 
@@ -154,6 +163,22 @@ class Engine:
         out = np.zeros(n)
         self._chk(self.L.pdac_gpu_mass_totals(self.h, abi.dptr(out), n), "mass_totals")
         return out
+
+    def stats(self):
+        out = (C.c_double * 4)()
+        self._chk(self.L.pdac_gpu_stats(self.h, out, 4), "stats")
+        return dict(launches=int(out[0]), sweeps=int(out[1]), corr_launches=int(out[2]), corr_ms=out[3])
+
+    def reset_stats(self, profile_corrector=False):
+        self._chk(self.L.pdac_gpu_reset_stats(self.h, int(profile_corrector)), "reset_stats")
+
+    def mark(self, slot):
+        self._chk(self.L.pdac_gpu_mark(self.h, slot), "mark")
+
+    def elapsed(self, a, b):
+        ms = C.c_double(0)
+        self._chk(self.L.pdac_gpu_elapsed(self.h, a, b, C.byref(ms)), "elapsed")
+        return ms.value
 
     def phase_times(self):
         out = (C.c_double * 7)()

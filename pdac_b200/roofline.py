@@ -1,0 +1,45 @@
+"""Algorithmic byte counts of the time step, per cell.
+
+Compulsory HBM traffic model: every array a pass needs is read once and
+every array it produces is written once, FP64 (8 B).  Symbols: S = 1 + ns
+phases, d dimensions, G gas species, N_app = d * S(S+1)/2 interphase terms.
+
+  corrector sweep (iter.f:204-410), per fluid cell:
+    R_sweep = 8 + G + 2 ns + 2 d S + N_app     (p, ep, rog, rgp, rgpn, tg,
+              conv, abeta, xgc, rlk/rlkn, face velocities, tilde momenta,
+              interphase terms)
+    W_sweep = 4 + ns + d S                      (p, ep, rog, rgp, rlk,
+              face velocities)
+  whole step (semi-implicit path, rungekut = 1):
+    B_step = 8 [ fixed + nit (R_sweep + W_sweep) ]
+"""
+from __future__ import annotations
+
+
+def sweep_doubles(ns, ng, d=2):
+    S = 1 + ns
+    n_app = d * S * (S + 1) // 2
+    r = 8 + ng + 2 * ns + 2 * d * S + n_app
+    w = 4 + ns + d * S
+    return r, w
+
+
+def step_fixed_doubles(ns, ng, d=2):
+    """Doubles per cell of the non-iterative passes of one step."""
+    S = 1 + ns
+    n_state = 6 + d + ns * (3 + d) + 2 * ng
+    n_old = 4 + 2 * ns + ng + d * S
+    n_app = d * S * (S + 1) // 2
+    # boundary + fieldn, tilde (+fluxes), predictor/betas, ygas, htilde, ftem
+    return (n_state + n_old + 2) + (n_state + d * S + n_app) + (d * S + n_app + 5 + d * S + 2) \
+        + (2 * ng + d + 2) + (2 * S + d * S + 2) + (2 * S + n_state)
+
+
+def corrector_bytes_per_cell_sweep(ns, ng, d=2):
+    r, w = sweep_doubles(ns, ng, d)
+    return 8 * (r + w)
+
+
+def step_bytes_per_cell(ns, ng, nit, d=2):
+    r, w = sweep_doubles(ns, ng, d)
+    return 8 * (step_fixed_doubles(ns, ng, d) + nit * (r + w))
