@@ -106,6 +106,7 @@ struct Oracle {
     vector<double> rgfe, rgfn, rgft, rsfe, rsfn, rsft, conv, abeta;
     vector<double> egfe, egft, esfe, esft, hgfe, hgft, hsfe, hsft, yfe, yft;
     vector<double> sink;
+    vector<double> mf3, ef3, yfn;   // 3D momentum / enthalpy face fluxes, species y-fluxes
     vector<double> dgres;   // |dg|/conv at the last corrector visit (diagnostic)
     vector<double> vent_fact, vent_fact0;
     // padjust SAVE variables (iter.f:1005)
@@ -151,7 +152,7 @@ void build_tables(Oracle &o) {
             o.rem[(size_t)s * o.ncell + c] = -1;  // undefined outside the interior
         }
         bool interior = i >= 2 && i <= o.nx - 1 && k >= 2 && k <= o.nz - 1 && (!o.d3 || (j >= 2 && j <= o.ny - 1));
-        if (!interior) continue;
+        if (!interior || o.d3) continue;
         auto R = [&](int s) { return o.raw[(size_t)s * o.ncell + c]; };
         auto F = [&](int s) { return o.flag[R(s)]; };
         auto setr = [&](int s, int v) { o.rem[(size_t)s * o.ncell + c] = v; };
@@ -1884,7 +1885,10 @@ void alloc(Oracle &o) {
         v->assign(n * ns, 0.0);
     for (auto *v : {&o.ygc, &o.xgc, &o.rgpgcn}) v->assign(n * ng, 0.0);
     for (auto *v : {&o.appu, &o.appv, &o.appw}) v->assign(n * o.nap, 0.0);
+    if (o.d3) o.mf3.assign((size_t)(ns + 1) * 9 * n, 0.0);
 }
+
+#include "pdac_oracle3d.inc"
 
 }  // namespace
 
@@ -1898,7 +1902,6 @@ int pdac_oracle_create(const pdac_cfg *cfg, void **out) {
     Oracle *o = new Oracle();
     o->cfg = *cfg;
     o->d3 = cfg->job_type == 3;
-    if (o->d3) { delete o; return PDAC_ERR_CONFIG; }  // 3D restatement not in this file yet
     o->nx = cfg->nx; o->ny = o->d3 ? cfg->ny : 1; o->nz = cfg->nz;
     o->ncell = o->nx * o->ny * o->nz;
     o->ns = cfg->nsolid; o->ng = cfg->ngas; o->nph = o->ns + 1; o->nap = o->nph * (o->nph + 1) / 2;
@@ -1912,9 +1915,10 @@ int pdac_oracle_create(const pdac_cfg *cfg, void **out) {
     fill1(o->dx, cfg->dx, o->nx);
     fill1(o->dz, cfg->dz, o->nz);
     if (o->d3) fill1(o->dy, cfg->dy, o->ny); else o->dy.assign(4, 0.0);
+    if (o->d3) { o->indy.resize(o->dy.size()); for (size_t q = 0; q < o->dy.size(); ++q) o->indy[q] = 1.0 / o->dy[q]; }
     auto inv = [](vector<double> &out, const vector<double> &in) { out.resize(in.size()); for (size_t q = 0; q < in.size(); ++q) out[q] = 1.0 / in[q]; };
     inv(o->indx, o->dx); inv(o->indz, o->dz);
-    o->indy.assign(o->dy.size(), 0.0);
+    if (!o->d3) o->indy.assign(o->dy.size(), 0.0);
     // grid.f:306-345
     int nx = o->nx;
     o->r.assign(nx + 4, 1.0); o->rb.assign(nx + 4, 1.0); o->inr.assign(nx + 4, 1.0); o->inrb.assign(nx + 4, 1.0);
@@ -1941,6 +1945,7 @@ int pdac_oracle_create(const pdac_cfg *cfg, void **out) {
     o->cfg.vent_ijk = vl;
     setc(*o);
     build_tables(*o);
+    if (o->d3) build_tables3(*o);
     alloc(*o);
     *out = o;
     return PDAC_OK;
@@ -1990,20 +1995,43 @@ int pdac_oracle_get_state(void *h, pdac_state_view *s) {
     return PDAC_OK;
 }
 
-int pdac_oracle_boundary(void *h, int sweep) { boundary_2d(*(Oracle *)h, sweep); return PDAC_OK; }
+int pdac_oracle_boundary(void *h, int sweep) {
+    Oracle &o = *(Oracle *)h;
+    if (o.d3) boundary_3d(o, sweep); else boundary_2d(o, sweep);
+    return PDAC_OK;
+}
 int pdac_oracle_fieldn(void *h) {
     Oracle &o = *(Oracle *)h;
-    fieldn(o);
+    if (o.d3) fieldn3(o); else fieldn(o);
     // allocate_fluxes (tilde.f:56-102): tilde/app terms zeroed once per step
     for (auto *v : {&o.rug, &o.rwg, &o.rhg}) std::fill(v->begin(), v->end(), 0.0);
     for (auto *v : {&o.rus, &o.rws, &o.rhs, &o.appu, &o.appw}) std::fill(v->begin(), v->end(), 0.0);
+    if (o.d3) for (auto *v : {&o.rvg, &o.rvs, &o.appv}) std::fill(v->begin(), v->end(), 0.0);
     return PDAC_OK;
 }
-int pdac_oracle_tilde(void *h, double dt) { tilde_2d(*(Oracle *)h, dt); return PDAC_OK; }
-int pdac_oracle_iter(void *h, double dt, int *nit) { return iter_2d(*(Oracle *)h, dt, nit); }
-int pdac_oracle_ygas(void *h, double dt) { ygas_2d(*(Oracle *)h, dt); return PDAC_OK; }
-int pdac_oracle_htilde(void *h, double dt) { htilde_2d(*(Oracle *)h, dt); return PDAC_OK; }
-int pdac_oracle_ftem(void *h, double dt) { return ftem_2d(*(Oracle *)h, dt); }
+int pdac_oracle_tilde(void *h, double dt) {
+    Oracle &o = *(Oracle *)h;
+    if (o.d3) tilde_3d(o, dt); else tilde_2d(o, dt);
+    return PDAC_OK;
+}
+int pdac_oracle_iter(void *h, double dt, int *nit) {
+    Oracle &o = *(Oracle *)h;
+    return o.d3 ? iter_3d(o, dt, nit) : iter_2d(o, dt, nit);
+}
+int pdac_oracle_ygas(void *h, double dt) {
+    Oracle &o = *(Oracle *)h;
+    if (o.d3) ygas_3d(o, dt); else ygas_2d(o, dt);
+    return PDAC_OK;
+}
+int pdac_oracle_htilde(void *h, double dt) {
+    Oracle &o = *(Oracle *)h;
+    if (o.d3) htilde_3d(o, dt); else htilde_2d(o, dt);
+    return PDAC_OK;
+}
+int pdac_oracle_ftem(void *h, double dt) {
+    Oracle &o = *(Oracle *)h;
+    return o.d3 ? ftem_3d(o, dt) : ftem_2d(o, dt);
+}
 
 // prog.f:143-417 for one step (time_integration = 0)
 int pdac_oracle_step(void *h, int sweep, int *nit) {
@@ -2048,7 +2076,10 @@ int pdac_oracle_get_array(void *h, const char *name, double *out, long *n_inout)
                {"wsfe", &o.wsfe}, {"wsft", &o.wsft}, {"rgfe", &o.rgfe}, {"rgft", &o.rgft},
                {"rsfe", &o.rsfe}, {"rsft", &o.rsft}, {"conv", &o.conv}, {"abeta", &o.abeta},
                {"rhg", &o.rhg}, {"rhs", &o.rhs}, {"egfe", &o.egfe}, {"egft", &o.egft},
-               {"esfe", &o.esfe}, {"esft", &o.esft}, {"dgres", &o.dgres}};
+               {"esfe", &o.esfe}, {"esft", &o.esft}, {"dgres", &o.dgres},
+               {"rvgn", &o.rvgn}, {"rvsn", &o.rvsn}, {"rvg", &o.rvg}, {"rvs", &o.rvs}, {"appv", &o.appv},
+               {"rgfn", &o.rgfn}, {"rsfn", &o.rsfn}, {"mf3", &o.mf3}, {"ef3", &o.ef3},
+               {"gvisy", &o.gvisy}, {"pvisy", &o.pvisy}};
     for (auto &e : tab) {
         if (std::strcmp(e.n, name) == 0) {
             long need = (long)e.v->size();

@@ -42,6 +42,44 @@ def small_2d(nx=12, nz=16, **kw):
     return plume_2d(nx=nx, nz=nz, **kw)
 
 
+def plume_3d(nx=256, ny=256, nz=192, dxyz=20.0, dt=0.02, vent_cells=5, w_gas=150.0, t_gas=1000.0,
+             diameters=(30.0, 250.0, 1000.0), density=2400.0, ep_solid=(0.005, 0.01, 0.005), muscl=1,
+             limiter=2, delg=1.0e-8, maxout=500):
+    """3D Cartesian plume over flat ground on a uniform grid.
+
+    Defaults are the 256 x 256 x 192, 20 m, three-class, 300-step workload: the
+    same stratified air atmosphere, a square vent of 5 x 5 cells at the domain
+    centre (a FIXED_FLOWS inlet block in the ground row) injecting water vapour
+    at 1000 K and 150 m/s with classes of 30, 250 and 1000 um (2400 kg/m3) at
+    volume fractions 0.005, 0.01 and 0.005.  Lateral and top boundaries are
+    free in/outflow, the ground is a no-slip wall.
+    """
+    d = Deck()
+    ns = len(diameters)
+    d.set("control", job_type="3D", dt=dt, tstop=1.0e9)
+    d.set("model", iturb=0, ngas=2, gravz=-9.81, pmodel=2, drag_model=1)
+    d.set("mesh", nx=nx, ny=ny, nz=nz, itc=0, iuni=1, dx0=dxyz, dy0=dxyz, dz0=dxyz, grigen=0)
+    d.set("boundaries", west=4, east=4, south=4, north=4, bottom=3, top=4)
+    d.set("atmosphere", stratification=True, t_ground=288.0, troposphere_grad=-6.5e-3,
+          p_ground=1.01325e5, atm_Air=1.0)
+    d.set("particles", nsolid=ns, diameter=list(diameters), density=[density] * ns)
+    d.set("numeric", muscl=muscl, vel_limiter=limiter, mass_limiter=limiter, delg=delg, maxout=maxout)
+    lo_i = nx // 2 - vent_cells // 2 + 1
+    lo_j = ny // 2 - vent_cells // 2 + 1
+    d.blocks = [dict(typ=5, xlo=lo_i, xhi=lo_i + vent_cells - 1, ylo=lo_j, yhi=lo_j + vent_cells - 1, zlo=1, zhi=1,
+                     ug=0.0, vg=0.0, wg=w_gas, p=1.01325e5, ep=1.0 - sum(ep_solid), tg=t_gas,
+                     solids=[dict(u=0.0, v=0.0, w=w_gas, eps=e, t=t_gas) for e in ep_solid],
+                     ygc=[0.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0])]
+    return d
+
+
+def small_3d(nx=10, ny=9, nz=12, **kw):
+    """A tiny version of the 3D plume for parity tests (2 x 2 vent)."""
+    kw.setdefault("vent_cells", 2)
+    return plume_3d(nx=nx, ny=ny, nz=nz, **kw)
+
+
 WORKLOADS = {
     "plume2d_128x192": dict(builder="plume_2d", kw={}, steps=500),
+    "plume3d_256x256x192": dict(builder="plume_3d", kw={}, steps=300),
 }

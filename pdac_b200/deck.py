@@ -367,6 +367,4 @@ class Deck:
             bad.append("ipro>0 or iali=5")
         if self["optimization"] not in (1,):
             bad.append("optimization!=1")
-        if self.is3d:
-            bad.append("3D job (not yet built)")
         return bad
