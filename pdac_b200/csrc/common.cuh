@@ -23,6 +23,7 @@ enum : int { FLUID = 1, SLIP = 2, NOSLIP = 4, BL_CELL = 5, FREE_IO = 8, INLET = 
 // Scalar run parameters, passed by value to every kernel.
 struct Prm {
     int nx, ny, nz, ncell, ns, ng, nph, nap;
+    int d3;  // 1 for the 3D Cartesian path, 0 for 2D (x, z)
     int itc, muscl, lv, lm, pmodel, drag_model, icpc;
     int gas_viscosity, part_viscosity, repulsive_model, inmax;
     int gas_type[PDAC_MAXG];
@@ -46,12 +47,13 @@ struct Fld {
     double *p, *ep, *rog, *rgp, *tg, *sieg, *cg, *ug, *vg, *wg;
     double *rlk, *ts, *sies, *us, *vs, *ws, *ygc, *xgc;
     double *pn, *epn, *rgpn, *siegn, *rlkn, *siesn, *rgpgcn, *mug, *kapg;
-    double *rugn, *rwgn, *rusn, *rwsn;
-    double *rug, *rwg, *rus, *rws, *appu, *appw;
-    double *ugfe, *ugft, *wgfe, *wgft, *usfe, *usft, *wsfe, *wsft;
-    double *rgfe, *rgft, *rsfe, *rsft, *conv, *abeta;
-    double *egfe, *egft, *esfe, *esft, *rhg, *rhs;
-    double *yfe, *yft;
+    double *rugn, *rvgn, *rwgn, *rusn, *rvsn, *rwsn;
+    double *rug, *rvg, *rwg, *rus, *rvs, *rws, *appu, *appv, *appw;
+    double *ugfe, *ugft, *wgfe, *wgft, *usfe, *usft, *wsfe, *wsft;  // 2D momentum fluxes
+    double *mf;  // 3D momentum fluxes, block ((phase*3 + component)*3 + face) of ncell values
+    double *rgfe, *rgfn, *rgft, *rsfe, *rsfn, *rsft, *conv, *abeta;
+    double *egfe, *egfn, *egft, *esfe, *esfn, *esft, *rhg, *rhs;
+    double *yfe, *yfn, *yft;
     double *sink;
     int *counters;  // [0] non-converged cells this sweep, [1] eos failures, [2] rls>1 cells, [3] boundary errors
 };

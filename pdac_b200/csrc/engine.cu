@@ -14,7 +14,7 @@
 #include <algorithm>
 
 #include "../../include/pdac_gpu.h"
-#include "kernels2d.cuh"
+#include "kernels3d.cuh"
 
 using namespace pdac;
 
@@ -30,7 +30,7 @@ struct pdac_ctx {
     double *metric = nullptr;
     int *d_flag = nullptr, *d_vent = nullptr, *d_counters = nullptr, *h_counters = nullptr;
     double *d_vfact = nullptr, *d_vfact0 = nullptr;
-    double *d_app0u = nullptr, *d_app0w = nullptr;
+    double *d_app0u = nullptr, *d_app0v = nullptr, *d_app0w = nullptr;
     double *d_partial = nullptr;
     int nvent = 0;
     std::string err;
@@ -102,8 +102,12 @@ void set_constants(pdac_ctx *ctx) {
 }
 
 int validate(const pdac_cfg *c, std::string &why) {
-    if (c->job_type != 2) { why = "only job_type 2 (2D) is built in this engine"; return 1; }
+    if (c->job_type != 2 && c->job_type != 3) { why = "job_type must be 2 (2D) or 3 (3D)"; return 1; }
     if (c->nx < 5 || c->nz < 5) { why = "nx and nz must be >= 5"; return 1; }
+    if (c->job_type == 3 && c->ny < 5) { why = "ny must be >= 5 in 3D"; return 1; }
+    if (c->job_type == 3 && c->itc != 0) { why = "3D runs are Cartesian (itc = 0)"; return 1; }
+    if (c->job_type == 3 && !c->dy) { why = "dy pointer is NULL"; return 1; }
+    if ((long)c->nx * (c->job_type == 3 ? c->ny : 1) * c->nz > 2000000000L) { why = "mesh too large"; return 1; }
     if (c->nsolid < 1 || c->nsolid > PDAC_MAX_NSOLID) { why = "nsolid out of range"; return 1; }
     if (c->ngas < 1 || c->ngas > PDAC_MAX_NGAS) { why = "ngas out of range"; return 1; }
     for (int ig = 0; ig < c->ngas; ++ig)
@@ -132,14 +136,14 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     }
     pdac_ctx *ctx = new pdac_ctx();
     ctx->cfg = *cfg;
-    ctx->d3 = false;
-    ctx->nx = cfg->nx; ctx->ny = 1; ctx->nz = cfg->nz;
+    ctx->d3 = cfg->job_type == 3;
+    ctx->nx = cfg->nx; ctx->ny = ctx->d3 ? cfg->ny : 1; ctx->nz = cfg->nz;
     ctx->ncell = ctx->nx * ctx->ny * ctx->nz;
     ctx->ns = cfg->nsolid; ctx->ng = cfg->ngas; ctx->nph = ctx->ns + 1; ctx->nap = ctx->nph * (ctx->nph + 1) / 2;
     int n = ctx->ncell, ns = ctx->ns, ng = ctx->ng, nap = ctx->nap;
     Prm &P = ctx->P;
     std::memset(&P, 0, sizeof(P));
-    P.nx = ctx->nx; P.ny = 1; P.nz = ctx->nz; P.ncell = n; P.ns = ns; P.ng = ng; P.nph = ctx->nph; P.nap = nap;
+    P.nx = ctx->nx; P.ny = ctx->ny; P.nz = ctx->nz; P.ncell = n; P.d3 = ctx->d3 ? 1 : 0; P.ns = ns; P.ng = ng; P.nph = ctx->nph; P.nap = nap;
     P.itc = cfg->itc; P.muscl = cfg->muscl; P.lv = cfg->lv; P.lm = cfg->lm; P.pmodel = cfg->pmodel;
     P.drag_model = cfg->drag_model; P.icpc = cfg->icpc; P.gas_viscosity = cfg->gas_viscosity;
     P.part_viscosity = cfg->part_viscosity; P.repulsive_model = cfg->repulsive_model; P.inmax = cfg->inmax;
@@ -151,15 +155,20 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     set_constants(ctx);
 
     // host metric, 1-based padded, grid.f:306-345
-    int nx = ctx->nx, nz = ctx->nz;
+    int nx = ctx->nx, ny = ctx->ny, nz = ctx->nz;
     std::vector<double> dx(nx + 4), dz(nz + 4), indx(nx + 4), indz(nz + 4), r(nx + 4, 1.0), rb(nx + 4, 1.0),
-        inr(nx + 4, 1.0), inrb(nx + 4, 1.0), patm(nz + 2, 0.0), tatm(nz + 2, 0.0), dy(4, 0.0), indy(4, 0.0);
+        inr(nx + 4, 1.0), inrb(nx + 4, 1.0), patm(nz + 2, 0.0), tatm(nz + 2, 0.0), dy(ny + 4, 0.0), indy(ny + 4, 0.0);
     for (int i = 1; i <= nx; ++i) dx[i] = cfg->dx[i - 1];
     dx[0] = dx[1]; dx[nx + 1] = dx[nx + 2] = dx[nx + 3] = dx[nx];
     for (int k = 1; k <= nz; ++k) dz[k] = cfg->dz[k - 1];
     dz[0] = dz[1]; dz[nz + 1] = dz[nz + 2] = dz[nz + 3] = dz[nz];
     for (int i = 0; i < nx + 4; ++i) indx[i] = 1.0 / dx[i];
     for (int k = 0; k < nz + 4; ++k) indz[k] = 1.0 / dz[k];
+    if (ctx->d3) {
+        for (int j = 1; j <= ny; ++j) dy[j] = cfg->dy[j - 1];
+        dy[0] = dy[1]; dy[ny + 1] = dy[ny + 2] = dy[ny + 3] = dy[ny];
+        for (int j = 0; j < ny + 4; ++j) indy[j] = 1.0 / dy[j];
+    }
     if (cfg->itc == 1) {
         std::vector<double> xb(nx + 4, 0.0), x(nx + 4, 0.0);
         xb[1] = 0.0; x[1] = -0.5 * dx[1] + xb[1];
@@ -212,6 +221,9 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     // field arena: (name, number of ncell blocks)
     Fld &F = ctx->F;
     struct Slot { const char *name; double **ptr; int blocks; };
+    // 2D-only and 3D-only slots get zero blocks on the other path, the
+    // previous-visit interphase copies exist only when alpha < 1
+    int d3 = ctx->d3 ? 1 : 0, d2 = 1 - d3, a0 = cfg->alpha != 1.0 ? 1 : 0;
     std::vector<Slot> slots = {
         {"p", &F.p, 1}, {"ep", &F.ep, 1}, {"rog", &F.rog, 1}, {"rgp", &F.rgp, 1}, {"tg", &F.tg, 1},
         {"sieg", &F.sieg, 1}, {"cg", &F.cg, 1}, {"ug", &F.ug, 1}, {"vg", &F.vg, 1}, {"wg", &F.wg, 1},
@@ -219,16 +231,22 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
         {"ws", &F.ws, ns}, {"ygc", &F.ygc, ng}, {"xgc", &F.xgc, ng},
         {"pn", &F.pn, 1}, {"epn", &F.epn, 1}, {"rgpn", &F.rgpn, 1}, {"siegn", &F.siegn, 1},
         {"rlkn", &F.rlkn, ns}, {"siesn", &F.siesn, ns}, {"rgpgcn", &F.rgpgcn, ng}, {"mug", &F.mug, 1},
-        {"kapg", &F.kapg, 1}, {"rugn", &F.rugn, 1}, {"rwgn", &F.rwgn, 1}, {"rusn", &F.rusn, ns},
-        {"rwsn", &F.rwsn, ns}, {"rug", &F.rug, 1}, {"rwg", &F.rwg, 1}, {"rus", &F.rus, ns},
-        {"rws", &F.rws, ns}, {"appu", &F.appu, nap}, {"appw", &F.appw, nap},
-        {"ugfe", &F.ugfe, 1}, {"ugft", &F.ugft, 1}, {"wgfe", &F.wgfe, 1}, {"wgft", &F.wgft, 1},
-        {"usfe", &F.usfe, ns}, {"usft", &F.usft, ns}, {"wsfe", &F.wsfe, ns}, {"wsft", &F.wsft, ns},
-        {"rgfe", &F.rgfe, 1}, {"rgft", &F.rgft, 1}, {"rsfe", &F.rsfe, ns}, {"rsft", &F.rsft, ns},
-        {"conv", &F.conv, 1}, {"abeta", &F.abeta, 1}, {"egfe", &F.egfe, 1}, {"egft", &F.egft, 1},
-        {"esfe", &F.esfe, ns}, {"esft", &F.esft, ns}, {"rhg", &F.rhg, 1}, {"rhs", &F.rhs, ns},
-        {"yfe", &F.yfe, ng}, {"yft", &F.yft, ng}, {"sink", &F.sink, ns},
-        {"app0u", &ctx->d_app0u, nap}, {"app0w", &ctx->d_app0w, nap}};
+        {"kapg", &F.kapg, 1}, {"rugn", &F.rugn, 1}, {"rvgn", &F.rvgn, d3}, {"rwgn", &F.rwgn, 1},
+        {"rusn", &F.rusn, ns}, {"rvsn", &F.rvsn, ns * d3}, {"rwsn", &F.rwsn, ns},
+        {"rug", &F.rug, 1}, {"rvg", &F.rvg, d3}, {"rwg", &F.rwg, 1}, {"rus", &F.rus, ns},
+        {"rvs", &F.rvs, ns * d3}, {"rws", &F.rws, ns}, {"appu", &F.appu, nap}, {"appv", &F.appv, nap * d3},
+        {"appw", &F.appw, nap},
+        {"ugfe", &F.ugfe, d2}, {"ugft", &F.ugft, d2}, {"wgfe", &F.wgfe, d2}, {"wgft", &F.wgft, d2},
+        {"usfe", &F.usfe, ns * d2}, {"usft", &F.usft, ns * d2}, {"wsfe", &F.wsfe, ns * d2},
+        {"wsft", &F.wsft, ns * d2}, {"mf", &F.mf, 9 * (ns + 1) * d3},
+        {"rgfe", &F.rgfe, 1}, {"rgfn", &F.rgfn, d3}, {"rgft", &F.rgft, 1}, {"rsfe", &F.rsfe, ns},
+        {"rsfn", &F.rsfn, ns * d3}, {"rsft", &F.rsft, ns},
+        {"conv", &F.conv, 1}, {"abeta", &F.abeta, 1}, {"egfe", &F.egfe, 1}, {"egfn", &F.egfn, d3},
+        {"egft", &F.egft, 1}, {"esfe", &F.esfe, ns}, {"esfn", &F.esfn, ns * d3}, {"esft", &F.esft, ns},
+        {"rhg", &F.rhg, 1}, {"rhs", &F.rhs, ns},
+        {"yfe", &F.yfe, ng}, {"yfn", &F.yfn, ng * d3}, {"yft", &F.yft, ng}, {"sink", &F.sink, ns},
+        {"app0u", &ctx->d_app0u, nap * a0}, {"app0v", &ctx->d_app0v, nap * a0 * d3},
+        {"app0w", &ctx->d_app0w, nap * a0}};
     // each field starts on a 256-byte boundary
     size_t stride = ((size_t)n + 31) / 32 * 32;
     size_t total = 0;
@@ -238,6 +256,7 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     CK(cudaMemset(ctx->arena, 0, total * sizeof(double)));
     size_t o2 = 0;
     for (auto &s : slots) {
+        if (s.blocks == 0) { *s.ptr = nullptr; continue; }
         *s.ptr = ctx->arena + o2;
         ctx->names.push_back({s.name, {*s.ptr, (size_t)n * s.blocks}});
         o2 += stride * s.blocks;
@@ -278,9 +297,9 @@ static int xfer_state(pdac_ctx *ctx, pdac_state_view *s, bool up) {
     struct X { double *h; double *d; size_t cnt; bool need; };
     X xs[] = {{s->p, F.p, n, true}, {s->ep, F.ep, n, true}, {s->rog, F.rog, n, true}, {s->rgp, F.rgp, n, true},
               {s->tg, F.tg, n, true}, {s->sieg, F.sieg, n, true}, {s->cg, F.cg, n, true},
-              {s->ug, F.ug, n, true}, {s->vg, F.vg, n, false}, {s->wg, F.wg, n, true},
+              {s->ug, F.ug, n, true}, {s->vg, F.vg, n, ctx->d3}, {s->wg, F.wg, n, true},
               {s->rlk, F.rlk, n * ns, true}, {s->ts, F.ts, n * ns, true}, {s->sies, F.sies, n * ns, true},
-              {s->us, F.us, n * ns, true}, {s->vs, F.vs, n * ns, false}, {s->ws, F.ws, n * ns, true},
+              {s->us, F.us, n * ns, true}, {s->vs, F.vs, n * ns, ctx->d3}, {s->ws, F.ws, n * ns, true},
               {s->ygc, F.ygc, n * ng, true}, {s->xgc, F.xgc, n * ng, true}};
     for (auto &x : xs) {
         if (!x.h) {
@@ -304,7 +323,9 @@ int pdac_gpu_boundary(pdac_ctx *ctx, int sweep) {
     CK(cudaEventRecord(ctx->ev[0], st));
     if (ctx->nvent > 0 && ctx->cfg.irand >= 1)
         pdac::k_vent<<<blocks(ctx->nvent), TPB, 0, st>>>(ctx->P, ctx->F, ctx->d_vent, ctx->nvent, ctx->d_vfact, ctx->d_vfact0), ctx->launches++;
-    pdac::k_boundary2d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F), ctx->launches++;
+    if (ctx->d3) pdac::k_boundary3d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F);
+    else pdac::k_boundary2d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F);
+    ctx->launches++;
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[1], st));
     return PDAC_OK;
@@ -314,19 +335,19 @@ int pdac_gpu_fieldn(pdac_ctx *ctx) {
     if (!ctx) return PDAC_ERR_ARG;
     cudaStream_t st = ctx->stream;
     CK(cudaEventRecord(ctx->ev[2], st));
-    pdac::k_fieldn2d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F), ctx->launches++;
+    if (ctx->d3) pdac::k_fieldn3d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F);
+    else pdac::k_fieldn2d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F);
+    ctx->launches++;
     // allocate_fluxes (tilde.f:56-102): tilde and interphase terms start from
     // zero in every step
     size_t n = ctx->ncell;
     Fld &F = ctx->F;
-    CK(cudaMemsetAsync(F.rug, 0, n * sizeof(double), st));
-    CK(cudaMemsetAsync(F.rwg, 0, n * sizeof(double), st));
-    CK(cudaMemsetAsync(F.rus, 0, n * ctx->ns * sizeof(double), st));
-    CK(cudaMemsetAsync(F.rws, 0, n * ctx->ns * sizeof(double), st));
-    CK(cudaMemsetAsync(F.appu, 0, n * ctx->nap * sizeof(double), st));
-    CK(cudaMemsetAsync(F.appw, 0, n * ctx->nap * sizeof(double), st));
-    CK(cudaMemsetAsync(ctx->d_app0u, 0, n * ctx->nap * sizeof(double), st));
-    CK(cudaMemsetAsync(ctx->d_app0w, 0, n * ctx->nap * sizeof(double), st));
+    for (double *a : {F.rug, F.rvg, F.rwg})
+        if (a) CK(cudaMemsetAsync(a, 0, n * sizeof(double), st));
+    for (double *a : {F.rus, F.rvs, F.rws})
+        if (a) CK(cudaMemsetAsync(a, 0, n * ctx->ns * sizeof(double), st));
+    for (double *a : {F.appu, F.appv, F.appw, ctx->d_app0u, ctx->d_app0v, ctx->d_app0w})
+        if (a) CK(cudaMemsetAsync(a, 0, n * ctx->nap * sizeof(double), st));
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[3], st));
     return PDAC_OK;
@@ -338,13 +359,20 @@ int pdac_gpu_tilde(pdac_ctx *ctx, double dt) {
     size_t n = ctx->ncell, ns = ctx->ns;
     Fld &F = ctx->F;
     CK(cudaEventRecord(ctx->ev[4], st));
-    for (double *a : {F.ugfe, F.ugft, F.wgfe, F.wgft}) CK(cudaMemsetAsync(a, 0, n * sizeof(double), st));
-    for (double *a : {F.usfe, F.usft, F.wsfe, F.wsft}) CK(cudaMemsetAsync(a, 0, n * ns * sizeof(double), st));
-    pdac::k_tilde_flux2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F), ctx->launches++;
-    pdac::k_tilde2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt, ctx->d_app0u, ctx->d_app0w), ctx->launches++;
+    if (ctx->d3) {
+        CK(cudaMemsetAsync(F.mf, 0, n * 9 * (ns + 1) * sizeof(double), st));
+        pdac::k_tilde_flux3d<<<blocks(n), TPB, 0, st>>>(ctx->P, F), ctx->launches++;
+        pdac::k_tilde3d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt, ctx->d_app0u, ctx->d_app0v, ctx->d_app0w), ctx->launches++;
+    } else {
+        for (double *a : {F.ugfe, F.ugft, F.wgfe, F.wgft}) CK(cudaMemsetAsync(a, 0, n * sizeof(double), st));
+        for (double *a : {F.usfe, F.usft, F.wsfe, F.wsft}) CK(cudaMemsetAsync(a, 0, n * ns * sizeof(double), st));
+        pdac::k_tilde_flux2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F), ctx->launches++;
+        pdac::k_tilde2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt, ctx->d_app0u, ctx->d_app0w), ctx->launches++;
+    }
     if (ctx->P.alpha != 1.0 && ctx->cfg.rungekut > 1) {
         CK(cudaMemcpyAsync(ctx->d_app0u, F.appu, n * ctx->nap * sizeof(double), cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(ctx->d_app0w, F.appw, n * ctx->nap * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        if (ctx->d3) CK(cudaMemcpyAsync(ctx->d_app0v, F.appv, n * ctx->nap * sizeof(double), cudaMemcpyDeviceToDevice, st));
     }
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[5], st));
@@ -357,19 +385,27 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
     size_t n = ctx->ncell, ns = ctx->ns;
     Fld &F = ctx->F;
     CK(cudaEventRecord(ctx->ev[6], st));
-    for (double *a : {F.rgfe, F.rgft, F.conv, F.abeta}) CK(cudaMemsetAsync(a, 0, n * sizeof(double), st));
-    for (double *a : {F.rsfe, F.rsft}) CK(cudaMemsetAsync(a, 0, n * ns * sizeof(double), st));
-    pdac::k_predictor2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt), ctx->launches++;
-    pdac::k_mflux_init2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt), ctx->launches++;
+    for (double *a : {F.rgfe, F.rgfn, F.rgft, F.conv, F.abeta})
+        if (a) CK(cudaMemsetAsync(a, 0, n * sizeof(double), st));
+    for (double *a : {F.rsfe, F.rsfn, F.rsft})
+        if (a) CK(cudaMemsetAsync(a, 0, n * ns * sizeof(double), st));
+    if (ctx->d3) {
+        pdac::k_predictor3d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt), ctx->launches++;
+        pdac::k_mflux_init3d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt), ctx->launches++;
+    } else {
+        pdac::k_predictor2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt), ctx->launches++;
+        pdac::k_mflux_init2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt), ctx->launches++;
+    }
     CK(cudaGetLastError());
     int m = (ctx->nx + 2) / 3;
-    long nthr = (long)m * ctx->nz;
+    long nthr = (long)m * ctx->ny * ctx->nz;
     int nit;
     for (nit = 1; nit <= ctx->cfg.maxout; ++nit) {
         CK(cudaMemsetAsync(ctx->d_counters, 0, sizeof(int), st));
         for (int col = 0; col < 3; ++col) {
             if (ctx->prof) CK(cudaEventRecord(ctx->cev[2 * col], st));
-            pdac::k_corrector2d<<<blocks(nthr, TPB_CORR), TPB_CORR, 0, st>>>(ctx->P, F, dt, col, nit);
+            if (ctx->d3) pdac::k_corrector3d<<<blocks(nthr, TPB_CORR), TPB_CORR, 0, st>>>(ctx->P, F, dt, col, nit);
+            else pdac::k_corrector2d<<<blocks(nthr, TPB_CORR), TPB_CORR, 0, st>>>(ctx->P, F, dt, col, nit);
             ctx->launches++;
             if (ctx->prof) CK(cudaEventRecord(ctx->cev[2 * col + 1], st));
         }
@@ -403,10 +439,15 @@ int pdac_gpu_ygas(pdac_ctx *ctx, double dt) {
         CK(cudaMemcpyAsync(ctx->F.xgc, one.data(), n * sizeof(double), cudaMemcpyHostToDevice, st));
         CK(cudaStreamSynchronize(st));
     } else {
-        CK(cudaMemsetAsync(ctx->F.yfe, 0, n * ctx->ng * sizeof(double), st));
-        CK(cudaMemsetAsync(ctx->F.yft, 0, n * ctx->ng * sizeof(double), st));
-        pdac::k_ygas_flux2d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F), ctx->launches++;
-        pdac::k_ygas2d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F, dt), ctx->launches++;
+        for (double *a : {ctx->F.yfe, ctx->F.yfn, ctx->F.yft})
+            if (a) CK(cudaMemsetAsync(a, 0, n * ctx->ng * sizeof(double), st));
+        if (ctx->d3) {
+            pdac::k_ygas_flux3d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F), ctx->launches++;
+            pdac::k_ygas3d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F, dt), ctx->launches++;
+        } else {
+            pdac::k_ygas_flux2d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F), ctx->launches++;
+            pdac::k_ygas2d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F, dt), ctx->launches++;
+        }
     }
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[9], st));
@@ -419,12 +460,17 @@ int pdac_gpu_htilde(pdac_ctx *ctx, double dt) {
     size_t n = ctx->ncell, ns = ctx->ns;
     Fld &F = ctx->F;
     CK(cudaEventRecord(ctx->ev[10], st));
-    CK(cudaMemsetAsync(F.egfe, 0, n * sizeof(double), st));
-    CK(cudaMemsetAsync(F.egft, 0, n * sizeof(double), st));
-    CK(cudaMemsetAsync(F.esfe, 0, n * ns * sizeof(double), st));
-    CK(cudaMemsetAsync(F.esft, 0, n * ns * sizeof(double), st));
-    pdac::k_htilde_flux2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F), ctx->launches++;
-    pdac::k_htilde2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt), ctx->launches++;
+    for (double *a : {F.egfe, F.egfn, F.egft})
+        if (a) CK(cudaMemsetAsync(a, 0, n * sizeof(double), st));
+    for (double *a : {F.esfe, F.esfn, F.esft})
+        if (a) CK(cudaMemsetAsync(a, 0, n * ns * sizeof(double), st));
+    if (ctx->d3) {
+        pdac::k_htilde_flux3d<<<blocks(n), TPB, 0, st>>>(ctx->P, F), ctx->launches++;
+        pdac::k_htilde3d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt), ctx->launches++;
+    } else {
+        pdac::k_htilde_flux2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F), ctx->launches++;
+        pdac::k_htilde2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt), ctx->launches++;
+    }
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[11], st));
     return PDAC_OK;
@@ -435,7 +481,9 @@ int pdac_gpu_ftem(pdac_ctx *ctx, double dt) {
     cudaStream_t st = ctx->stream;
     CK(cudaEventRecord(ctx->ev[12], st));
     CK(cudaMemsetAsync(ctx->d_counters + 1, 0, sizeof(int), st));
-    pdac::k_ftem2d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F, dt), ctx->launches++;
+    if (ctx->d3) pdac::k_ftem3d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F, dt);
+    else pdac::k_ftem2d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F, dt);
+    ctx->launches++;
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[13], st));
     CK(cudaMemcpyAsync(ctx->h_counters + 1, ctx->d_counters + 1, sizeof(int), cudaMemcpyDeviceToHost, st));

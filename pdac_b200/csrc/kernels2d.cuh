@@ -30,9 +30,11 @@ __global__ void k_vent(Prm P, Fld F, const int *vent, int nvent, double *fact, d
     double rann = fact[q] * intensity, ranold = fact0[q] * intensity;
     fact0[q] = fact[q];
     F.ug[c] = F.ug[c] * (1.0 + rann) / (1.0 + ranold);
+    if (P.d3) F.vg[c] = F.vg[c] * (1.0 + rann) / (1.0 + ranold);
     F.wg[c] = F.wg[c] * (1.0 + rann) / (1.0 + ranold);
     for (int is = 1; is <= P.ns; ++is) {
         SOL(F.us, c, is) = SOL(F.us, c, is) * (1.0 + rann) / (1.0 + ranold);
+        if (P.d3) SOL(F.vs, c, is) = SOL(F.vs, c, is) * (1.0 + rann) / (1.0 + ranold);
         SOL(F.ws, c, is) = SOL(F.ws, c, is) * (1.0 + rann) / (1.0 + ranold);
     }
 }
@@ -1078,8 +1080,8 @@ __global__ void k_mass_partial(Prm P, Fld F, double *partial, int nq) {
     for (int q = 0; q < nq; ++q) sh[q * blockDim.x + tid] = 0.0;
     for (int c = blockIdx.x * blockDim.x + tid; c < P.ncell; c += gridDim.x * blockDim.x) {
         if (!fluid(P, c)) continue;
-        int i = c % P.nx + 1, k = c / P.nx + 1;
-        double vol = P.dx[i] * P.dz[k] * (P.itc == 1 ? P.r[i] : 1.0);
+        int i = c % P.nx + 1, j = (c / P.nx) % P.ny + 1, k = c / (P.nx * P.ny) + 1;
+        double vol = P.dx[i] * P.dz[k] * (P.itc == 1 ? P.r[i] : 1.0) * (P.d3 ? P.dy[j] : 1.0);
         sh[tid] += F.rgp[c] * vol;
         for (int is = 1; is <= P.ns; ++is) sh[is * blockDim.x + tid] += SOL(F.rlk, c, is) * vol;
         for (int ig = 0; ig < P.ng; ++ig) sh[(1 + P.ns + ig) * blockDim.x + tid] += F.rgp[c] * GAS(F.ygc, c, ig) * vol;
