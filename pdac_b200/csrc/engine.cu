@@ -37,10 +37,12 @@ struct pdac_ctx {
     cudaEvent_t ev[16];
     float phase_ms[7] = {0};
     // statistics: kernel launches, corrector launch timing (when profiling)
-    long long launches = 0, sweeps = 0, corr_launches = 0;
-    double corr_ms = 0.0;
+    long long launches = 0, sweeps = 0, corr_launches = 0, work_cells = 0;
+    double corr_ms = 0.0, resid_ms = 0.0, inner_ms = 0.0;
+    int *d_work = nullptr, *d_wcount = nullptr;  // corrector worklist and its per-colour lengths
+    int inner_grid = 0;
     bool prof = false;
-    cudaEvent_t cev[6];
+    cudaEvent_t cev[9];
     cudaEvent_t user_ev[32];
     std::vector<std::pair<std::string, std::pair<double *, size_t>>> names;
 };
@@ -62,6 +64,20 @@ int fail(pdac_ctx *c, int code, const std::string &msg) {
     } while (0)
 
 inline int blocks(long n, int tpb = TPB) { return (int)((n + tpb - 1) / tpb); }
+
+// launch a kernel template instantiated for the run's phase count (gas +
+// solid classes): 2, 3, 4 and 6 phases have register-resident phase systems,
+// any other count runs the generic instantiation
+#define PHASE_LAUNCH(nph, KERNEL, grid, tpb, st, ...)                              \
+    do {                                                                           \
+        switch (nph) {                                                             \
+            case 2: KERNEL<2><<<grid, tpb, 0, st>>>(__VA_ARGS__); break;           \
+            case 3: KERNEL<3><<<grid, tpb, 0, st>>>(__VA_ARGS__); break;           \
+            case 4: KERNEL<4><<<grid, tpb, 0, st>>>(__VA_ARGS__); break;           \
+            case 6: KERNEL<6><<<grid, tpb, 0, st>>>(__VA_ARGS__); break;           \
+            default: KERNEL<0><<<grid, tpb, 0, st>>>(__VA_ARGS__); break;          \
+        }                                                                          \
+    } while (0)
 
 // setup.f:551-616 and particles.f:35-79: gas and particle constants
 void set_constants(pdac_ctx *ctx) {
@@ -214,6 +230,14 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
         CK(cudaMemcpy(ctx->d_vfact, one.data(), cfg->nvent * sizeof(double), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(ctx->d_vfact0, zero.data(), cfg->nvent * sizeof(double), cudaMemcpyHostToDevice));
     }
+    CK(cudaMalloc(&ctx->d_work, (size_t)n * sizeof(int)));
+    CK(cudaMalloc(&ctx->d_wcount, 4 * sizeof(int)));
+    {
+        int dev = 0, nsm = 148;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        ctx->inner_grid = nsm * 16;
+    }
     CK(cudaMalloc(&ctx->d_counters, 8 * sizeof(int)));
     CK(cudaMemset(ctx->d_counters, 0, 8 * sizeof(int)));
     CK(cudaMallocHost(&ctx->h_counters, 8 * sizeof(int)));
@@ -280,6 +304,8 @@ int pdac_gpu_destroy(pdac_ctx *ctx) {
     cudaFree(ctx->d_vfact);
     cudaFree(ctx->d_vfact0);
     cudaFree(ctx->d_counters);
+    cudaFree(ctx->d_work);
+    cudaFree(ctx->d_wcount);
     cudaFree(ctx->d_partial);
     cudaFreeHost(ctx->h_counters);
     for (auto &e : ctx->ev) cudaEventDestroy(e);
@@ -389,38 +415,50 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
         if (a) CK(cudaMemsetAsync(a, 0, n * sizeof(double), st));
     for (double *a : {F.rsfe, F.rsfn, F.rsft})
         if (a) CK(cudaMemsetAsync(a, 0, n * ns * sizeof(double), st));
+    int nph = ctx->nph;
     if (ctx->d3) {
-        pdac::k_predictor3d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt), ctx->launches++;
-        pdac::k_mflux_init3d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt), ctx->launches++;
+        PHASE_LAUNCH(nph, pdac::k_predictor3d, blocks(n), TPB, st, ctx->P, F, dt);
+        pdac::k_mflux_init3d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt);
     } else {
-        pdac::k_predictor2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt), ctx->launches++;
-        pdac::k_mflux_init2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt), ctx->launches++;
+        PHASE_LAUNCH(nph, pdac::k_predictor2d, blocks(n), TPB, st, ctx->P, F, dt);
+        pdac::k_mflux_init2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt);
     }
+    ctx->launches += 2;
     CK(cudaGetLastError());
     int m = (ctx->nx + 2) / 3;
     long nthr = (long)m * ctx->ny * ctx->nz;
     int nit;
     for (nit = 1; nit <= ctx->cfg.maxout; ++nit) {
-        CK(cudaMemsetAsync(ctx->d_counters, 0, sizeof(int), st));
+        CK(cudaMemsetAsync(ctx->d_wcount, 0, 3 * sizeof(int), st));
         for (int col = 0; col < 3; ++col) {
-            if (ctx->prof) CK(cudaEventRecord(ctx->cev[2 * col], st));
-            if (ctx->d3) pdac::k_corrector3d<<<blocks(nthr, TPB_CORR), TPB_CORR, 0, st>>>(ctx->P, F, dt, col, nit);
-            else pdac::k_corrector2d<<<blocks(nthr, TPB_CORR), TPB_CORR, 0, st>>>(ctx->P, F, dt, col, nit);
-            ctx->launches++;
-            if (ctx->prof) CK(cudaEventRecord(ctx->cev[2 * col + 1], st));
+            int *cnt = ctx->d_wcount + col;
+            if (ctx->prof) CK(cudaEventRecord(ctx->cev[3 * col], st));
+            if (ctx->d3) PHASE_LAUNCH(nph, pdac::k_resid3d, blocks(nthr), TPB, st, ctx->P, F, dt, col, ctx->d_work, cnt);
+            else PHASE_LAUNCH(nph, pdac::k_resid2d, blocks(nthr), TPB, st, ctx->P, F, dt, col, ctx->d_work, cnt);
+            if (ctx->prof) CK(cudaEventRecord(ctx->cev[3 * col + 1], st));
+            int g = std::min(ctx->inner_grid, blocks(nthr, TPB_CORR));
+            if (ctx->d3) PHASE_LAUNCH(nph, pdac::k_inner3d, g, TPB_CORR, st, ctx->P, F, dt, nit, ctx->d_work, cnt);
+            else PHASE_LAUNCH(nph, pdac::k_inner2d, g, TPB_CORR, st, ctx->P, F, dt, nit, ctx->d_work, cnt);
+            if (ctx->prof) CK(cudaEventRecord(ctx->cev[3 * col + 2], st));
+            ctx->launches += 2;
         }
-        CK(cudaMemcpyAsync(ctx->h_counters, ctx->d_counters, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(ctx->h_counters, ctx->d_wcount, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         ctx->sweeps++;
+        long unconverged = (long)ctx->h_counters[0] + ctx->h_counters[1] + ctx->h_counters[2];
         if (ctx->prof) {
             for (int col = 0; col < 3; ++col) {
-                float t = 0;
-                CK(cudaEventElapsedTime(&t, ctx->cev[2 * col], ctx->cev[2 * col + 1]));
-                ctx->corr_ms += t;
+                float t0 = 0, t1 = 0;
+                CK(cudaEventElapsedTime(&t0, ctx->cev[3 * col], ctx->cev[3 * col + 1]));
+                CK(cudaEventElapsedTime(&t1, ctx->cev[3 * col + 1], ctx->cev[3 * col + 2]));
+                ctx->resid_ms += t0;
+                ctx->inner_ms += t1;
+                ctx->corr_ms += t0 + t1;
                 ctx->corr_launches++;
             }
+            ctx->work_cells += unconverged;
         }
-        if (ctx->h_counters[0] == 0) break;
+        if (unconverged == 0) break;
     }
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[7], st));
@@ -576,13 +614,18 @@ int pdac_gpu_stats(pdac_ctx *ctx, double *out, int nout) {
     out[1] = (double)ctx->sweeps;
     out[2] = (double)ctx->corr_launches;
     out[3] = ctx->corr_ms;
+    if (nout >= 7) {
+        out[4] = ctx->resid_ms;
+        out[5] = ctx->inner_ms;
+        out[6] = (double)ctx->work_cells;
+    }
     return PDAC_OK;
 }
 
 int pdac_gpu_reset_stats(pdac_ctx *ctx, int profile_corrector) {
     if (!ctx) return PDAC_ERR_ARG;
-    ctx->launches = ctx->sweeps = ctx->corr_launches = 0;
-    ctx->corr_ms = 0.0;
+    ctx->launches = ctx->sweeps = ctx->corr_launches = ctx->work_cells = 0;
+    ctx->corr_ms = ctx->resid_ms = ctx->inner_ms = 0.0;
     ctx->prof = profile_corrector != 0;
     return PDAC_OK;
 }

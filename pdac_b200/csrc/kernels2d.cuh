@@ -10,7 +10,7 @@
 // that cross of each other, so a phase is race free and equals a
 // Gauss-Seidel sweep in colour-major order.
 #pragma once
-#include "phys2d.cuh"
+#include "solve.cuh"
 
 namespace pdac {
 
@@ -524,101 +524,8 @@ __global__ void k_tilde2d(Prm P, Fld F, double dt, const double *app0u, const do
     for (int is = 1; is <= ns; ++is) { SOL(F.rus, c, is) = rus[is]; SOL(F.rws, c, is) = rws[is]; }
 }
 
-// ---------------------------------------------------------------------------
-// phase matrix, matrix.f:38-328 (2D): E/T faces and W/B faces of a cell
-// ---------------------------------------------------------------------------
-typedef double Mat[PDAC_MAXP + 1][PDAC_MAXP + 1];
-
-__device__ __forceinline__ void assemble_et_2d(const Prm &P, const Fld &F, const Raw2 &R, const Rem2 &M, int i, int k,
-                                               double dt, Mat &au, double *bu, Mat &aw, double *bw) {
-    const double *dx = P.dx, *dz = P.dz;
-    int c = R.c, ijke = M.e, ijkt = M.t;
-    double alpha = P.alpha, ag = P.alphagrav;
-    double dxi = dx[i], dxip1 = dx[i + 1], dzk = dz[k], dzkp1 = dz[k + 1];
-    double pijk = F.p[c];
-    double indxp = 1.0 / (dxi + dxip1), indzp = 1.0 / (dzk + dzkp1);
-    double ep_e = 1.0, ep_t = 1.0;
-    if (P.pmodel == 1) {
-        ep_e = (dxi * F.ep[ijke] + dxip1 * F.ep[c]) * indxp;
-        ep_t = (dzk * F.ep[ijkt] + dzkp1 * F.ep[c]) * indzp;
-    }
-    bu[1] = F.rug[c] + alpha * dt * indxp * 2.0 * ep_e * (pijk - F.p[ijke]);
-    bw[1] = F.rwg[c] + alpha * dt * indzp * 2.0 * ep_t * (pijk - F.p[ijkt]);
-    bu[1] = bu[1] + dt * ag * indxp * P.gravx * (dxi * F.rgp[ijke] + dxip1 * F.rgp[c]);
-    bw[1] = bw[1] + dt * ag * indzp * P.gravz * (dzk * F.rgp[ijkt] + dzkp1 * F.rgp[c]);
-    au[1][1] = alpha * (dxi * APP(F.appu, ijke, 1) + dxip1 * APP(F.appu, c, 1)) * indxp;
-    au[1][1] = au[1][1] + (dxi * F.rgp[ijke] + dxip1 * F.rgp[c]) * indxp;
-    aw[1][1] = alpha * (dzk * APP(F.appw, ijkt, 1) + dzkp1 * APP(F.appw, c, 1)) * indzp;
-    aw[1][1] = aw[1][1] + (dzk * F.rgp[ijkt] + dzkp1 * F.rgp[c]) * indzp;
-    for (int l = 2; l <= P.nph; ++l) {
-        double eps_e = 0, eps_t = 0;
-        if (P.pmodel == 1) {
-            eps_e = (dxi * SOL(F.rlk, ijke, l - 1) + dxip1 * SOL(F.rlk, c, l - 1)) * indxp * P.inrl[l - 1];
-            eps_t = (dzk * SOL(F.rlk, ijkt, l - 1) + dzkp1 * SOL(F.rlk, c, l - 1)) * indzp * P.inrl[l - 1];
-        }
-        bu[l] = SOL(F.rus, c, l - 1) + alpha * dt * indxp * 2.0 * eps_e * (pijk - F.p[ijke]);
-        bw[l] = SOL(F.rws, c, l - 1) + alpha * dt * indzp * 2.0 * eps_t * (pijk - F.p[ijkt]);
-        bu[l] = bu[l] + dt * ag * indxp * P.gravx * (dxi * SOL(F.rlk, ijke, l - 1) + dxip1 * SOL(F.rlk, c, l - 1));
-        bw[l] = bw[l] + dt * ag * indzp * P.gravz * (dzk * SOL(F.rlk, ijkt, l - 1) + dzkp1 * SOL(F.rlk, c, l - 1));
-        int ls1 = l * (l - 1) / 2;
-        for (int ll = 1; ll <= l; ++ll) {
-            int ls = ls1 + ll;
-            au[l][ll] = alpha * (dxi * APP(F.appu, ijke, ls) + dxip1 * APP(F.appu, c, ls)) * indxp;
-            au[ll][l] = au[l][ll];
-            aw[l][ll] = alpha * (dzk * APP(F.appw, ijkt, ls) + dzkp1 * APP(F.appw, c, ls)) * indzp;
-            aw[ll][l] = aw[l][ll];
-        }
-        au[l][l] = au[l][l] + (dxi * SOL(F.rlk, ijke, l - 1) + dxip1 * SOL(F.rlk, c, l - 1)) * indxp;
-        aw[l][l] = aw[l][l] + (dzk * SOL(F.rlk, ijkt, l - 1) + dzkp1 * SOL(F.rlk, c, l - 1)) * indzp;
-    }
-}
-
-__device__ __forceinline__ void assemble_wb_2d(const Prm &P, const Fld &F, const Raw2 &R, const Rem2 &M, int i, int k,
-                                               double dt, Mat &au1, double *bu1, Mat &aw1, double *bw1) {
-    const double *dx = P.dx, *dz = P.dz;
-    int c = R.c, imjk = R.w, ijkm = R.b, ijkw = M.w, ijkb = M.b;
-    double alpha = P.alpha, ag = P.alphagrav;
-    double dxi = dx[i], dxim1 = dx[i - 1], dzk = dz[k], dzkm1 = dz[k - 1];
-    double pijk = F.p[c], epijk = F.ep[c], rgpijk = F.rgp[c];
-    double indxm = 1.0 / (dx[i] + dx[i - 1]), indzm = 1.0 / (dz[k] + dz[k - 1]);
-    double ep_w = 1.0, ep_b = 1.0;
-    if (P.pmodel == 1) {
-        ep_w = (dxi * F.ep[ijkw] + dxim1 * epijk) * indxm;
-        ep_b = (dzk * F.ep[ijkb] + dzkm1 * epijk) * indzm;
-    }
-    bu1[1] = F.rug[imjk] + alpha * dt * indxm * 2.0 * ep_w * (F.p[ijkw] - pijk);
-    bw1[1] = F.rwg[ijkm] + alpha * dt * indzm * 2.0 * ep_b * (F.p[ijkb] - pijk);
-    bu1[1] = bu1[1] + dt * ag * indxm * P.gravx * (dxi * F.rgp[ijkw] + dxim1 * F.rgp[c]);
-    bw1[1] = bw1[1] + dt * ag * indzm * P.gravz * (dzk * F.rgp[ijkb] + dzkm1 * F.rgp[c]);
-    au1[1][1] = alpha * (dxi * APP(F.appu, ijkw, 1) + dxim1 * APP(F.appu, c, 1)) * indxm;
-    au1[1][1] = au1[1][1] + (dxi * F.rgp[ijkw] + dxim1 * rgpijk) * indxm;
-    aw1[1][1] = alpha * (dzk * APP(F.appw, ijkb, 1) + dzkm1 * APP(F.appw, c, 1)) * indzm;
-    aw1[1][1] = aw1[1][1] + (dzk * F.rgp[ijkb] + dzkm1 * rgpijk) * indzm;
-    for (int l = 2; l <= P.nph; ++l) {
-        double rlklm1 = SOL(F.rlk, c, l - 1);
-        double eps_w = 0, eps_b = 0;
-        if (P.pmodel == 1) {
-            eps_w = (dxi * SOL(F.rlk, ijkw, l - 1) + dxim1 * rlklm1) * indxm * P.inrl[l - 1];
-            eps_b = (dzk * SOL(F.rlk, ijkb, l - 1) + dzkm1 * rlklm1) * indzm * P.inrl[l - 1];
-        }
-        bu1[l] = SOL(F.rus, imjk, l - 1) + alpha * dt * indxm * 2.0 * eps_w * (F.p[ijkw] - pijk);
-        bw1[l] = SOL(F.rws, ijkm, l - 1) + alpha * dt * indzm * 2.0 * eps_b * (F.p[ijkb] - pijk);
-        bu1[l] = bu1[l] + dt * ag * indxm * P.gravx * (dxi * SOL(F.rlk, ijkw, l - 1) + dxim1 * SOL(F.rlk, c, l - 1));
-        bw1[l] = bw1[l] + dt * ag * indzm * P.gravz * (dzk * SOL(F.rlk, ijkb, l - 1) + dzkm1 * SOL(F.rlk, c, l - 1));
-        int ls1 = l * (l - 1) / 2;
-        for (int ll = 1; ll <= l; ++ll) {
-            int ls = ls1 + ll;
-            au1[ll][l] = alpha * (dxi * APP(F.appu, ijkw, ls) + dxim1 * APP(F.appu, c, ls)) * indxm;
-            au1[l][ll] = au1[ll][l];
-            aw1[ll][l] = alpha * (dzk * APP(F.appw, ijkb, ls) + dzkm1 * APP(F.appw, c, ls)) * indzm;
-            aw1[l][ll] = aw1[ll][l];
-        }
-        au1[l][l] = au1[l][l] + (dxi * SOL(F.rlk, ijkw, l - 1) + dxim1 * rlklm1) * indxm;
-        aw1[l][l] = aw1[l][l] + (dzk * SOL(F.rlk, ijkb, l - 1) + dzkm1 * rlklm1) * indzm;
-    }
-}
-
 // predictor, iter.f:135-145
+template <int NP>
 __global__ void k_predictor2d(Prm P, Fld F, double dt) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.ncell || !fluid(P, c)) return;
@@ -627,19 +534,8 @@ __global__ void k_predictor2d(Prm P, Fld F, double dt) {
     Rem2 M;
     raw2(P, i, k, R);
     rem2(P, i, k, R, M);
-    Mat au, aw;
-    double bu[PDAC_MAXP + 1], bw[PDAC_MAXP + 1];
-    assemble_et_2d(P, F, R, M, i, k, dt, au, bu, aw, bw);
-    if (fluid(P, R.e)) {
-        gauss_jordan(P, au, bu);
-        F.ug[c] = bu[1];
-        for (int l = 2; l <= P.nph; ++l) SOL(F.us, c, l - 1) = bu[l];
-    }
-    if (fluid(P, R.t)) {
-        gauss_jordan(P, aw, bw);
-        F.wg[c] = bw[1];
-        for (int l = 2; l <= P.nph; ++l) SOL(F.ws, c, l - 1) = bw[l];
-    }
+    face_solve<NP>(P, F, c, M.e, R.e, i, 0, +1, dt);
+    face_solve<NP>(P, F, c, M.t, R.t, k, 2, +1, dt);
 }
 
 // gas mass flux of one cell over its four faces (calc_gas_mass_flux,
@@ -767,92 +663,98 @@ __device__ __forceinline__ void padjust(PAdj &s, double &p, int &kros, double d3
     p3 = p;
 }
 
-// one colour phase of an outer sweep: corrector + inner_loop, iter.f:241-319, 480-580
-__global__ void k_corrector2d(Prm P, Fld F, double dt, int colour, int nit) {
+// One colour phase of an outer sweep (iter.f:241-319) runs as two launches:
+// k_resid2d tests every cell of the colour, updates the volume fractions of
+// converged cells (calc_eps) and appends unconverged ones to a worklist;
+// k_inner2d runs inner_loop (iter.f:480-580) on the worklist.  Cells of one
+// colour never touch each other's data, so the split changes no result.
+__device__ __forceinline__ int colour_cell2d(const Prm &P, int t, int colour, int &i, int &k) {
     int m = (P.nx + 2) / 3;
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= m * P.nz) return;
-    int k = t / m + 1, q = t % m;
+    if (t >= m * P.nz) return -1;
+    k = t / m + 1;
+    int q = t % m;
     int i0 = (((colour - 1 - k) % 3) + 3) % 3;
     if (i0 == 0) i0 = 3;
-    int i = i0 + 3 * q;
-    if (i > P.nx) return;
-    int c = (i - 1) + P.nx * (k - 1);
-    if (!fluid(P, c)) return;
-    Raw2 R;
-    Rem2 M;
-    raw2(P, i, k, R);
-    rem2(P, i, k, R, M);
-    double dg = calc_res_2d(P, F, R, i, k, dt);
-    double dgorig = dg;
-    double conv = F.conv[c];
-    if (fabs(dg) <= conv) {
-        calc_eps_2d(P, F, R, i, k, dt);
-        F.rgp[c] = F.ep[c] * F.rog[c];
-        return;
-    }
-    atomicAdd(&F.counters[0], 1);
-    double d3 = dg, p3 = F.p[c], abeta = F.abeta[c];
-    double xg[PDAC_MAXG];
-    for (int ig = 0; ig < P.ng; ++ig) xg[ig] = GAS(F.xgc, c, ig);
-    double tgc = F.tg[c];
-    int kros = -1;
-    PAdj s = {0, 0, 0, 0, 0, 0};
-    double p = F.p[c];
-    for (int loop = 1; loop <= P.inmax; ++loop) {
-        if (loop > 1 || nit > 1) padjust(s, p, kros, d3, p3, P.omega, abeta);
-        F.p[c] = p;
-        double rog = thermal_eosg(P, tgc, p, xg);
-        F.rog[c] = rog;
-        F.rgp[c] = F.ep[c] * rog;
-        {
-            Mat au1, aw1, au, aw;
-            double bu1[PDAC_MAXP + 1], bw1[PDAC_MAXP + 1], bu[PDAC_MAXP + 1], bw[PDAC_MAXP + 1];
-            assemble_wb_2d(P, F, R, M, i, k, dt, au1, bu1, aw1, bw1);
-            assemble_et_2d(P, F, R, M, i, k, dt, au, bu, aw, bw);
-            if (fluid(P, R.w)) {
-                gauss_jordan(P, au1, bu1);
-                F.ug[R.w] = bu1[1];
-                for (int l = 2; l <= P.nph; ++l) SOL(F.us, R.w, l - 1) = bu1[l];
-            }
-            if (fluid(P, R.b)) {
-                gauss_jordan(P, aw1, bw1);
-                F.wg[R.b] = bw1[1];
-                for (int l = 2; l <= P.nph; ++l) SOL(F.ws, R.b, l - 1) = bw1[l];
-            }
-            if (fluid(P, R.e)) {
-                gauss_jordan(P, au, bu);
-                F.ug[c] = bu[1];
-                for (int l = 2; l <= P.nph; ++l) SOL(F.us, c, l - 1) = bu[l];
-            }
-            if (fluid(P, R.t)) {
-                gauss_jordan(P, aw, bw);
-                F.wg[c] = bw[1];
-                for (int l = 2; l <= P.nph; ++l) SOL(F.ws, c, l - 1) = bw[l];
-            }
-        }
-        for (int is = 1; is <= P.ns; ++is) {
-            size_t off = (size_t)(is - 1) * P.ncell;
-            MF2 f;
-            cell_massflux(P, F.rlk + off, F.us + off, F.ws + off, R, M, i, k, f);
-            F.rsfe[off + c] = f.e; F.rsft[off + c] = f.t; F.rsfe[off + R.w] = f.w; F.rsft[off + R.b] = f.b;
-        }
-        calc_eps_2d(P, F, R, i, k, dt);
-        F.rgp[c] = F.ep[c] * rog;
-        {
-            MF2 f;
-            cell_massflux(P, F.rgp, F.ug, F.wg, R, M, i, k, f);
-            F.rgfe[c] = f.e; F.rgft[c] = f.t; F.rgfe[R.w] = f.w; F.rgft[R.b] = f.b;
-        }
-        dg = calc_res_2d(P, F, R, i, k, dt);
-        if (fabs(dg) > conv || fabs(dg) >= fabs(dgorig)) {
-            if (nit == 1 && loop == 1) dgorig = dg;
-            d3 = dg;
-        } else if (fabs(dg) <= conv) {
-            break;
+    i = i0 + 3 * q;
+    if (i > P.nx) return -1;
+    return (i - 1) + P.nx * (k - 1);
+}
+
+template <int NP>
+__global__ void k_resid2d(Prm P, Fld F, double dt, int colour, int *list, int *count) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int i = 0, k = 0;
+    int c = colour_cell2d(P, t, colour, i, k);
+    bool want = false;
+    if (c >= 0 && fluid(P, c)) {
+        Raw2 R;
+        raw2(P, i, k, R);
+        double dg = calc_res_2d(P, F, R, i, k, dt);
+        if (fabs(dg) <= F.conv[c]) {
+            calc_eps_2d(P, F, R, i, k, dt);
+            F.rgp[c] = F.ep[c] * F.rog[c];
+        } else {
+            want = true;
         }
     }
-    F.abeta[c] = abeta;
+    work_append(list, count, c, want);
+}
+
+template <int NP>
+__global__ void __launch_bounds__(64) k_inner2d(Prm P, Fld F, double dt, int nit, const int *list, const int *count) {
+    const int nwork = *count;
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nwork; w += gridDim.x * blockDim.x) {
+        int c = list[w];
+        int i = c % P.nx + 1, k = c / P.nx + 1;
+        Raw2 R;
+        Rem2 M;
+        raw2(P, i, k, R);
+        rem2(P, i, k, R, M);
+        double dg = calc_res_2d(P, F, R, i, k, dt);
+        double dgorig = dg;
+        double conv = F.conv[c];
+        double d3 = dg, p3 = F.p[c], abeta = F.abeta[c];
+        double xg[PDAC_MAXG];
+        for (int ig = 0; ig < P.ng; ++ig) xg[ig] = GAS(F.xgc, c, ig);
+        double tgc = F.tg[c];
+        int kros = -1;
+        PAdj s = {0, 0, 0, 0, 0, 0};
+        double p = F.p[c];
+        for (int loop = 1; loop <= P.inmax; ++loop) {
+            if (loop > 1 || nit > 1) padjust(s, p, kros, d3, p3, P.omega, abeta);
+            F.p[c] = p;
+            double rog = thermal_eosg(P, tgc, p, xg);
+            F.rog[c] = rog;
+            F.rgp[c] = F.ep[c] * rog;
+            // W, B then E, T faces (matrix.f:351-479)
+            face_solve<NP>(P, F, c, M.w, R.w, i, 0, -1, dt);
+            face_solve<NP>(P, F, c, M.b, R.b, k, 2, -1, dt);
+            face_solve<NP>(P, F, c, M.e, R.e, i, 0, +1, dt);
+            face_solve<NP>(P, F, c, M.t, R.t, k, 2, +1, dt);
+#pragma unroll
+            for (int is = 1; is <= nphases<NP>(P) - 1; ++is) {
+                size_t off = (size_t)(is - 1) * P.ncell;
+                MF2 f;
+                cell_massflux(P, F.rlk + off, F.us + off, F.ws + off, R, M, i, k, f);
+                F.rsfe[off + c] = f.e; F.rsft[off + c] = f.t; F.rsfe[off + R.w] = f.w; F.rsft[off + R.b] = f.b;
+            }
+            calc_eps_2d(P, F, R, i, k, dt);
+            F.rgp[c] = F.ep[c] * rog;
+            {
+                MF2 f;
+                cell_massflux(P, F.rgp, F.ug, F.wg, R, M, i, k, f);
+                F.rgfe[c] = f.e; F.rgft[c] = f.t; F.rgfe[R.w] = f.w; F.rgft[R.b] = f.b;
+            }
+            dg = calc_res_2d(P, F, R, i, k, dt);
+            if (fabs(dg) > conv || fabs(dg) >= fabs(dgorig)) {
+                if (nit == 1 && loop == 1) dgorig = dg;
+                d3 = dg;
+            } else if (fabs(dg) <= conv) {
+                break;
+            }
+        }
+        F.abeta[c] = abeta;
+    }
 }
 
 // ---------------------------------------------------------------------------

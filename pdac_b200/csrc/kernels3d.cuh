@@ -470,92 +470,8 @@ __global__ void k_tilde3d(Prm P, Fld F, double dt, const double *app0u, const do
     for (int is = 1; is <= ns; ++is) { SOL(F.rus, c, is) = rr[is][0]; SOL(F.rvs, c, is) = rr[is][1]; SOL(F.rws, c, is) = rr[is][2]; }
 }
 
-// ---------------------------------------------------------------------------
-// phase matrix of one face, matrix.f:38-328 (3D).  dir 0/1/2 = x/y/z,
-// side +1 = E/N/T face (assemble_matrix), -1 = W/S/B face (assemble_all_matrix)
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void assemble_3d(const Prm &P, const Fld &F, const Raw3 &R, const Rem3 &M, int i, int j,
-                                            int k, double dt, int dir, int side, Mat &a, double *b) {
-    int c = R.c;
-    const double *dd = dir == 0 ? P.dx : (dir == 1 ? P.dy : P.dz);
-    int ii = dir == 0 ? i : (dir == 1 ? j : k);
-    double grav = dir == 0 ? P.gravx : (dir == 1 ? P.gravy : P.gravz);
-    const double *app = dir == 0 ? F.appu : (dir == 1 ? F.appv : F.appw);
-    const double *rg = dir == 0 ? F.rug : (dir == 1 ? F.rvg : F.rwg);
-    const double *rs = dir == 0 ? F.rus : (dir == 1 ? F.rvs : F.rws);
-    double alpha = P.alpha, ag = P.alphagrav, pijk = F.p[c];
-    if (side > 0) {
-        int nb = dir == 0 ? M.e : (dir == 1 ? M.n : M.t);
-        double d0 = dd[ii], d1 = dd[ii + 1];
-        double inp = 1.0 / (d0 + d1);
-        double ep_f = 1.0;
-        if (P.pmodel == 1) ep_f = (d0 * F.ep[nb] + d1 * F.ep[c]) * inp;
-        b[1] = rg[c] + alpha * dt * inp * 2.0 * ep_f * (pijk - F.p[nb]);
-        b[1] = b[1] + dt * ag * inp * grav * (d0 * F.rgp[nb] + d1 * F.rgp[c]);
-        a[1][1] = alpha * (d0 * APP(app, nb, 1) + d1 * APP(app, c, 1)) * inp;
-        a[1][1] = a[1][1] + (d0 * F.rgp[nb] + d1 * F.rgp[c]) * inp;
-        for (int l = 2; l <= P.nph; ++l) {
-            double rn = SOL(F.rlk, nb, l - 1), rc = SOL(F.rlk, c, l - 1);
-            double eps_f = 0.0;
-            if (P.pmodel == 1) eps_f = (d0 * rn + d1 * rc) * inp * P.inrl[l - 1];
-            b[l] = SOL(rs, c, l - 1) + alpha * dt * inp * 2.0 * eps_f * (pijk - F.p[nb]);
-            b[l] = b[l] + dt * ag * inp * grav * (d0 * rn + d1 * rc);
-            int ls1 = l * (l - 1) / 2;
-            for (int ll = 1; ll <= l; ++ll) {
-                int ls = ls1 + ll;
-                a[l][ll] = alpha * (d0 * APP(app, nb, ls) + d1 * APP(app, c, ls)) * inp;
-                a[ll][l] = a[l][ll];
-            }
-            a[l][l] = a[l][l] + (d0 * rn + d1 * rc) * inp;
-        }
-    } else {
-        int nb = dir == 0 ? M.w : (dir == 1 ? M.s : M.b);
-        int rawm = dir == 0 ? R.w : (dir == 1 ? R.s : R.b);
-        double d0 = dd[ii], dm1 = dd[ii - 1];
-        double inm = 1.0 / (d0 + dm1);
-        double ep_f = 1.0;
-        if (P.pmodel == 1) ep_f = (d0 * F.ep[nb] + dm1 * F.ep[c]) * inm;
-        b[1] = rg[rawm] + alpha * dt * inm * 2.0 * ep_f * (F.p[nb] - pijk);
-        b[1] = b[1] + dt * ag * inm * grav * (d0 * F.rgp[nb] + dm1 * F.rgp[c]);
-        a[1][1] = alpha * (d0 * APP(app, nb, 1) + dm1 * APP(app, c, 1)) * inm;
-        a[1][1] = a[1][1] + (d0 * F.rgp[nb] + dm1 * F.rgp[c]) * inm;
-        for (int l = 2; l <= P.nph; ++l) {
-            double rn = SOL(F.rlk, nb, l - 1), rc = SOL(F.rlk, c, l - 1);
-            double eps_f = 0.0;
-            if (P.pmodel == 1) eps_f = (d0 * rn + dm1 * rc) * inm * P.inrl[l - 1];
-            b[l] = SOL(rs, rawm, l - 1) + alpha * dt * inm * 2.0 * eps_f * (F.p[nb] - pijk);
-            b[l] = b[l] + dt * ag * inm * grav * (d0 * rn + dm1 * rc);
-            int ls1 = l * (l - 1) / 2;
-            for (int ll = 1; ll <= l; ++ll) {
-                int ls = ls1 + ll;
-                a[ll][l] = alpha * (d0 * APP(app, nb, ls) + dm1 * APP(app, c, ls)) * inm;
-                a[l][ll] = a[ll][l];
-            }
-            a[l][l] = a[l][l] + (d0 * rn + dm1 * rc) * inm;
-        }
-    }
-}
-
-// assemble one face's phase matrix and, when the face neighbour is fluid,
-// solve it and store the face velocities (matrix.f:351-630).  The six faces
-// of a cell are independent: no assembly reads what another face's solve
-// writes, so solving them one at a time equals assembling all first.
-__device__ __forceinline__ void face_solve_3d(const Prm &P, const Fld &F, const Raw3 &R, const Rem3 &M, int i, int j,
-                                              int k, double dt, int dir, int side) {
-    int nbr = side > 0 ? (dir == 0 ? R.e : (dir == 1 ? R.n : R.t)) : (dir == 0 ? R.w : (dir == 1 ? R.s : R.b));
-    if (!fluid(P, nbr)) return;
-    Mat a;
-    double b[PDAC_MAXP + 1];
-    assemble_3d(P, F, R, M, i, j, k, dt, dir, side, a, b);
-    gauss_jordan(P, a, b);
-    int store = side > 0 ? R.c : nbr;
-    double *g = dir == 0 ? F.ug : (dir == 1 ? F.vg : F.wg);
-    double *s = dir == 0 ? F.us : (dir == 1 ? F.vs : F.ws);
-    g[store] = b[1];
-    for (int l = 2; l <= P.nph; ++l) SOL(s, store, l - 1) = b[l];
-}
-
 // predictor, iter.f:135-145
+template <int NP>
 __global__ void k_predictor3d(Prm P, Fld F, double dt) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.ncell || !fluid(P, c)) return;
@@ -565,7 +481,9 @@ __global__ void k_predictor3d(Prm P, Fld F, double dt) {
     Rem3 M;
     raw3(P, i, j, k, R);
     rem3(P, i, j, k, R, M);
-    for (int d = 0; d < 3; ++d) face_solve_3d(P, F, R, M, i, j, k, dt, d, +1);
+    face_solve<NP>(P, F, c, M.e, R.e, i, 0, +1, dt);
+    face_solve<NP>(P, F, c, M.n, R.n, j, 1, +1, dt);
+    face_solve<NP>(P, F, c, M.t, R.t, k, 2, +1, dt);
 }
 
 // mass flux of one cell over its six faces (calc_gas_mass_flux and
@@ -640,10 +558,12 @@ __device__ __forceinline__ double calc_res_3d(const Prm &P, const Fld &F, const 
 }
 
 // calc_eps, iter.f:927-994 (3D)
+template <int NP>
 __device__ __forceinline__ void calc_eps_3d(const Prm &P, const Fld &F, const Raw3 &R, int i, int j, int k, double dt) {
     int c = R.c;
     double rls = 0;
-    for (int is = 1; is <= P.ns; ++is) {
+#pragma unroll
+    for (int is = 1; is <= nphases<NP>(P) - 1; ++is) {
         double rlkx = (1.0 * SOL(F.rsfe, c, is) - 1.0 * SOL(F.rsfe, R.w, is)) * P.indx[i] * 1.0;
         double rlkz = (1.0 * SOL(F.rsft, c, is) - 1.0 * SOL(F.rsft, R.b, is)) * P.indz[k];
         double rlky = (1.0 * SOL(F.rsfn, c, is) - 1.0 * SOL(F.rsfn, R.s, is)) * P.indy[j];
@@ -657,72 +577,104 @@ __device__ __forceinline__ void calc_eps_3d(const Prm &P, const Fld &F, const Ra
     if (rls > 1.0) atomicAdd(&F.counters[2], 1);
 }
 
-// one colour phase of an outer sweep: corrector + inner_loop, iter.f:241-319, 480-580 (3D)
-__global__ void k_corrector3d(Prm P, Fld F, double dt, int colour, int nit) {
+// One colour phase of an outer sweep (iter.f:241-319) runs as two launches.
+// k_resid3d tests every cell of the colour: a converged cell only updates its
+// volume fractions (calc_eps), an unconverged one is appended to a worklist;
+// k_inner3d then runs inner_loop (iter.f:480-580) on the worklist.  Cells of
+// one colour never touch each other's data, so the split changes no result.
+__device__ __forceinline__ int colour_cell3d(const Prm &P, long t, int colour, int &i, int &j, int &k) {
     int m = (P.nx + 2) / 3;
-    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)m * P.ny * P.nz) return;
+    if (t >= (long)m * P.ny * P.nz) return -1;
     int q = (int)(t % m);
     long rest = t / m;
-    int j = (int)(rest % P.ny) + 1, k = (int)(rest / P.ny) + 1;
+    j = (int)(rest % P.ny) + 1;
+    k = (int)(rest / P.ny) + 1;
     int i0 = (((colour - j - k) % 3) + 3) % 3;
     if (i0 == 0) i0 = 3;
-    int i = i0 + 3 * q;
-    if (i > P.nx) return;
-    int c = at3(P, i, j, k);
-    if (!fluid(P, c)) return;
-    Raw3 R;
-    Rem3 M;
-    raw3(P, i, j, k, R);
-    rem3(P, i, j, k, R, M);
-    double dg = calc_res_3d(P, F, R, i, j, k, dt);
-    double dgorig = dg;
-    double conv = F.conv[c];
-    if (fabs(dg) <= conv) {
-        calc_eps_3d(P, F, R, i, j, k, dt);
-        F.rgp[c] = F.ep[c] * F.rog[c];
-        return;
-    }
-    atomicAdd(&F.counters[0], 1);
-    double d3 = dg, p3 = F.p[c], abeta = F.abeta[c];
-    double xg[PDAC_MAXG];
-    for (int ig = 0; ig < P.ng; ++ig) xg[ig] = GAS(F.xgc, c, ig);
-    double tgc = F.tg[c];
-    int kros = -1;
-    PAdj s = {0, 0, 0, 0, 0, 0};
-    double p = F.p[c];
-    for (int loop = 1; loop <= P.inmax; ++loop) {
-        if (loop > 1 || nit > 1) padjust(s, p, kros, d3, p3, P.omega, abeta);
-        F.p[c] = p;
-        double rog = thermal_eosg(P, tgc, p, xg);
-        F.rog[c] = rog;
-        F.rgp[c] = F.ep[c] * rog;
-        for (int d = 0; d < 3; ++d) face_solve_3d(P, F, R, M, i, j, k, dt, d, -1);
-        for (int d = 0; d < 3; ++d) face_solve_3d(P, F, R, M, i, j, k, dt, d, +1);
-        for (int is = 1; is <= P.ns; ++is) {
-            size_t off = (size_t)(is - 1) * P.ncell;
-            F6d f;
-            cell_massflux3d(P, F.rlk + off, F.us + off, F.vs + off, F.ws + off, R, M, i, j, k, f);
-            F.rsfe[off + c] = f.e; F.rsfn[off + c] = f.n; F.rsft[off + c] = f.t;
-            F.rsfe[off + R.w] = f.w; F.rsfn[off + R.s] = f.s; F.rsft[off + R.b] = f.b;
-        }
-        calc_eps_3d(P, F, R, i, j, k, dt);
-        F.rgp[c] = F.ep[c] * rog;
-        {
-            F6d f;
-            cell_massflux3d(P, F.rgp, F.ug, F.vg, F.wg, R, M, i, j, k, f);
-            F.rgfe[c] = f.e; F.rgfn[c] = f.n; F.rgft[c] = f.t;
-            F.rgfe[R.w] = f.w; F.rgfn[R.s] = f.s; F.rgft[R.b] = f.b;
-        }
-        dg = calc_res_3d(P, F, R, i, j, k, dt);
-        if (fabs(dg) > conv || fabs(dg) >= fabs(dgorig)) {
-            if (nit == 1 && loop == 1) dgorig = dg;
-            d3 = dg;
-        } else if (fabs(dg) <= conv) {
-            break;
+    i = i0 + 3 * q;
+    if (i > P.nx) return -1;
+    return at3(P, i, j, k);
+}
+
+template <int NP>
+__global__ void k_resid3d(Prm P, Fld F, double dt, int colour, int *list, int *count) {
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i = 0, j = 0, k = 0;
+    int c = colour_cell3d(P, t, colour, i, j, k);
+    bool want = false;
+    if (c >= 0 && fluid(P, c)) {
+        Raw3 R;
+        raw3(P, i, j, k, R);
+        double dg = calc_res_3d(P, F, R, i, j, k, dt);
+        if (fabs(dg) <= F.conv[c]) {
+            calc_eps_3d<NP>(P, F, R, i, j, k, dt);
+            F.rgp[c] = F.ep[c] * F.rog[c];
+        } else {
+            want = true;
         }
     }
-    F.abeta[c] = abeta;
+    work_append(list, count, c, want);
+}
+
+template <int NP>
+__global__ void __launch_bounds__(64) k_inner3d(Prm P, Fld F, double dt, int nit, const int *list, const int *count) {
+    const int nwork = *count;
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nwork; w += gridDim.x * blockDim.x) {
+        int c = list[w], i, j, k;
+        ijk_of(P, c, i, j, k);
+        Raw3 R;
+        Rem3 M;
+        raw3(P, i, j, k, R);
+        rem3(P, i, j, k, R, M);
+        double dg = calc_res_3d(P, F, R, i, j, k, dt);
+        double dgorig = dg;
+        double conv = F.conv[c];
+        double d3 = dg, p3 = F.p[c], abeta = F.abeta[c];
+        double xg[PDAC_MAXG];
+        for (int ig = 0; ig < P.ng; ++ig) xg[ig] = GAS(F.xgc, c, ig);
+        double tgc = F.tg[c];
+        int kros = -1;
+        PAdj s = {0, 0, 0, 0, 0, 0};
+        double p = F.p[c];
+        for (int loop = 1; loop <= P.inmax; ++loop) {
+            if (loop > 1 || nit > 1) padjust(s, p, kros, d3, p3, P.omega, abeta);
+            F.p[c] = p;
+            double rog = thermal_eosg(P, tgc, p, xg);
+            F.rog[c] = rog;
+            F.rgp[c] = F.ep[c] * rog;
+            // W, S, B then E, N, T faces (matrix.f:351-479, 494-630)
+            face_solve<NP>(P, F, c, M.w, R.w, i, 0, -1, dt);
+            face_solve<NP>(P, F, c, M.s, R.s, j, 1, -1, dt);
+            face_solve<NP>(P, F, c, M.b, R.b, k, 2, -1, dt);
+            face_solve<NP>(P, F, c, M.e, R.e, i, 0, +1, dt);
+            face_solve<NP>(P, F, c, M.n, R.n, j, 1, +1, dt);
+            face_solve<NP>(P, F, c, M.t, R.t, k, 2, +1, dt);
+#pragma unroll
+            for (int is = 1; is <= nphases<NP>(P) - 1; ++is) {
+                size_t off = (size_t)(is - 1) * P.ncell;
+                F6d f;
+                cell_massflux3d(P, F.rlk + off, F.us + off, F.vs + off, F.ws + off, R, M, i, j, k, f);
+                F.rsfe[off + c] = f.e; F.rsfn[off + c] = f.n; F.rsft[off + c] = f.t;
+                F.rsfe[off + R.w] = f.w; F.rsfn[off + R.s] = f.s; F.rsft[off + R.b] = f.b;
+            }
+            calc_eps_3d<NP>(P, F, R, i, j, k, dt);
+            F.rgp[c] = F.ep[c] * rog;
+            {
+                F6d f;
+                cell_massflux3d(P, F.rgp, F.ug, F.vg, F.wg, R, M, i, j, k, f);
+                F.rgfe[c] = f.e; F.rgfn[c] = f.n; F.rgft[c] = f.t;
+                F.rgfe[R.w] = f.w; F.rgfn[R.s] = f.s; F.rgft[R.b] = f.b;
+            }
+            dg = calc_res_3d(P, F, R, i, j, k, dt);
+            if (fabs(dg) > conv || fabs(dg) >= fabs(dgorig)) {
+                if (nit == 1 && loop == 1) dgorig = dg;
+                d3 = dg;
+            } else if (fabs(dg) <= conv) {
+                break;
+            }
+        }
+        F.abeta[c] = abeta;
+    }
 }
 
 // ---------------------------------------------------------------------------

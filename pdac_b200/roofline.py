@@ -12,6 +12,14 @@ phases, d dimensions, G gas species, N_app = d * S(S+1)/2 interphase terms.
               face velocities)
   whole step (semi-implicit path, rungekut = 1):
     B_step = 8 [ fixed + nit (R_sweep + W_sweep) ]
+
+  A colour phase of the corrector runs as two kernels:
+    residual test, per cell of the colour: mass-flux faces (2d), rgp, rgpn,
+      conv; a converged cell also reads its particle mass-flux faces
+      (2d ns), rlkn, sink (2 ns) and rog, and writes rlk (ns), ep and rgp:
+        converged    8 [(2d + 3) + (2d + 2) ns + 1 + ns + 2]
+        unconverged  8 (2d + 3) + 4 (worklist entry)
+    inner loop, per unconverged cell: 8 (R_sweep + W_sweep) + 4
 """
 from __future__ import annotations
 
@@ -43,3 +51,16 @@ def corrector_bytes_per_cell_sweep(ns, ng, d=2):
 def step_bytes_per_cell(ns, ng, nit, d=2):
     r, w = sweep_doubles(ns, ng, d)
     return 8 * (step_fixed_doubles(ns, ng, d) + nit * (r + w))
+
+
+def resid_bytes(ns, d, converged, unconverged):
+    """Algorithmic bytes of residual-test launches covering the given cells."""
+    conv = 8 * ((2 * d + 3) + (2 * d + 2) * ns + 1 + ns + 2)
+    unconv = 8 * (2 * d + 3) + 4
+    return conv * converged + unconv * unconverged
+
+
+def inner_bytes(ns, ng, d, unconverged):
+    """Algorithmic bytes of inner-loop launches over the given worklist cells."""
+    r, w = sweep_doubles(ns, ng, d)
+    return (8 * (r + w) + 4) * unconverged
