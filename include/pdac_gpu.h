@@ -168,8 +168,9 @@ int pdac_gpu_phase_times(pdac_ctx *ctx, double *ms7);
  * sweeps of iter, out[2] timed colour phases of the corrector, out[3] their
  * device time in ms; with nout >= 7 also out[4] / out[5] the device time of
  * the residual-test and inner-loop kernels of those phases and out[6] the
- * number of unconverged cells they processed (timed only when the reset
- * enabled profiling); nout >= 4                                           */
+ * number of unconverged cells they processed, with nout >= 8 also out[7]
+ * the number of cells the residual tests evaluated (all counted only when
+ * the reset enabled profiling); nout >= 4                                 */
 int pdac_gpu_stats(pdac_ctx *ctx, double *out, int nout);
 int pdac_gpu_reset_stats(pdac_ctx *ctx, int profile_corrector);
 /* stream-ordered timing marks (slots 0..31) and the device time between two */

@@ -37,9 +37,10 @@ struct pdac_ctx {
     cudaEvent_t ev[16];
     float phase_ms[7] = {0};
     // statistics: kernel launches, corrector launch timing (when profiling)
-    long long launches = 0, sweeps = 0, corr_launches = 0, work_cells = 0;
+    long long launches = 0, sweeps = 0, corr_launches = 0, work_cells = 0, tested_cells = 0;
     double corr_ms = 0.0, resid_ms = 0.0, inner_ms = 0.0;
     int *d_work = nullptr, *d_wcount = nullptr;  // corrector worklist and its per-colour lengths
+    unsigned char *d_dirty = nullptr;            // corrector active set, one byte per cell
     int inner_grid = 0;
     bool prof = false;
     cudaEvent_t cev[9];
@@ -231,7 +232,8 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
         CK(cudaMemcpy(ctx->d_vfact0, zero.data(), cfg->nvent * sizeof(double), cudaMemcpyHostToDevice));
     }
     CK(cudaMalloc(&ctx->d_work, (size_t)n * sizeof(int)));
-    CK(cudaMalloc(&ctx->d_wcount, 4 * sizeof(int)));
+    CK(cudaMalloc(&ctx->d_wcount, 8 * sizeof(int)));
+    CK(cudaMalloc(&ctx->d_dirty, (size_t)n));
     {
         int dev = 0, nsm = 148;
         CK(cudaGetDevice(&dev));
@@ -306,6 +308,7 @@ int pdac_gpu_destroy(pdac_ctx *ctx) {
     cudaFree(ctx->d_counters);
     cudaFree(ctx->d_work);
     cudaFree(ctx->d_wcount);
+    cudaFree(ctx->d_dirty);
     cudaFree(ctx->d_partial);
     cudaFreeHost(ctx->h_counters);
     for (auto &e : ctx->ev) cudaEventDestroy(e);
@@ -427,22 +430,26 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
     CK(cudaGetLastError());
     int m = (ctx->nx + 2) / 3;
     long nthr = (long)m * ctx->ny * ctx->nz;
+    // every cell is tested in the first sweep
+    CK(cudaMemsetAsync(ctx->d_dirty, 1, n, st));
     int nit;
     for (nit = 1; nit <= ctx->cfg.maxout; ++nit) {
-        CK(cudaMemsetAsync(ctx->d_wcount, 0, 3 * sizeof(int), st));
+        // [col] worklist length, [3 + col] cells tested, of colour col
+        CK(cudaMemsetAsync(ctx->d_wcount, 0, 6 * sizeof(int), st));
         for (int col = 0; col < 3; ++col) {
             int *cnt = ctx->d_wcount + col;
             if (ctx->prof) CK(cudaEventRecord(ctx->cev[3 * col], st));
-            if (ctx->d3) PHASE_LAUNCH(nph, pdac::k_resid3d, blocks(nthr), TPB, st, ctx->P, F, dt, col, ctx->d_work, cnt);
-            else PHASE_LAUNCH(nph, pdac::k_resid2d, blocks(nthr), TPB, st, ctx->P, F, dt, col, ctx->d_work, cnt);
+            unsigned char *dirty = ctx->d_dirty;
+            if (ctx->d3) PHASE_LAUNCH(nph, pdac::k_resid3d, blocks(nthr), TPB, st, ctx->P, F, dt, col, ctx->d_work, cnt, dirty);
+            else PHASE_LAUNCH(nph, pdac::k_resid2d, blocks(nthr), TPB, st, ctx->P, F, dt, col, ctx->d_work, cnt, dirty);
             if (ctx->prof) CK(cudaEventRecord(ctx->cev[3 * col + 1], st));
             int g = std::min(ctx->inner_grid, blocks(nthr, TPB_CORR));
-            if (ctx->d3) PHASE_LAUNCH(nph, pdac::k_inner3d, g, TPB_CORR, st, ctx->P, F, dt, nit, ctx->d_work, cnt);
-            else PHASE_LAUNCH(nph, pdac::k_inner2d, g, TPB_CORR, st, ctx->P, F, dt, nit, ctx->d_work, cnt);
+            if (ctx->d3) PHASE_LAUNCH(nph, pdac::k_inner3d, g, TPB_CORR, st, ctx->P, F, dt, nit, ctx->d_work, cnt, dirty);
+            else PHASE_LAUNCH(nph, pdac::k_inner2d, g, TPB_CORR, st, ctx->P, F, dt, nit, ctx->d_work, cnt, dirty);
             if (ctx->prof) CK(cudaEventRecord(ctx->cev[3 * col + 2], st));
             ctx->launches += 2;
         }
-        CK(cudaMemcpyAsync(ctx->h_counters, ctx->d_wcount, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(ctx->h_counters, ctx->d_wcount, 6 * sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         ctx->sweeps++;
         long unconverged = (long)ctx->h_counters[0] + ctx->h_counters[1] + ctx->h_counters[2];
@@ -457,6 +464,7 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
                 ctx->corr_launches++;
             }
             ctx->work_cells += unconverged;
+            ctx->tested_cells += (long)ctx->h_counters[3] + ctx->h_counters[4] + ctx->h_counters[5];
         }
         if (unconverged == 0) break;
     }
@@ -619,12 +627,13 @@ int pdac_gpu_stats(pdac_ctx *ctx, double *out, int nout) {
         out[5] = ctx->inner_ms;
         out[6] = (double)ctx->work_cells;
     }
+    if (nout >= 8) out[7] = (double)ctx->tested_cells;
     return PDAC_OK;
 }
 
 int pdac_gpu_reset_stats(pdac_ctx *ctx, int profile_corrector) {
     if (!ctx) return PDAC_ERR_ARG;
-    ctx->launches = ctx->sweeps = ctx->corr_launches = ctx->work_cells = 0;
+    ctx->launches = ctx->sweeps = ctx->corr_launches = ctx->work_cells = ctx->tested_cells = 0;
     ctx->corr_ms = ctx->resid_ms = ctx->inner_ms = 0.0;
     ctx->prof = profile_corrector != 0;
     return PDAC_OK;

@@ -668,6 +668,8 @@ __device__ __forceinline__ void padjust(PAdj &s, double &p, int &kros, double d3
 // converged cells (calc_eps) and appends unconverged ones to a worklist;
 // k_inner2d runs inner_loop (iter.f:480-580) on the worklist.  Cells of one
 // colour never touch each other's data, so the split changes no result.
+// Clean cells (no inner loop at the cell or a face neighbour since their
+// last test) are skipped: their test would reproduce the values they hold.
 __device__ __forceinline__ int colour_cell2d(const Prm &P, int t, int colour, int &i, int &k) {
     int m = (P.nx + 2) / 3;
     if (t >= m * P.nz) return -1;
@@ -681,12 +683,14 @@ __device__ __forceinline__ int colour_cell2d(const Prm &P, int t, int colour, in
 }
 
 template <int NP>
-__global__ void k_resid2d(Prm P, Fld F, double dt, int colour, int *list, int *count) {
+__global__ void k_resid2d(Prm P, Fld F, double dt, int colour, int *list, int *count, unsigned char *dirty) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     int i = 0, k = 0;
     int c = colour_cell2d(P, t, colour, i, k);
-    bool want = false;
-    if (c >= 0 && fluid(P, c)) {
+    bool want = false, tested = false;
+    if (c >= 0 && dirty[c] && fluid(P, c)) {
+        dirty[c] = 0;
+        tested = true;
         Raw2 R;
         raw2(P, i, k, R);
         double dg = calc_res_2d(P, F, R, i, k, dt);
@@ -698,10 +702,12 @@ __global__ void k_resid2d(Prm P, Fld F, double dt, int colour, int *list, int *c
         }
     }
     work_append(list, count, c, want);
+    warp_count(count + 3, tested);
 }
 
 template <int NP>
-__global__ void __launch_bounds__(64) k_inner2d(Prm P, Fld F, double dt, int nit, const int *list, const int *count) {
+__global__ void __launch_bounds__(64) k_inner2d(Prm P, Fld F, double dt, int nit, const int *list, const int *count,
+                                                unsigned char *dirty) {
     const int nwork = *count;
     for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nwork; w += gridDim.x * blockDim.x) {
         int c = list[w];
@@ -754,6 +760,8 @@ __global__ void __launch_bounds__(64) k_inner2d(Prm P, Fld F, double dt, int nit
             }
         }
         F.abeta[c] = abeta;
+        dirty[c] = 1;
+        dirty[R.e] = 1; dirty[R.w] = 1; dirty[R.t] = 1; dirty[R.b] = 1;
     }
 }
 

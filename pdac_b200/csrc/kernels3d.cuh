@@ -582,6 +582,12 @@ __device__ __forceinline__ void calc_eps_3d(const Prm &P, const Fld &F, const Ra
 // volume fractions (calc_eps), an unconverged one is appended to a worklist;
 // k_inner3d then runs inner_loop (iter.f:480-580) on the worklist.  Cells of
 // one colour never touch each other's data, so the split changes no result.
+//
+// Active set: the test of a cell reads only its own p/rog/rgp and the mass
+// fluxes of its six faces, which change only when the cell or a face
+// neighbour runs the inner loop.  Such a run marks the cell and its six face
+// neighbours dirty; a clean cell was converged at its last test and would
+// recompute exactly the values it holds, so the test skips it.
 __device__ __forceinline__ int colour_cell3d(const Prm &P, long t, int colour, int &i, int &j, int &k) {
     int m = (P.nx + 2) / 3;
     if (t >= (long)m * P.ny * P.nz) return -1;
@@ -597,12 +603,14 @@ __device__ __forceinline__ int colour_cell3d(const Prm &P, long t, int colour, i
 }
 
 template <int NP>
-__global__ void k_resid3d(Prm P, Fld F, double dt, int colour, int *list, int *count) {
+__global__ void k_resid3d(Prm P, Fld F, double dt, int colour, int *list, int *count, unsigned char *dirty) {
     long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     int i = 0, j = 0, k = 0;
     int c = colour_cell3d(P, t, colour, i, j, k);
-    bool want = false;
-    if (c >= 0 && fluid(P, c)) {
+    bool want = false, tested = false;
+    if (c >= 0 && dirty[c] && fluid(P, c)) {
+        dirty[c] = 0;
+        tested = true;
         Raw3 R;
         raw3(P, i, j, k, R);
         double dg = calc_res_3d(P, F, R, i, j, k, dt);
@@ -614,10 +622,12 @@ __global__ void k_resid3d(Prm P, Fld F, double dt, int colour, int *list, int *c
         }
     }
     work_append(list, count, c, want);
+    warp_count(count + 3, tested);
 }
 
 template <int NP>
-__global__ void __launch_bounds__(64) k_inner3d(Prm P, Fld F, double dt, int nit, const int *list, const int *count) {
+__global__ void __launch_bounds__(64) k_inner3d(Prm P, Fld F, double dt, int nit, const int *list, const int *count,
+                                                unsigned char *dirty) {
     const int nwork = *count;
     for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nwork; w += gridDim.x * blockDim.x) {
         int c = list[w], i, j, k;
@@ -674,6 +684,8 @@ __global__ void __launch_bounds__(64) k_inner3d(Prm P, Fld F, double dt, int nit
             }
         }
         F.abeta[c] = abeta;
+        dirty[c] = 1;
+        dirty[R.e] = 1; dirty[R.w] = 1; dirty[R.n] = 1; dirty[R.s] = 1; dirty[R.t] = 1; dirty[R.b] = 1;
     }
 }
 

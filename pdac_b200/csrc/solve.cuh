@@ -124,4 +124,11 @@ __device__ __forceinline__ void work_append(int *list, int *count, int c, bool w
     if (want) list[base + __popc(m & ((1u << lane) - 1u))] = c;
 }
 
+// Warp-aggregated count of the lanes with flag set.  Every lane of the warp
+// must reach this call.
+__device__ __forceinline__ void warp_count(int *count, bool flag) {
+    unsigned m = __ballot_sync(0xffffffffu, flag);
+    if (m != 0 && (threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(count, __popc(m));
+}
+
 }  // namespace pdac

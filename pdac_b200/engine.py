@@ -165,10 +165,10 @@ class Engine:
         return out
 
     def stats(self):
-        out = (C.c_double * 7)()
-        self._chk(self.L.pdac_gpu_stats(self.h, out, 7), "stats")
+        out = (C.c_double * 8)()
+        self._chk(self.L.pdac_gpu_stats(self.h, out, 8), "stats")
         return dict(launches=int(out[0]), sweeps=int(out[1]), corr_launches=int(out[2]), corr_ms=out[3],
-                    resid_ms=out[4], inner_ms=out[5], work_cells=int(out[6]))
+                    resid_ms=out[4], inner_ms=out[5], work_cells=int(out[6]), tested_cells=int(out[7]))
 
     def reset_stats(self, profile_corrector=False):
         self._chk(self.L.pdac_gpu_reset_stats(self.h, int(profile_corrector)), "reset_stats")
