@@ -54,17 +54,17 @@ __device__ __forceinline__ void gauss_jordan_t(const Prm &P, double (&a)[M][M], 
     }
 }
 
-// Phase matrix of one face, matrix.f:38-328, then its solution stored as the
-// face velocities (matrix.f:351-630).  dir 0/1/2 = x/y/z; side +1 = the
-// E/N/T face of cell c (assemble_matrix), side -1 = its W/S/B face
+// Phase matrix of one face, matrix.f:38-328, solved (matrix.f:351-630) into
+// the face velocities v[0..nph-1] (gas first).  dir 0/1/2 = x/y/z; side +1 =
+// the E/N/T face of cell c (assemble_matrix), side -1 = its W/S/B face
 // (assemble_all_matrix).  nb = remapped face neighbour, raw = raw face
-// neighbour (the cell whose face velocity is stored for side -1), ii = the
-// cell's index along dir.  The system is solved only when the raw
-// neighbour is fluid.
+// neighbour (whose row holds the tilde momentum of a W/S/B face), ii = the
+// cell's index along dir.  The cell's own p, ep, rgp and rlk come in
+// registers; neighbour values and the tilde terms are read-only here.
 template <int NP>
-__device__ __forceinline__ void face_solve(const Prm &P, const Fld &F, int c, int nb, int raw, int ii, int dir,
-                                           int side, double dt) {
-    if (!(P.flag[raw] & 1)) return;
+__device__ __forceinline__ void face_system(const Prm &P, const Fld &F, int c, int nb, int raw, int ii, int dir,
+                                            int side, double dt, double pc, double epc, double rgpc,
+                                            const double *rlkc, double *v) {
     constexpr int M = Sys<NP>::M;
     const int nph = nphases<NP>(P);
     const size_t n = P.ncell;
@@ -73,44 +73,67 @@ __device__ __forceinline__ void face_solve(const Prm &P, const Fld &F, int c, in
     const double *app = dir == 0 ? F.appu : (dir == 1 ? F.appv : F.appw);
     const double *rg = dir == 0 ? F.rug : (dir == 1 ? F.rvg : F.rwg);
     const double *rs = dir == 0 ? F.rus : (dir == 1 ? F.rvs : F.rws);
-    double alpha = P.alpha, ag = P.alphagrav, pijk = F.p[c];
+    double alpha = P.alpha, ag = P.alphagrav;
     double a[M][M], b[M];
-    // side +1: d0 = d(ii), d1 = d(ii+1), the face value of c's own row;
-    // side -1: d0 = d(ii), d1 = d(ii-1), the row of the lower neighbour
+    // side +1: d0 = d(ii), d1 = d(ii+1); side -1: d0 = d(ii), d1 = d(ii-1)
     double d0 = dd[ii], d1 = side > 0 ? dd[ii + 1] : dd[ii - 1];
     double inv = 1.0 / (d0 + d1);
-    int rowc = side > 0 ? c : raw;  // cell holding the tilde momentum of this face
-    double dp = side > 0 ? pijk - F.p[nb] : F.p[nb] - pijk;
+    int rowc = side > 0 ? c : raw;
+    double pnb = __ldg(F.p + nb), rgpnb = __ldg(F.rgp + nb);
+    double dp = side > 0 ? pc - pnb : pnb - pc;
     double ep_f = 1.0;
-    if (P.pmodel == 1) ep_f = (d0 * F.ep[nb] + d1 * F.ep[c]) * inv;
-    b[1] = rg[rowc] + alpha * dt * inv * 2.0 * ep_f * dp;
-    b[1] = b[1] + dt * ag * inv * grav * (d0 * F.rgp[nb] + d1 * F.rgp[c]);
-    a[1][1] = alpha * (d0 * app[nb] + d1 * app[c]) * inv;
-    a[1][1] = a[1][1] + (d0 * F.rgp[nb] + d1 * F.rgp[c]) * inv;
+    if (P.pmodel == 1) ep_f = (d0 * __ldg(F.ep + nb) + d1 * epc) * inv;
+    b[1] = __ldg(rg + rowc) + alpha * dt * inv * 2.0 * ep_f * dp;
+    b[1] = b[1] + dt * ag * inv * grav * (d0 * rgpnb + d1 * rgpc);
+    a[1][1] = alpha * (d0 * __ldg(app + nb) + d1 * __ldg(app + c)) * inv;
+    a[1][1] = a[1][1] + (d0 * rgpnb + d1 * rgpc) * inv;
 #pragma unroll
     for (int l = 2; l <= nph; ++l) {
-        double rn = F.rlk[(l - 2) * n + nb], rc = F.rlk[(l - 2) * n + c];
+        double rn = __ldg(F.rlk + (l - 2) * n + nb), rc = rlkc[l - 2];
         double eps_f = 0.0;
         if (P.pmodel == 1) eps_f = (d0 * rn + d1 * rc) * inv * P.inrl[l - 1];
-        b[l] = rs[(l - 2) * n + rowc] + alpha * dt * inv * 2.0 * eps_f * dp;
+        b[l] = __ldg(rs + (l - 2) * n + rowc) + alpha * dt * inv * 2.0 * eps_f * dp;
         b[l] = b[l] + dt * ag * inv * grav * (d0 * rn + d1 * rc);
         int ls1 = l * (l - 1) / 2;
 #pragma unroll
         for (int ll = 1; ll <= l; ++ll) {
             int ls = ls1 + ll;
-            double v = alpha * (d0 * app[(ls - 1) * n + nb] + d1 * app[(ls - 1) * n + c]) * inv;
-            a[l][ll] = v;
-            a[ll][l] = v;
+            double val = alpha * (d0 * __ldg(app + (ls - 1) * n + nb) + d1 * __ldg(app + (ls - 1) * n + c)) * inv;
+            a[l][ll] = val;
+            a[ll][l] = val;
         }
         a[l][l] = a[l][l] + (d0 * rn + d1 * rc) * inv;
     }
     gauss_jordan_t<NP>(P, a, b);
+#pragma unroll
+    for (int l = 1; l <= nph; ++l) v[l - 1] = b[l];
+}
+
+// face_system with the cell's state read from and the velocities stored to
+// memory, when the raw face neighbour is fluid (the predictor, iter.f:135-145)
+template <int NP>
+__device__ __forceinline__ void face_solve(const Prm &P, const Fld &F, int c, int nb, int raw, int ii, int dir,
+                                           int side, double dt) {
+    if (!(P.flag[raw] & 1)) return;
+    constexpr int M = Sys<NP>::M;
+    const int nph = nphases<NP>(P);
+    const size_t n = P.ncell;
+    double rlkc[M - 1], v[M - 1];
+#pragma unroll
+    for (int l = 2; l <= nph; ++l) rlkc[l - 2] = F.rlk[(l - 2) * n + c];
+    face_system<NP>(P, F, c, nb, raw, ii, dir, side, dt, F.p[c], F.ep[c], F.rgp[c], rlkc, v);
     int store = side > 0 ? c : raw;
     double *g = dir == 0 ? F.ug : (dir == 1 ? F.vg : F.wg);
     double *s = dir == 0 ? F.us : (dir == 1 ? F.vs : F.ws);
-    g[store] = b[1];
+    g[store] = v[0];
 #pragma unroll
-    for (int l = 2; l <= nph; ++l) s[(l - 2) * n + store] = b[l];
+    for (int l = 2; l <= nph; ++l) s[(l - 2) * n + store] = v[l - 1];
+}
+
+// value of a stencil slot: the cell's own current value where the (remapped)
+// slot index is the cell itself, else the read-only neighbour value
+__device__ __forceinline__ double slot(const double *a, int idx, int c, double own) {
+    return idx == c ? own : __ldg(a + idx);
 }
 
 // Warp-aggregated append of cell c to a worklist when want is set: one
