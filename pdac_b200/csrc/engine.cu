@@ -14,7 +14,7 @@
 #include <algorithm>
 
 #include "../../include/pdac_gpu.h"
-#include "kernels3d.cuh"
+#include "inner.cuh"
 
 using namespace pdac;
 
@@ -52,6 +52,7 @@ namespace {
 
 const int TPB = 128;
 const int TPB_CORR = 64;
+const int TPB_TEAM = 128;
 
 int fail(pdac_ctx *c, int code, const std::string &msg) {
     if (c) c->err = msg;
@@ -77,6 +78,18 @@ inline int blocks(long n, int tpb = TPB) { return (int)((n + tpb - 1) / tpb); }
             case 4: KERNEL<4><<<grid, tpb, 0, st>>>(__VA_ARGS__); break;           \
             case 6: KERNEL<6><<<grid, tpb, 0, st>>>(__VA_ARGS__); break;           \
             default: KERNEL<0><<<grid, tpb, 0, st>>>(__VA_ARGS__); break;          \
+        }                                                                          \
+    } while (0)
+
+// the same for a kernel template over (phases, dimensions)
+#define PHASE_LAUNCH_D(nph, KERNEL, D, grid, tpb, st, ...)                         \
+    do {                                                                           \
+        switch (nph) {                                                             \
+            case 2: KERNEL<2, D><<<grid, tpb, 0, st>>>(__VA_ARGS__); break;        \
+            case 3: KERNEL<3, D><<<grid, tpb, 0, st>>>(__VA_ARGS__); break;        \
+            case 4: KERNEL<4, D><<<grid, tpb, 0, st>>>(__VA_ARGS__); break;        \
+            case 6: KERNEL<6, D><<<grid, tpb, 0, st>>>(__VA_ARGS__); break;        \
+            default: KERNEL<0, D><<<grid, tpb, 0, st>>>(__VA_ARGS__); break;       \
         }                                                                          \
     } while (0)
 
@@ -443,9 +456,11 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
             if (ctx->d3) PHASE_LAUNCH(nph, pdac::k_resid3d, blocks(nthr), TPB, st, ctx->P, F, dt, col, ctx->d_work, cnt, dirty);
             else PHASE_LAUNCH(nph, pdac::k_resid2d, blocks(nthr), TPB, st, ctx->P, F, dt, col, ctx->d_work, cnt, dirty);
             if (ctx->prof) CK(cudaEventRecord(ctx->cev[3 * col + 1], st));
-            int g = std::min(ctx->inner_grid, blocks(nthr, TPB_CORR));
-            if (ctx->d3) PHASE_LAUNCH(nph, pdac::k_inner3d, g, TPB_CORR, st, ctx->P, F, dt, nit, ctx->d_work, cnt, dirty);
-            else PHASE_LAUNCH(nph, pdac::k_inner2d, g, TPB_CORR, st, ctx->P, F, dt, nit, ctx->d_work, cnt, dirty);
+            // one team of lanes per worklist cell (8 in 3D, 4 in 2D)
+            long team_threads = nthr * (ctx->d3 ? 8 : 4);
+            int g = std::min(ctx->inner_grid, blocks(team_threads, TPB_TEAM));
+            if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_inner_team, 3, g, TPB_TEAM, st, ctx->P, F, dt, nit, ctx->d_work, cnt, dirty);
+            else PHASE_LAUNCH_D(nph, pdac::k_inner_team, 2, g, TPB_TEAM, st, ctx->P, F, dt, nit, ctx->d_work, cnt, dirty);
             if (ctx->prof) CK(cudaEventRecord(ctx->cev[3 * col + 2], st));
             ctx->launches += 2;
         }

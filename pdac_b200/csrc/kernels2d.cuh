@@ -666,7 +666,7 @@ __device__ __forceinline__ void padjust(PAdj &s, double &p, int &kros, double d3
 // One colour phase of an outer sweep (iter.f:241-319) runs as two launches:
 // k_resid2d tests every cell of the colour, updates the volume fractions of
 // converged cells (calc_eps) and appends unconverged ones to a worklist;
-// k_inner2d runs inner_loop (iter.f:480-580) on the worklist.  Cells of one
+// k_inner_team (inner.cuh) runs inner_loop (iter.f:480-580) on the worklist.  Cells of one
 // colour never touch each other's data, so the split changes no result.
 // Clean cells (no inner loop at the cell or a face neighbour since their
 // last test) are skipped: their test would reproduce the values they hold.
@@ -703,140 +703,6 @@ __global__ void k_resid2d(Prm P, Fld F, double dt, int colour, int *list, int *c
     }
     work_append(list, count, c, want);
     warp_count(count + 3, tested);
-}
-
-// inner_loop of one unconverged cell with its state, face velocities and
-// fluxes in registers (nothing else touches the cell's neighbourhood within a
-// colour phase); the final values are stored as the reference leaves them.
-template <int NP>
-__global__ void __launch_bounds__(64) k_inner2d(Prm P, Fld F, double dt, int nit, const int *list, const int *count,
-                                                unsigned char *dirty) {
-    constexpr int NC = Sys<NP>::M - 1;
-    const int nph = nphases<NP>(P), ns = nph - 1;
-    const size_t n = P.ncell;
-    const int nwork = *count;
-    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nwork; w += gridDim.x * blockDim.x) {
-        int c = list[w];
-        int i = c % P.nx + 1, k = c / P.nx + 1;
-        Raw2 R;
-        Rem2 M;
-        raw2(P, i, k, R);
-        rem2(P, i, k, R, M);
-        const int *fl = P.flag;
-        double dg = calc_res_2d(P, F, R, i, k, dt);
-        double dgorig = dg;
-        double conv = F.conv[c];
-        double d3 = dg, p3 = F.p[c], abeta = F.abeta[c];
-        double xg[PDAC_MAXG];
-        for (int ig = 0; ig < P.ng; ++ig) xg[ig] = GAS(F.xgc, c, ig);
-        double tgc = F.tg[c];
-        int kros = -1;
-        PAdj s = {0, 0, 0, 0, 0, 0};
-        double p = F.p[c], ep = F.ep[c], rog = F.rog[c], rgp = F.rgp[c];
-        double rlk[NC];
-#pragma unroll
-        for (int is = 1; is <= ns; ++is) rlk[is - 1] = F.rlk[(is - 1) * n + c];
-        // faces W, B, E, T: raw neighbour, remapped neighbour, axis index,
-        // direction (0 = x, 2 = z) and the cell holding the face velocity
-        const int fnb[4] = {R.w, R.b, R.e, R.t};
-        const int frm[4] = {M.w, M.b, M.e, M.t};
-        const int fii[4] = {i, k, i, k};
-        const int fdir[4] = {0, 2, 0, 2};
-        const int fcell[4] = {R.w, R.b, c, c};
-        double vel[4][NC];
-        bool solved[4];
-#pragma unroll
-        for (int f = 0; f < 4; ++f) {
-            solved[f] = (fl[fnb[f]] & 1) != 0;
-            const double *g = fdir[f] == 0 ? F.ug : F.wg;
-            const double *sv = fdir[f] == 0 ? F.us : F.ws;
-            vel[f][0] = g[fcell[f]];
-#pragma unroll
-            for (int l = 2; l <= nph; ++l) vel[f][l - 1] = sv[(l - 2) * n + fcell[f]];
-        }
-        bool mus = P.muscl > 0 && fl[c] == FLUID;
-        for (int loop = 1; loop <= P.inmax; ++loop) {
-            if (loop > 1 || nit > 1) padjust(s, p, kros, d3, p3, P.omega, abeta);
-            rog = thermal_eosg(P, tgc, p, xg);
-            rgp = ep * rog;
-            // W, B then E, T faces (matrix.f:351-479)
-#pragma unroll
-            for (int f = 0; f < 4; ++f)
-                if (solved[f]) face_system<NP>(P, F, c, frm[f], fnb[f], fii[f], fdir[f], f < 2 ? -1 : +1, dt, p, ep, rgp, rlk, vel[f]);
-            // particle mass fluxes and volume fractions (iter.f:778-994)
-            double rls = 0;
-#pragma unroll
-            for (int is = 1; is <= ns; ++is) {
-                size_t off = (size_t)(is - 1) * n;
-                const double *D = F.rlk + off;
-                double own = rlk[is - 1];
-                St d;
-                d.c = own;
-                d.e = slot(D, M.e, c, own); d.w = slot(D, M.w, c, own);
-                d.t = slot(D, M.t, c, own); d.b = slot(D, M.b, c, own);
-                if (mus) {
-                    d.ee = slot(D, M.ee, c, own); d.tt = slot(D, M.tt, c, own);
-                    d.ww = slot(D, M.ww, c, own); d.bb = slot(D, M.bb, c, own);
-                }
-                MF2 f;
-                massflux_2d(P, d, vel[0][is], vel[2][is], vel[1][is], vel[3][is], i, k, mus, fl[R.w], fl[R.e], fl[R.b],
-                            fl[R.t], f);
-                F.rsfe[off + c] = f.e; F.rsft[off + c] = f.t; F.rsfe[off + R.w] = f.w; F.rsft[off + R.b] = f.b;
-                double rlkx = (1.0 * f.e - 1.0 * f.w) * P.indx[i] * P.inr[i];
-                double rlkz = (1.0 * f.t - 1.0 * f.b) * P.indz[k];
-                double rlky = 0.0;
-                double t = F.rlkn[off + c] - dt * 1.0 * (rlkx + rlky + rlkz);
-                t = t + dt * 1.0 * F.sink[off + c];
-                double v = fmax(0.0, t);
-                rlk[is - 1] = v;
-                rls = rls + v * P.inrl[is];
-            }
-            ep = 1.0 - rls;
-            if (rls > 1.0) atomicAdd(&F.counters[2], 1);
-            rgp = ep * rog;
-            // gas mass flux and continuity residual (iter.f:597-771)
-            {
-                const double *D = F.rgp;
-                St d;
-                d.c = rgp;
-                d.e = slot(D, M.e, c, rgp); d.w = slot(D, M.w, c, rgp);
-                d.t = slot(D, M.t, c, rgp); d.b = slot(D, M.b, c, rgp);
-                if (mus) {
-                    d.ee = slot(D, M.ee, c, rgp); d.tt = slot(D, M.tt, c, rgp);
-                    d.ww = slot(D, M.ww, c, rgp); d.bb = slot(D, M.bb, c, rgp);
-                }
-                MF2 f;
-                massflux_2d(P, d, vel[0][0], vel[2][0], vel[1][0], vel[3][0], i, k, mus, fl[R.w], fl[R.e], fl[R.b],
-                            fl[R.t], f);
-                F.rgfe[c] = f.e; F.rgft[c] = f.t; F.rgfe[R.w] = f.w; F.rgft[R.b] = f.b;
-                double resx = (1.0 * f.e - 1.0 * f.w) * P.indx[i] * P.inr[i];
-                double resz = (1.0 * f.t - 1.0 * f.b) * P.indz[k];
-                double resy = 0.0;
-                dg = rgp - F.rgpn[c] + dt * 1.0 * (resx + resy + resz);
-            }
-            if (fabs(dg) > conv || fabs(dg) >= fabs(dgorig)) {
-                if (nit == 1 && loop == 1) dgorig = dg;
-                d3 = dg;
-            } else if (fabs(dg) <= conv) {
-                break;
-            }
-        }
-        F.p[c] = p; F.rog[c] = rog; F.rgp[c] = rgp; F.ep[c] = ep;
-#pragma unroll
-        for (int is = 1; is <= ns; ++is) F.rlk[(is - 1) * n + c] = rlk[is - 1];
-#pragma unroll
-        for (int f = 0; f < 4; ++f) {
-            if (!solved[f]) continue;
-            double *g = fdir[f] == 0 ? F.ug : F.wg;
-            double *sv = fdir[f] == 0 ? F.us : F.ws;
-            g[fcell[f]] = vel[f][0];
-#pragma unroll
-            for (int l = 2; l <= nph; ++l) sv[(l - 2) * n + fcell[f]] = vel[f][l - 1];
-        }
-        F.abeta[c] = abeta;
-        dirty[c] = 1;
-        dirty[R.e] = 1; dirty[R.w] = 1; dirty[R.t] = 1; dirty[R.b] = 1;
-    }
 }
 
 // ---------------------------------------------------------------------------

@@ -580,7 +580,7 @@ __device__ __forceinline__ void calc_eps_3d(const Prm &P, const Fld &F, const Ra
 // One colour phase of an outer sweep (iter.f:241-319) runs as two launches.
 // k_resid3d tests every cell of the colour: a converged cell only updates its
 // volume fractions (calc_eps), an unconverged one is appended to a worklist;
-// k_inner3d then runs inner_loop (iter.f:480-580) on the worklist.  Cells of
+// k_inner_team (inner.cuh) then runs inner_loop (iter.f:480-580) on it.  Cells of
 // one colour never touch each other's data, so the split changes no result.
 //
 // Active set: the test of a cell reads only its own p/rog/rgp and the mass
@@ -623,143 +623,6 @@ __global__ void k_resid3d(Prm P, Fld F, double dt, int colour, int *list, int *c
     }
     work_append(list, count, c, want);
     warp_count(count + 3, tested);
-}
-
-// inner_loop of one unconverged cell with its state, face velocities and
-// fluxes in registers: within a colour phase nothing else reads or writes the
-// cell's neighbourhood, so intermediate values need not pass through memory;
-// the final values are stored as the reference leaves them.
-template <int NP>
-__global__ void __launch_bounds__(64) k_inner3d(Prm P, Fld F, double dt, int nit, const int *list, const int *count,
-                                                unsigned char *dirty) {
-    constexpr int NC = Sys<NP>::M - 1;  // phase capacity of the register arrays
-    const int nph = nphases<NP>(P), ns = nph - 1;
-    const size_t n = P.ncell;
-    const int nwork = *count;
-    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nwork; w += gridDim.x * blockDim.x) {
-        int c = list[w], i, j, k;
-        ijk_of(P, c, i, j, k);
-        Raw3 R;
-        Rem3 M;
-        raw3(P, i, j, k, R);
-        rem3(P, i, j, k, R, M);
-        const int *fl = P.flag;
-        double dg = calc_res_3d(P, F, R, i, j, k, dt);
-        double dgorig = dg;
-        double conv = F.conv[c];
-        double d3 = dg, p3 = F.p[c], abeta = F.abeta[c];
-        double xg[PDAC_MAXG];
-        for (int ig = 0; ig < P.ng; ++ig) xg[ig] = GAS(F.xgc, c, ig);
-        double tgc = F.tg[c];
-        int kros = -1;
-        PAdj s = {0, 0, 0, 0, 0, 0};
-        double p = F.p[c], ep = F.ep[c], rog = F.rog[c], rgp = F.rgp[c];
-        double rlk[NC];
-#pragma unroll
-        for (int is = 1; is <= ns; ++is) rlk[is - 1] = F.rlk[(is - 1) * n + c];
-        // face velocities by phase: a face whose raw neighbour is not fluid
-        // is never solved and keeps its stored value
-        const int fnb[6] = {R.w, R.s, R.b, R.e, R.n, R.t};
-        const int frm[6] = {M.w, M.s, M.b, M.e, M.n, M.t};
-        const int fii[6] = {i, j, k, i, j, k};
-        const int fcell[6] = {R.w, R.s, R.b, c, c, c};  // where the face velocity is stored
-        double *const gv[3] = {F.ug, F.vg, F.wg};
-        double *const sv[3] = {F.us, F.vs, F.ws};
-        double vel[6][NC];
-        bool solved[6];
-#pragma unroll
-        for (int f = 0; f < 6; ++f) {
-            solved[f] = (fl[fnb[f]] & 1) != 0;
-            vel[f][0] = gv[f % 3][fcell[f]];
-#pragma unroll
-            for (int l = 2; l <= nph; ++l) vel[f][l - 1] = sv[f % 3][(l - 2) * n + fcell[f]];
-        }
-        bool mus = P.muscl > 0 && fl[c] == FLUID;
-        for (int loop = 1; loop <= P.inmax; ++loop) {
-            if (loop > 1 || nit > 1) padjust(s, p, kros, d3, p3, P.omega, abeta);
-            rog = thermal_eosg(P, tgc, p, xg);
-            rgp = ep * rog;
-            // W, S, B then E, N, T faces (matrix.f:351-479, 494-630)
-#pragma unroll
-            for (int f = 0; f < 6; ++f)
-                if (solved[f]) face_system<NP>(P, F, c, frm[f], fnb[f], fii[f], f % 3, f < 3 ? -1 : +1, dt, p, ep, rgp, rlk, vel[f]);
-            // particle mass fluxes and volume fractions (calc_part_mass_flux,
-            // calc_eps, iter.f:778-994)
-            double rls = 0;
-#pragma unroll
-            for (int is = 1; is <= ns; ++is) {
-                size_t off = (size_t)(is - 1) * n;
-                const double *D = F.rlk + off;
-                double own = rlk[is - 1];
-                S3 d;
-                d.c = own;
-                d.e = slot(D, M.e, c, own); d.w = slot(D, M.w, c, own); d.n = slot(D, M.n, c, own);
-                d.s = slot(D, M.s, c, own); d.t = slot(D, M.t, c, own); d.b = slot(D, M.b, c, own);
-                if (mus) {
-                    d.ee = slot(D, M.ee, c, own); d.ww = slot(D, M.ww, c, own); d.nn = slot(D, M.nn, c, own);
-                    d.ss = slot(D, M.ss, c, own); d.tt = slot(D, M.tt, c, own); d.bb = slot(D, M.bb, c, own);
-                }
-                F6d f;
-                massflux_3d(P, d, vel[0][is], vel[3][is], vel[1][is], vel[4][is], vel[2][is], vel[5][is], i, j, k, mus,
-                            fl[R.w], fl[R.e], fl[R.s], fl[R.n], fl[R.b], fl[R.t], f);
-                F.rsfe[off + c] = f.e; F.rsfn[off + c] = f.n; F.rsft[off + c] = f.t;
-                F.rsfe[off + R.w] = f.w; F.rsfn[off + R.s] = f.s; F.rsft[off + R.b] = f.b;
-                double rlkx = (1.0 * f.e - 1.0 * f.w) * P.indx[i] * 1.0;
-                double rlkz = (1.0 * f.t - 1.0 * f.b) * P.indz[k];
-                double rlky = (1.0 * f.n - 1.0 * f.s) * P.indy[j];
-                double t = F.rlkn[off + c] - dt * 1.0 * (rlkx + rlky + rlkz);
-                t = t + dt * 1.0 * F.sink[off + c];
-                double v = fmax(0.0, t);
-                rlk[is - 1] = v;
-                rls = rls + v * P.inrl[is];
-            }
-            ep = 1.0 - rls;
-            if (rls > 1.0) atomicAdd(&F.counters[2], 1);
-            rgp = ep * rog;
-            // gas mass flux and continuity residual (calc_gas_mass_flux,
-            // calc_res, iter.f:597-771)
-            {
-                const double *D = F.rgp;
-                S3 d;
-                d.c = rgp;
-                d.e = slot(D, M.e, c, rgp); d.w = slot(D, M.w, c, rgp); d.n = slot(D, M.n, c, rgp);
-                d.s = slot(D, M.s, c, rgp); d.t = slot(D, M.t, c, rgp); d.b = slot(D, M.b, c, rgp);
-                if (mus) {
-                    d.ee = slot(D, M.ee, c, rgp); d.ww = slot(D, M.ww, c, rgp); d.nn = slot(D, M.nn, c, rgp);
-                    d.ss = slot(D, M.ss, c, rgp); d.tt = slot(D, M.tt, c, rgp); d.bb = slot(D, M.bb, c, rgp);
-                }
-                F6d f;
-                massflux_3d(P, d, vel[0][0], vel[3][0], vel[1][0], vel[4][0], vel[2][0], vel[5][0], i, j, k, mus,
-                            fl[R.w], fl[R.e], fl[R.s], fl[R.n], fl[R.b], fl[R.t], f);
-                F.rgfe[c] = f.e; F.rgfn[c] = f.n; F.rgft[c] = f.t;
-                F.rgfe[R.w] = f.w; F.rgfn[R.s] = f.s; F.rgft[R.b] = f.b;
-                double resx = (1.0 * f.e - 1.0 * f.w) * P.indx[i] * 1.0;
-                double resz = (1.0 * f.t - 1.0 * f.b) * P.indz[k];
-                double resy = (1.0 * f.n - 1.0 * f.s) * P.indy[j];
-                dg = rgp - F.rgpn[c] + dt * 1.0 * (resx + resy + resz);
-            }
-            if (fabs(dg) > conv || fabs(dg) >= fabs(dgorig)) {
-                if (nit == 1 && loop == 1) dgorig = dg;
-                d3 = dg;
-            } else if (fabs(dg) <= conv) {
-                break;
-            }
-        }
-        // final state of the cell and its solved faces
-        F.p[c] = p; F.rog[c] = rog; F.rgp[c] = rgp; F.ep[c] = ep;
-#pragma unroll
-        for (int is = 1; is <= ns; ++is) F.rlk[(is - 1) * n + c] = rlk[is - 1];
-#pragma unroll
-        for (int f = 0; f < 6; ++f) {
-            if (!solved[f]) continue;
-            gv[f % 3][fcell[f]] = vel[f][0];
-#pragma unroll
-            for (int l = 2; l <= nph; ++l) sv[f % 3][(l - 2) * n + fcell[f]] = vel[f][l - 1];
-        }
-        F.abeta[c] = abeta;
-        dirty[c] = 1;
-        dirty[R.e] = 1; dirty[R.w] = 1; dirty[R.n] = 1; dirty[R.s] = 1; dirty[R.t] = 1; dirty[R.b] = 1;
-    }
 }
 
 // ---------------------------------------------------------------------------
