@@ -456,8 +456,9 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
             if (ctx->d3) PHASE_LAUNCH(nph, pdac::k_resid3d, blocks(nthr), TPB, st, ctx->P, F, dt, col, ctx->d_work, cnt, dirty);
             else PHASE_LAUNCH(nph, pdac::k_resid2d, blocks(nthr), TPB, st, ctx->P, F, dt, col, ctx->d_work, cnt, dirty);
             if (ctx->prof) CK(cudaEventRecord(ctx->cev[3 * col + 1], st));
-            // one team of lanes per worklist cell (8 in 3D, 4 in 2D)
-            long team_threads = nthr * (ctx->d3 ? 8 : 4);
+            // one team of lanes per worklist cell (5 teams of 6 lanes per warp
+            // in 3D, 8 of 4 in 2D)
+            long team_threads = (nthr + (ctx->d3 ? 4 : 7)) / (ctx->d3 ? 5 : 8) * 32;
             int g = std::min(ctx->inner_grid, blocks(team_threads, TPB_TEAM));
             if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_inner_team, 3, g, TPB_TEAM, st, ctx->P, F, dt, nit, ctx->d_work, cnt, dirty);
             else PHASE_LAUNCH_D(nph, pdac::k_inner_team, 2, g, TPB_TEAM, st, ctx->P, F, dt, nit, ctx->d_work, cnt, dirty);

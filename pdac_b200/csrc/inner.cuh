@@ -1,7 +1,7 @@
 // inner.cuh -- inner_loop of the corrector (iter.f:480-580) on a team of
 // lanes per cell.
 //
-// A team of T lanes (8 in 3D, 4 in 2D) owns one unconverged cell of the
+// A team of T lanes (6 in 3D, 4 in 2D) owns one unconverged cell of the
 // worklist.  Lane q < NF owns face q of the cell (3D: W, S, B, E, N, T; 2D:
 // W, B, E, T): it assembles and solves that face's phase system and computes
 // that face's mass fluxes.  The per-cell quantities (pressure adjustment,
@@ -50,56 +50,135 @@ __device__ __forceinline__ double face_mflux(const Prm &P, const FaceGeo &g, boo
     return f + upwnd * cs * g.r;
 }
 
+// Loop-invariant part of one face's phase system (matrix.f:38-328) for the
+// cell's inner loop: everything that does not depend on the cell's own p,
+// ep, rgp and rlk, evaluated once with the operations of face_system so that
+// the in-loop assembly (face_assemble) reproduces face_system bit for bit.
+template <int NP>
+struct FaceK {
+    static constexpr int NA = Sys<NP>::M * (Sys<NP>::M - 1) / 2;
+    double A[NA];               // alpha (d0 app(nb) + d1 app(c)) / (d0 + d1), by interphase index
+    double brow[Sys<NP>::M - 1];  // tilde momenta of the face, gas first
+    double d0rn[Sys<NP>::M - 1];  // d0 x neighbour particle bulk densities (index 0 = gas: d0 rgp(nb))
+    double pnb, d0epnb, K1, K2, d1, inv;
+};
+
+template <int NP>
+__device__ __forceinline__ void face_prepare(const Prm &P, const Fld &F, int c, int nb, int raw, int ii, int dir,
+                                             int side, double dt, FaceK<NP> &K) {
+    const int nph = nphases<NP>(P);
+    const size_t n = P.ncell;
+    const double *dd = dir == 0 ? P.dx : (dir == 1 ? P.dy : P.dz);
+    double grav = dir == 0 ? P.gravx : (dir == 1 ? P.gravy : P.gravz);
+    const double *app = dir == 0 ? F.appu : (dir == 1 ? F.appv : F.appw);
+    const double *rg = dir == 0 ? F.rug : (dir == 1 ? F.rvg : F.rwg);
+    const double *rs = dir == 0 ? F.rus : (dir == 1 ? F.rvs : F.rws);
+    double alpha = P.alpha, ag = P.alphagrav;
+    double d0 = dd[ii], d1 = side > 0 ? dd[ii + 1] : dd[ii - 1];
+    double inv = 1.0 / (d0 + d1);
+    int rowc = side > 0 ? c : raw;
+    K.d1 = d1;
+    K.inv = inv;
+    K.pnb = __ldg(F.p + nb);
+    K.d0epnb = P.pmodel == 1 ? d0 * __ldg(F.ep + nb) : 0.0;
+    K.K1 = alpha * dt * inv * 2.0;
+    K.K2 = dt * ag * inv * grav;
+    K.brow[0] = __ldg(rg + rowc);
+    K.d0rn[0] = d0 * __ldg(F.rgp + nb);
+#pragma unroll
+    for (int l = 2; l <= nph; ++l) {
+        K.brow[l - 1] = __ldg(rs + (l - 2) * n + rowc);
+        K.d0rn[l - 1] = d0 * __ldg(F.rlk + (l - 2) * n + nb);
+    }
+    const int nap = nph * (nph + 1) / 2;
+#pragma unroll
+    for (int ls = 1; ls <= nap; ++ls)
+        K.A[ls - 1] = alpha * (d0 * __ldg(app + (ls - 1) * n + nb) + d1 * __ldg(app + (ls - 1) * n + c)) * inv;
+}
+
+// the in-loop assembly and solution; side as in face_system
+template <int NP>
+__device__ __forceinline__ void face_assemble(const Prm &P, const FaceK<NP> &K, int side, double pc, double epc,
+                                              double rgpc, const double *rlkc, double *v) {
+    constexpr int M = Sys<NP>::M;
+    const int nph = nphases<NP>(P);
+    double a[M][M], b[M];
+    double d1 = K.d1, inv = K.inv;
+    double dp = side > 0 ? pc - K.pnb : K.pnb - pc;
+    double ep_f = 1.0;
+    if (P.pmodel == 1) ep_f = (K.d0epnb + d1 * epc) * inv;
+    b[1] = K.brow[0] + K.K1 * ep_f * dp;
+    b[1] = b[1] + K.K2 * (K.d0rn[0] + d1 * rgpc);
+    a[1][1] = K.A[0] + (K.d0rn[0] + d1 * rgpc) * inv;
+#pragma unroll
+    for (int l = 2; l <= nph; ++l) {
+        double rc = rlkc[l - 2];
+        double eps_f = 0.0;
+        if (P.pmodel == 1) eps_f = (K.d0rn[l - 1] + d1 * rc) * inv * P.inrl[l - 1];
+        b[l] = K.brow[l - 1] + K.K1 * eps_f * dp;
+        b[l] = b[l] + K.K2 * (K.d0rn[l - 1] + d1 * rc);
+        int ls1 = l * (l - 1) / 2;
+#pragma unroll
+        for (int ll = 1; ll <= l; ++ll) {
+            double val = K.A[ls1 + ll - 1];
+            a[l][ll] = val;
+            a[ll][l] = val;
+        }
+        a[l][l] = a[l][l] + (K.d0rn[l - 1] + d1 * rc) * inv;
+    }
+    gauss_jordan_t<NP>(P, a, b);
+#pragma unroll
+    for (int l = 1; l <= nph; ++l) v[l - 1] = b[l];
+}
+
 template <int NP, int D>
 __global__ void __launch_bounds__(128) k_inner_team(Prm P, Fld F, double dt, int nit, const int *list, const int *count,
                                                     unsigned char *dirty) {
-    constexpr int T = D == 3 ? 8 : 4;    // lanes per cell
+    constexpr int T = D == 3 ? 6 : 4;    // lanes per cell
+    constexpr int TPW = 32 / T;          // teams per warp (3D: 5, lanes 30 and 31 idle)
     constexpr int NF = D == 3 ? 6 : 4;   // faces per cell
     constexpr int NC = Sys<NP>::M - 1;   // phase capacity
     const int nph = nphases<NP>(P), ns = nph - 1;
     const size_t n = P.ncell;
-    const int lane = threadIdx.x & 31, q = lane & (T - 1), tb = lane & ~(T - 1);
-    const unsigned tmask = (T == 32 ? 0xffffffffu : ((1u << T) - 1u)) << tb;
+    const int lane = threadIdx.x & 31, tw = lane / T;
+    if (tw >= TPW) return;  // idle lanes take no part in any team
+    const int q = lane - tw * T, tb = tw * T;
+    const unsigned tmask = ((1u << T) - 1u) << tb;
     const int nwork = *count;
-    const int team0 = (blockIdx.x * blockDim.x + threadIdx.x) / T, nteams = gridDim.x * blockDim.x / T;
-    for (int w = team0; w < nwork; w += nteams) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int w = warp * TPW + tw; w < nwork; w += nwarps * TPW) {
         const int c = list[w];
         int i, j, k;
         if (D == 3) ijk_of(P, c, i, j, k);
         else { i = c % P.nx + 1; j = 1; k = c / P.nx + 1; }
         const int *fl = P.flag;
-        // ---- this lane's face ------------------------------------------------
-        // axis and side; raw / remapped neighbours on both sides along the
-        // axis (first and second); cell holding the face velocity
-        int dir = 0, ii = i, nax = P.nx;
-        bool minus = true, own_face = q < NF;
-        int raw_m = c, raw_p = c, rm = c, rmm = c, rp = c, rpp = c, rawnb = c;
-        if (own_face) {
-            int a = D == 3 ? q % 3 : q % 2;  // axis slot
-            minus = D == 3 ? q < 3 : q < 2;
-            dir = D == 3 ? a : (a == 0 ? 0 : 2);
-            ii = dir == 0 ? i : (dir == 1 ? j : k);
-            nax = dir == 0 ? P.nx : (dir == 1 ? P.ny : P.nz);
-            if (D == 3) {
-                Raw3 R;
-                Rem3 M;
-                raw3(P, i, j, k, R);
-                rem3(P, i, j, k, R, M);
-                if (dir == 0) { raw_m = R.w; raw_p = R.e; rm = M.w; rmm = M.ww; rp = M.e; rpp = M.ee; }
-                else if (dir == 1) { raw_m = R.s; raw_p = R.n; rm = M.s; rmm = M.ss; rp = M.n; rpp = M.nn; }
-                else { raw_m = R.b; raw_p = R.t; rm = M.b; rmm = M.bb; rp = M.t; rpp = M.tt; }
-            } else {
-                Raw2 R;
-                Rem2 M;
-                raw2(P, i, k, R);
-                rem2(P, i, k, R, M);
-                if (dir == 0) { raw_m = R.w; raw_p = R.e; rm = M.w; rmm = M.ww; rp = M.e; rpp = M.ee; }
-                else { raw_m = R.b; raw_p = R.t; rm = M.b; rmm = M.bb; rp = M.t; rpp = M.tt; }
-            }
-            rawnb = minus ? raw_m : raw_p;
+        // ---- this lane's face: axis, side, raw and remapped neighbours -------
+        const int a = D == 3 ? q % 3 : q % 2;
+        const bool minus = D == 3 ? q < 3 : q < 2;
+        const int dir = D == 3 ? a : (a == 0 ? 0 : 2);
+        const int ii = dir == 0 ? i : (dir == 1 ? j : k);
+        const int nax = dir == 0 ? P.nx : (dir == 1 ? P.ny : P.nz);
+        int raw_m, raw_p, rm, rmm, rp, rpp;
+        if (D == 3) {
+            Raw3 R;
+            Rem3 M;
+            raw3(P, i, j, k, R);
+            rem3(P, i, j, k, R, M);
+            if (dir == 0) { raw_m = R.w; raw_p = R.e; rm = M.w; rmm = M.ww; rp = M.e; rpp = M.ee; }
+            else if (dir == 1) { raw_m = R.s; raw_p = R.n; rm = M.s; rmm = M.ss; rp = M.n; rpp = M.nn; }
+            else { raw_m = R.b; raw_p = R.t; rm = M.b; rmm = M.bb; rp = M.t; rpp = M.tt; }
+        } else {
+            Raw2 R;
+            Rem2 M;
+            raw2(P, i, k, R);
+            rem2(P, i, k, R, M);
+            if (dir == 0) { raw_m = R.w; raw_p = R.e; rm = M.w; rmm = M.ww; rp = M.e; rpp = M.ee; }
+            else { raw_m = R.b; raw_p = R.t; rm = M.b; rmm = M.bb; rp = M.t; rpp = M.tt; }
         }
-        const bool solved = own_face && (fl[rawnb] & 1);
+        const int rawnb = minus ? raw_m : raw_p;
+        const bool solved = (fl[rawnb] & 1) != 0;
         const int fcell = minus ? rawnb : c;  // where this face's velocity and fluxes live
+        const bool mus = P.muscl > 0 && fl[c] == FLUID;
         FaceGeo g;
         {
             const double *dd = dir == 0 ? P.dx : (dir == 1 ? P.dy : P.dz);
@@ -111,23 +190,41 @@ __global__ void __launch_bounds__(128) k_inner_team(Prm P, Fld F, double dt, int
             g.incr_p = minus ? 0.5 * dd[ii - 1] : 0.5 * dd[ii];
             g.incr_m = minus ? -0.5 * dd[ii] : -0.5 * dd[ii + 1];
             g.r = (D == 2 && dir == 0) ? (minus ? P.rb[i - 1] : P.rb[i]) : 1.0;
-            g.lim_on = own_face && (minus ? (ii != 2 && fl[raw_m] == FLUID) : (ii != nax - 1 && fl[raw_p] == FLUID));
+            g.lim_on = minus ? (ii != 2 && fl[raw_m] == FLUID) : (ii != nax - 1 && fl[raw_p] == FLUID);
         }
         double *const gvel = dir == 0 ? F.ug : (dir == 1 ? F.vg : F.wg);
         double *const svel = dir == 0 ? F.us : (dir == 1 ? F.vs : F.ws);
         double vel[NC];
-        if (own_face) {
-            vel[0] = gvel[fcell];
+        vel[0] = gvel[fcell];
 #pragma unroll
-            for (int l = 2; l <= nph; ++l) vel[l - 1] = svel[(l - 2) * n + fcell];
+        for (int l = 2; l <= nph; ++l) vel[l - 1] = svel[(l - 2) * n + fcell];
+        FaceK<NP> K;
+        if (solved) face_prepare<NP>(P, F, c, minus ? rm : rp, rawnb, ii, dir, minus ? -1 : +1, dt, K);
+        // mass-flux stencil of this face by phase (gas first): neighbour
+        // values, or the cell's own current value where the slot is the cell
+        const int rfar = minus ? rmm : rpp;
+        const bool sm = rm == c, sp = rp == c, sfar = rfar == c;
+        double cm[NC], cp[NC], cfar[NC];
+        cm[0] = __ldg(F.rgp + rm); cp[0] = __ldg(F.rgp + rp); cfar[0] = mus ? __ldg(F.rgp + rfar) : 0.0;
+#pragma unroll
+        for (int l = 2; l <= nph; ++l) {
+            const double *D_ = F.rlk + (size_t)(l - 2) * n;
+            cm[l - 1] = __ldg(D_ + rm); cp[l - 1] = __ldg(D_ + rp); cfar[l - 1] = mus ? __ldg(D_ + rfar) : 0.0;
         }
+        auto mflux = [&](int ph, double own) {
+            double dm = sm ? own : cm[ph], dp = sp ? own : cp[ph], df = sfar ? own : cfar[ph];
+            return minus ? face_mflux(P, g, true, vel[ph], own, dm, df, dp, 0.0, mus)
+                         : face_mflux(P, g, false, vel[ph], own, dm, 0.0, dp, df, mus);
+        };
         // ---- cell state (identical in every lane) ------------------------------
         const double rx = D == 2 ? P.inr[i] : 1.0;
+        const double idx_i = P.indx[i], idz_k = P.indz[k], idy_j = D == 3 ? P.indy[j] : 0.0;
+        const double rgpn_c = F.rgpn[c];
         auto resid = [&](double fe, double fw, double fn, double fs, double ft, double fb, double rgpc) {
-            double resx = (1.0 * fe - 1.0 * fw) * P.indx[i] * rx;
-            double resz = (1.0 * ft - 1.0 * fb) * P.indz[k];
-            double resy = D == 3 ? (1.0 * fn - 1.0 * fs) * P.indy[j] : 0.0;
-            return rgpc - F.rgpn[c] + dt * 1.0 * (resx + resy + resz);
+            double resx = (1.0 * fe - 1.0 * fw) * idx_i * rx;
+            double resz = (1.0 * ft - 1.0 * fb) * idz_k;
+            double resy = D == 3 ? (1.0 * fn - 1.0 * fs) * idy_j : 0.0;
+            return rgpc - rgpn_c + dt * 1.0 * (resx + resy + resz);
         };
         double dg;  // calc_res of the stored state (raw W/S/B neighbours)
         if (D == 3) {
@@ -146,50 +243,40 @@ __global__ void __launch_bounds__(128) k_inner_team(Prm P, Fld F, double dt, int
         int kros = -1;
         PAdj s = {0, 0, 0, 0, 0, 0};
         double p = F.p[c], ep = F.ep[c], rog = F.rog[c], rgp = F.rgp[c];
-        double rlk[NC];
+        double rlk[NC], rlkn[NC], sink[NC];
 #pragma unroll
-        for (int is = 1; is <= ns; ++is) rlk[is - 1] = F.rlk[(is - 1) * n + c];
+        for (int is = 1; is <= ns; ++is) {
+            rlk[is - 1] = F.rlk[(is - 1) * n + c];
+            rlkn[is - 1] = F.rlkn[(is - 1) * n + c];
+            sink[is - 1] = F.sink[(is - 1) * n + c];
+        }
         double flux[NC];  // this lane's face mass flux by phase (gas first)
 #pragma unroll
         for (int l = 0; l < NC; ++l) flux[l] = 0.0;
-        const bool mus = P.muscl > 0 && fl[c] == FLUID;
         // source lanes of the faces (3D: W S B E N T = 0..5; 2D: W B E T = 0..3)
         const int lW = tb + 0, lE = tb + (D == 3 ? 3 : 2), lB = tb + (D == 3 ? 2 : 1), lT = tb + (D == 3 ? 5 : 3);
         const int lS = tb + 1, lN = tb + 4;
-        auto stencil = [&](const double *a, double own, double &dm, double &dmm, double &dp, double &dpp) {
-            dm = slot(a, rm, c, own);
-            dp = slot(a, rp, c, own);
-            if (mus) {
-                if (minus) dmm = slot(a, rmm, c, own);
-                else dpp = slot(a, rpp, c, own);
-            }
-        };
         for (int loop = 1; loop <= P.inmax; ++loop) {
             if (loop > 1 || nit > 1) padjust(s, p, kros, d3, p3, P.omega, abeta);
             rog = thermal_eosg(P, tgc, p, xg);
             rgp = ep * rog;
             // this lane's face system (matrix.f:351-630)
-            if (solved) face_system<NP>(P, F, c, minus ? rm : rp, rawnb, ii, dir, minus ? -1 : +1, dt, p, ep, rgp, rlk, vel);
+            if (solved) face_assemble<NP>(P, K, minus ? -1 : +1, p, ep, rgp, rlk, vel);
             // particle mass fluxes and volume fractions (iter.f:778-994)
+#pragma unroll
+            for (int is = 1; is <= ns; ++is) flux[is] = mflux(is, rlk[is - 1]);
             double rls = 0;
 #pragma unroll
             for (int is = 1; is <= ns; ++is) {
-                double own = rlk[is - 1];
-                if (own_face) {
-                    double dm = 0, dmm = 0, dp = 0, dpp = 0;
-                    stencil(F.rlk + (size_t)(is - 1) * n, own, dm, dmm, dp, dpp);
-                    flux[is] = face_mflux(P, g, minus, vel[is], own, dm, dmm, dp, dpp, mus);
-                }
                 double fW = __shfl_sync(tmask, flux[is], lW), fE = __shfl_sync(tmask, flux[is], lE);
                 double fB = __shfl_sync(tmask, flux[is], lB), fT = __shfl_sync(tmask, flux[is], lT);
                 double fS = 0, fN = 0;
                 if (D == 3) { fS = __shfl_sync(tmask, flux[is], lS); fN = __shfl_sync(tmask, flux[is], lN); }
-                size_t off = (size_t)(is - 1) * n;
-                double rlkx = (1.0 * fE - 1.0 * fW) * P.indx[i] * rx;
-                double rlkz = (1.0 * fT - 1.0 * fB) * P.indz[k];
-                double rlky = D == 3 ? (1.0 * fN - 1.0 * fS) * P.indy[j] : 0.0;
-                double t = F.rlkn[off + c] - dt * 1.0 * (rlkx + rlky + rlkz);
-                t = t + dt * 1.0 * F.sink[off + c];
+                double rlkx = (1.0 * fE - 1.0 * fW) * idx_i * rx;
+                double rlkz = (1.0 * fT - 1.0 * fB) * idz_k;
+                double rlky = D == 3 ? (1.0 * fN - 1.0 * fS) * idy_j : 0.0;
+                double t = rlkn[is - 1] - dt * 1.0 * (rlkx + rlky + rlkz);
+                t = t + dt * 1.0 * sink[is - 1];
                 double v = fmax(0.0, t);
                 rlk[is - 1] = v;
                 rls = rls + v * P.inrl[is];
@@ -198,11 +285,7 @@ __global__ void __launch_bounds__(128) k_inner_team(Prm P, Fld F, double dt, int
             if (rls > 1.0 && q == 0) atomicAdd(&F.counters[2], 1);
             rgp = ep * rog;
             // gas mass flux and continuity residual (iter.f:597-771)
-            if (own_face) {
-                double dm = 0, dmm = 0, dp = 0, dpp = 0;
-                stencil(F.rgp, rgp, dm, dmm, dp, dpp);
-                flux[0] = face_mflux(P, g, minus, vel[0], rgp, dm, dmm, dp, dpp, mus);
-            }
+            flux[0] = mflux(0, rgp);
             {
                 double fW = __shfl_sync(tmask, flux[0], lW), fE = __shfl_sync(tmask, flux[0], lE);
                 double fB = __shfl_sync(tmask, flux[0], lB), fT = __shfl_sync(tmask, flux[0], lT);
@@ -218,7 +301,7 @@ __global__ void __launch_bounds__(128) k_inner_team(Prm P, Fld F, double dt, int
             }
         }
         // ---- final values -----------------------------------------------------
-        if (own_face) {
+        {
             // face mass fluxes (every face, as calc_*_mass_flux writes them)
             double *gfa = dir == 0 ? F.rgfe : (dir == 1 ? F.rgfn : F.rgft);
             double *sfa = dir == 0 ? F.rsfe : (dir == 1 ? F.rsfn : F.rsft);
