@@ -140,6 +140,29 @@ int pdac_gpu_fieldn(pdac_ctx *ctx);
 int pdac_gpu_tilde(pdac_ctx *ctx, double dt);
 /* iter (iter.f:38-477); *nit receives the number of outer sweeps          */
 int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit);
+/* Variant of pdac_gpu_iter with no counterpart in the reference: the same
+ * computation and results, but the corrector's scratch (per-colour
+ * counters, worklist, active-set flags) lives in one fixed static device
+ * array of PDAC_ITER_STATIC_SCRATCH_BYTES instead of the context's buffers,
+ * and the call allocates no memory of any kind.  It serves hosts that fix
+ * their device footprint themselves -- e.g. a driver that reserves all
+ * device memory for its own pool at start-up and must not see later
+ * allocations, or whose memory accounting admits only the buffers it
+ * created.  Limits and rules:
+ *  - the mesh must fit: 256 + 4 * ceil((nx + 2) / 3) * ny * nz (rounded up
+ *    to 256) + nx * ny * nz bytes <= PDAC_ITER_STATIC_SCRATCH_BYTES, else the
+ *    call returns PDAC_ERR_ARG with the sizes in pdac_gpu_last_error;
+ *  - the context's device must be current; the first call on a device looks
+ *    up the array's address once (cudaGetSymbolAddress), so make that first
+ *    call before any stream capture on the device;
+ *  - nothing in the array needs to start at zero: the call clears the
+ *    counters on the context's stream before every sweep and sets the
+ *    active-set bytes before the first one;
+ *  - one array per device is shared by every context on it, so calls that
+ *    overlap in time on one device (other threads or streams) race and are
+ *    not allowed.                                                          */
+#define PDAC_ITER_STATIC_SCRATCH_BYTES (8 * 1024 * 1024)
+int pdac_gpu_iter_static(pdac_ctx *ctx, double dt, int *nit);
 /* ygas (ygas.f:27-156)                                                    */
 int pdac_gpu_ygas(pdac_ctx *ctx, double dt);
 /* htilde (htilde.f:25-178)                                                */

@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <mutex>
 
 #include "../../include/pdac_gpu.h"
 #include "inner.cuh"
@@ -486,6 +487,101 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
     }
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[7], st));
+    if (nit_out) *nit_out = nit;
+    return PDAC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// pdac_gpu_iter_static: pdac_gpu_iter with its corrector scratch (per-colour
+// counters, worklist, active-set flags) in one fixed static device array
+// instead of the context's buffers; the call allocates nothing.
+//
+// Layout of the static array: bytes [0, 256) hold the six int counters
+// (worklist length and tested cells per colour), then the worklist (one int
+// per cell of the largest colour phase, from byte 256, 256-aligned length),
+// then one active-set byte per cell.  The counters must be zero when a
+// residual-test launch starts: the call clears them itself on its stream
+// before every sweep, and sets every active-set byte before the first
+// sweep, so no part of the array has to start at zero.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_iter_scratch[PDAC_ITER_STATIC_SCRATCH_BYTES];
+
+namespace {
+std::mutex g_scratch_mutex;
+unsigned char *g_scratch_ptr[64] = {nullptr};  // device address of g_iter_scratch, by device ordinal
+
+// one-time set-up per device, with that device current
+int static_scratch(pdac_ctx *ctx, unsigned char **out) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(ctx, PDAC_ERR_ARG, "iter_static: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_ptr[dev]) {
+        void *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_iter_scratch);
+        if (e != cudaSuccess)
+            return fail(ctx, PDAC_ERR_CUDA, std::string("iter_static: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        g_scratch_ptr[dev] = static_cast<unsigned char *>(ptr);
+    }
+    *out = g_scratch_ptr[dev];
+    return PDAC_OK;
+}
+}  // namespace
+
+int pdac_gpu_iter_static(pdac_ctx *ctx, double dt, int *nit_out) {
+    if (!ctx) return PDAC_ERR_ARG;
+    int m = (ctx->nx + 2) / 3;
+    long nthr = (long)m * ctx->ny * ctx->nz;
+    size_t n = ctx->ncell, ns = ctx->ns;
+    size_t work_bytes = ((size_t)nthr * sizeof(int) + 255) / 256 * 256;
+    size_t need = 256 + work_bytes + n;
+    if (need > (size_t)PDAC_ITER_STATIC_SCRATCH_BYTES)
+        return fail(ctx, PDAC_ERR_ARG, "iter_static: this mesh needs " + std::to_string(need) +
+                                           " bytes of static scratch, the limit is " +
+                                           std::to_string((size_t)PDAC_ITER_STATIC_SCRATCH_BYTES));
+    unsigned char *base = nullptr;
+    int st_ = static_scratch(ctx, &base);
+    if (st_) return st_;
+    int *wcount = reinterpret_cast<int *>(base);
+    int *work = reinterpret_cast<int *>(base + 256);
+    unsigned char *dirty = base + 256 + work_bytes;
+    cudaStream_t st = ctx->stream;
+    Fld &F = ctx->F;
+    for (double *a : {F.rgfe, F.rgfn, F.rgft, F.conv, F.abeta})
+        if (a) CK(cudaMemsetAsync(a, 0, n * sizeof(double), st));
+    for (double *a : {F.rsfe, F.rsfn, F.rsft})
+        if (a) CK(cudaMemsetAsync(a, 0, n * ns * sizeof(double), st));
+    int nph = ctx->nph;
+    if (ctx->d3) {
+        PHASE_LAUNCH(nph, pdac::k_predictor3d, blocks(n), TPB, st, ctx->P, F, dt);
+        pdac::k_mflux_init3d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt);
+    } else {
+        PHASE_LAUNCH(nph, pdac::k_predictor2d, blocks(n), TPB, st, ctx->P, F, dt);
+        pdac::k_mflux_init2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt);
+    }
+    ctx->launches += 2;
+    CK(cudaGetLastError());
+    CK(cudaMemsetAsync(dirty, 1, n, st));
+    int nit;
+    for (nit = 1; nit <= ctx->cfg.maxout; ++nit) {
+        CK(cudaMemsetAsync(wcount, 0, 6 * sizeof(int), st));
+        for (int col = 0; col < 3; ++col) {
+            int *cnt = wcount + col;
+            if (ctx->d3) PHASE_LAUNCH(nph, pdac::k_resid3d, blocks(nthr), TPB, st, ctx->P, F, dt, col, work, cnt, dirty);
+            else PHASE_LAUNCH(nph, pdac::k_resid2d, blocks(nthr), TPB, st, ctx->P, F, dt, col, work, cnt, dirty);
+            long team_threads = (nthr + (ctx->d3 ? 4 : 7)) / (ctx->d3 ? 5 : 8) * 32;
+            int g = std::min(ctx->inner_grid, blocks(team_threads, TPB_TEAM));
+            if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_inner_team, 3, g, TPB_TEAM, st, ctx->P, F, dt, nit, work, cnt, dirty);
+            else PHASE_LAUNCH_D(nph, pdac::k_inner_team, 2, g, TPB_TEAM, st, ctx->P, F, dt, nit, work, cnt, dirty);
+            ctx->launches += 2;
+        }
+        CK(cudaMemcpyAsync(ctx->h_counters, wcount, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        ctx->sweeps++;
+        long unconverged = (long)ctx->h_counters[0] + ctx->h_counters[1] + ctx->h_counters[2];
+        if (unconverged == 0) break;
+    }
+    CK(cudaGetLastError());
     if (nit_out) *nit_out = nit;
     return PDAC_OK;
 }
