@@ -149,15 +149,16 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit);
  * device memory for its own pool at start-up and must not see later
  * allocations, or whose memory accounting admits only the buffers it
  * created.  Limits and rules:
- *  - the mesh must fit: 256 + 4 * ceil((nx + 2) / 3) * ny * nz (rounded up
- *    to 256) + nx * ny * nz bytes <= PDAC_ITER_STATIC_SCRATCH_BYTES, else the
+ *  - the mesh must fit: 256 + 2 * (4 * ceil((nx + 2) / 3) * ny * nz rounded
+ *    up to 256) + 4 * ceil(nx * ny * nz / 32) bytes
+ *    <= PDAC_ITER_STATIC_SCRATCH_BYTES, else the
  *    call returns PDAC_ERR_ARG with the sizes in pdac_gpu_last_error;
  *  - the context's device must be current; the first call on a device looks
  *    up the array's address once (cudaGetSymbolAddress), so make that first
  *    call before any stream capture on the device;
  *  - nothing in the array needs to start at zero: the call clears the
  *    counters on the context's stream before every sweep and sets the
- *    active-set bytes before the first one;
+ *    active-set bits before the first one;
  *  - one array per device is shared by every context on it, so calls that
  *    overlap in time on one device (other threads or streams) race and are
  *    not allowed.                                                          */

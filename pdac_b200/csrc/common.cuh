@@ -13,6 +13,7 @@
 #define PDAC_MAXS 8          // max solid classes
 #define PDAC_MAXP (PDAC_MAXS + 1)
 #define PDAC_MAXG 7
+#define TPB_RESID 256        // threads per block of the corrector's residual test
 
 namespace pdac {
 

@@ -41,7 +41,8 @@ struct pdac_ctx {
     long long launches = 0, sweeps = 0, corr_launches = 0, work_cells = 0, tested_cells = 0;
     double corr_ms = 0.0, resid_ms = 0.0, inner_ms = 0.0;
     int *d_work = nullptr, *d_wcount = nullptr;  // corrector worklist and its per-colour lengths
-    unsigned char *d_dirty = nullptr;            // corrector active set, one byte per cell
+    unsigned *d_dirty = nullptr;                 // corrector active set, one bit per cell
+    int *d_cand = nullptr;                       // candidate cells of one colour phase
     int inner_grid = 0;
     bool prof = false;
     cudaEvent_t cev[9];
@@ -246,8 +247,9 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
         CK(cudaMemcpy(ctx->d_vfact0, zero.data(), cfg->nvent * sizeof(double), cudaMemcpyHostToDevice));
     }
     CK(cudaMalloc(&ctx->d_work, (size_t)n * sizeof(int)));
-    CK(cudaMalloc(&ctx->d_wcount, 8 * sizeof(int)));
-    CK(cudaMalloc(&ctx->d_dirty, (size_t)n));
+    CK(cudaMalloc(&ctx->d_wcount, 16 * sizeof(int)));
+    CK(cudaMalloc(&ctx->d_dirty, ((size_t)n + 31) / 32 * sizeof(unsigned)));
+    CK(cudaMalloc(&ctx->d_cand, (size_t)n * sizeof(int)));
     {
         int dev = 0, nsm = 148;
         CK(cudaGetDevice(&dev));
@@ -323,6 +325,7 @@ int pdac_gpu_destroy(pdac_ctx *ctx) {
     cudaFree(ctx->d_work);
     cudaFree(ctx->d_wcount);
     cudaFree(ctx->d_dirty);
+    cudaFree(ctx->d_cand);
     cudaFree(ctx->d_partial);
     cudaFreeHost(ctx->h_counters);
     for (auto &e : ctx->ev) cudaEventDestroy(e);
@@ -404,8 +407,9 @@ int pdac_gpu_tilde(pdac_ctx *ctx, double dt) {
     CK(cudaEventRecord(ctx->ev[4], st));
     if (ctx->d3) {
         CK(cudaMemsetAsync(F.mf, 0, n * 9 * (ns + 1) * sizeof(double), st));
-        pdac::k_tilde_flux3d<<<blocks(n), TPB, 0, st>>>(ctx->P, F), ctx->launches++;
-        pdac::k_tilde3d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt, ctx->d_app0u, ctx->d_app0v, ctx->d_app0w), ctx->launches++;
+        pdac::k_tilde_flux3d<<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F), ctx->launches++;
+        PHASE_LAUNCH(ctx->nph, pdac::k_tilde3d, blocks(n), TPB, st, ctx->P, F, dt, ctx->d_app0u, ctx->d_app0v, ctx->d_app0w);
+        ctx->launches++;
     } else {
         for (double *a : {F.ugfe, F.ugft, F.wgfe, F.wgft}) CK(cudaMemsetAsync(a, 0, n * sizeof(double), st));
         for (double *a : {F.usfe, F.usft, F.wsfe, F.wsft}) CK(cudaMemsetAsync(a, 0, n * ns * sizeof(double), st));
@@ -445,17 +449,21 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
     int m = (ctx->nx + 2) / 3;
     long nthr = (long)m * ctx->ny * ctx->nz;
     // every cell is tested in the first sweep
-    CK(cudaMemsetAsync(ctx->d_dirty, 1, n, st));
+    const size_t nwords = (n + 31) / 32;
+    CK(cudaMemsetAsync(ctx->d_dirty, 0xff, nwords * sizeof(unsigned), st));
+    const int test_grid = std::max(1, ctx->inner_grid / 2);
     int nit;
     for (nit = 1; nit <= ctx->cfg.maxout; ++nit) {
-        // [col] worklist length, [3 + col] cells tested, of colour col
-        CK(cudaMemsetAsync(ctx->d_wcount, 0, 6 * sizeof(int), st));
+        // [col] worklist length, [3 + col] cells tested, [6 + col] candidates, of colour col
+        CK(cudaMemsetAsync(ctx->d_wcount, 0, 9 * sizeof(int), st));
         for (int col = 0; col < 3; ++col) {
-            int *cnt = ctx->d_wcount + col;
+            int *cnt = ctx->d_wcount + col, *ncand = ctx->d_wcount + 6 + col;
             if (ctx->prof) CK(cudaEventRecord(ctx->cev[3 * col], st));
-            unsigned char *dirty = ctx->d_dirty;
-            if (ctx->d3) PHASE_LAUNCH(nph, pdac::k_resid3d, blocks(nthr), TPB, st, ctx->P, F, dt, col, ctx->d_work, cnt, dirty);
-            else PHASE_LAUNCH(nph, pdac::k_resid2d, blocks(nthr), TPB, st, ctx->P, F, dt, col, ctx->d_work, cnt, dirty);
+            unsigned *dirty = ctx->d_dirty;
+            pdac::k_resid_collect<<<blocks((long)nwords, TPB_RESID), TPB_RESID, 0, st>>>(ctx->P, col, dirty, ctx->d_cand, ncand);
+            if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_resid_test, 3, test_grid, TPB_RESID, st, ctx->P, F, dt, ctx->d_cand, ncand, ctx->d_work, cnt);
+            else PHASE_LAUNCH_D(nph, pdac::k_resid_test, 2, test_grid, TPB_RESID, st, ctx->P, F, dt, ctx->d_cand, ncand, ctx->d_work, cnt);
+            ctx->launches++;
             if (ctx->prof) CK(cudaEventRecord(ctx->cev[3 * col + 1], st));
             // one team of lanes per worklist cell (5 teams of 6 lanes per warp
             // in 3D, 8 of 4 in 2D)
@@ -496,13 +504,13 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
 // counters, worklist, active-set flags) in one fixed static device array
 // instead of the context's buffers; the call allocates nothing.
 //
-// Layout of the static array: bytes [0, 256) hold the six int counters
-// (worklist length and tested cells per colour), then the worklist (one int
-// per cell of the largest colour phase, from byte 256, 256-aligned length),
-// then one active-set byte per cell.  The counters must be zero when a
-// residual-test launch starts: the call clears them itself on its stream
-// before every sweep, and sets every active-set byte before the first
-// sweep, so no part of the array has to start at zero.
+// Layout of the static array: bytes [0, 256) hold the nine int counters
+// (worklist length, tested cells and candidates per colour), then the
+// worklist and the candidate list (one int per cell of the largest colour
+// phase each, 256-aligned lengths), then the active set (one bit per cell).
+// The counters must be zero when a colour phase starts: the call clears them
+// itself on its stream before every sweep, and sets every active-set bit
+// before the first sweep, so no part of the array has to start at zero.
 // ---------------------------------------------------------------------------
 static __device__ __align__(256) unsigned char g_iter_scratch[PDAC_ITER_STATIC_SCRATCH_BYTES];
 
@@ -534,7 +542,8 @@ int pdac_gpu_iter_static(pdac_ctx *ctx, double dt, int *nit_out) {
     long nthr = (long)m * ctx->ny * ctx->nz;
     size_t n = ctx->ncell, ns = ctx->ns;
     size_t work_bytes = ((size_t)nthr * sizeof(int) + 255) / 256 * 256;
-    size_t need = 256 + work_bytes + n;
+    size_t nwords = (n + 31) / 32;
+    size_t need = 256 + 2 * work_bytes + nwords * sizeof(unsigned);
     if (need > (size_t)PDAC_ITER_STATIC_SCRATCH_BYTES)
         return fail(ctx, PDAC_ERR_ARG, "iter_static: this mesh needs " + std::to_string(need) +
                                            " bytes of static scratch, the limit is " +
@@ -544,7 +553,8 @@ int pdac_gpu_iter_static(pdac_ctx *ctx, double dt, int *nit_out) {
     if (st_) return st_;
     int *wcount = reinterpret_cast<int *>(base);
     int *work = reinterpret_cast<int *>(base + 256);
-    unsigned char *dirty = base + 256 + work_bytes;
+    int *cand = reinterpret_cast<int *>(base + 256 + work_bytes);
+    unsigned *dirty = reinterpret_cast<unsigned *>(base + 256 + 2 * work_bytes);
     cudaStream_t st = ctx->stream;
     Fld &F = ctx->F;
     for (double *a : {F.rgfe, F.rgfn, F.rgft, F.conv, F.abeta})
@@ -561,14 +571,17 @@ int pdac_gpu_iter_static(pdac_ctx *ctx, double dt, int *nit_out) {
     }
     ctx->launches += 2;
     CK(cudaGetLastError());
-    CK(cudaMemsetAsync(dirty, 1, n, st));
+    CK(cudaMemsetAsync(dirty, 0xff, nwords * sizeof(unsigned), st));
+    const int test_grid = std::max(1, ctx->inner_grid / 2);
     int nit;
     for (nit = 1; nit <= ctx->cfg.maxout; ++nit) {
-        CK(cudaMemsetAsync(wcount, 0, 6 * sizeof(int), st));
+        CK(cudaMemsetAsync(wcount, 0, 9 * sizeof(int), st));
         for (int col = 0; col < 3; ++col) {
-            int *cnt = wcount + col;
-            if (ctx->d3) PHASE_LAUNCH(nph, pdac::k_resid3d, blocks(nthr), TPB, st, ctx->P, F, dt, col, work, cnt, dirty);
-            else PHASE_LAUNCH(nph, pdac::k_resid2d, blocks(nthr), TPB, st, ctx->P, F, dt, col, work, cnt, dirty);
+            int *cnt = wcount + col, *ncand = wcount + 6 + col;
+            pdac::k_resid_collect<<<blocks((long)nwords, TPB_RESID), TPB_RESID, 0, st>>>(ctx->P, col, dirty, cand, ncand);
+            if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_resid_test, 3, test_grid, TPB_RESID, st, ctx->P, F, dt, cand, ncand, work, cnt);
+            else PHASE_LAUNCH_D(nph, pdac::k_resid_test, 2, test_grid, TPB_RESID, st, ctx->P, F, dt, cand, ncand, work, cnt);
+            ctx->launches++;
             long team_threads = (nthr + (ctx->d3 ? 4 : 7)) / (ctx->d3 ? 5 : 8) * 32;
             int g = std::min(ctx->inner_grid, blocks(team_threads, TPB_TEAM));
             if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_inner_team, 3, g, TPB_TEAM, st, ctx->P, F, dt, nit, work, cnt, dirty);

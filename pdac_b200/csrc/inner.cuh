@@ -133,7 +133,7 @@ __device__ __forceinline__ void face_assemble(const Prm &P, const FaceK<NP> &K, 
 
 template <int NP, int D>
 __global__ void __launch_bounds__(128) k_inner_team(Prm P, Fld F, double dt, int nit, const int *list, const int *count,
-                                                    unsigned char *dirty) {
+                                                    unsigned *dirty) {
     constexpr int T = D == 3 ? 6 : 4;    // lanes per cell
     constexpr int TPW = 32 / T;          // teams per warp (3D: 5, lanes 30 and 31 idle)
     constexpr int NF = D == 3 ? 6 : 4;   // faces per cell
@@ -313,15 +313,78 @@ __global__ void __launch_bounds__(128) k_inner_team(Prm P, Fld F, double dt, int
 #pragma unroll
                 for (int l = 2; l <= nph; ++l) svel[(l - 2) * n + fcell] = vel[l - 1];
             }
-            dirty[rawnb] = 1;
+            mark_dirty(dirty, rawnb);
         }
         if (q == 0) {
             F.p[c] = p; F.rog[c] = rog; F.rgp[c] = rgp; F.ep[c] = ep;
 #pragma unroll
             for (int is = 1; is <= ns; ++is) F.rlk[(is - 1) * n + c] = rlk[is - 1];
             F.abeta[c] = abeta;
-            dirty[c] = 1;
+            mark_dirty(dirty, c);
         }
+    }
+}
+
+// Residual test of one colour phase (iter.f:241-319) in two launches.
+// The active set is one bit per cell: the test of a cell reads only its own
+// p/rog/rgp and the mass fluxes of its faces, which change only when the
+// cell or a face neighbour runs the inner loop; such a run sets the bits of
+// those cells (mark_dirty), and a clean cell would recompute exactly the
+// values it holds, so it is not tested.  k_resid_collect turns the set bits
+// of one colour's fluid cells into a candidate list (clearing them, and the
+// bits of non-fluid cells, which are never tested); k_resid_test tests each
+// candidate: a converged cell updates its volume fractions (calc_eps) and
+// rgp, an unconverged one goes to the worklist of k_inner_team.
+__global__ void __launch_bounds__(TPB_RESID) k_resid_collect(Prm P, int colour, unsigned *dirty, int *cand,
+                                                             int *ncand) {
+    const unsigned nwords = ((unsigned)P.ncell + 31u) / 32u;
+    unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    int mine[32], nmine = 0;
+    if (t < nwords) {
+        unsigned w = dirty[t], keep = w;
+        while (w) {
+            int b = __ffs(w) - 1;
+            w &= w - 1u;
+            int c = (int)(32u * t) + b;
+            if (c >= P.ncell) break;
+            if (!(P.flag[c] & 1)) { keep &= ~(1u << b); continue; }
+            int i = c % P.nx + 1, r = c / P.nx, j = r % P.ny + 1, k = r / P.ny + 1;
+            if ((i + j + k) % 3 != colour) continue;
+            keep &= ~(1u << b);
+            mine[nmine++] = c;
+        }
+        if (keep != dirty[t]) dirty[t] = keep;
+    }
+    block_append_n<TPB_RESID, 32>(cand, ncand, mine, nmine, nullptr, 0);
+}
+
+template <int NP, int D>
+__global__ void __launch_bounds__(TPB_RESID) k_resid_test(Prm P, Fld F, double dt, const int *cand, const int *ncand,
+                                                          int *work, int *count) {
+    const int len = *ncand;
+    for (int base = blockIdx.x * TPB_RESID; base < len; base += gridDim.x * TPB_RESID) {
+        int idx = base + threadIdx.x, c = -1, nmine = 0;
+        if (idx < len) {
+            c = cand[idx];
+            double dg;
+            if (D == 3) {
+                int i, j, k;
+                ijk_of(P, c, i, j, k);
+                Raw3 R;
+                raw3(P, i, j, k, R);
+                dg = calc_res_3d(P, F, R, i, j, k, dt);
+                if (fabs(dg) <= F.conv[c]) calc_eps_3d<NP>(P, F, R, i, j, k, dt);
+            } else {
+                int i = c % P.nx + 1, k = c / P.nx + 1;
+                Raw2 R;
+                raw2(P, i, k, R);
+                dg = calc_res_2d(P, F, R, i, k, dt);
+                if (fabs(dg) <= F.conv[c]) calc_eps_2d(P, F, R, i, k, dt);
+            }
+            if (fabs(dg) <= F.conv[c]) F.rgp[c] = F.ep[c] * F.rog[c];
+            else nmine = 1;
+        }
+        block_append_n<TPB_RESID, 1>(work, count, &c, nmine, count + 3, idx < len ? 1 : 0);
     }
 }
 

@@ -663,47 +663,6 @@ __device__ __forceinline__ void padjust(PAdj &s, double &p, int &kros, double d3
     p3 = p;
 }
 
-// One colour phase of an outer sweep (iter.f:241-319) runs as two launches:
-// k_resid2d tests every cell of the colour, updates the volume fractions of
-// converged cells (calc_eps) and appends unconverged ones to a worklist;
-// k_inner_team (inner.cuh) runs inner_loop (iter.f:480-580) on the worklist.  Cells of one
-// colour never touch each other's data, so the split changes no result.
-// Clean cells (no inner loop at the cell or a face neighbour since their
-// last test) are skipped: their test would reproduce the values they hold.
-__device__ __forceinline__ int colour_cell2d(const Prm &P, int t, int colour, int &i, int &k) {
-    int m = (P.nx + 2) / 3;
-    if (t >= m * P.nz) return -1;
-    k = t / m + 1;
-    int q = t % m;
-    int i0 = (((colour - 1 - k) % 3) + 3) % 3;
-    if (i0 == 0) i0 = 3;
-    i = i0 + 3 * q;
-    if (i > P.nx) return -1;
-    return (i - 1) + P.nx * (k - 1);
-}
-
-template <int NP>
-__global__ void k_resid2d(Prm P, Fld F, double dt, int colour, int *list, int *count, unsigned char *dirty) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    int i = 0, k = 0;
-    int c = colour_cell2d(P, t, colour, i, k);
-    bool want = false, tested = false;
-    if (c >= 0 && dirty[c] && fluid(P, c)) {
-        dirty[c] = 0;
-        tested = true;
-        Raw2 R;
-        raw2(P, i, k, R);
-        double dg = calc_res_2d(P, F, R, i, k, dt);
-        if (fabs(dg) <= F.conv[c]) {
-            calc_eps_2d(P, F, R, i, k, dt);
-            F.rgp[c] = F.ep[c] * F.rog[c];
-        } else {
-            want = true;
-        }
-    }
-    work_append(list, count, c, want);
-    warp_count(count + 3, tested);
-}
 
 // ---------------------------------------------------------------------------
 // ygas, ygas.f:27-325 (2D)

@@ -239,9 +239,13 @@ __global__ void k_fieldn3d(Prm P, Fld F) {
 // ---------------------------------------------------------------------------
 // tilde momentum fluxes, compute_all_fluxes_tilde tilde.f:850-1326 (3D)
 // ---------------------------------------------------------------------------
+// one thread per (cell, phase): consecutive threads take consecutive cells
+// of one phase
 __global__ void k_tilde_flux3d(Prm P, Fld F) {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= P.ncell || !fluid(P, c)) return;
+    unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (unsigned)P.ncell * (unsigned)(P.ns + 1)) return;
+    int ph = (int)(t / (unsigned)P.ncell), c = (int)(t % (unsigned)P.ncell);
+    if (!fluid(P, c)) return;
     int i, j, k;
     ijk_of(P, c, i, j, k);
     Raw3 R;
@@ -251,7 +255,7 @@ __global__ void k_tilde_flux3d(Prm P, Fld F) {
     bool dw = !fluid(P, R.w), ds = !fluid(P, R.s), db = !fluid(P, R.b);
     bool mus = P.muscl > 0 && P.flag[c] == FLUID;
     size_t n = P.ncell;
-    for (int ph = 0; ph <= P.ns; ++ph) {
+    {
         size_t off = (size_t)(ph > 0 ? ph - 1 : 0) * n;
         const double *U = ph == 0 ? F.ug : F.us + off;
         const double *V = ph == 0 ? F.vg : F.vs + off;
@@ -295,7 +299,9 @@ __global__ void k_tilde_flux3d(Prm P, Fld F) {
 // tilde mesh loop, tilde.f:276-848 (3D), with stress3D, kdrags/sdrag and
 // inter (drag.f:11-298).  app0 holds the interphase matrix of the previous
 // visit of each cell in this step; it is read only when alpha < 1.
+template <int NP>
 __global__ void k_tilde3d(Prm P, Fld F, double dt, const double *app0u, const double *app0v, const double *app0w) {
+    constexpr int MP = Sys<NP>::M;  // phase capacity + 1
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.ncell || !fluid(P, c)) return;
     int i, j, k;
@@ -306,14 +312,15 @@ __global__ void k_tilde3d(Prm P, Fld F, double dt, const double *app0u, const do
     rem3(P, i, j, k, R, M);
     const double *dx = P.dx, *dy = P.dy, *dz = P.dz, *indx = P.indx, *indy = P.indy, *indz = P.indz;
     size_t n = P.ncell;
-    int ns = P.ns;
+    const int ns = nphases<NP>(P) - 1, nph = ns + 1;
     int imjk = R.w, ijmk = R.s, ijkm = R.b, ijke = M.e, ijkn = M.n, ijkt = M.t;
     double alpha = P.alpha, ag = P.alphagrav;
     double dxi = dx[i], dxip1 = dx[i + 1], dyj = dy[j], dyjp1 = dy[j + 1], dzk = dz[k], dzkp1 = dz[k + 1];
     double indxp = 1.0 / (dx[i] + dx[i + 1]), indyp = 1.0 / (dy[j] + dy[j + 1]), indzp = 1.0 / (dz[k] + dz[k + 1]);
-    double rr[PDAC_MAXP + 1][3];
-    double kpgv[PDAC_MAXP];
+    double rr[MP][3];
+    double kpgv[MP];
     const double a_rep = -8.76, b_rep = -0.27;
+#pragma unroll
     for (int ph = 0; ph <= ns; ++ph) {
         size_t off = (size_t)(ph > 0 ? ph - 1 : 0) * n;
         double vx = 0, vy = 0, vz = 0;
@@ -404,14 +411,17 @@ __global__ void k_tilde3d(Prm P, Fld F, double dt, const double *app0u, const do
         }
     }
     // inter, drag.f:173-246
-    const int NA = PDAC_MAXP * (PDAC_MAXP + 1) / 2 + 1;
+    constexpr int NA = MP * (MP - 1) / 2 + 1;
     double au[NA], av[NA], aw[NA];
-    double rlkc[PDAC_MAXP];
+    double rlkc[MP];
+#pragma unroll
     for (int is = 1; is <= ns; ++is) rlkc[is] = SOL(F.rlk, c, is);
     int ks = 0;
-    for (int kk1 = 1; kk1 <= P.nph; ++kk1) {
+#pragma unroll
+    for (int kk1 = 1; kk1 <= nph; ++kk1) {
         if (kk1 == 1) { ks++; au[ks] = av[ks] = aw[ks] = 0; }
         else {
+#pragma unroll
             for (int kk = 1; kk <= kk1; ++kk) {
                 ks++;
                 if (kk == 1) { au[ks] = -kpgv[kk1 - 1] * dt; av[ks] = -kpgv[kk1 - 1] * dt; aw[ks] = -kpgv[kk1 - 1] * dt; }
@@ -428,28 +438,39 @@ __global__ void k_tilde3d(Prm P, Fld F, double dt, const double *app0u, const do
             }
         }
     }
-    for (int kk1 = 1; kk1 <= P.nph; ++kk1) {
+#pragma unroll
+    for (int kk1 = 1; kk1 <= nph; ++kk1) {
         double sx = 0, sy = 0, sz = 0;
+#pragma unroll
         for (int kk = 1; kk <= kk1; ++kk) { int q = kk + kk1 * (kk1 - 1) / 2; sx = sx + au[q]; sy = sy + av[q]; sz = sz + aw[q]; }
-        for (int kk = kk1; kk <= P.nph; ++kk) { int q = kk1 + kk * (kk - 1) / 2; sx = sx + au[q]; sy = sy + av[q]; sz = sz + aw[q]; }
+#pragma unroll
+        for (int kk = kk1; kk <= nph; ++kk) { int q = kk1 + kk * (kk - 1) / 2; sx = sx + au[q]; sy = sy + av[q]; sz = sz + aw[q]; }
         int q = kk1 * (kk1 + 1) / 2;
         au[q] = -sx; av[q] = -sy; aw[q] = -sz;
     }
-    for (int q = 1; q <= P.nap; ++q) { APP(F.appu, c, q) = au[q]; APP(F.appv, c, q) = av[q]; APP(F.appw, c, q) = aw[q]; }
+    const int nap = nph * (nph + 1) / 2;
+#pragma unroll
+    for (int q = 1; q <= nap; ++q) { APP(F.appu, c, q) = au[q]; APP(F.appv, c, q) = av[q]; APP(F.appw, c, q) = aw[q]; }
     // (1 - alpha) explicit interphase part, tilde.f:597-680
     if (alpha != 1.0) {
-        const double *a0[3] = {app0u, app0v, app0w};
-        const double *an[3] = {au, av, aw};
         double coef0[3] = {dxi, dyj, dzk}, coef1[3] = {dxip1, dyjp1, dzkp1}, inv[3] = {indxp, indyp, indzp};
         int nbr[3] = {ijke, ijkn, ijkt};
-        const double *gv[3] = {F.ug, F.vg, F.wg}, *sv[3] = {F.us, F.vs, F.ws};
+#pragma unroll
         for (int q = 0; q < 3; ++q) {
-            auto A = [&](int cell, int ls) { return cell == c ? an[q][ls] : APP(a0[q], cell, ls); };
+            const double *a0 = q == 0 ? app0u : (q == 1 ? app0v : app0w);
+            const double *gvq = q == 0 ? F.ug : (q == 1 ? F.vg : F.wg);
+            const double *svq = q == 0 ? F.us : (q == 1 ? F.vs : F.ws);
+            auto A = [&](int cell, int ls) {
+                double own = q == 0 ? au[ls] : (q == 1 ? av[ls] : aw[ls]);
+                return cell == c ? own : APP(a0, cell, ls);
+            };
             auto AP = [&](int ls) { return (1.0 - alpha) * (coef0[q] * A(nbr[q], ls) + coef1[q] * A(c, ls)) * inv[q]; };
-            auto vel = [&](int ph) { return ph == 0 ? gv[q][c] : SOL(sv[q], c, ph); };
+            auto vel = [&](int ph) { return ph == 0 ? gvq[c] : SOL(svq, c, ph); };
             rr[0][q] = rr[0][q] - AP(1) * vel(0);
-            for (int l = 2; l <= P.nph; ++l) {
+#pragma unroll
+            for (int l = 2; l <= nph; ++l) {
                 int ls1 = l * (l - 1) / 2;
+#pragma unroll
                 for (int ll = 1; ll <= l; ++ll) {
                     int ls = ls1 + ll;
                     double f = AP(ls);
@@ -467,6 +488,7 @@ __global__ void k_tilde3d(Prm P, Fld F, double dt, const double *app0u, const do
         }
     }
     F.rug[c] = rr[0][0]; F.rvg[c] = rr[0][1]; F.rwg[c] = rr[0][2];
+#pragma unroll
     for (int is = 1; is <= ns; ++is) { SOL(F.rus, c, is) = rr[is][0]; SOL(F.rvs, c, is) = rr[is][1]; SOL(F.rws, c, is) = rr[is][2]; }
 }
 
@@ -577,53 +599,6 @@ __device__ __forceinline__ void calc_eps_3d(const Prm &P, const Fld &F, const Ra
     if (rls > 1.0) atomicAdd(&F.counters[2], 1);
 }
 
-// One colour phase of an outer sweep (iter.f:241-319) runs as two launches.
-// k_resid3d tests every cell of the colour: a converged cell only updates its
-// volume fractions (calc_eps), an unconverged one is appended to a worklist;
-// k_inner_team (inner.cuh) then runs inner_loop (iter.f:480-580) on it.  Cells of
-// one colour never touch each other's data, so the split changes no result.
-//
-// Active set: the test of a cell reads only its own p/rog/rgp and the mass
-// fluxes of its six faces, which change only when the cell or a face
-// neighbour runs the inner loop.  Such a run marks the cell and its six face
-// neighbours dirty; a clean cell was converged at its last test and would
-// recompute exactly the values it holds, so the test skips it.
-__device__ __forceinline__ int colour_cell3d(const Prm &P, long t, int colour, int &i, int &j, int &k) {
-    int m = (P.nx + 2) / 3;
-    if (t >= (long)m * P.ny * P.nz) return -1;
-    int q = (int)(t % m);
-    long rest = t / m;
-    j = (int)(rest % P.ny) + 1;
-    k = (int)(rest / P.ny) + 1;
-    int i0 = (((colour - j - k) % 3) + 3) % 3;
-    if (i0 == 0) i0 = 3;
-    i = i0 + 3 * q;
-    if (i > P.nx) return -1;
-    return at3(P, i, j, k);
-}
-
-template <int NP>
-__global__ void k_resid3d(Prm P, Fld F, double dt, int colour, int *list, int *count, unsigned char *dirty) {
-    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    int i = 0, j = 0, k = 0;
-    int c = colour_cell3d(P, t, colour, i, j, k);
-    bool want = false, tested = false;
-    if (c >= 0 && dirty[c] && fluid(P, c)) {
-        dirty[c] = 0;
-        tested = true;
-        Raw3 R;
-        raw3(P, i, j, k, R);
-        double dg = calc_res_3d(P, F, R, i, j, k, dt);
-        if (fabs(dg) <= F.conv[c]) {
-            calc_eps_3d<NP>(P, F, R, i, j, k, dt);
-            F.rgp[c] = F.ep[c] * F.rog[c];
-        } else {
-            want = true;
-        }
-    }
-    work_append(list, count, c, want);
-    warp_count(count + 3, tested);
-}
 
 // ---------------------------------------------------------------------------
 // ygas, ygas.f:27-325 (3D)

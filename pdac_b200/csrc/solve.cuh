@@ -136,22 +136,42 @@ __device__ __forceinline__ double slot(const double *a, int idx, int c, double o
     return idx == c ? own : __ldg(a + idx);
 }
 
-// Warp-aggregated append of cell c to a worklist when want is set: one
-// atomic per warp.  Every lane of the warp must reach this call.
-__device__ __forceinline__ void work_append(int *list, int *count, int c, bool want) {
-    unsigned m = __ballot_sync(0xffffffffu, want);
-    if (m == 0) return;
-    int lane = threadIdx.x & 31, leader = __ffs(m) - 1, base = 0;
-    if (lane == leader) base = atomicAdd(count, __popc(m));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (want) list[base + __popc(m & ((1u << lane) - 1u))] = c;
+// Block-aggregated append of up to CAP cells per thread (cells[0..ncand))
+// and count of tested cells (tested_count may be NULL): one atomic per block
+// and counter.  Every thread of the block (TPBK threads) must reach this call.
+template <int TPBK, int CAP>
+__device__ __forceinline__ void block_append_n(int *list, int *count, const int *cells, int ncand, int *tested_count,
+                                               int ntested) {
+    constexpr int NW = TPBK / 32;
+    __shared__ int s_off[NW], s_tst[NW], s_base;
+    const unsigned full = 0xffffffffu;
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int incl = ncand;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int v = __shfl_up_sync(full, incl, o);
+        if (lane >= o) incl += v;
+    }
+    int tst = ntested;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) tst += __shfl_xor_sync(full, tst, o);
+    if (lane == 31) s_off[wid] = incl;
+    if (lane == 0) s_tst[wid] = tst;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int tot = 0, tt = 0;
+        for (int w = 0; w < NW; ++w) { int v = s_off[w]; s_off[w] = tot; tot += v; tt += s_tst[w]; }
+        s_base = tot ? atomicAdd(count, tot) : 0;
+        if (tt && tested_count) atomicAdd(tested_count, tt);
+    }
+    __syncthreads();
+    int off = s_base + s_off[wid] + incl - ncand;
+#pragma unroll 1
+    for (int q = 0; q < ncand && q < CAP; ++q) list[off + q] = cells[q];
+    __syncthreads();
 }
 
-// Warp-aggregated count of the lanes with flag set.  Every lane of the warp
-// must reach this call.
-__device__ __forceinline__ void warp_count(int *count, bool flag) {
-    unsigned m = __ballot_sync(0xffffffffu, flag);
-    if (m != 0 && (threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(count, __popc(m));
-}
+// set the active-set bit of cell x (one bit per cell, 32 per word)
+__device__ __forceinline__ void mark_dirty(unsigned *dirty, int x) { atomicOr(dirty + (x >> 5), 1u << (x & 31)); }
 
 }  // namespace pdac

@@ -13,14 +13,14 @@ phases, d dimensions, G gas species, N_app = d * S(S+1)/2 interphase terms.
   whole step (semi-implicit path, rungekut = 1):
     B_step = 8 [ fixed + nit (R_sweep + W_sweep) ]
 
-  A colour phase of the corrector runs as two kernels:
-    residual test, per cell of the colour: its active-set byte; a tested
-      cell reads its mass-flux faces (2d), rgp, rgpn, conv; a converged one
-      also reads its particle mass-flux faces (2d ns), rlkn, sink (2 ns) and
-      rog, and writes rlk (ns), ep and rgp:
-        skipped      1
-        converged    8 [(2d + 3) + (2d + 2) ns + 1 + ns + 2] + 1
-        unconverged  8 (2d + 3) + 4 (worklist entry) + 1
+  A colour phase of the corrector runs as three kernels:
+    collect: the active-set bitmask (ncell / 8 bytes) and 4 bytes per
+      candidate written;
+    residual test, per candidate: mass-flux faces (2d), rgp, rgpn, conv; a
+      converged cell also reads its particle mass-flux faces (2d ns), rlkn,
+      sink (2 ns) and rog, and writes rlk (ns), ep and rgp:
+        converged    8 [(2d + 3) + (2d + 2) ns + 1 + ns + 2] + 4
+        unconverged  8 (2d + 3) + 4 + 4 (worklist entry)
     inner loop, per unconverged cell: 8 (R_sweep + W_sweep) + 4
 """
 from __future__ import annotations
@@ -55,11 +55,12 @@ def step_bytes_per_cell(ns, ng, nit, d=2):
     return 8 * (step_fixed_doubles(ns, ng, d) + nit * (r + w))
 
 
-def resid_bytes(ns, d, converged, unconverged, skipped=0):
-    """Algorithmic bytes of residual-test launches covering the given cells."""
-    conv = 8 * ((2 * d + 3) + (2 * d + 2) * ns + 1 + ns + 2) + 1
-    unconv = 8 * (2 * d + 3) + 4 + 1
-    return conv * converged + unconv * unconverged + skipped
+def resid_bytes(ns, d, converged, unconverged, ncell=0, phases=0):
+    """Algorithmic bytes of the collect + residual-test launches of `phases`
+    colour phases that tested the given cells."""
+    conv = 8 * ((2 * d + 3) + (2 * d + 2) * ns + 1 + ns + 2) + 4
+    unconv = 8 * (2 * d + 3) + 8
+    return conv * converged + unconv * unconverged + phases * (ncell // 8)
 
 
 def inner_bytes(ns, ng, d, unconverged):
