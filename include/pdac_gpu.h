@@ -197,6 +197,11 @@ int pdac_gpu_phase_times(pdac_ctx *ctx, double *ms7);
  * the reset enabled profiling); nout >= 4                                 */
 int pdac_gpu_stats(pdac_ctx *ctx, double *out, int nout);
 int pdac_gpu_reset_stats(pdac_ctx *ctx, int profile_corrector);
+/* per colour phase of the corrector since the last profiling reset, six
+ * doubles each: sweep, colour, worklist length, cells tested, device ms of
+ * the residual test and of the inner loop; *n_inout holds the capacity in
+ * doubles on entry and the count on return                                */
+int pdac_gpu_sweep_log(pdac_ctx *ctx, double *out, long *n_inout);
 /* stream-ordered timing marks (slots 0..31) and the device time between two */
 int pdac_gpu_mark(pdac_ctx *ctx, int slot);
 int pdac_gpu_elapsed(pdac_ctx *ctx, int a, int b, double *ms);

@@ -44,6 +44,7 @@ struct pdac_ctx {
     unsigned *d_dirty = nullptr;                 // corrector active set, one bit per cell
     int *d_cand = nullptr;                       // candidate cells of one colour phase
     int inner_grid = 0;
+    std::vector<double> sweep_log;  // per colour phase when profiling: sweep, colour, worklist, tested, ms x2
     bool prof = false;
     cudaEvent_t cev[9];
     cudaEvent_t user_ev[32];
@@ -53,7 +54,6 @@ struct pdac_ctx {
 namespace {
 
 const int TPB = 128;
-const int TPB_CORR = 64;
 const int TPB_TEAM = 128;
 
 int fail(pdac_ctx *c, int code, const std::string &msg) {
@@ -490,6 +490,13 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
             }
             ctx->work_cells += unconverged;
             ctx->tested_cells += (long)ctx->h_counters[3] + ctx->h_counters[4] + ctx->h_counters[5];
+            for (int col = 0; col < 3; ++col) {
+                float t0 = 0, t1 = 0;
+                CK(cudaEventElapsedTime(&t0, ctx->cev[3 * col], ctx->cev[3 * col + 1]));
+                CK(cudaEventElapsedTime(&t1, ctx->cev[3 * col + 1], ctx->cev[3 * col + 2]));
+                double rec[6] = {(double)nit, (double)col, (double)ctx->h_counters[col], (double)ctx->h_counters[3 + col], t0, t1};
+                ctx->sweep_log.insert(ctx->sweep_log.end(), rec, rec + 6);
+            }
         }
         if (unconverged == 0) break;
     }
@@ -760,7 +767,19 @@ int pdac_gpu_reset_stats(pdac_ctx *ctx, int profile_corrector) {
     if (!ctx) return PDAC_ERR_ARG;
     ctx->launches = ctx->sweeps = ctx->corr_launches = ctx->work_cells = ctx->tested_cells = 0;
     ctx->corr_ms = ctx->resid_ms = ctx->inner_ms = 0.0;
+    ctx->sweep_log.clear();
     ctx->prof = profile_corrector != 0;
+    return PDAC_OK;
+}
+
+// per colour phase since the last profiling reset: sweep, colour, worklist
+// length, cells tested, residual-test ms, inner-loop ms (6 doubles each)
+int pdac_gpu_sweep_log(pdac_ctx *ctx, double *out, long *n_inout) {
+    if (!ctx || !n_inout) return PDAC_ERR_ARG;
+    long need = (long)ctx->sweep_log.size();
+    if (!out || *n_inout < need) { *n_inout = need; return need ? PDAC_ERR_ARG : PDAC_OK; }
+    std::copy(ctx->sweep_log.begin(), ctx->sweep_log.end(), out);
+    *n_inout = need;
     return PDAC_OK;
 }
 

@@ -131,12 +131,16 @@ __device__ __forceinline__ void face_assemble(const Prm &P, const FaceK<NP> &K, 
     for (int l = 1; l <= nph; ++l) v[l - 1] = b[l];
 }
 
+// minimum resident blocks per SM the register allocation must allow
+#ifndef PDAC_INNER_MINB
+#define PDAC_INNER_MINB 2
+#endif
+
 template <int NP, int D>
-__global__ void __launch_bounds__(128) k_inner_team(Prm P, Fld F, double dt, int nit, const int *list, const int *count,
+__global__ void __launch_bounds__(128, PDAC_INNER_MINB) k_inner_team(Prm P, Fld F, double dt, int nit, const int *list, const int *count,
                                                     unsigned *dirty) {
     constexpr int T = D == 3 ? 6 : 4;    // lanes per cell
     constexpr int TPW = 32 / T;          // teams per warp (3D: 5, lanes 30 and 31 idle)
-    constexpr int NF = D == 3 ? 6 : 4;   // faces per cell
     constexpr int NC = Sys<NP>::M - 1;   // phase capacity
     const int nph = nphases<NP>(P), ns = nph - 1;
     const size_t n = P.ncell;

@@ -170,6 +170,18 @@ class Engine:
         return dict(launches=int(out[0]), sweeps=int(out[1]), corr_launches=int(out[2]), corr_ms=out[3],
                     resid_ms=out[4], inner_ms=out[5], work_cells=int(out[6]), tested_cells=int(out[7]))
 
+    def sweep_log(self):
+        """Per colour phase since the last profiling reset: array of rows
+        (sweep, colour, worklist, tested, resid_ms, inner_ms)."""
+        L = self.L
+        L.pdac_gpu_sweep_log.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_long)]
+        L.pdac_gpu_sweep_log.restype = C.c_int
+        n = C.c_long(0)
+        L.pdac_gpu_sweep_log(self.h, None, C.byref(n))
+        buf = np.zeros(max(n.value, 1))
+        self._chk(L.pdac_gpu_sweep_log(self.h, buf.ctypes.data_as(C.POINTER(C.c_double)), C.byref(n)), "sweep_log")
+        return buf[:n.value].reshape(-1, 6)
+
     def reset_stats(self, profile_corrector=False):
         self._chk(self.L.pdac_gpu_reset_stats(self.h, int(profile_corrector)), "reset_stats")
 
