@@ -52,6 +52,7 @@ struct Fld {
     double *rug, *rvg, *rwg, *rus, *rvs, *rws, *appu, *appv, *appw;
     double *ugfe, *ugft, *wgfe, *wgft, *usfe, *usft, *wsfe, *wsft;  // 2D momentum fluxes
     double *mf;  // 3D momentum fluxes, block ((phase*3 + component)*3 + face) of ncell values
+    double *vis; // 3D viscous stress divergence, block (phase*3 + component) of ncell values
     double *rgfe, *rgfn, *rgft, *rsfe, *rsfn, *rsft, *conv, *abeta;
     double *egfe, *egfn, *egft, *esfe, *esfn, *esft, *rhg, *rhs;
     double *yfe, *yfn, *yft;

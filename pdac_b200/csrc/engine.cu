@@ -44,6 +44,12 @@ struct pdac_ctx {
     unsigned *d_dirty = nullptr;                 // corrector active set, one bit per cell
     int *d_cand = nullptr;                       // candidate cells of one colour phase
     int inner_grid = 0;
+    int *d_nit = nullptr, *h_nit = nullptr;  // outer sweep number (device, pinned host)
+    // the outer sweep loop as a graph: a conditional WHILE node whose body is
+    // one sweep, instantiated for one dt
+    cudaGraph_t it_graph = nullptr;
+    cudaGraphExec_t it_exec = nullptr;
+    double it_dt = 0.0;
     std::vector<double> sweep_log;  // per colour phase when profiling: sweep, colour, worklist, tested, ms x2
     bool prof = false;
     cudaEvent_t cev[9];
@@ -256,6 +262,8 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
         CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
         ctx->inner_grid = nsm * 16;
     }
+    CK(cudaMalloc(&ctx->d_nit, sizeof(int)));
+    CK(cudaMallocHost(&ctx->h_nit, sizeof(int)));
     CK(cudaMalloc(&ctx->d_counters, 8 * sizeof(int)));
     CK(cudaMemset(ctx->d_counters, 0, 8 * sizeof(int)));
     CK(cudaMallocHost(&ctx->h_counters, 8 * sizeof(int)));
@@ -280,7 +288,7 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
         {"appw", &F.appw, nap},
         {"ugfe", &F.ugfe, d2}, {"ugft", &F.ugft, d2}, {"wgfe", &F.wgfe, d2}, {"wgft", &F.wgft, d2},
         {"usfe", &F.usfe, ns * d2}, {"usft", &F.usft, ns * d2}, {"wsfe", &F.wsfe, ns * d2},
-        {"wsft", &F.wsft, ns * d2}, {"mf", &F.mf, 9 * (ns + 1) * d3},
+        {"wsft", &F.wsft, ns * d2}, {"mf", &F.mf, 9 * (ns + 1) * d3}, {"vis", &F.vis, 3 * (ns + 1) * d3},
         {"rgfe", &F.rgfe, 1}, {"rgfn", &F.rgfn, d3}, {"rgft", &F.rgft, 1}, {"rsfe", &F.rsfe, ns},
         {"rsfn", &F.rsfn, ns * d3}, {"rsft", &F.rsft, ns},
         {"conv", &F.conv, 1}, {"abeta", &F.abeta, 1}, {"egfe", &F.egfe, 1}, {"egfn", &F.egfn, d3},
@@ -325,6 +333,10 @@ int pdac_gpu_destroy(pdac_ctx *ctx) {
     cudaFree(ctx->d_work);
     cudaFree(ctx->d_wcount);
     cudaFree(ctx->d_dirty);
+    if (ctx->it_exec) cudaGraphExecDestroy(ctx->it_exec);
+    if (ctx->it_graph) cudaGraphDestroy(ctx->it_graph);
+    cudaFree(ctx->d_nit);
+    cudaFreeHost(ctx->h_nit);
     cudaFree(ctx->d_cand);
     cudaFree(ctx->d_partial);
     cudaFreeHost(ctx->h_counters);
@@ -407,7 +419,12 @@ int pdac_gpu_tilde(pdac_ctx *ctx, double dt) {
     CK(cudaEventRecord(ctx->ev[4], st));
     if (ctx->d3) {
         CK(cudaMemsetAsync(F.mf, 0, n * 9 * (ns + 1) * sizeof(double), st));
-        pdac::k_tilde_flux3d<<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F), ctx->launches++;
+        pdac::k_visc3d<<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
+        ctx->launches++;
+        pdac::k_tilde_flux3d<0><<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
+        pdac::k_tilde_flux3d<1><<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
+        pdac::k_tilde_flux3d<2><<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
+        ctx->launches += 3;
         PHASE_LAUNCH(ctx->nph, pdac::k_tilde3d, blocks(n), TPB, st, ctx->P, F, dt, ctx->d_app0u, ctx->d_app0v, ctx->d_app0w);
         ctx->launches++;
     } else {
@@ -423,6 +440,71 @@ int pdac_gpu_tilde(pdac_ctx *ctx, double dt) {
     }
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[5], st));
+    return PDAC_OK;
+}
+
+// one outer sweep of the corrector (iter.f:241-410): three colour phases of
+// candidate collection, residual test and inner loop; the sweep number is
+// read on the device from d_nit
+static int enqueue_sweep(pdac_ctx *ctx, double dt, cudaStream_t st, bool prof) {
+    Fld &F = ctx->F;
+    const int nph = ctx->nph;
+    const size_t n = ctx->ncell, nwords = (n + 31) / 32;
+    const long nthr = (long)((ctx->nx + 2) / 3) * ctx->ny * ctx->nz;
+    const int test_grid = std::max(1, ctx->inner_grid / 2);
+    // one team of lanes per worklist cell (5 teams of 6 lanes per warp in
+    // 3D, 8 of 4 in 2D)
+    const long team_threads = (nthr + (ctx->d3 ? 4 : 7)) / (ctx->d3 ? 5 : 8) * 32;
+    const int g = std::min(ctx->inner_grid, blocks(team_threads, TPB_TEAM));
+    unsigned *dirty = ctx->d_dirty;
+    // [col] worklist length, [3 + col] cells tested, [6 + col] candidates, of colour col
+    CK(cudaMemsetAsync(ctx->d_wcount, 0, 9 * sizeof(int), st));
+    for (int col = 0; col < 3; ++col) {
+        int *cnt = ctx->d_wcount + col, *ncand = ctx->d_wcount + 6 + col;
+        if (prof) CK(cudaEventRecord(ctx->cev[3 * col], st));
+        pdac::k_resid_collect<<<blocks((long)nwords, TPB_RESID), TPB_RESID, 0, st>>>(ctx->P, col, dirty, ctx->d_cand, ncand);
+        if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_resid_test, 3, test_grid, TPB_RESID, st, ctx->P, F, dt, ctx->d_cand, ncand, ctx->d_work, cnt);
+        else PHASE_LAUNCH_D(nph, pdac::k_resid_test, 2, test_grid, TPB_RESID, st, ctx->P, F, dt, ctx->d_cand, ncand, ctx->d_work, cnt);
+        if (prof) CK(cudaEventRecord(ctx->cev[3 * col + 1], st));
+        if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_inner_team, 3, g, TPB_TEAM, st, ctx->P, F, dt, ctx->d_nit, ctx->d_work, cnt, dirty);
+        else PHASE_LAUNCH_D(nph, pdac::k_inner_team, 2, g, TPB_TEAM, st, ctx->P, F, dt, ctx->d_nit, ctx->d_work, cnt, dirty);
+        if (prof) CK(cudaEventRecord(ctx->cev[3 * col + 2], st));
+    }
+    CK(cudaGetLastError());
+    return PDAC_OK;
+}
+
+// (re)build the graph of the outer sweep loop for time step dt: a WHILE
+// conditional node around one sweep plus k_sweep_check, which clears the
+// condition when the sweep left no unconverged cell or maxout is reached
+static int build_iter_graph(pdac_ctx *ctx, double dt) {
+    if (ctx->it_exec) { cudaGraphExecDestroy(ctx->it_exec); ctx->it_exec = nullptr; }
+    if (ctx->it_graph) { cudaGraphDestroy(ctx->it_graph); ctx->it_graph = nullptr; }
+    cudaStream_t st = ctx->stream;
+    CK(cudaGraphCreate(&ctx->it_graph, 0));
+    cudaGraphConditionalHandle loop;
+    CK(cudaGraphConditionalHandleCreate(&loop, ctx->it_graph, 1, cudaGraphCondAssignDefault));
+    // the union inside cudaGraphNodeParams has no default constructor:
+    // build the parameters in zeroed storage
+    alignas(cudaGraphNodeParams) unsigned char cp_storage[sizeof(cudaGraphNodeParams)] = {};
+    cudaGraphNodeParams &cp = *reinterpret_cast<cudaGraphNodeParams *>(cp_storage);
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = loop;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, ctx->it_graph, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CK(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    int s = enqueue_sweep(ctx, dt, st, false);
+    if (!s) pdac::k_sweep_check<<<1, 1, 0, st>>>(ctx->d_wcount, ctx->d_nit, ctx->cfg.maxout, loop);
+    cudaGraph_t captured = nullptr;
+    cudaError_t e = cudaStreamEndCapture(st, &captured);
+    if (s) return s;
+    if (e != cudaSuccess) return fail(ctx, PDAC_ERR_CUDA, std::string("iter graph capture: ") + cudaGetErrorString(e));
+    CK(cudaGetLastError());
+    CK(cudaGraphInstantiate(&ctx->it_exec, ctx->it_graph, 0));
+    ctx->it_dt = dt;
     return PDAC_OK;
 }
 
@@ -446,39 +528,38 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
     }
     ctx->launches += 2;
     CK(cudaGetLastError());
-    int m = (ctx->nx + 2) / 3;
-    long nthr = (long)m * ctx->ny * ctx->nz;
     // every cell is tested in the first sweep
-    const size_t nwords = (n + 31) / 32;
-    CK(cudaMemsetAsync(ctx->d_dirty, 0xff, nwords * sizeof(unsigned), st));
-    const int test_grid = std::max(1, ctx->inner_grid / 2);
+    CK(cudaMemsetAsync(ctx->d_dirty, 0xff, (n + 31) / 32 * sizeof(unsigned), st));
     int nit;
-    for (nit = 1; nit <= ctx->cfg.maxout; ++nit) {
-        // [col] worklist length, [3 + col] cells tested, [6 + col] candidates, of colour col
-        CK(cudaMemsetAsync(ctx->d_wcount, 0, 9 * sizeof(int), st));
-        for (int col = 0; col < 3; ++col) {
-            int *cnt = ctx->d_wcount + col, *ncand = ctx->d_wcount + 6 + col;
-            if (ctx->prof) CK(cudaEventRecord(ctx->cev[3 * col], st));
-            unsigned *dirty = ctx->d_dirty;
-            pdac::k_resid_collect<<<blocks((long)nwords, TPB_RESID), TPB_RESID, 0, st>>>(ctx->P, col, dirty, ctx->d_cand, ncand);
-            if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_resid_test, 3, test_grid, TPB_RESID, st, ctx->P, F, dt, ctx->d_cand, ncand, ctx->d_work, cnt);
-            else PHASE_LAUNCH_D(nph, pdac::k_resid_test, 2, test_grid, TPB_RESID, st, ctx->P, F, dt, ctx->d_cand, ncand, ctx->d_work, cnt);
-            ctx->launches++;
-            if (ctx->prof) CK(cudaEventRecord(ctx->cev[3 * col + 1], st));
-            // one team of lanes per worklist cell (5 teams of 6 lanes per warp
-            // in 3D, 8 of 4 in 2D)
-            long team_threads = (nthr + (ctx->d3 ? 4 : 7)) / (ctx->d3 ? 5 : 8) * 32;
-            int g = std::min(ctx->inner_grid, blocks(team_threads, TPB_TEAM));
-            if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_inner_team, 3, g, TPB_TEAM, st, ctx->P, F, dt, nit, ctx->d_work, cnt, dirty);
-            else PHASE_LAUNCH_D(nph, pdac::k_inner_team, 2, g, TPB_TEAM, st, ctx->P, F, dt, nit, ctx->d_work, cnt, dirty);
-            if (ctx->prof) CK(cudaEventRecord(ctx->cev[3 * col + 2], st));
-            ctx->launches += 2;
+    if (!ctx->prof) {
+        // the sweep loop runs on the device; one read-back of its count
+        if (!ctx->it_exec || ctx->it_dt != dt) {
+            int s = build_iter_graph(ctx, dt);
+            if (s) return s;
         }
-        CK(cudaMemcpyAsync(ctx->h_counters, ctx->d_wcount, 6 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        *ctx->h_nit = 1;
+        CK(cudaMemcpyAsync(ctx->d_nit, ctx->h_nit, sizeof(int), cudaMemcpyHostToDevice, st));
+        CK(cudaGraphLaunch(ctx->it_exec, st));
+        CK(cudaMemcpyAsync(ctx->h_nit, ctx->d_nit, sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
-        ctx->sweeps++;
-        long unconverged = (long)ctx->h_counters[0] + ctx->h_counters[1] + ctx->h_counters[2];
-        if (ctx->prof) {
+        nit = *ctx->h_nit;
+        int done = std::min(nit, ctx->cfg.maxout);
+        ctx->sweeps += done;
+        ctx->launches += 10L * done;
+    } else {
+        // host loop with per-colour-phase timing
+        for (nit = 1; nit <= ctx->cfg.maxout; ++nit) {
+            *ctx->h_nit = nit;
+            CK(cudaMemcpyAsync(ctx->d_nit, ctx->h_nit, sizeof(int), cudaMemcpyHostToDevice, st));
+            int s = enqueue_sweep(ctx, dt, st, true);
+            if (s) return s;
+            ctx->launches += 9;
+            CK(cudaMemcpyAsync(ctx->h_counters, ctx->d_wcount, 6 * sizeof(int), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            ctx->sweeps++;
+            long unconverged = (long)ctx->h_counters[0] + ctx->h_counters[1] + ctx->h_counters[2];
+            ctx->work_cells += unconverged;
+            ctx->tested_cells += (long)ctx->h_counters[3] + ctx->h_counters[4] + ctx->h_counters[5];
             for (int col = 0; col < 3; ++col) {
                 float t0 = 0, t1 = 0;
                 CK(cudaEventElapsedTime(&t0, ctx->cev[3 * col], ctx->cev[3 * col + 1]));
@@ -487,18 +568,12 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
                 ctx->inner_ms += t1;
                 ctx->corr_ms += t0 + t1;
                 ctx->corr_launches++;
-            }
-            ctx->work_cells += unconverged;
-            ctx->tested_cells += (long)ctx->h_counters[3] + ctx->h_counters[4] + ctx->h_counters[5];
-            for (int col = 0; col < 3; ++col) {
-                float t0 = 0, t1 = 0;
-                CK(cudaEventElapsedTime(&t0, ctx->cev[3 * col], ctx->cev[3 * col + 1]));
-                CK(cudaEventElapsedTime(&t1, ctx->cev[3 * col + 1], ctx->cev[3 * col + 2]));
-                double rec[6] = {(double)nit, (double)col, (double)ctx->h_counters[col], (double)ctx->h_counters[3 + col], t0, t1};
+                double rec[6] = {(double)nit, (double)col, (double)ctx->h_counters[col],
+                                 (double)ctx->h_counters[3 + col], t0, t1};
                 ctx->sweep_log.insert(ctx->sweep_log.end(), rec, rec + 6);
             }
+            if (unconverged == 0) break;
         }
-        if (unconverged == 0) break;
     }
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[7], st));
@@ -512,7 +587,8 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
 // instead of the context's buffers; the call allocates nothing.
 //
 // Layout of the static array: bytes [0, 256) hold the nine int counters
-// (worklist length, tested cells and candidates per colour), then the
+// (worklist length, tested cells and candidates per colour) and the sweep
+// number (int 12), then the
 // worklist and the candidate list (one int per cell of the largest colour
 // phase each, 256-aligned lengths), then the active set (one bit per cell).
 // The counters must be zero when a colour phase starts: the call clears them
@@ -559,6 +635,7 @@ int pdac_gpu_iter_static(pdac_ctx *ctx, double dt, int *nit_out) {
     int st_ = static_scratch(ctx, &base);
     if (st_) return st_;
     int *wcount = reinterpret_cast<int *>(base);
+    int *dnit = wcount + 12;  // sweep number, read by the inner loop
     int *work = reinterpret_cast<int *>(base + 256);
     int *cand = reinterpret_cast<int *>(base + 256 + work_bytes);
     unsigned *dirty = reinterpret_cast<unsigned *>(base + 256 + 2 * work_bytes);
@@ -582,6 +659,8 @@ int pdac_gpu_iter_static(pdac_ctx *ctx, double dt, int *nit_out) {
     const int test_grid = std::max(1, ctx->inner_grid / 2);
     int nit;
     for (nit = 1; nit <= ctx->cfg.maxout; ++nit) {
+        *ctx->h_nit = nit;
+        CK(cudaMemcpyAsync(dnit, ctx->h_nit, sizeof(int), cudaMemcpyHostToDevice, st));
         CK(cudaMemsetAsync(wcount, 0, 9 * sizeof(int), st));
         for (int col = 0; col < 3; ++col) {
             int *cnt = wcount + col, *ncand = wcount + 6 + col;
@@ -591,8 +670,8 @@ int pdac_gpu_iter_static(pdac_ctx *ctx, double dt, int *nit_out) {
             ctx->launches++;
             long team_threads = (nthr + (ctx->d3 ? 4 : 7)) / (ctx->d3 ? 5 : 8) * 32;
             int g = std::min(ctx->inner_grid, blocks(team_threads, TPB_TEAM));
-            if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_inner_team, 3, g, TPB_TEAM, st, ctx->P, F, dt, nit, work, cnt, dirty);
-            else PHASE_LAUNCH_D(nph, pdac::k_inner_team, 2, g, TPB_TEAM, st, ctx->P, F, dt, nit, work, cnt, dirty);
+            if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_inner_team, 3, g, TPB_TEAM, st, ctx->P, F, dt, dnit, work, cnt, dirty);
+            else PHASE_LAUNCH_D(nph, pdac::k_inner_team, 2, g, TPB_TEAM, st, ctx->P, F, dt, dnit, work, cnt, dirty);
             ctx->launches += 2;
         }
         CK(cudaMemcpyAsync(ctx->h_counters, wcount, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -137,8 +137,9 @@ __device__ __forceinline__ void face_assemble(const Prm &P, const FaceK<NP> &K, 
 #endif
 
 template <int NP, int D>
-__global__ void __launch_bounds__(128, PDAC_INNER_MINB) k_inner_team(Prm P, Fld F, double dt, int nit, const int *list, const int *count,
-                                                    unsigned *dirty) {
+__global__ void __launch_bounds__(128, PDAC_INNER_MINB) k_inner_team(Prm P, Fld F, double dt, const int *nitp, const int *list,
+                                                                     const int *count, unsigned *dirty) {
+    const int nit = *nitp;  // outer sweep number, 1-based
     constexpr int T = D == 3 ? 6 : 4;    // lanes per cell
     constexpr int TPW = 32 / T;          // teams per warp (3D: 5, lanes 30 and 31 idle)
     constexpr int NC = Sys<NP>::M - 1;   // phase capacity
@@ -390,6 +391,18 @@ __global__ void __launch_bounds__(TPB_RESID) k_resid_test(Prm P, Fld F, double d
         }
         block_append_n<TPB_RESID, 1>(work, count, &c, nmine, count + 3, idx < len ? 1 : 0);
     }
+}
+
+// End of one outer sweep on the device (iter.f:388-410): with no unconverged
+// cell left, or after maxout sweeps, the sweep loop stops; otherwise the
+// sweep number advances.  *nit ends as the host loop's nit (maxout + 1 when
+// the sweeps did not converge).
+__global__ void k_sweep_check(const int *wcount, int *nit, int maxout, cudaGraphConditionalHandle loop) {
+    long unconverged = (long)wcount[0] + wcount[1] + wcount[2];
+    if (unconverged == 0) { cudaGraphSetConditional(loop, 0); return; }
+    if (*nit >= maxout) { *nit = maxout + 1; cudaGraphSetConditional(loop, 0); return; }
+    *nit += 1;
+    cudaGraphSetConditional(loop, 1);
 }
 
 }  // namespace pdac

@@ -239,8 +239,9 @@ __global__ void k_fieldn3d(Prm P, Fld F) {
 // ---------------------------------------------------------------------------
 // tilde momentum fluxes, compute_all_fluxes_tilde tilde.f:850-1326 (3D)
 // ---------------------------------------------------------------------------
-// one thread per (cell, phase): consecutive threads take consecutive cells
-// of one phase
+// one thread per (cell, phase) for one momentum component COMP (0 = x,
+// 1 = y, 2 = z): consecutive threads take consecutive cells of one phase
+template <int COMP>
 __global__ void k_tilde_flux3d(Prm P, Fld F) {
     unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (unsigned)P.ncell * (unsigned)(P.ns + 1)) return;
@@ -255,50 +256,90 @@ __global__ void k_tilde_flux3d(Prm P, Fld F) {
     bool dw = !fluid(P, R.w), ds = !fluid(P, R.s), db = !fluid(P, R.b);
     bool mus = P.muscl > 0 && P.flag[c] == FLUID;
     size_t n = P.ncell;
-    {
-        size_t off = (size_t)(ph > 0 ? ph - 1 : 0) * n;
-        const double *U = ph == 0 ? F.ug : F.us + off;
-        const double *V = ph == 0 ? F.vg : F.vs + off;
-        const double *W = ph == 0 ? F.wg : F.ws + off;
-        const double *D = ph == 0 ? F.rgp : F.rlk + off;
-        S3 u, v, w, d, ds3;
-        rnb3(u, U, R);
-        rnb3(v, V, R);
-        rnb3(w, W, R);
-        nb3(d, D, R, M);
-        F6d f = {0, 0, 0, 0, 0, 0};
-        // x momentum
+    size_t off = (size_t)(ph > 0 ? ph - 1 : 0) * n;
+    const double *U = ph == 0 ? F.ug : F.us + off;
+    const double *V = ph == 0 ? F.vg : F.vs + off;
+    const double *W = ph == 0 ? F.wg : F.ws + off;
+    const double *D = ph == 0 ? F.rgp : F.rlk + off;
+    S3 u, v, w, d, ds3;
+    rnb3(u, U, R);
+    rnb3(v, V, R);
+    rnb3(w, W, R);
+    nb3(d, D, R, M);
+    F6d f = {0, 0, 0, 0, 0, 0};
+    if (COMP == 0) {  // x momentum
         interp_x3(P, d, i, ds3);
         flu_3d(P, f, dw, ds, db, ds3, u, v, w, i);
         if (mus && i != P.nx - 1) muscl_flu_3d(P, f, ds3, u, v, w, i, j, k);
-        MFX(ph, 0, 0)[c] = f.e; MFX(ph, 0, 1)[c] = f.n; MFX(ph, 0, 2)[c] = f.t;
-        if (dw) MFX(ph, 0, 0)[R.w] = f.w;
-        if (ds) MFX(ph, 0, 1)[R.s] = f.s;
-        if (db) MFX(ph, 0, 2)[R.b] = f.b;
-        // y momentum
-        f = {0, 0, 0, 0, 0, 0};
+    } else if (COMP == 1) {  // y momentum
         interp_y3(P, d, j, ds3);
         flv_3d(P, f, dw, ds, db, ds3, u, v, w, j);
         if (mus && j != P.ny - 1) muscl_flv_3d(P, f, ds3, u, v, w, i, j, k);
-        MFX(ph, 1, 0)[c] = f.e; MFX(ph, 1, 1)[c] = f.n; MFX(ph, 1, 2)[c] = f.t;
-        if (dw) MFX(ph, 1, 0)[R.w] = f.w;
-        if (ds) MFX(ph, 1, 1)[R.s] = f.s;
-        if (db) MFX(ph, 1, 2)[R.b] = f.b;
-        // z momentum
-        f = {0, 0, 0, 0, 0, 0};
+    } else {  // z momentum
         interp_z3(P, d, k, ds3);
         flw_3d(P, f, dw, ds, db, ds3, u, v, w, k);
         if (mus && k != P.nz - 1) muscl_flw_3d(P, f, ds3, u, v, w, i, j, k);
-        MFX(ph, 2, 0)[c] = f.e; MFX(ph, 2, 1)[c] = f.n; MFX(ph, 2, 2)[c] = f.t;
-        if (dw) MFX(ph, 2, 0)[R.w] = f.w;
-        if (ds) MFX(ph, 2, 1)[R.s] = f.s;
-        if (db) MFX(ph, 2, 2)[R.b] = f.b;
     }
+    MFX(ph, COMP, 0)[c] = f.e; MFX(ph, COMP, 1)[c] = f.n; MFX(ph, COMP, 2)[c] = f.t;
+    if (dw) MFX(ph, COMP, 0)[R.w] = f.w;
+    if (ds) MFX(ph, COMP, 1)[R.s] = f.s;
+    if (db) MFX(ph, COMP, 2)[R.b] = f.b;
 }
 
 // tilde mesh loop, tilde.f:276-848 (3D), with stress3D, kdrags/sdrag and
 // inter (drag.f:11-298).  app0 holds the interphase matrix of the previous
 // visit of each cell in this step; it is read only when alpha < 1.
+// viscous stress divergence of one phase of one cell (viscg / viscs,
+// visc.f:150-291, stress3D visc.f:293-559) with the particle repulsion term
+// (tilde.f:362-416); one thread per (cell, phase), consecutive threads take
+// consecutive cells of one phase
+__global__ void k_visc3d(Prm P, Fld F) {
+    unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (unsigned)P.ncell * (unsigned)(P.ns + 1)) return;
+    int ph = (int)(t / (unsigned)P.ncell), c = (int)(t % (unsigned)P.ncell);
+    if (!fluid(P, c)) return;
+    int i, j, k;
+    ijk_of(P, c, i, j, k);
+    Raw3 R;
+    Rem3 M;
+    raw3(P, i, j, k, R);
+    rem3(P, i, j, k, R, M);
+    const double *dx = P.dx, *dy = P.dy, *dz = P.dz;
+    size_t n = P.ncell;
+    size_t off = (size_t)(ph > 0 ? ph - 1 : 0) * n;
+    int ijke = M.e, ijkn = M.n, ijkt = M.t;
+    double indxp = 1.0 / (dx[i] + dx[i + 1]), indyp = 1.0 / (dy[j] + dy[j + 1]), indzp = 1.0 / (dz[k] + dz[k + 1]);
+    const double a_rep = -8.76, b_rep = -0.27;
+    double vx = 0, vy = 0, vz = 0;
+    if (ph == 0) {
+        if (P.gas_viscosity) {
+            const double *mug = F.mug, *ep = F.ep;
+            stress3d_cell(P, R, M, i, j, k, [&](int q) { return mug[q]; }, [&](int q) { return ep[q]; }, F.ug, F.vg,
+                          F.wg, vx, vy, vz);
+        }
+    } else if (P.part_viscosity) {
+        const double cm = P.cmus[ph], ir = P.inrl[ph];
+        const double *rl = F.rlk + off;
+        stress3d_cell(P, R, M, i, j, k, [&](int) { return cm; }, [&](int q) { return rl[q] * ir; }, F.us + off,
+                      F.vs + off, F.ws + off, vx, vy, vz);
+        if (P.repulsive_model == 1) {
+            double rc = rl[c], re = rl[ijke], rn = rl[ijkn], rt = rl[ijkt];
+            double epsx = (dx[i + 1] * rc + dx[i] * re) * indxp * ir;
+            double gepx = pow(10.0, -a_rep * epsx + b_rep);
+            vx = vx - gepx * indxp * 2.0 * (re - rc) * ir;
+            double epsz = (dz[k + 1] * rc + dz[k] * rt) * indzp * ir;
+            double gepz = pow(10.0, -a_rep * epsz + b_rep);
+            vz = vz - gepz * indzp * 2.0 * (rt - rc) * ir;
+            double epsy = (dy[j + 1] * rc + dy[j] * rn) * indyp * ir;
+            double gepy = pow(10.0, -a_rep * epsy + b_rep);
+            vy = vy - gepy * indyp * 2.0 * (rn - rc) * ir;
+        }
+    }
+    F.vis[(size_t)(ph * 3 + 0) * n + c] = vx;
+    F.vis[(size_t)(ph * 3 + 1) * n + c] = vy;
+    F.vis[(size_t)(ph * 3 + 2) * n + c] = vz;
+}
+
 template <int NP>
 __global__ void k_tilde3d(Prm P, Fld F, double dt, const double *app0u, const double *app0v, const double *app0w) {
     constexpr int MP = Sys<NP>::M;  // phase capacity + 1
@@ -319,35 +360,12 @@ __global__ void k_tilde3d(Prm P, Fld F, double dt, const double *app0u, const do
     double indxp = 1.0 / (dx[i] + dx[i + 1]), indyp = 1.0 / (dy[j] + dy[j + 1]), indzp = 1.0 / (dz[k] + dz[k + 1]);
     double rr[MP][3];
     double kpgv[MP];
-    const double a_rep = -8.76, b_rep = -0.27;
 #pragma unroll
     for (int ph = 0; ph <= ns; ++ph) {
         size_t off = (size_t)(ph > 0 ? ph - 1 : 0) * n;
-        double vx = 0, vy = 0, vz = 0;
-        if (ph == 0) {
-            if (P.gas_viscosity) {
-                const double *mug = F.mug, *ep = F.ep;
-                stress3d_cell(P, R, M, i, j, k, [&](int q) { return mug[q]; }, [&](int q) { return ep[q]; }, F.ug, F.vg,
-                              F.wg, vx, vy, vz);
-            }
-        } else if (P.part_viscosity) {
-            const double cm = P.cmus[ph], ir = P.inrl[ph];
-            const double *rl = F.rlk + off;
-            stress3d_cell(P, R, M, i, j, k, [&](int) { return cm; }, [&](int q) { return rl[q] * ir; }, F.us + off,
-                          F.vs + off, F.ws + off, vx, vy, vz);
-            if (P.repulsive_model == 1) {
-                double rc = rl[c], re = rl[ijke], rn = rl[ijkn], rt = rl[ijkt];
-                double epsx = (dx[i + 1] * rc + dx[i] * re) * indxp * ir;
-                double gepx = pow(10.0, -a_rep * epsx + b_rep);
-                vx = vx - gepx * indxp * 2.0 * (re - rc) * ir;
-                double epsz = (dz[k + 1] * rc + dz[k] * rt) * indzp * ir;
-                double gepz = pow(10.0, -a_rep * epsz + b_rep);
-                vz = vz - gepz * indzp * 2.0 * (rt - rc) * ir;
-                double epsy = (dy[j + 1] * rc + dy[j] * rn) * indyp * ir;
-                double gepy = pow(10.0, -a_rep * epsy + b_rep);
-                vy = vy - gepy * indyp * 2.0 * (rn - rc) * ir;
-            }
-        }
+        // viscous terms from k_visc3d
+        double vx = F.vis[(size_t)(ph * 3 + 0) * n + c], vy = F.vis[(size_t)(ph * 3 + 1) * n + c];
+        double vz = F.vis[(size_t)(ph * 3 + 2) * n + c];
         double ufx = MFX(ph, 0, 0)[c] - MFX(ph, 0, 0)[imjk], ufy = MFX(ph, 0, 1)[c] - MFX(ph, 0, 1)[ijmk];
         double ufz = MFX(ph, 0, 2)[c] - MFX(ph, 0, 2)[ijkm];
         double vfx = MFX(ph, 1, 0)[c] - MFX(ph, 1, 0)[imjk], vfy = MFX(ph, 1, 1)[c] - MFX(ph, 1, 1)[ijmk];
