@@ -65,6 +65,8 @@ typedef struct pdac_cfg {
     /* &numeric */
     double dt;
     int    rungekut;
+    int    time_integration;    /* 0 = semi-implicit (tilde/iter/htilde/ftem),
+                                   1 = explicit SSP-RK3 (explicit_solver.f)  */
     double alpha, alphagrav;
     double omega, delg;
     int    inmax, maxout;
@@ -170,7 +172,17 @@ int pdac_gpu_ygas(pdac_ctx *ctx, double dt);
 int pdac_gpu_htilde(pdac_ctx *ctx, double dt);
 /* ftem (ftem.f:19-199)                                                    */
 int pdac_gpu_ftem(pdac_ctx *ctx, double dt);
-/* one whole time step: boundary, fieldn, RK loop of tilde/iter/ygas/htilde/ftem */
+/* explicit SSP-RK3 solver, contexts created with time_integration = 1:
+ * initialize_fieldn (explicit_solver.f:419-564) in place of fieldn, and
+ * explicit_iter (explicit_solver.f:996-1223) in place of tilde / iter /
+ * htilde / ftem; explicit_iter returns PDAC_ERR_EOS where the reference
+ * stops on more than one caloric failure (explicit_solver.f:1214-1215).
+ * Both return PDAC_ERR_CONFIG on a time_integration = 0 context.           */
+int pdac_gpu_initialize_fieldn(pdac_ctx *ctx);
+int pdac_gpu_explicit_iter(pdac_ctx *ctx, double dt);
+/* one whole time step: boundary, fieldn, RK loop of tilde/iter/ygas/htilde/ftem
+ * (time_integration = 0), or boundary, initialize_fieldn, RK loop of
+ * explicit_iter/ygas (time_integration = 1, *nit = 0)                      */
 int pdac_gpu_step(pdac_ctx *ctx, int sweep, int *nit);
 
 /* vent fluctuation factors for the next boundary call, one per vent cell in

@@ -69,8 +69,19 @@ struct Sten {
     double eet = 0, ett = 0, eee = 0, nnn = 0, ttt = 0, een = 0, enn = 0, nnt = 0, ntt = 0;
 };
 
+// fields of the SSP-RK3 explicit path (explicit_solver.f:15-83)
+struct RK3State {
+    int neq = 0;
+    std::vector<double> rgpS, rlkS, ugS, usS, vgS, vsS, wgS, wsS, tgS, tsS, siegS, siesS, pS, epS, rhogS;
+    std::vector<double> ugN, usN, vgN, vsN, wgN, wsN;
+    std::vector<double> hv, kpgv;            // (ncell, ns) column-major
+    std::vector<double> rhs3, k1, k2, k3;    // row per cell: [c * neq + eq]
+    std::vector<double> hf3;                 // 3D diffusive heat fluxes, [phase][face e,n,t]
+};
+
 struct Oracle {
     pdac_cfg cfg{};
+    RK3State rk;
     bool d3 = false;
     int nx = 0, ny = 1, nz = 0, ncell = 0, ns = 0, ng = 0, nph = 0, nap = 0;
     int order = 0;                 // 0 colored, 1 lexicographic
@@ -1889,6 +1900,7 @@ void alloc(Oracle &o) {
 }
 
 #include "pdac_oracle3d.inc"
+#include "pdac_oracle_rk3.inc"
 
 }  // namespace
 
@@ -2033,7 +2045,23 @@ int pdac_oracle_ftem(void *h, double dt) {
     return o.d3 ? ftem_3d(o, dt) : ftem_2d(o, dt);
 }
 
-// prog.f:143-417 for one step (time_integration = 0)
+// initialize_fieldn (explicit_solver.f:419-564), the time_integration = 1
+// counterpart of fieldn; coefficients use the full time step
+int pdac_oracle_initialize_fieldn(void *h) {
+    Oracle &o = *(Oracle *)h;
+    rk3_fieldn(o, o.cfg.dt);
+    return PDAC_OK;
+}
+// explicit_iter (explicit_solver.f:996-1223); PDAC_ERR_EOS when more than
+// one caloric failure, as explicit_solver.f:1214-1215 aborts
+int pdac_oracle_explicit_iter(void *h, double dt) {
+    Oracle &o = *(Oracle *)h;
+    if (o.rk.neq == 0) return PDAC_ERR_ARG;
+    int num = rk3_iter(o, dt);
+    return num > 1 ? PDAC_ERR_EOS : PDAC_OK;
+}
+
+// prog.f:143-417 for one step
 int pdac_oracle_step(void *h, int sweep, int *nit) {
     Oracle &o = *(Oracle *)h;
     pdac_oracle_boundary(h, sweep);
@@ -2045,9 +2073,20 @@ int pdac_oracle_step(void *h, int sweep, int *nit) {
             o.rgp[c] = o.rog[c] * o.ep[c];
         }
     }
-    pdac_oracle_fieldn(h);
     double dt0 = o.cfg.dt;
     int st = PDAC_OK;
+    if (o.cfg.time_integration == 1) {
+        pdac_oracle_initialize_fieldn(h);
+        if (nit) *nit = 0;
+        for (int rk = 1; rk <= o.cfg.rungekut; ++rk) {
+            double dt = dt0 / (o.cfg.rungekut + 1 - rk);
+            int s2 = pdac_oracle_explicit_iter(h, dt);
+            if (s2 != PDAC_OK) st = s2;
+            pdac_oracle_ygas(h, dt);
+        }
+        return st;
+    }
+    pdac_oracle_fieldn(h);
     for (int rk = 1; rk <= o.cfg.rungekut; ++rk) {
         double dt = dt0 / (o.cfg.rungekut + 1 - rk);
         pdac_oracle_tilde(h, dt);
@@ -2079,7 +2118,16 @@ int pdac_oracle_get_array(void *h, const char *name, double *out, long *n_inout)
                {"esfe", &o.esfe}, {"esft", &o.esft}, {"dgres", &o.dgres},
                {"rvgn", &o.rvgn}, {"rvsn", &o.rvsn}, {"rvg", &o.rvg}, {"rvs", &o.rvs}, {"appv", &o.appv},
                {"rgfn", &o.rgfn}, {"rsfn", &o.rsfn}, {"mf3", &o.mf3}, {"ef3", &o.ef3},
-               {"gvisy", &o.gvisy}, {"pvisy", &o.pvisy}};
+               {"gvisy", &o.gvisy}, {"pvisy", &o.pvisy}, {"hgfe", &o.hgfe}, {"hgft", &o.hgft},
+               {"hsfe", &o.hsfe}, {"hsft", &o.hsft},
+               // explicit-solver fields (explicit_solver.f:15-83)
+               {"rgpstar", &o.rk.rgpS}, {"rlkstar", &o.rk.rlkS}, {"ugstar", &o.rk.ugS}, {"usstar", &o.rk.usS},
+               {"vgstar", &o.rk.vgS}, {"vsstar", &o.rk.vsS}, {"wgstar", &o.rk.wgS}, {"wsstar", &o.rk.wsS},
+               {"tgstar", &o.rk.tgS}, {"tsstar", &o.rk.tsS}, {"siegstar", &o.rk.siegS}, {"siesstar", &o.rk.siesS},
+               {"pstar", &o.rk.pS}, {"epstar", &o.rk.epS}, {"rhogstar", &o.rk.rhogS}, {"ugn", &o.rk.ugN},
+               {"usn", &o.rk.usN}, {"vgn", &o.rk.vgN}, {"vsn", &o.rk.vsN}, {"wgn", &o.rk.wgN}, {"wsn", &o.rk.wsN},
+               {"hv", &o.rk.hv}, {"kpgv", &o.rk.kpgv}, {"rhs3", &o.rk.rhs3}, {"k1", &o.rk.k1}, {"k2", &o.rk.k2},
+               {"k3", &o.rk.k3}, {"hf3", &o.rk.hf3}};
     for (auto &e : tab) {
         if (std::strcmp(e.n, name) == 0) {
             long need = (long)e.v->size();

@@ -24,8 +24,9 @@ _lib = None
 
 def build(force=False):
     """Compile the oracle with its Makefile (g++ only; seconds)."""
+    srcs = ("pdac_oracle.cpp", "pdac_oracle3d.inc", "pdac_oracle_rk3.inc")
     if force or not os.path.exists(LIB_PATH) or \
-            os.path.getmtime(LIB_PATH) < os.path.getmtime(os.path.join(HERE, "pdac_oracle.cpp")):
+            os.path.getmtime(LIB_PATH) < max(os.path.getmtime(os.path.join(HERE, f)) for f in srcs):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
     return LIB_PATH
 
@@ -120,6 +121,12 @@ class Oracle:
 
     def ftem(self, dt):
         self._chk(self.L.pdac_oracle_ftem(self.h, dt), "ftem")
+
+    def initialize_fieldn(self):
+        self._chk(self.L.pdac_oracle_initialize_fieldn(self.h), "initialize_fieldn")
+
+    def explicit_iter(self, dt):
+        self._chk(self.L.pdac_oracle_explicit_iter(self.h, dt), "explicit_iter")
 
     def step(self, sweep):
         nit = C.c_int(0)

@@ -40,7 +40,7 @@ class PdacCfg(C.Structure):
         ("job_type", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
         ("itc", C.c_int), ("nsolid", C.c_int), ("ngas", C.c_int),
         ("gas_type", C.c_int * MAX_NGAS),
-        ("dt", C.c_double), ("rungekut", C.c_int),
+        ("dt", C.c_double), ("rungekut", C.c_int), ("time_integration", C.c_int),
         ("alpha", C.c_double), ("alphagrav", C.c_double),
         ("omega", C.c_double), ("delg", C.c_double),
         ("inmax", C.c_int), ("maxout", C.c_int),
@@ -108,7 +108,9 @@ def declare(lib, prefix, handle_type):
     sigs = {
         "boundary": [h, C.c_int],
         "fieldn": [h],
+        "initialize_fieldn": [h],
         "tilde": [h, C.c_double],
+        "explicit_iter": [h, C.c_double],
         "iter": [h, C.c_double, C.POINTER(C.c_int)],
         "ygas": [h, C.c_double],
         "htilde": [h, C.c_double],

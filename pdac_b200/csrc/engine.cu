@@ -16,6 +16,7 @@
 
 #include "../../include/pdac_gpu.h"
 #include "inner.cuh"
+#include "rk3.cuh"
 
 using namespace pdac;
 
@@ -55,6 +56,14 @@ struct pdac_ctx {
     cudaEvent_t cev[9];
     cudaEvent_t user_ev[32];
     std::vector<std::pair<std::string, std::pair<double *, size_t>>> names;
+    // explicit SSP-RK3 solver (time_integration = 1): its fields and the
+    // graph of one explicit_iter, instantiated for one dt
+    int ti = 0;
+    RkF K{};
+    cudaGraph_t ex_graph = nullptr;
+    cudaGraphExec_t ex_exec = nullptr;
+    double ex_dt = 0.0;
+    long long ex_launches = 0;  // kernel launches of one explicit_iter
 };
 
 namespace {
@@ -155,6 +164,11 @@ int validate(const pdac_cfg *c, std::string &why) {
     if (!c->dx || !c->dz || !c->flag || !c->p_atm || !c->t_atm) { why = "metric, flag or atmosphere pointer is NULL"; return 1; }
     if (c->nvent > 0 && !c->vent_ijk) { why = "vent_ijk is NULL"; return 1; }
     if (c->precision != PDAC_PREC_FP64) { why = "only PDAC_PREC_FP64 is built"; return 1; }
+    if (c->time_integration != 0 && c->time_integration != 1) { why = "time_integration must be 0 or 1"; return 1; }
+    if (c->time_integration == 1 && c->pmodel != 1 && c->pmodel != 2) {
+        why = "time_integration = 1 needs pmodel 1 or 2 (explicit_solver.f:632-642)";
+        return 1;
+    }
     return 0;
 }
 
@@ -274,6 +288,11 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     // 2D-only and 3D-only slots get zero blocks on the other path, the
     // previous-visit interphase copies exist only when alpha < 1
     int d3 = ctx->d3 ? 1 : 0, d2 = 1 - d3, a0 = cfg->alpha != 1.0 ? 1 : 0;
+    ctx->ti = cfg->time_integration;
+    // the explicit solver's own fields exist only when it is selected; its
+    // right-hand-side rows: mass, momentum per axis and enthalpy of each phase
+    int t1 = ctx->ti == 1 ? 1 : 0, neq = (ctx->d3 ? 5 : 4) * ctx->nph;
+    RkF &K = ctx->K;
     std::vector<Slot> slots = {
         {"p", &F.p, 1}, {"ep", &F.ep, 1}, {"rog", &F.rog, 1}, {"rgp", &F.rgp, 1}, {"tg", &F.tg, 1},
         {"sieg", &F.sieg, 1}, {"cg", &F.cg, 1}, {"ug", &F.ug, 1}, {"vg", &F.vg, 1}, {"wg", &F.wg, 1},
@@ -288,7 +307,8 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
         {"appw", &F.appw, nap},
         {"ugfe", &F.ugfe, d2}, {"ugft", &F.ugft, d2}, {"wgfe", &F.wgfe, d2}, {"wgft", &F.wgft, d2},
         {"usfe", &F.usfe, ns * d2}, {"usft", &F.usft, ns * d2}, {"wsfe", &F.wsfe, ns * d2},
-        {"wsft", &F.wsft, ns * d2}, {"mf", &F.mf, 9 * (ns + 1) * d3}, {"vis", &F.vis, 3 * (ns + 1) * d3},
+        {"wsft", &F.wsft, ns * d2}, {"mf", &F.mf, 9 * (ns + 1) * d3},
+        {"vis", &F.vis, 3 * (ns + 1) * std::max(d3, t1)},
         {"rgfe", &F.rgfe, 1}, {"rgfn", &F.rgfn, d3}, {"rgft", &F.rgft, 1}, {"rsfe", &F.rsfe, ns},
         {"rsfn", &F.rsfn, ns * d3}, {"rsft", &F.rsft, ns},
         {"conv", &F.conv, 1}, {"abeta", &F.abeta, 1}, {"egfe", &F.egfe, 1}, {"egfn", &F.egfn, d3},
@@ -296,7 +316,11 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
         {"rhg", &F.rhg, 1}, {"rhs", &F.rhs, ns},
         {"yfe", &F.yfe, ng}, {"yfn", &F.yfn, ng * d3}, {"yft", &F.yft, ng}, {"sink", &F.sink, ns},
         {"app0u", &ctx->d_app0u, nap * a0}, {"app0v", &ctx->d_app0v, nap * a0 * d3},
-        {"app0w", &ctx->d_app0w, nap * a0}};
+        {"app0w", &ctx->d_app0w, nap * a0},
+        {"ugn", &K.ugn, t1}, {"vgn", &K.vgn, t1 * d3}, {"wgn", &K.wgn, t1}, {"usn", &K.usn, ns * t1},
+        {"vsn", &K.vsn, ns * t1 * d3}, {"wsn", &K.wsn, ns * t1}, {"hv", &K.hv, ns * t1},
+        {"k1", &K.k1, neq * t1}, {"k2", &K.k2, neq * t1}, {"xrgp", &K.xrgp, t1}, {"xrlk", &K.xrlk, ns * t1},
+        {"xep", &K.xep, t1}, {"xug", &K.xug, t1}, {"xvg", &K.xvg, t1 * d3}, {"xwg", &K.xwg, t1}};
     // each field starts on a 256-byte boundary
     size_t stride = ((size_t)n + 31) / 32 * 32;
     size_t total = 0;
@@ -335,6 +359,8 @@ int pdac_gpu_destroy(pdac_ctx *ctx) {
     cudaFree(ctx->d_dirty);
     if (ctx->it_exec) cudaGraphExecDestroy(ctx->it_exec);
     if (ctx->it_graph) cudaGraphDestroy(ctx->it_graph);
+    if (ctx->ex_exec) cudaGraphExecDestroy(ctx->ex_exec);
+    if (ctx->ex_graph) cudaGraphDestroy(ctx->ex_graph);
     cudaFree(ctx->d_nit);
     cudaFreeHost(ctx->h_nit);
     cudaFree(ctx->d_cand);
@@ -722,10 +748,10 @@ int pdac_gpu_htilde(pdac_ctx *ctx, double dt) {
     for (double *a : {F.esfe, F.esfn, F.esft})
         if (a) CK(cudaMemsetAsync(a, 0, n * ns * sizeof(double), st));
     if (ctx->d3) {
-        pdac::k_htilde_flux3d<<<blocks(n), TPB, 0, st>>>(ctx->P, F), ctx->launches++;
+        pdac::k_htilde_flux3d<true><<<blocks(n), TPB, 0, st>>>(ctx->P, F), ctx->launches++;
         pdac::k_htilde3d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt), ctx->launches++;
     } else {
-        pdac::k_htilde_flux2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F), ctx->launches++;
+        pdac::k_htilde_flux2d<true><<<blocks(n), TPB, 0, st>>>(ctx->P, F), ctx->launches++;
         pdac::k_htilde2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt), ctx->launches++;
     }
     CK(cudaGetLastError());
@@ -749,14 +775,161 @@ int pdac_gpu_ftem(pdac_ctx *ctx, double dt) {
     return PDAC_OK;
 }
 
+// ---------------------------------------------------------------------------
+// explicit SSP-RK3 solver (time_integration = 1), explicit_solver.f
+// ---------------------------------------------------------------------------
+int pdac_gpu_initialize_fieldn(pdac_ctx *ctx) {
+    if (!ctx) return PDAC_ERR_ARG;
+    if (ctx->ti != 1) return fail(ctx, PDAC_ERR_CONFIG, "initialize_fieldn: the context runs time_integration = 0");
+    cudaStream_t st = ctx->stream;
+    size_t n = ctx->ncell, ns = ctx->ns;
+    Fld &F = ctx->F;
+    CK(cudaEventRecord(ctx->ev[2], st));
+    // fluxes and stresses start from zero (explicit_solver.f:446-509)
+    for (double *a : {F.rgfe, F.rgfn, F.rgft, F.egfe, F.egfn, F.egft, F.ugfe, F.ugft, F.wgfe, F.wgft})
+        if (a) CK(cudaMemsetAsync(a, 0, n * sizeof(double), st));
+    for (double *a : {F.rsfe, F.rsfn, F.rsft, F.esfe, F.esfn, F.esft, F.usfe, F.usft, F.wsfe, F.wsft})
+        if (a) CK(cudaMemsetAsync(a, 0, n * ns * sizeof(double), st));
+    if (F.mf) CK(cudaMemsetAsync(F.mf, 0, n * 9 * (ns + 1) * sizeof(double), st));
+    CK(cudaMemsetAsync(F.vis, 0, n * 3 * (ns + 1) * sizeof(double), st));
+    if (ctx->d3) {
+        PHASE_LAUNCH_D(ctx->nph, pdac::k_rk3_fieldn, 3, blocks(n), TPB, st, ctx->P, F, ctx->K, ctx->cfg.dt);
+        pdac::k_visc3d<<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
+    } else {
+        PHASE_LAUNCH_D(ctx->nph, pdac::k_rk3_fieldn, 2, blocks(n), TPB, st, ctx->P, F, ctx->K, ctx->cfg.dt);
+        pdac::k_visc2d<<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
+    }
+    ctx->launches += 2;
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev[3], st));
+    return PDAC_OK;
+}
+
+// the kernels of one explicit_iter on stream st; returns their count
+static long long enqueue_explicit(pdac_ctx *ctx, double dt, cudaStream_t st) {
+    const Prm &P = ctx->P;
+    const Fld &F = ctx->F;
+    const RkF &K = ctx->K;
+    const long n = ctx->ncell, nphc = (long)n * (ctx->ns + 1);
+    const int nph = ctx->nph, nx = ctx->nx, ny = ctx->ny, nz = ctx->nz;
+    long long L = 0;
+    // compute_fluxes: mass, momentum and enthalpy face fluxes of the state
+    auto fluxes = [&]() {
+        if (ctx->d3) {
+            pdac::k_rk3_mflux<3><<<blocks(n), TPB, 0, st>>>(P, F);
+            pdac::k_tilde_flux3d<0><<<blocks(nphc), TPB, 0, st>>>(P, F);
+            pdac::k_tilde_flux3d<1><<<blocks(nphc), TPB, 0, st>>>(P, F);
+            pdac::k_tilde_flux3d<2><<<blocks(nphc), TPB, 0, st>>>(P, F);
+            pdac::k_htilde_flux3d<false><<<blocks(n), TPB, 0, st>>>(P, F);
+            L += 5;
+        } else {
+            pdac::k_rk3_mflux<2><<<blocks(n), TPB, 0, st>>>(P, F);
+            pdac::k_tilde_flux2d<<<blocks(n), TPB, 0, st>>>(P, F);
+            pdac::k_htilde_flux2d<false><<<blocks(n), TPB, 0, st>>>(P, F);
+            L += 3;
+        }
+    };
+    for (int stage = 1; stage <= 2; ++stage) {
+        fluxes();
+        if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_rk3_stage, 3, blocks(n), TPB, st, P, F, K, dt, stage);
+        else PHASE_LAUNCH_D(nph, pdac::k_rk3_stage, 2, blocks(n), TPB, st, P, F, K, dt, stage);
+        L++;
+        // gas-enthalpy wavefront over the hyperplanes i + j + k = d of the
+        // interior (2 <= i <= nx - 1 ...), in increasing d
+        if (ctx->d3) {
+            const int nj = ny - 2, dmax = (nx - 1) + (ny - 1) + (nz - 1);
+            for (int d = 6; d <= dmax; ++d) {
+                int kmin = std::max(2, d - (nx - 1) - (ny - 1)), kmax = std::min(nz - 1, d - 4);
+                int nt = nj * (kmax - kmin + 1);
+                pdac::k_rk3_wave<3><<<blocks(nt), TPB, 0, st>>>(P, F, K, dt, stage, d, kmin, nt);
+                L++;
+            }
+        } else {
+            const int dmax = (nx - 1) + (nz - 1);
+            for (int d = 4; d <= dmax; ++d) {
+                int kmin = std::max(2, d - (nx - 1)), kmax = std::min(nz - 1, d - 2);
+                int nt = kmax - kmin + 1;
+                pdac::k_rk3_wave<2><<<blocks(nt), TPB, 0, st>>>(P, F, K, dt, stage, d, kmin, nt);
+                L++;
+            }
+        }
+    }
+    fluxes();
+    cudaMemsetAsync(ctx->d_counters + 1, 0, sizeof(int), st);
+    if (ctx->d3) {
+        PHASE_LAUNCH_D(nph, pdac::k_rk3_final_rhs, 3, blocks(n), TPB, st, P, F, K, dt);
+        PHASE_LAUNCH_D(nph, pdac::k_rk3_final_phys, 3, blocks(n), TPB, st, P, F, K, dt);
+        PHASE_LAUNCH_D(nph, pdac::k_rk3_solve, 3, blocks(n), TPB, st, P, F, K, dt);
+    } else {
+        PHASE_LAUNCH_D(nph, pdac::k_rk3_final_rhs, 2, blocks(n), TPB, st, P, F, K, dt);
+        PHASE_LAUNCH_D(nph, pdac::k_rk3_final_phys, 2, blocks(n), TPB, st, P, F, K, dt);
+        PHASE_LAUNCH_D(nph, pdac::k_rk3_solve, 2, blocks(n), TPB, st, P, F, K, dt);
+    }
+    L += 3;
+    return L;
+}
+
+// explicit_iter as one graph for time step dt
+static int build_explicit_graph(pdac_ctx *ctx, double dt) {
+    if (ctx->ex_exec) { cudaGraphExecDestroy(ctx->ex_exec); ctx->ex_exec = nullptr; }
+    if (ctx->ex_graph) { cudaGraphDestroy(ctx->ex_graph); ctx->ex_graph = nullptr; }
+    cudaStream_t st = ctx->stream;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+    long long L = enqueue_explicit(ctx, dt, st);
+    cudaError_t e = cudaStreamEndCapture(st, &ctx->ex_graph);
+    if (e != cudaSuccess) return fail(ctx, PDAC_ERR_CUDA, std::string("explicit_iter graph capture: ") + cudaGetErrorString(e));
+    CK(cudaGetLastError());
+    CK(cudaGraphInstantiate(&ctx->ex_exec, ctx->ex_graph, 0));
+    ctx->ex_dt = dt;
+    ctx->ex_launches = L;
+    return PDAC_OK;
+}
+
+int pdac_gpu_explicit_iter(pdac_ctx *ctx, double dt) {
+    if (!ctx) return PDAC_ERR_ARG;
+    if (ctx->ti != 1) return fail(ctx, PDAC_ERR_CONFIG, "explicit_iter: the context runs time_integration = 0");
+    cudaStream_t st = ctx->stream;
+    CK(cudaEventRecord(ctx->ev[6], st));
+    if (ctx->prof) {
+        ctx->launches += enqueue_explicit(ctx, dt, st);
+        CK(cudaGetLastError());
+    } else {
+        if (!ctx->ex_exec || ctx->ex_dt != dt) {
+            int s = build_explicit_graph(ctx, dt);
+            if (s) return s;
+        }
+        CK(cudaGraphLaunch(ctx->ex_exec, st));
+        ctx->launches += ctx->ex_launches;
+    }
+    CK(cudaEventRecord(ctx->ev[7], st));
+    CK(cudaMemcpyAsync(ctx->h_counters + 1, ctx->d_counters + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    // explicit_solver.f:1214-1215 stops the run on more than one failure
+    if (ctx->h_counters[1] > 1) return fail(ctx, PDAC_ERR_EOS, "explicit_iter: caloric equation of state failed");
+    return PDAC_OK;
+}
+
 int pdac_gpu_step(pdac_ctx *ctx, int sweep, int *nit) {
     if (!ctx) return PDAC_ERR_ARG;
     int s;
     if ((s = pdac_gpu_boundary(ctx, sweep))) return s;
     if (ctx->cfg.update_eosg) return fail(ctx, PDAC_ERR_CONFIG, "update_eosg is not built");
-    if ((s = pdac_gpu_fieldn(ctx))) return s;
     double dt0 = ctx->cfg.dt;
     int status = PDAC_OK;
+    if (ctx->ti == 1) {
+        // prog.f:191-274 with time_integration = 1
+        if ((s = pdac_gpu_initialize_fieldn(ctx))) return s;
+        if (nit) *nit = 0;
+        for (int rk = 1; rk <= ctx->cfg.rungekut; ++rk) {
+            double dt = dt0 / (ctx->cfg.rungekut + 1 - rk);
+            s = pdac_gpu_explicit_iter(ctx, dt);
+            if (s == PDAC_ERR_EOS) status = s;
+            else if (s) return s;
+            if ((s = pdac_gpu_ygas(ctx, dt))) return s;
+        }
+        return status;
+    }
+    if ((s = pdac_gpu_fieldn(ctx))) return s;
     for (int rk = 1; rk <= ctx->cfg.rungekut; ++rk) {
         double dt = dt0 / (ctx->cfg.rungekut + 1 - rk);
         if ((s = pdac_gpu_tilde(ctx, dt))) return s;

@@ -728,6 +728,9 @@ __global__ void k_ygas2d(Prm P, Fld F, double dt) {
 // ---------------------------------------------------------------------------
 // htilde, htilde.f:25-575 (2D)
 // ---------------------------------------------------------------------------
+// GRAV adds the work of gravity to the convective flux (htilde); the
+// explicit solver's calc_all_fluxes (explicit_solver.f:2165-2885) has none
+template <bool GRAV>
 __global__ void k_htilde_flux2d(Prm P, Fld F) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.ncell || !fluid(P, c)) return;
@@ -775,8 +778,13 @@ __global__ void k_htilde_flux2d(Prm P, Fld F) {
             hotc_2d(P, he, ht, hwv, hbv, hw, hb, ep, te, ka, i, k);
         }
         double gx = P.gravx, gz = P.gravz;
-        fE[c] = fe - he + DE[c] * gx * uc;
-        fT[c] = ft - ht + DE[c] * gz * wc;
+        if (GRAV) {
+            fE[c] = fe - he + DE[c] * gx * uc;
+            fT[c] = ft - ht + DE[c] * gz * wc;
+        } else {
+            fE[c] = fe - he;
+            fT[c] = ft - ht;
+        }
         // W/B faces towards non-fluid cells; when the neighbour's flag is not
         // exactly 1 but still fluid (dome/immb), hotc writes hgfw yet htilde
         // does not subtract it (htilde.f:338-339) -- only non-fluid matter here.

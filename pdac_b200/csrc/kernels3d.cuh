@@ -687,6 +687,8 @@ __global__ void k_ygas3d(Prm P, Fld F, double dt) {
 // ---------------------------------------------------------------------------
 // htilde, htilde.f:25-575 (3D)
 // ---------------------------------------------------------------------------
+// GRAV as in k_htilde_flux2d
+template <bool GRAV>
 __global__ void k_htilde_flux3d(Prm P, Fld F) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.ncell || !fluid(P, c)) return;
@@ -738,9 +740,15 @@ __global__ void k_htilde_flux3d(Prm P, Fld F) {
             }
             hotc_3d(P, h, hw, hs, hb, ep, te, ka, i, j, k);
         }
-        fE[c] = f.e - h.e + DE[c] * P.gravx * uc;
-        fT[c] = f.t - h.t + DE[c] * P.gravz * wc;
-        fN[c] = f.n - h.n + DE[c] * P.gravy * vc;
+        if (GRAV) {
+            fE[c] = f.e - h.e + DE[c] * P.gravx * uc;
+            fT[c] = f.t - h.t + DE[c] * P.gravz * wc;
+            fN[c] = f.n - h.n + DE[c] * P.gravy * vc;
+        } else {
+            fE[c] = f.e - h.e;
+            fT[c] = f.t - h.t;
+            fN[c] = f.n - h.n;
+        }
         // W/S/B faces towards non-fluid cells (a non-fluid flag is never 1,
         // so hotc has produced the conductive part there)
         if (dw) fE[R.w] = f.w - h.w;

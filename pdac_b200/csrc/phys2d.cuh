@@ -458,12 +458,12 @@ __device__ __forceinline__ int caloric_eosg(const Prm &P, double &cgas, double &
     return info;
 }
 
-// drag.f:60-157 (kdrags) and 11-58 (sdrag)
-__device__ __forceinline__ double drag_coeff(const Prm &P, double du, double dv, double dw, double ep, double rgp, double rlk,
-                                             double mug, int is) {
+// drag.f:60-157 (kdrags)
+__device__ __forceinline__ double kdrags(const Prm &P, double du, double dv, double dw, double ep, double rgp, double rlk,
+                                         double mug, int is) {
     double vrel = sqrt(du * du + dv * dv + dw * dw);
     double drag;
-    if (P.drag_model == 1) {
+    {
         if (ep < 0.8) {
             double denom = 1.0 / (P.dk[is] * P.phis[is] * ep);
             drag = 150.0 * ep * rlk * P.inrl[is] * mug * denom + 1.75 * rgp * vrel;
@@ -478,7 +478,16 @@ __device__ __forceinline__ double drag_coeff(const Prm &P, double du, double dv,
             drag = 0.75 * dc * eps / (P.dk[is] * P.phis[is]) * rgp * vrel;
             drag = drag * pow(ep, (double)(-2.65f));
         }
-    } else {
+    }
+    return drag;
+}
+
+// drag.f:11-58 (sdrag)
+__device__ __forceinline__ double sdrag(const Prm &P, double du, double dv, double dw, double ep, double rgp, double rlk,
+                                        double mug, int is) {
+    double vrel = sqrt(du * du + dv * dv + dw * dw);
+    double drag;
+    {
         double eps = rlk * P.inrl[is];
         double reynum = rgp * P.dk[is] * P.phis[is] * vrel / mug;
         double a = pow(ep, (double)4.14f), b;
@@ -493,6 +502,12 @@ __device__ __forceinline__ double drag_coeff(const Prm &P, double du, double dv,
         drag = drag / vr;
     }
     return drag;
+}
+
+// the drag law the run selects (tilde.f:617-623)
+__device__ __forceinline__ double drag_coeff(const Prm &P, double du, double dv, double dw, double ep, double rgp, double rlk,
+                                             double mug, int is) {
+    return P.drag_model == 1 ? kdrags(P, du, dv, dw, ep, rgp, rlk, mug, is) : sdrag(P, du, dv, dw, ep, rgp, rlk, mug, is);
 }
 
 // drag.f:248-298

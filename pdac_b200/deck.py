@@ -351,8 +351,12 @@ class Deck:
             bad.append("ctu>0 (corner transport upwind)")
         if self["implicit_fluxes"] or self["implicit_enthalpy"]:
             bad.append("implicit_fluxes/implicit_enthalpy")
-        if self["time_integration"] != 0:
-            bad.append("time_integration=1 (RK3 explicit solver)")
+        if self["time_integration"] not in (0, 1):
+            bad.append("time_integration other than 0 or 1")
+        elif self["time_integration"] == 1 and self["pmodel"] not in (1, 2):
+            # compute_rhs (explicit_solver.f:632-642) defines the face volume
+            # fractions only for pmodel 1 and 2
+            bad.append("time_integration=1 with pmodel other than 1 or 2")
         if self["irex"] > 1:
             bad.append("irex>1 (reactions)")
         if self["immb"] != 0 or self["itp"] != 0:

@@ -398,6 +398,7 @@ class Case:
             c.gas_type[ig] = gt
         c.dt = d["dt"]
         c.rungekut = d["rungekut"]
+        c.time_integration = d["time_integration"]
         c.alpha, c.alphagrav = d["alpha"], d["alphagrav"]
         c.omega, c.delg = d["omega"], d["delg"]
         c.inmax, c.maxout = d["inmax"], d["maxout"]
