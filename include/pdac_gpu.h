@@ -206,7 +206,11 @@ int pdac_gpu_phase_times(pdac_ctx *ctx, double *ms7);
  * the residual-test and inner-loop kernels of those phases and out[6] the
  * number of unconverged cells they processed, with nout >= 8 also out[7]
  * the number of cells the residual tests evaluated (all counted only when
- * the reset enabled profiling); nout >= 4                                 */
+ * the reset enabled profiling); with nout >= 13 also the device ms of the
+ * explicit solver's kernel groups over the profiled explicit_iter calls,
+ * out[8] flux passes, out[9] stage kernels, out[10] gas-enthalpy
+ * wavefronts, out[11] final solve, and out[12] the number of those calls;
+ * nout >= 4                                                               */
 int pdac_gpu_stats(pdac_ctx *ctx, double *out, int nout);
 int pdac_gpu_reset_stats(pdac_ctx *ctx, int profile_corrector);
 /* per colour phase of the corrector since the last profiling reset, six

@@ -64,6 +64,12 @@ struct pdac_ctx {
     cudaGraphExec_t ex_exec = nullptr;
     double ex_dt = 0.0;
     long long ex_launches = 0;  // kernel launches of one explicit_iter
+    // profiling of explicit_iter: marks between its kernel groups and the
+    // accumulated device ms of the groups [flux passes, stage kernels,
+    // gas-enthalpy wavefronts, final rhs + coefficients + solve]
+    cudaEvent_t xev[9];
+    double ex_ms[4] = {0, 0, 0, 0};
+    long long ex_calls = 0;
 };
 
 namespace {
@@ -237,6 +243,7 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     for (auto &e : ctx->ev) CK(cudaEventCreate(&e));
     for (auto &e : ctx->cev) CK(cudaEventCreate(&e));
     for (auto &e : ctx->user_ev) CK(cudaEventCreate(&e));
+    for (auto &e : ctx->xev) CK(cudaEventCreate(&e));
     std::vector<std::vector<double> *> mets = {&dx, &dy, &dz, &indx, &indy, &indz, &r, &rb, &inr, &inrb, &patm, &tatm};
     size_t mtot = 0;
     for (auto *v : mets) mtot += v->size();
@@ -369,6 +376,7 @@ int pdac_gpu_destroy(pdac_ctx *ctx) {
     for (auto &e : ctx->ev) cudaEventDestroy(e);
     for (auto &e : ctx->cev) cudaEventDestroy(e);
     for (auto &e : ctx->user_ev) cudaEventDestroy(e);
+    for (auto &e : ctx->xev) cudaEventDestroy(e);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return PDAC_OK;
@@ -805,8 +813,12 @@ int pdac_gpu_initialize_fieldn(pdac_ctx *ctx) {
     return PDAC_OK;
 }
 
-// the kernels of one explicit_iter on stream st; returns their count
-static long long enqueue_explicit(pdac_ctx *ctx, double dt, cudaStream_t st) {
+// the kernels of one explicit_iter on stream st; returns their count.  With
+// prof, events xev[0..8] mark the group boundaries: flux pass, stage 1,
+// wavefront 1, flux pass, stage 2, wavefront 2, flux pass, final kernels
+static long long enqueue_explicit(pdac_ctx *ctx, double dt, cudaStream_t st, bool prof) {
+    int q = 0;
+    auto mark = [&]() { if (prof) cudaEventRecord(ctx->xev[q++], st); };
     const Prm &P = ctx->P;
     const Fld &F = ctx->F;
     const RkF &K = ctx->K;
@@ -830,10 +842,13 @@ static long long enqueue_explicit(pdac_ctx *ctx, double dt, cudaStream_t st) {
         }
     };
     for (int stage = 1; stage <= 2; ++stage) {
+        mark();
         fluxes();
+        mark();
         if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_rk3_stage, 3, blocks(n), TPB, st, P, F, K, dt, stage);
         else PHASE_LAUNCH_D(nph, pdac::k_rk3_stage, 2, blocks(n), TPB, st, P, F, K, dt, stage);
         L++;
+        mark();
         // gas-enthalpy wavefront over the hyperplanes i + j + k = d of the
         // interior (2 <= i <= nx - 1 ...), in increasing d
         if (ctx->d3) {
@@ -854,7 +869,9 @@ static long long enqueue_explicit(pdac_ctx *ctx, double dt, cudaStream_t st) {
             }
         }
     }
+    mark();
     fluxes();
+    mark();
     cudaMemsetAsync(ctx->d_counters + 1, 0, sizeof(int), st);
     if (ctx->d3) {
         PHASE_LAUNCH_D(nph, pdac::k_rk3_final_rhs, 3, blocks(n), TPB, st, P, F, K, dt);
@@ -866,6 +883,7 @@ static long long enqueue_explicit(pdac_ctx *ctx, double dt, cudaStream_t st) {
         PHASE_LAUNCH_D(nph, pdac::k_rk3_solve, 2, blocks(n), TPB, st, P, F, K, dt);
     }
     L += 3;
+    mark();
     return L;
 }
 
@@ -875,7 +893,7 @@ static int build_explicit_graph(pdac_ctx *ctx, double dt) {
     if (ctx->ex_graph) { cudaGraphDestroy(ctx->ex_graph); ctx->ex_graph = nullptr; }
     cudaStream_t st = ctx->stream;
     CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
-    long long L = enqueue_explicit(ctx, dt, st);
+    long long L = enqueue_explicit(ctx, dt, st, false);
     cudaError_t e = cudaStreamEndCapture(st, &ctx->ex_graph);
     if (e != cudaSuccess) return fail(ctx, PDAC_ERR_CUDA, std::string("explicit_iter graph capture: ") + cudaGetErrorString(e));
     CK(cudaGetLastError());
@@ -891,7 +909,7 @@ int pdac_gpu_explicit_iter(pdac_ctx *ctx, double dt) {
     cudaStream_t st = ctx->stream;
     CK(cudaEventRecord(ctx->ev[6], st));
     if (ctx->prof) {
-        ctx->launches += enqueue_explicit(ctx, dt, st);
+        ctx->launches += enqueue_explicit(ctx, dt, st, true);
         CK(cudaGetLastError());
     } else {
         if (!ctx->ex_exec || ctx->ex_dt != dt) {
@@ -904,6 +922,15 @@ int pdac_gpu_explicit_iter(pdac_ctx *ctx, double dt) {
     CK(cudaEventRecord(ctx->ev[7], st));
     CK(cudaMemcpyAsync(ctx->h_counters + 1, ctx->d_counters + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    if (ctx->prof) {
+        float t[8];
+        for (int q = 0; q < 8; ++q) CK(cudaEventElapsedTime(&t[q], ctx->xev[q], ctx->xev[q + 1]));
+        ctx->ex_ms[0] += t[0] + t[3] + t[6];
+        ctx->ex_ms[1] += t[1] + t[4];
+        ctx->ex_ms[2] += t[2] + t[5];
+        ctx->ex_ms[3] += t[7];
+        ctx->ex_calls++;
+    }
     // explicit_solver.f:1214-1215 stops the run on more than one failure
     if (ctx->h_counters[1] > 1) return fail(ctx, PDAC_ERR_EOS, "explicit_iter: caloric equation of state failed");
     return PDAC_OK;
@@ -1012,6 +1039,10 @@ int pdac_gpu_stats(pdac_ctx *ctx, double *out, int nout) {
         out[6] = (double)ctx->work_cells;
     }
     if (nout >= 8) out[7] = (double)ctx->tested_cells;
+    if (nout >= 13) {
+        for (int q = 0; q < 4; ++q) out[8 + q] = ctx->ex_ms[q];
+        out[12] = (double)ctx->ex_calls;
+    }
     return PDAC_OK;
 }
 
@@ -1019,6 +1050,8 @@ int pdac_gpu_reset_stats(pdac_ctx *ctx, int profile_corrector) {
     if (!ctx) return PDAC_ERR_ARG;
     ctx->launches = ctx->sweeps = ctx->corr_launches = ctx->work_cells = ctx->tested_cells = 0;
     ctx->corr_ms = ctx->resid_ms = ctx->inner_ms = 0.0;
+    for (double &x : ctx->ex_ms) x = 0.0;
+    ctx->ex_calls = 0;
     ctx->sweep_log.clear();
     ctx->prof = profile_corrector != 0;
     return PDAC_OK;

@@ -172,10 +172,12 @@ class Engine:
         return out
 
     def stats(self):
-        out = (C.c_double * 8)()
-        self._chk(self.L.pdac_gpu_stats(self.h, out, 8), "stats")
+        out = (C.c_double * 13)()
+        self._chk(self.L.pdac_gpu_stats(self.h, out, 13), "stats")
         return dict(launches=int(out[0]), sweeps=int(out[1]), corr_launches=int(out[2]), corr_ms=out[3],
-                    resid_ms=out[4], inner_ms=out[5], work_cells=int(out[6]), tested_cells=int(out[7]))
+                    resid_ms=out[4], inner_ms=out[5], work_cells=int(out[6]), tested_cells=int(out[7]),
+                    rk3_ms={"flux": out[8], "stage": out[9], "wave": out[10], "final": out[11]},
+                    rk3_calls=int(out[12]))
 
     def sweep_log(self):
         """Per colour phase since the last profiling reset: array of rows

@@ -93,3 +93,20 @@ def test_unsupported_options_are_rejected():
     d.set("model", iturb=1)
     with pytest.raises(ValueError, match="iturb"):
         Case(d)
+
+
+def test_explicit_solver_selection():
+    """time_integration = 1 selects the explicit SSP-RK3 solver; it needs
+    pmodel 1 or 2 (compute_rhs, explicit_solver.f:632-642) and reaches the
+    C configuration struct."""
+    d = configs.plume_2d_rk3()
+    case = Case(d)
+    assert case.cfg().time_integration == 1
+    d.set("model", pmodel=0)
+    with pytest.raises(ValueError, match="pmodel"):
+        Case(d)
+    d = configs.plume_2d()
+    d.set("numeric", time_integration=2)
+    with pytest.raises(ValueError, match="time_integration"):
+        Case(d)
+    assert Case(configs.plume_2d()).cfg().time_integration == 0

@@ -15,13 +15,15 @@ GOLDEN = json.load(open(os.path.join(HERE, "golden", "oracle_small.json")))
 TOL = 1e-9
 
 
-@pytest.mark.parametrize("deck", ["small_2d", "small_3d"])
+@pytest.mark.parametrize("deck", ["small_2d", "small_3d", "small_2d_rk3", "small_3d_rk3"])
 def test_engine_matches_colored_fixture(deck):
+    """The explicit-solver decks (no corrector, no sweep order) have one
+    fixture, stored under the lexicographic key."""
     from pdac_b200 import configs
     from pdac_b200.engine import Engine
     from pdac_b200.setup_state import Case
     from golden.make_golden import summarize
-    ref = GOLDEN[f"{deck}/colored"]
+    ref = GOLDEN.get(f"{deck}/colored") or GOLDEN[f"{deck}/lexicographic"]
     case = Case(getattr(configs, deck)())
     eng = Engine(case)
     cells = ref["probe_cells"]
