@@ -185,6 +185,35 @@ int pdac_gpu_explicit_iter(pdac_ctx *ctx, double dt);
  * explicit_iter/ygas (time_integration = 1, *nit = 0)                      */
 int pdac_gpu_step(pdac_ctx *ctx, int sweep, int *nit);
 
+/* ---- files of the time loop, in the reference's formats -------------- */
+/* tapewr (io_restart.f:31-124): the restart file (pdac.res) as Fortran
+ * unformatted sequential records, 4-byte little-endian length markers:
+ * (time, nx, ny, nz, nsolid, ngas, nfil), gas_type(ngas), then one REAL*8
+ * record of ncell values each for p, ug, [vg], wg, sieg, rlk per class, per
+ * class us, [vs], ws, sies per class, ygc per gas, rgp, rog, tg, ts per
+ * class ([] = 3D only).                                                    */
+int pdac_gpu_write_restart(pdac_ctx *ctx, const char *path, double time, int nfil);
+/* taperd (io_restart.f:126-339) + the restart branch of cnvert
+ * (setup.f:359-391): reads such a file into the context (the file's gas
+ * types replace the run's, as in the reference), derives xgc, ep and cg,
+ * and returns its time and output counter; PDAC_ERR_ARG with the reason in
+ * pdac_gpu_last_error on a missing file, bad framing or a dimension that
+ * differs from the context's.                                              */
+int pdac_gpu_read_restart(pdac_ctx *ctx, const char *path, double *time, int *nfil);
+/* outp (outp.f:194-384), unformatted form: REAL(time, 4), then REAL*4
+ * records of p, ug, [vg], wg, tg, xgc per gas, and per class rlk / rl, us,
+ * [vs], ws, ts.  The caller names the file output.NNNN (lettera, letter.f). */
+int pdac_gpu_write_output(pdac_ctx *ctx, const char *path, double time);
+/* print_mass_residuals (residuals.f:15-136): out = [res_g, res_s(nsolid),
+ * res_gc(ngas), mfr], masses in the fluid cells minus the mass that entered
+ * through inlet and vent cells in nswp steps of dt, and the vent mass flow
+ * rate (compute_mass_flow_rate, residuals.f:171-251); nout >= 2 + nsolid +
+ * ngas                                                                     */
+int pdac_gpu_mass_residuals(pdac_ctx *ctx, int nswp, double dt, double *out, int nout);
+/* the same values appended to path as one pdac.chm line,
+ * FORMAT(I8,15(G30.20E3)) (residuals.f:123-127)                           */
+int pdac_gpu_append_mass_check(pdac_ctx *ctx, const char *path, int nswp, double dt);
+
 /* vent fluctuation factors for the next boundary call, one per vent cell in
  * cfg->vent_ijk order (vent.f:824-873 random_switch draws them in 3D).     */
 int pdac_gpu_set_vent_factors(pdac_ctx *ctx, const double *fact, int nvent);

@@ -119,6 +119,14 @@ def declare(lib, prefix, handle_type):
         "get_array": [h, C.c_char_p, _dp, C.POINTER(C.c_long)],
         "mass_totals": [h, _dp, C.c_int],
     }
+    if prefix == "pdac_gpu":
+        sigs.update({
+            "write_restart": [h, C.c_char_p, C.c_double, C.c_int],
+            "read_restart": [h, C.c_char_p, _dp, C.POINTER(C.c_int)],
+            "write_output": [h, C.c_char_p, C.c_double],
+            "mass_residuals": [h, C.c_int, C.c_double, _dp, C.c_int],
+            "append_mass_check": [h, C.c_char_p, C.c_int, C.c_double],
+        })
     for name, args in sigs.items():
         fn = getattr(lib, f"{prefix}_{name}")
         fn.argtypes = args

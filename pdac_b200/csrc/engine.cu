@@ -17,6 +17,7 @@
 #include "../../include/pdac_gpu.h"
 #include "inner.cuh"
 #include "rk3.cuh"
+#include "io.cuh"
 
 using namespace pdac;
 
@@ -1013,6 +1014,203 @@ int pdac_gpu_phase_times(pdac_ctx *ctx, double *ms7) {
         ms7[q] = t;
     }
     cudaGetLastError();
+    return PDAC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// files of the time loop: pdac.res, output.NNNN, pdac.chm
+// ---------------------------------------------------------------------------
+// the state arrays of tapewr / taperd in file order (io_restart.f:52-118)
+static std::vector<std::pair<double *, const char *>> restart_arrays(pdac_ctx *ctx) {
+    Fld &F = ctx->F;
+    const size_t n = ctx->ncell;
+    std::vector<std::pair<double *, const char *>> a;
+    a.push_back({F.p, "p"});
+    a.push_back({F.ug, "ug"});
+    if (ctx->d3) a.push_back({F.vg, "vg"});
+    a.push_back({F.wg, "wg"});
+    a.push_back({F.sieg, "sieg"});
+    for (int is = 0; is < ctx->ns; ++is) a.push_back({F.rlk + is * n, "rlk"});
+    for (int is = 0; is < ctx->ns; ++is) {
+        a.push_back({F.us + is * n, "us"});
+        if (ctx->d3) a.push_back({F.vs + is * n, "vs"});
+        a.push_back({F.ws + is * n, "ws"});
+    }
+    for (int is = 0; is < ctx->ns; ++is) a.push_back({F.sies + is * n, "sies"});
+    for (int ig = 0; ig < ctx->ng; ++ig) a.push_back({F.ygc + ig * n, "ygc"});
+    a.push_back({F.rgp, "rgp"});
+    a.push_back({F.rog, "rog"});
+    a.push_back({F.tg, "tg"});
+    for (int is = 0; is < ctx->ns; ++is) a.push_back({F.ts + is * n, "ts"});
+    return a;
+}
+
+// tapewr (io_restart.f:31-124): header (time, nx, ny, nz, nsolid, ngas,
+// nfil), gas_type, then one REAL*8 record per array
+int pdac_gpu_write_restart(pdac_ctx *ctx, const char *path, double time, int nfil) {
+    if (!ctx || !path) return PDAC_ERR_ARG;
+    const size_t n = ctx->ncell;
+    pdac::io::Writer w(path);
+    if (!w.ok) return fail(ctx, PDAC_ERR_ARG, std::string("write_restart: cannot open ") + path);
+    unsigned char head[32];
+    int32_t dims[6] = {ctx->nx, ctx->ny, ctx->nz, ctx->ns, ctx->ng, nfil};
+    std::memcpy(head, &time, 8);
+    std::memcpy(head + 8, dims, 24);
+    w.record(head, 32);
+    std::vector<int32_t> gt(ctx->cfg.gas_type, ctx->cfg.gas_type + ctx->ng);
+    w.record(gt.data(), gt.size() * 4);
+    std::vector<double> buf(n);
+    for (auto &a : restart_arrays(ctx)) {
+        CK(cudaMemcpyAsync(buf.data(), a.first, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        w.record(buf.data(), n * sizeof(double));
+    }
+    if (!w.close()) return fail(ctx, PDAC_ERR_ARG, std::string("write_restart: write error on ") + path);
+    return PDAC_OK;
+}
+
+// taperd (io_restart.f:126-339) followed by cnvert's restart branch
+// (setup.f:359-391): the file's gas types replace the run's; xgc, ep and cg
+// are derived from the arrays read
+int pdac_gpu_read_restart(pdac_ctx *ctx, const char *path, double *time, int *nfil) {
+    if (!ctx || !path) return PDAC_ERR_ARG;
+    const size_t n = ctx->ncell;
+    pdac::io::Reader r(path);
+    if (!r.f) return fail(ctx, PDAC_ERR_ARG, "read_restart: " + r.err);
+    unsigned char head[32];
+    if (!r.record(head, 32, "the header")) return fail(ctx, PDAC_ERR_ARG, "read_restart: " + r.err);
+    double t;
+    int32_t dims[6];
+    std::memcpy(&t, head, 8);
+    std::memcpy(dims, head + 8, 24);
+    const char *dn[5] = {"nx", "ny", "nz", "nsolid", "ngas"};
+    int want[5] = {ctx->nx, ctx->ny, ctx->nz, ctx->ns, ctx->ng};
+    for (int q = 0; q < 5; ++q)
+        if (dims[q] != want[q])
+            return fail(ctx, PDAC_ERR_ARG, std::string("read_restart: inconsistent dimension ") + dn[q] + " (file " +
+                                               std::to_string(dims[q]) + ", run " + std::to_string(want[q]) + ")");
+    std::vector<int32_t> gt(ctx->ng);
+    if (!r.record(gt.data(), gt.size() * 4, "gas_type")) return fail(ctx, PDAC_ERR_ARG, "read_restart: " + r.err);
+    for (int ig = 0; ig < ctx->ng; ++ig)
+        if (gt[ig] < 1 || gt[ig] > 7) return fail(ctx, PDAC_ERR_ARG, "read_restart: gas_type out of range");
+    bool regas = false;
+    for (int ig = 0; ig < ctx->ng; ++ig) regas |= gt[ig] != ctx->cfg.gas_type[ig];
+    if (regas) {
+        // kernels and captured graphs carry the gas table by value
+        for (int ig = 0; ig < ctx->ng; ++ig) ctx->cfg.gas_type[ig] = ctx->P.gas_type[ig] = gt[ig];
+        if (ctx->it_exec) { cudaGraphExecDestroy(ctx->it_exec); ctx->it_exec = nullptr; }
+        if (ctx->it_graph) { cudaGraphDestroy(ctx->it_graph); ctx->it_graph = nullptr; }
+        if (ctx->ex_exec) { cudaGraphExecDestroy(ctx->ex_exec); ctx->ex_exec = nullptr; }
+        if (ctx->ex_graph) { cudaGraphDestroy(ctx->ex_graph); ctx->ex_graph = nullptr; }
+    }
+    std::vector<double> buf(n);
+    for (auto &a : restart_arrays(ctx)) {
+        if (!r.record(buf.data(), n * sizeof(double), a.second)) return fail(ctx, PDAC_ERR_ARG, "read_restart: " + r.err);
+        bool neg = false;
+        for (size_t c = 0; c < n && !neg; ++c) neg = buf[c] < 0.0;
+        const char *ch = a.second;
+        if (neg && std::strcmp(ch, "ug") && std::strcmp(ch, "vg") && std::strcmp(ch, "wg") && std::strcmp(ch, "us") &&
+            std::strcmp(ch, "vs") && std::strcmp(ch, "ws"))
+            fprintf(stderr, "WARNING reading restart, %s < 0\n", ch);
+        CK(cudaMemcpyAsync(a.first, buf.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    pdac::k_restart_derive<<<blocks(n), TPB, 0, ctx->stream>>>(ctx->P, ctx->F);
+    ctx->launches++;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (time) *time = t;
+    if (nfil) *nfil = dims[5];
+    return PDAC_OK;
+}
+
+// outp (outp.f:194-384), unformatted: REAL(time, 4), then single-precision
+// records of p, gas velocity, tg, xgc per gas, and per class eps = rlk/rl,
+// particle velocity and ts
+int pdac_gpu_write_output(pdac_ctx *ctx, const char *path, double time) {
+    if (!ctx || !path) return PDAC_ERR_ARG;
+    const size_t n = ctx->ncell;
+    Fld &F = ctx->F;
+    pdac::io::Writer w(path);
+    if (!w.ok) return fail(ctx, PDAC_ERR_ARG, std::string("write_output: cannot open ") + path);
+    float t4 = (float)time;
+    w.record(&t4, 4);
+    std::vector<double> buf(n);
+    std::vector<float> sgl(n);
+    auto put = [&](const double *d, double scale, bool scaled) -> int {
+        CK(cudaMemcpyAsync(buf.data(), d, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        for (size_t c = 0; c < n; ++c) sgl[c] = (float)(scaled ? buf[c] * scale : buf[c]);
+        w.record(sgl.data(), n * sizeof(float));
+        return PDAC_OK;
+    };
+    int s;
+    if ((s = put(F.p, 1.0, false))) return s;
+    if ((s = put(F.ug, 1.0, false))) return s;
+    if (ctx->d3 && (s = put(F.vg, 1.0, false))) return s;
+    if ((s = put(F.wg, 1.0, false))) return s;
+    if ((s = put(F.tg, 1.0, false))) return s;
+    for (int ig = 0; ig < ctx->ng; ++ig)
+        if ((s = put(F.xgc + ig * n, 1.0, false))) return s;
+    for (int is = 1; is <= ctx->ns; ++is) {
+        size_t off = (size_t)(is - 1) * n;
+        if ((s = put(F.rlk + off, ctx->P.inrl[is], true))) return s;
+        if ((s = put(F.us + off, 1.0, false))) return s;
+        if (ctx->d3 && (s = put(F.vs + off, 1.0, false))) return s;
+        if ((s = put(F.ws + off, 1.0, false))) return s;
+        if ((s = put(F.ts + off, 1.0, false))) return s;
+    }
+    if (!w.close()) return fail(ctx, PDAC_ERR_ARG, std::string("write_output: write error on ") + path);
+    return PDAC_OK;
+}
+
+// print_mass_residuals (residuals.f:15-136) and the mass flow rate of
+// compute_mass_flow_rate (residuals.f:171-251): out = [res_g, res_s(ns),
+// res_gc(ng), mfr]
+int pdac_gpu_mass_residuals(pdac_ctx *ctx, int nswp, double dt, double *out, int nout) {
+    if (!ctx || !out) return PDAC_ERR_ARG;
+    const int ns = ctx->ns, ng = ctx->ng, nres = 2 + ns + ng, nq = 4 + 2 * ns + ng;
+    if (nout < nres) return PDAC_ERR_ARG;
+    // the partial sums fit the reduction buffer of mass_totals, which holds
+    // (1 + ns + ng) x 1024 doubles
+    const int nb = 148, tpb = 128;
+    double *part = ctx->d_partial;
+    pdac::k_mass_resid<<<nb, tpb, (size_t)nq * tpb * sizeof(double), ctx->stream>>>(ctx->P, ctx->F, nswp, dt, part, nq);
+    ctx->launches++;
+    CK(cudaGetLastError());
+    std::vector<double> h((size_t)nq * nb);
+    CK(cudaMemcpyAsync(h.data(), part, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    std::vector<double> tot(nq, 0.0);
+    for (int q = 0; q < nq; ++q)
+        for (int b = 0; b < nb; ++b) tot[q] += h[(size_t)q * nb + b];
+    for (int q = 0; q < 1 + ns + ng; ++q) out[q] = tot[q];
+    out[1 + ns + ng] = tot[1 + ns + ng];  // mfr
+    return PDAC_OK;
+}
+
+// one line of pdac.chm, FORMAT(I8,15(G30.20E3)) (residuals.f:123-127),
+// appended to path
+int pdac_gpu_append_mass_check(pdac_ctx *ctx, const char *path, int nswp, double dt) {
+    if (!ctx || !path) return PDAC_ERR_ARG;
+    const int nres = 2 + ctx->ns + ctx->ng;
+    std::vector<double> v(nres);
+    int s = pdac_gpu_mass_residuals(ctx, nswp, dt, v.data(), nres);
+    if (s) return s;
+    char head[32];
+    std::snprintf(head, sizeof head, "%8d", nswp);
+    std::string line = head;
+    for (int q = 0; q < nres; ++q) {
+        // format reversion: after 15 items the line ends and the group repeats
+        if (q > 0 && q % 15 == 0) line += "\n";
+        line += pdac::io::fortran_g(v[q], 30, 20, 3);
+    }
+    line += "\n";
+    FILE *f = std::fopen(path, "a");
+    if (!f) return fail(ctx, PDAC_ERR_ARG, std::string("append_mass_check: cannot open ") + path);
+    bool ok = std::fputs(line.c_str(), f) >= 0;
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) return fail(ctx, PDAC_ERR_ARG, std::string("append_mass_check: write error on ") + path);
     return PDAC_OK;
 }
 

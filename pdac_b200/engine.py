@@ -69,6 +69,8 @@ EXPORTED = (
     "pdac_gpu_ygas", "pdac_gpu_htilde", "pdac_gpu_ftem", "pdac_gpu_step", "pdac_gpu_set_vent_factors",
     "pdac_gpu_get_array", "pdac_gpu_mass_totals", "pdac_gpu_phase_times", "pdac_gpu_stats",
     "pdac_gpu_reset_stats", "pdac_gpu_mark", "pdac_gpu_elapsed",
+    "pdac_gpu_write_restart", "pdac_gpu_read_restart", "pdac_gpu_write_output", "pdac_gpu_mass_residuals",
+    "pdac_gpu_append_mass_check",
 )
 
 
@@ -160,6 +162,36 @@ class Engine:
         nit = C.c_int(0)
         self._chk(self.L.pdac_gpu_step(self.h, sweep, C.byref(nit)), "step")
         return nit.value
+
+    # ---- files of the time loop (pdac.res, output.NNNN, pdac.chm) --------
+    def write_restart(self, path, time, nfil):
+        """tapewr: the restart file in the reference's record layout."""
+        self._chk(self.L.pdac_gpu_write_restart(self.h, os.fsencode(path), float(time), int(nfil)), "write_restart")
+
+    def read_restart(self, path):
+        """taperd + cnvert: load a restart file; returns (time, nfil)."""
+        t = C.c_double(0)
+        nf = C.c_int(0)
+        self._chk(self.L.pdac_gpu_read_restart(self.h, os.fsencode(path), C.byref(t), C.byref(nf)), "read_restart")
+        return t.value, nf.value
+
+    def write_output(self, path, time):
+        """outp (unformatted form) into path, e.g. output_name(nfil)."""
+        self._chk(self.L.pdac_gpu_write_output(self.h, os.fsencode(path), float(time)), "write_output")
+
+    def mass_residuals(self, nswp, dt=None):
+        """print_mass_residuals values: dict res_g, res_s, res_gc, mfr."""
+        n = 2 + self.case.nsolid + self.case.ngas
+        out = np.zeros(n)
+        dt = self.case.deck["dt"] if dt is None else dt
+        self._chk(self.L.pdac_gpu_mass_residuals(self.h, int(nswp), float(dt), abi.dptr(out), n), "mass_residuals")
+        ns = self.case.nsolid
+        return dict(res_g=out[0], res_s=out[1:1 + ns], res_gc=out[1 + ns:-1], mfr=out[-1])
+
+    def append_mass_check(self, path, nswp, dt=None):
+        """Append the pdac.chm line of step nswp to path."""
+        dt = self.case.deck["dt"] if dt is None else dt
+        self._chk(self.L.pdac_gpu_append_mass_check(self.h, os.fsencode(path), int(nswp), float(dt)), "append_mass_check")
 
     def set_vent_factors(self, fact):
         fact = np.ascontiguousarray(fact, dtype=np.float64)

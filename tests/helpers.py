@@ -60,3 +60,47 @@ def frame_agreement(got, ref, names, ncell, fluid, tol=1e-9):
         tot += d.size
         ok += int(np.count_nonzero(d <= tol))
     return ok / max(tot, 1)
+
+
+def fortran_records(path):
+    """The records of a Fortran unformatted sequential file, as bytes:
+    4-byte little-endian length markers around each record; a negative
+    leading marker continues the record in the next subrecord."""
+    import struct
+    data = open(path, "rb").read()
+    out, pos, cur = [], 0, b""
+    while pos < len(data):
+        (m1,) = struct.unpack_from("<i", data, pos)
+        n = abs(m1)
+        body = data[pos + 4:pos + 4 + n]
+        (m2,) = struct.unpack_from("<i", data, pos + 4 + n)
+        assert abs(m2) == n, "record framing"
+        pos += 8 + n
+        cur += body
+        if m1 >= 0:
+            out.append(cur)
+            cur = b""
+    assert cur == b"", "unterminated record"
+    return out
+
+
+def fortran_g(x, w=30, d=20, e=3):
+    """Fortran Gw.dEe output of one value (F2008 10.7.5.2.2), written out
+    with Python's decimal rounding of the exact binary value."""
+    from decimal import Decimal, ROUND_HALF_EVEN
+    n = e + 2
+    if x == 0.0:
+        return f"{x:{w - n}.{d - 1}f}" + " " * n
+    dec = Decimal(x)
+    ex = dec.adjusted()  # exponent of the leading digit before rounding
+    q = dec.scaleb(-ex).quantize(Decimal(1).scaleb(-(d - 1)), rounding=ROUND_HALF_EVEN)
+    if abs(q) >= 10:
+        ex += 1
+    s = ex + 1
+    if 0 <= s <= d:
+        return f"{x:{w - n}.{d - s}f}" + " " * n
+    digits = format(abs(dec).scaleb(-ex).quantize(Decimal(1).scaleb(-(d - 1)), rounding=ROUND_HALF_EVEN), "f").replace(".", "")[:d]
+    if abs(q) >= 10:
+        digits = "1" + "0" * (d - 1)
+    body = ("-" if x < 0 else "") + "0." + digits + "E" + ("-" if s < 0 else "+") + f"{abs(s):0{e}d}"
+    return f"{body:>{w}}"
