@@ -79,6 +79,11 @@ typedef struct pdac_cfg {
     int    pmodel, drag_model, icpc;
     double tref;
     int    gas_viscosity, part_viscosity, repulsive_model;
+    int    iturb;               /* 0 none, 1 Smagorinsky sub-grid model      */
+    int    modturbo;            /* 1 static Smagorinsky (2 dynamic: 2D falls
+                                   back to 1, turbo.f:173-177)               */
+    int    iss;                 /* 1 particle sub-grid stress (turbo.f:437)  */
+    double cmut;                /* Smagorinsky constant                      */
     double gravx, gravy, gravz;
 
     /* &particles */
@@ -166,6 +171,12 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit);
  *    not allowed.                                                          */
 #define PDAC_ITER_STATIC_SCRATCH_BYTES (8 * 1024 * 1024)
 int pdac_gpu_iter_static(pdac_ctx *ctx, double dt, int *nit);
+/* sub-grid turbulence model (cfg iturb = 1, iss = 1), called after fieldn
+ * or initialize_fieldn as prog.f:207-208 does: sgsg (turbo.f:145-349) sets
+ * the turbulent viscosity and conductivity from the strain rate, sgss
+ * (turbo.f:437-475) the particle sub-grid viscosity; no-ops without them  */
+int pdac_gpu_sgsg(pdac_ctx *ctx);
+int pdac_gpu_sgss(pdac_ctx *ctx);
 /* ygas (ygas.f:27-156)                                                    */
 int pdac_gpu_ygas(pdac_ctx *ctx, double dt);
 /* htilde (htilde.f:25-178)                                                */

@@ -118,6 +118,7 @@ struct Oracle {
     vector<double> egfe, egft, esfe, esft, hgfe, hgft, hsfe, hsft, yfe, yft;
     vector<double> sink;
     vector<double> mf3, ef3, yfn;   // 3D momentum / enthalpy face fluxes, species y-fluxes
+    vector<double> smag, mugt, kapgt, must;  // sub-grid model (turbo.f:10-14)
     vector<double> dgres;   // |dg|/conv at the last corrector visit (diagnostic)
     vector<double> vent_fact, vent_fact0;
     // padjust SAVE variables (iter.f:1005)
@@ -146,6 +147,8 @@ struct Oracle {
 // ---------------------------------------------------------------------------
 bool is_wall(int f) { return f == SLIP || f == NOSLIP; }
 bool is_wallf(int f) { return f == SLIP || f == NOSLIP || f == FILLED1; }
+
+#include "pdac_oracle_les.inc"
 
 void build_tables(Oracle &o) {
     o.raw.assign((size_t)NSLOT * o.ncell, 0);
@@ -1081,13 +1084,14 @@ void tilde_2d(Oracle &o, double dt) {
     std::fill(o.gvisz.begin(), o.gvisz.end(), 0.0);
     std::fill(o.pvisx.begin(), o.pvisx.end(), 0.0);
     std::fill(o.pvisz.begin(), o.pvisz.end(), 0.0);
-    if (o.cfg.gas_viscosity)  // viscg: mugt = mug (iturb = 0)
-        stress2d(o, o.gvisx.data(), o.gvisz.data(), o.mug.data(), o.mug.data(), o.ep.data(), o.ug.data(), o.wg.data());
+    if (o.cfg.gas_viscosity)  // viscg
+        stress2d(o, o.gvisx.data(), o.gvisz.data(), viscg_mu(o), o.mug.data(), o.ep.data(), o.ug.data(), o.wg.data());
     if (o.cfg.part_viscosity) {
-        vector<double> mus(n), rlkinrl(n);
+        vector<double> mus(n), must(n), rlkinrl(n);
         for (int is = 1; is <= ns; ++is) {
+            viscs_mu(o, is, must);
             for (int c = 0; c < n; ++c) { mus[c] = o.cmus[is]; rlkinrl[c] = o.S(o.rlk, c, is) * o.inrl[is]; }
-            stress2d(o, &o.pvisx[(size_t)(is - 1) * n], &o.pvisz[(size_t)(is - 1) * n], mus.data(), mus.data(),
+            stress2d(o, &o.pvisx[(size_t)(is - 1) * n], &o.pvisz[(size_t)(is - 1) * n], must.data(), mus.data(),
                      rlkinrl.data(), &o.us[(size_t)(is - 1) * n], &o.ws[(size_t)(is - 1) * n]);
         }
         if (o.cfg.repulsive_model == 1) repulsive_2d(o);
@@ -1497,6 +1501,7 @@ void ygas_2d(Oracle &o, double dt) {
 // ---------------------------------------------------------------------------
 void htilde_2d(Oracle &o, double dt) {
     int n = o.ncell, ns = o.ns;
+    const double *kapgt = flux_kapgt(o);
     o.egfe.assign(n, 0.0); o.egft.assign(n, 0.0); o.hgfe.assign(n, 0.0); o.hgft.assign(n, 0.0);
     o.esfe.assign((size_t)n * ns, 0.0); o.esft.assign((size_t)n * ns, 0.0);
     o.hsfe.assign((size_t)n * ns, 0.0); o.hsft.assign((size_t)n * ns, 0.0);
@@ -1517,7 +1522,7 @@ void htilde_2d(Oracle &o, double dt) {
         }
         if (o.cfg.gas_viscosity) {
             Sten kappa, eps, temp;
-            first_nb2(o, kappa, o.kapg.data(), c);
+            first_nb2(o, kappa, kapgt, c);
             first_nb2(o, eps, o.ep.data(), c);
             first_nb2(o, temp, o.tg.data(), c);
             hotc_2d(o, o.hgfe[c], o.hgft[c], o.hgfe[imjk], o.hgft[ijkm], eps, temp, kappa, c);
@@ -1959,6 +1964,7 @@ int pdac_oracle_create(const pdac_cfg *cfg, void **out) {
     build_tables(*o);
     if (o->d3) build_tables3(*o);
     alloc(*o);
+    les_setup(*o);
     *out = o;
     return PDAC_OK;
 }
@@ -2045,6 +2051,14 @@ int pdac_oracle_ftem(void *h, double dt) {
     return o.d3 ? ftem_3d(o, dt) : ftem_2d(o, dt);
 }
 
+// sgsg / sgss as prog.f:207-208 calls them after fieldn
+int pdac_oracle_sgs(void *h) {
+    Oracle &o = *(Oracle *)h;
+    if (o.cfg.iturb >= 1) sgsg(o);
+    if (o.cfg.iss == 1) sgss(o);
+    return PDAC_OK;
+}
+
 // initialize_fieldn (explicit_solver.f:419-564), the time_integration = 1
 // counterpart of fieldn; coefficients use the full time step
 int pdac_oracle_initialize_fieldn(void *h) {
@@ -2077,6 +2091,7 @@ int pdac_oracle_step(void *h, int sweep, int *nit) {
     int st = PDAC_OK;
     if (o.cfg.time_integration == 1) {
         pdac_oracle_initialize_fieldn(h);
+        pdac_oracle_sgs(h);
         if (nit) *nit = 0;
         for (int rk = 1; rk <= o.cfg.rungekut; ++rk) {
             double dt = dt0 / (o.cfg.rungekut + 1 - rk);
@@ -2087,6 +2102,7 @@ int pdac_oracle_step(void *h, int sweep, int *nit) {
         return st;
     }
     pdac_oracle_fieldn(h);
+    pdac_oracle_sgs(h);
     for (int rk = 1; rk <= o.cfg.rungekut; ++rk) {
         double dt = dt0 / (o.cfg.rungekut + 1 - rk);
         pdac_oracle_tilde(h, dt);
@@ -2119,7 +2135,8 @@ int pdac_oracle_get_array(void *h, const char *name, double *out, long *n_inout)
                {"rvgn", &o.rvgn}, {"rvsn", &o.rvsn}, {"rvg", &o.rvg}, {"rvs", &o.rvs}, {"appv", &o.appv},
                {"rgfn", &o.rgfn}, {"rsfn", &o.rsfn}, {"mf3", &o.mf3}, {"ef3", &o.ef3},
                {"gvisy", &o.gvisy}, {"pvisy", &o.pvisy}, {"hgfe", &o.hgfe}, {"hgft", &o.hgft},
-               {"hsfe", &o.hsfe}, {"hsft", &o.hsft},
+               {"hsfe", &o.hsfe}, {"hsft", &o.hsft}, {"smag", &o.smag}, {"mugt", &o.mugt}, {"kapgt", &o.kapgt},
+               {"must", &o.must},
                // explicit-solver fields (explicit_solver.f:15-83)
                {"rgpstar", &o.rk.rgpS}, {"rlkstar", &o.rk.rlkS}, {"ugstar", &o.rk.ugS}, {"usstar", &o.rk.usS},
                {"vgstar", &o.rk.vgS}, {"vsstar", &o.rk.vsS}, {"wgstar", &o.rk.wgS}, {"wsstar", &o.rk.wsS},

@@ -24,7 +24,7 @@ _lib = None
 
 def build(force=False):
     """Compile the oracle with its Makefile (g++ only; seconds)."""
-    srcs = ("pdac_oracle.cpp", "pdac_oracle3d.inc", "pdac_oracle_rk3.inc")
+    srcs = ("pdac_oracle.cpp", "pdac_oracle3d.inc", "pdac_oracle_rk3.inc", "pdac_oracle_les.inc")
     if force or not os.path.exists(LIB_PATH) or \
             os.path.getmtime(LIB_PATH) < max(os.path.getmtime(os.path.join(HERE, f)) for f in srcs):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
@@ -121,6 +121,10 @@ class Oracle:
 
     def ftem(self, dt):
         self._chk(self.L.pdac_oracle_ftem(self.h, dt), "ftem")
+
+    def sgs(self):
+        """sgsg and sgss as prog.f:207-208 call them after fieldn."""
+        self._chk(self.L.pdac_oracle_sgs(self.h), "sgs")
 
     def initialize_fieldn(self):
         self._chk(self.L.pdac_oracle_initialize_fieldn(self.h), "initialize_fieldn")

@@ -49,6 +49,7 @@ class PdacCfg(C.Structure):
         ("pmodel", C.c_int), ("drag_model", C.c_int), ("icpc", C.c_int),
         ("tref", C.c_double),
         ("gas_viscosity", C.c_int), ("part_viscosity", C.c_int), ("repulsive_model", C.c_int),
+        ("iturb", C.c_int), ("modturbo", C.c_int), ("iss", C.c_int), ("cmut", C.c_double),
         ("gravx", C.c_double), ("gravy", C.c_double), ("gravz", C.c_double),
         ("dk", C.c_double * MAX_NSOLID), ("rl", C.c_double * MAX_NSOLID),
         ("phis", C.c_double * MAX_NSOLID), ("cmus", C.c_double * MAX_NSOLID),
@@ -121,12 +122,16 @@ def declare(lib, prefix, handle_type):
     }
     if prefix == "pdac_gpu":
         sigs.update({
+            "sgsg": [h],
+            "sgss": [h],
             "write_restart": [h, C.c_char_p, C.c_double, C.c_int],
             "read_restart": [h, C.c_char_p, _dp, C.POINTER(C.c_int)],
             "write_output": [h, C.c_char_p, C.c_double],
             "mass_residuals": [h, C.c_int, C.c_double, _dp, C.c_int],
             "append_mass_check": [h, C.c_char_p, C.c_int, C.c_double],
         })
+    if prefix == "pdac_oracle":
+        sigs["sgs"] = [h]
     for name, args in sigs.items():
         fn = getattr(lib, f"{prefix}_{name}")
         fn.argtypes = args

@@ -119,3 +119,24 @@ def small_3d_rk3(**kw):
     """small_3d with the explicit SSP-RK3 solver at dt = 1 ms."""
     kw.setdefault("dt", 0.001)
     return _explicit(small_3d(**kw))
+
+
+def _les(deck):
+    deck.set("model", iturb=1, modturbo=1, iss=1)
+    return deck
+
+
+def small_2d_les(**kw):
+    """small_2d with the Smagorinsky sub-grid model (iturb = 1, the
+    reference's default) and the particle sub-grid stress (iss = 1)."""
+    return _les(small_2d(**kw))
+
+
+def small_3d_les(**kw):
+    """small_3d with the sub-grid models of small_2d_les."""
+    return _les(small_3d(**kw))
+
+
+def small_2d_rk3_les(**kw):
+    """small_2d_rk3 with the sub-grid models of small_2d_les."""
+    return _les(small_2d_rk3(**kw))

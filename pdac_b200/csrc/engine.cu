@@ -18,6 +18,7 @@
 #include "inner.cuh"
 #include "rk3.cuh"
 #include "io.cuh"
+#include "les.cuh"
 
 using namespace pdac;
 
@@ -172,6 +173,12 @@ int validate(const pdac_cfg *c, std::string &why) {
     if (c->nvent > 0 && !c->vent_ijk) { why = "vent_ijk is NULL"; return 1; }
     if (c->precision != PDAC_PREC_FP64) { why = "only PDAC_PREC_FP64 is built"; return 1; }
     if (c->time_integration != 0 && c->time_integration != 1) { why = "time_integration must be 0 or 1"; return 1; }
+    if (c->iturb != 0 && c->iturb != 1) { why = "iturb must be 0 or 1 (iturb = 2 needs the topography's roughness)"; return 1; }
+    if (c->iturb == 1 && c->modturbo != 1 && !(c->modturbo == 2 && c->job_type == 2)) {
+        why = "modturbo must be 1 (the dynamic model, 2, is built only as its 2D fall-back to 1)";
+        return 1;
+    }
+    if (c->iss != 0 && c->iss != 1) { why = "iss must be 0 or 1"; return 1; }
     if (c->time_integration == 1 && c->pmodel != 1 && c->pmodel != 2) {
         why = "time_integration = 1 needs pmodel 1 or 2 (explicit_solver.f:632-642)";
         return 1;
@@ -206,6 +213,7 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     P.itc = cfg->itc; P.muscl = cfg->muscl; P.lv = cfg->lv; P.lm = cfg->lm; P.pmodel = cfg->pmodel;
     P.drag_model = cfg->drag_model; P.icpc = cfg->icpc; P.gas_viscosity = cfg->gas_viscosity;
     P.part_viscosity = cfg->part_viscosity; P.repulsive_model = cfg->repulsive_model; P.inmax = cfg->inmax;
+    P.iturb = cfg->iturb; P.iss = cfg->iss;
     for (int ig = 0; ig < ng; ++ig) P.gas_type[ig] = cfg->gas_type[ig];
     P.alpha = cfg->alpha; P.alphagrav = cfg->alphagrav; P.omega = cfg->omega; P.delg = cfg->delg;
     P.beta = cfg->beta; P.flim = cfg->flim; P.tref = cfg->tref;
@@ -300,6 +308,7 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     // the explicit solver's own fields exist only when it is selected; its
     // right-hand-side rows: mass, momentum per axis and enthalpy of each phase
     int t1 = ctx->ti == 1 ? 1 : 0, neq = (ctx->d3 ? 5 : 4) * ctx->nph;
+    int lt = cfg->iturb >= 1 ? 1 : 0, ls = cfg->iss >= 1 ? 1 : 0;  // sub-grid model fields
     RkF &K = ctx->K;
     std::vector<Slot> slots = {
         {"p", &F.p, 1}, {"ep", &F.ep, 1}, {"rog", &F.rog, 1}, {"rgp", &F.rgp, 1}, {"tg", &F.tg, 1},
@@ -328,7 +337,8 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
         {"ugn", &K.ugn, t1}, {"vgn", &K.vgn, t1 * d3}, {"wgn", &K.wgn, t1}, {"usn", &K.usn, ns * t1},
         {"vsn", &K.vsn, ns * t1 * d3}, {"wsn", &K.wsn, ns * t1}, {"hv", &K.hv, ns * t1},
         {"k1", &K.k1, neq * t1}, {"k2", &K.k2, neq * t1}, {"xrgp", &K.xrgp, t1}, {"xrlk", &K.xrlk, ns * t1},
-        {"xep", &K.xep, t1}, {"xug", &K.xug, t1}, {"xvg", &K.xvg, t1 * d3}, {"xwg", &K.xwg, t1}};
+        {"xep", &K.xep, t1}, {"xug", &K.xug, t1}, {"xvg", &K.xvg, t1 * d3}, {"xwg", &K.xwg, t1},
+        {"smag", &F.smag, lt}, {"mugt", &F.mugt, lt}, {"kapgt", &F.kapgt, lt}, {"must", &F.must, ns * ls}};
     // each field starts on a 256-byte boundary
     size_t stride = ((size_t)n + 31) / 32 * 32;
     size_t total = 0;
@@ -346,6 +356,33 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     // per-class blocks inside a slot are exactly ncell apart, as the
     // reference's (ncell, n) column-major arrays; the stride pads slot ends
     F.counters = ctx->d_counters;
+    if (lt) {
+        // turbulence_setup (turbo.f:42-108), iturb = 1: smag = (cmut delta)^2,
+        // delta = sqrt(dz dx) in 2D, (dz dy dx)^(1/3) times anis in 3D
+        std::vector<double> smag(n);
+        for (int c = 0; c < n; ++c) {
+            int i = c % nx + 1, j = (c / nx) % ny + 1, k = c / (nx * ny) + 1;
+            double lm;
+            if (!ctx->d3) {
+                double delt = std::sqrt(dz[k] * dx[i]);
+                lm = cfg->cmut * delt;
+                smag[c] = lm * lm;
+            } else {
+                double delt = std::pow(dz[k] * dy[j] * dx[i], 1.0 / 3.0);
+                lm = cfg->cmut * delt;
+                smag[c] = lm * lm;
+                // anis, turbo.f:670-700
+                double deltamax = std::max(dx[i], std::max(dy[j], dz[k]));
+                double a1 = dx[i] / deltamax, a2 = dy[j] / deltamax, a3 = dz[k] / deltamax;
+                double la1 = std::log(a1), la2 = std::log(a2), la3 = std::log(a3);
+                double fla = la1 * la1 + la2 * la2 + la3 * la3 - la1 * la2 + la1 * la3 - la2 * la3;
+                fla = 4.0 / 27.0 * fla;
+                fla = std::sqrt(fla);
+                smag[c] = smag[c] * std::cosh(fla);
+            }
+        }
+        CK(cudaMemcpy(F.smag, smag.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    }
     int nq = 1 + ns + ng;
     CK(cudaMalloc(&ctx->d_partial, (size_t)nq * 1024 * sizeof(double)));
     *out = ctx;
@@ -446,12 +483,39 @@ int pdac_gpu_fieldn(pdac_ctx *ctx) {
     return PDAC_OK;
 }
 
+// viscg / viscs before a stress evaluation (visc.f:150-205): mugt = mug +
+// mugt with the sub-grid model, must = must + mus with the particle one
+static int accumulate_viscosities(pdac_ctx *ctx, cudaStream_t st) {
+    const size_t n = ctx->ncell;
+    if (ctx->P.iturb && ctx->P.gas_viscosity) {
+        pdac::k_accum<<<blocks((long)n), TPB, 0, st>>>(ctx->F.mugt, ctx->F.mug, n);
+        ctx->launches++;
+    }
+    if (ctx->P.iss && ctx->P.part_viscosity)
+        for (int is = 1; is <= ctx->ns; ++is) {
+            pdac::k_accum_const<<<blocks((long)n), TPB, 0, st>>>(ctx->F.must + (size_t)(is - 1) * n, ctx->P.cmus[is], n);
+            ctx->launches++;
+        }
+    CK(cudaGetLastError());
+    return PDAC_OK;
+}
+
+// the conductivity of an enthalpy flux pass: kapgt = kapgt + kapg with the
+// sub-grid model (htilde.f:218-224); the flux kernels then read kapgt
+static void accumulate_conductivity(pdac_ctx *ctx, cudaStream_t st) {
+    if (!ctx->P.iturb) return;
+    pdac::k_accum<<<blocks((long)ctx->ncell), TPB, 0, st>>>(ctx->F.kapgt, ctx->F.kapg, (size_t)ctx->ncell);
+    ctx->launches++;
+}
+
 int pdac_gpu_tilde(pdac_ctx *ctx, double dt) {
     if (!ctx) return PDAC_ERR_ARG;
     cudaStream_t st = ctx->stream;
     size_t n = ctx->ncell, ns = ctx->ns;
     Fld &F = ctx->F;
     CK(cudaEventRecord(ctx->ev[4], st));
+    int s = accumulate_viscosities(ctx, st);
+    if (s) return s;
     if (ctx->d3) {
         CK(cudaMemsetAsync(F.mf, 0, n * 9 * (ns + 1) * sizeof(double), st));
         pdac::k_visc3d<<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
@@ -756,6 +820,7 @@ int pdac_gpu_htilde(pdac_ctx *ctx, double dt) {
         if (a) CK(cudaMemsetAsync(a, 0, n * sizeof(double), st));
     for (double *a : {F.esfe, F.esfn, F.esft})
         if (a) CK(cudaMemsetAsync(a, 0, n * ns * sizeof(double), st));
+    accumulate_conductivity(ctx, st);
     if (ctx->d3) {
         pdac::k_htilde_flux3d<true><<<blocks(n), TPB, 0, st>>>(ctx->P, F), ctx->launches++;
         pdac::k_htilde3d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt), ctx->launches++;
@@ -803,14 +868,43 @@ int pdac_gpu_initialize_fieldn(pdac_ctx *ctx) {
     CK(cudaMemsetAsync(F.vis, 0, n * 3 * (ns + 1) * sizeof(double), st));
     if (ctx->d3) {
         PHASE_LAUNCH_D(ctx->nph, pdac::k_rk3_fieldn, 3, blocks(n), TPB, st, ctx->P, F, ctx->K, ctx->cfg.dt);
+        if (int s = accumulate_viscosities(ctx, st)) return s;
         pdac::k_visc3d<<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
     } else {
         PHASE_LAUNCH_D(ctx->nph, pdac::k_rk3_fieldn, 2, blocks(n), TPB, st, ctx->P, F, ctx->K, ctx->cfg.dt);
+        if (int s = accumulate_viscosities(ctx, st)) return s;
         pdac::k_visc2d<<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
     }
     ctx->launches += 2;
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[3], st));
+    return PDAC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// sub-grid turbulence model, turbo.f
+// ---------------------------------------------------------------------------
+// sgsg (turbo.f:145-349), called after fieldn / initialize_fieldn
+// (prog.f:207); nothing to do without the sub-grid model
+int pdac_gpu_sgsg(pdac_ctx *ctx) {
+    if (!ctx) return PDAC_ERR_ARG;
+    if (!ctx->P.iturb) return PDAC_OK;
+    if (ctx->d3) pdac::k_sgsg<3><<<blocks(ctx->ncell), TPB, 0, ctx->stream>>>(ctx->P, ctx->F);
+    else pdac::k_sgsg<2><<<blocks(ctx->ncell), TPB, 0, ctx->stream>>>(ctx->P, ctx->F);
+    ctx->launches++;
+    CK(cudaGetLastError());
+    return PDAC_OK;
+}
+
+// sgss (turbo.f:437-475), prog.f:208, with iss = 1
+int pdac_gpu_sgss(pdac_ctx *ctx) {
+    if (!ctx) return PDAC_ERR_ARG;
+    if (ctx->P.iss != 1) return PDAC_OK;
+    long nt = (long)ctx->ncell * ctx->ns;
+    if (ctx->d3) pdac::k_sgss<3><<<blocks(nt), TPB, 0, ctx->stream>>>(ctx->P, ctx->F);
+    else pdac::k_sgss<2><<<blocks(nt), TPB, 0, ctx->stream>>>(ctx->P, ctx->F);
+    ctx->launches++;
+    CK(cudaGetLastError());
     return PDAC_OK;
 }
 
@@ -828,6 +922,10 @@ static long long enqueue_explicit(pdac_ctx *ctx, double dt, cudaStream_t st, boo
     long long L = 0;
     // compute_fluxes: mass, momentum and enthalpy face fluxes of the state
     auto fluxes = [&]() {
+        if (P.iturb) {
+            pdac::k_accum<<<blocks(n), TPB, 0, st>>>(F.kapgt, F.kapg, (size_t)n);
+            L++;
+        }
         if (ctx->d3) {
             pdac::k_rk3_mflux<3><<<blocks(n), TPB, 0, st>>>(P, F);
             pdac::k_tilde_flux3d<0><<<blocks(nphc), TPB, 0, st>>>(P, F);
@@ -947,6 +1045,7 @@ int pdac_gpu_step(pdac_ctx *ctx, int sweep, int *nit) {
     if (ctx->ti == 1) {
         // prog.f:191-274 with time_integration = 1
         if ((s = pdac_gpu_initialize_fieldn(ctx))) return s;
+        if ((s = pdac_gpu_sgsg(ctx)) || (s = pdac_gpu_sgss(ctx))) return s;
         if (nit) *nit = 0;
         for (int rk = 1; rk <= ctx->cfg.rungekut; ++rk) {
             double dt = dt0 / (ctx->cfg.rungekut + 1 - rk);
@@ -958,6 +1057,7 @@ int pdac_gpu_step(pdac_ctx *ctx, int sweep, int *nit) {
         return status;
     }
     if ((s = pdac_gpu_fieldn(ctx))) return s;
+    if ((s = pdac_gpu_sgsg(ctx)) || (s = pdac_gpu_sgss(ctx))) return s;
     for (int rk = 1; rk <= ctx->cfg.rungekut; ++rk) {
         double dt = dt0 / (ctx->cfg.rungekut + 1 - rk);
         if ((s = pdac_gpu_tilde(ctx, dt))) return s;

@@ -316,8 +316,8 @@ __global__ void k_tilde_flux2d(Prm P, Fld F) {
 }
 
 // stress2D, visc.f:561-696, for one cell; mu/lambda/eps accessors
-template <typename MU, typename EPS>
-__device__ __forceinline__ void stress2d_cell(const Prm &P, const Raw2 &R, const Rem2 &M, int i, int k, MU mu, EPS eps,
+template <typename MU, typename LAM, typename EPS>
+__device__ __forceinline__ void stress2d_cell(const Prm &P, const Raw2 &R, const Rem2 &M, int i, int k, MU mu, LAM lam, EPS eps,
                                               const double *u, const double *w, double &visx, double &visz) {
     const double *dx = P.dx, *dz = P.dz, *indx = P.indx, *indz = P.indz, *r = P.r, *rb = P.rb, *inr = P.inr, *inrb = P.inrb;
     const double cm = 2.0 / 3.0;
@@ -331,10 +331,10 @@ __device__ __forceinline__ void stress2d_cell(const Prm &P, const Raw2 &R, const
     double txx1 = 2.0 * (u[c] - u[R.w]) * indx[i];
     double tyy2 = 2.0 * (w[R.t] - w[c]) * indz[k + 1];
     double tyy1 = 2.0 * (w[c] - w[R.b]) * indz[k];
-    txx2 = mu(M.e) * txx2 - cm * mu(M.e) * divr;
-    txx1 = mu(c) * txx1 - cm * mu(c) * divc;
-    tyy2 = mu(M.t) * tyy2 - cm * mu(M.t) * divt;
-    tyy1 = mu(c) * tyy1 - cm * mu(c) * divc;
+    txx2 = mu(M.e) * txx2 - cm * lam(M.e) * divr;
+    txx1 = mu(c) * txx1 - cm * lam(c) * divc;
+    tyy2 = mu(M.t) * tyy2 - cm * lam(M.t) * divt;
+    tyy1 = mu(c) * tyy1 - cm * lam(c) * divc;
     double tyx2 = (u[R.t] - u[c]) * indzp * 2.0 + (w[R.e] - w[c]) * indxp * 2.0;
     double tyx1 = (u[c] - u[R.b]) * indzm * 2.0 + (w[R.eb] - w[R.b]) * indxp * 2.0;
     double txy2 = tyx2;
@@ -343,7 +343,7 @@ __device__ __forceinline__ void stress2d_cell(const Prm &P, const Raw2 &R, const
     if (P.itc == 1) {
         eps0 = (eps(c) * dx[i + 1] + eps(M.e) * dx[i]) * indxp;
         double mu0 = (mu(c) * dx[i + 1] + mu(M.e) * dx[i]) * indxp;
-        double lambda0 = (mu(c) * dx[i + 1] + mu(M.e) * dx[i]) * indxp;
+        double lambda0 = (lam(c) * dx[i + 1] + lam(M.e) * dx[i]) * indxp;
         t0 = 2.0 * u[c] * inrb[i];
         double du = (rb[i + 1] * u[R.e] - rb[i - 1] * u[R.w]);
         double wm2 = (dx[i] * w[R.e] + dx[i + 1] * w[c]) * indxp;
@@ -390,8 +390,10 @@ __global__ void k_tilde2d(Prm P, Fld F, double dt, const double *app0u, const do
     // viscous stresses
     double gvx = 0, gvz = 0;
     if (P.gas_viscosity) {
-        const double *mug = F.mug, *ep = F.ep;
-        stress2d_cell(P, R, M, i, k, [&](int q) { return mug[q]; }, [&](int q) { return ep[q]; }, F.ug, F.wg, gvx, gvz);
+        // viscg: mu = mugt (the sub-grid model's, molecular part added) or mug, lambda = mug
+        const double *mug = F.mug, *mut = P.iturb ? F.mugt : F.mug, *ep = F.ep;
+        stress2d_cell(P, R, M, i, k, [&](int q) { return mut[q]; }, [&](int q) { return mug[q]; },
+                      [&](int q) { return ep[q]; }, F.ug, F.wg, gvx, gvz);
     }
     double alpha = P.alpha, ag = P.alphagrav;
     double dxi = dx[i], dxip1 = dx[i + 1], dzk = dz[k], dzkp1 = dz[k + 1];
@@ -422,7 +424,9 @@ __global__ void k_tilde2d(Prm P, Fld F, double dt, const double *app0u, const do
         if (P.part_viscosity) {
             const double cm = P.cmus[is], ir = P.inrl[is];
             const double *rl = F.rlk + (size_t)(is - 1) * n;
-            stress2d_cell(P, R, M, i, k, [&](int) { return cm; }, [&](int q) { return rl[q] * ir; },
+            const double *mst = P.iss ? F.must + (size_t)(is - 1) * n : nullptr;
+            stress2d_cell(P, R, M, i, k, [&](int q) { return mst ? mst[q] : cm; }, [&](int) { return cm; },
+                          [&](int q) { return rl[q] * ir; },
                           F.us + (size_t)(is - 1) * n, F.ws + (size_t)(is - 1) * n, pvx, pvz);
             if (P.repulsive_model == 1) {
                 double rc = rl[c], re = rl[ijke], rt = rl[ijkt];
@@ -766,7 +770,7 @@ __global__ void k_htilde_flux2d(Prm P, Fld F) {
         if (visc) {
             St ka, ep, te;
             if (ph == 0) {
-                first_nb2(ka, F.kapg, R, M);
+                first_nb2(ka, P.iturb ? F.kapgt : F.kapg, R, M);
                 first_nb2(ep, F.ep, R, M);
                 first_nb2(te, F.tg, R, M);
             } else {

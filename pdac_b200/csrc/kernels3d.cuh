@@ -313,14 +313,17 @@ __global__ void k_visc3d(Prm P, Fld F) {
     double vx = 0, vy = 0, vz = 0;
     if (ph == 0) {
         if (P.gas_viscosity) {
-            const double *mug = F.mug, *ep = F.ep;
-            stress3d_cell(P, R, M, i, j, k, [&](int q) { return mug[q]; }, [&](int q) { return ep[q]; }, F.ug, F.vg,
+            const double *mug = F.mug, *mut = P.iturb ? F.mugt : F.mug, *ep = F.ep;
+            stress3d_cell(P, R, M, i, j, k, [&](int q) { return mut[q]; }, [&](int q) { return mug[q]; },
+                          [&](int q) { return ep[q]; }, F.ug, F.vg,
                           F.wg, vx, vy, vz);
         }
     } else if (P.part_viscosity) {
         const double cm = P.cmus[ph], ir = P.inrl[ph];
         const double *rl = F.rlk + off;
-        stress3d_cell(P, R, M, i, j, k, [&](int) { return cm; }, [&](int q) { return rl[q] * ir; }, F.us + off,
+        const double *mst = P.iss ? F.must + off : nullptr;
+        stress3d_cell(P, R, M, i, j, k, [&](int q) { return mst ? mst[q] : cm; }, [&](int) { return cm; },
+                      [&](int q) { return rl[q] * ir; }, F.us + off,
                       F.vs + off, F.ws + off, vx, vy, vz);
         if (P.repulsive_model == 1) {
             double rc = rl[c], re = rl[ijke], rn = rl[ijkn], rt = rl[ijkt];
@@ -728,7 +731,7 @@ __global__ void k_htilde_flux3d(Prm P, Fld F) {
         if (visc) {
             S3 ka, ep, te;
             if (ph == 0) {
-                first_nb3(ka, F.kapg, R, M);
+                first_nb3(ka, P.iturb ? F.kapgt : F.kapg, R, M);
                 first_nb3(ep, F.ep, R, M);
                 first_nb3(te, F.tg, R, M);
             } else {

@@ -376,8 +376,8 @@ __device__ __forceinline__ void hotc_3d(const Prm &P, F6d &h, bool hw, bool hs, 
 }
 
 // stress3D (visc.f:293-559) for one cell; mu == lambda on this path
-template <typename MU, typename EPS>
-__device__ __forceinline__ void stress3d_cell(const Prm &P, const Raw3 &R, const Rem3 &M, int i, int j, int k, MU mu,
+template <typename MU, typename LAM, typename EPS>
+__device__ __forceinline__ void stress3d_cell(const Prm &P, const Raw3 &R, const Rem3 &M, int i, int j, int k, MU mu, LAM lam,
                                               EPS eps, const double *u, const double *v, const double *w,
                                               double &visx, double &visy, double &visz) {
     const double *dx = P.dx, *dy = P.dy, *dz = P.dz, *indx = P.indx, *indy = P.indy, *indz = P.indz;
@@ -399,12 +399,12 @@ __device__ __forceinline__ void stress3d_cell(const Prm &P, const Raw3 &R, const
     double txx2 = 2.0 * dup * indx[i + 1], txx1 = 2.0 * dum * indx[i];
     double tyy2 = 2.0 * dvp * indy[j + 1], tyy1 = 2.0 * dvm * indy[j];
     double tzz2 = 2.0 * dwp * indz[k + 1], tzz1 = 2.0 * dwm * indz[k];
-    txx2 = mu(M.e) * txx2 - cm * mu(M.e) * dive;
-    txx1 = mu(c) * txx1 - cm * mu(c) * divc;
-    tyy2 = mu(M.n) * tyy2 - cm * mu(M.n) * divn;
-    tyy1 = mu(c) * tyy1 - cm * mu(c) * divc;
-    tzz2 = mu(M.t) * tzz2 - cm * mu(M.t) * divt;
-    tzz1 = mu(c) * tzz1 - cm * mu(c) * divc;
+    txx2 = mu(M.e) * txx2 - cm * lam(M.e) * dive;
+    txx1 = mu(c) * txx1 - cm * lam(c) * divc;
+    tyy2 = mu(M.n) * tyy2 - cm * lam(M.n) * divn;
+    tyy1 = mu(c) * tyy1 - cm * lam(c) * divc;
+    tzz2 = mu(M.t) * tzz2 - cm * lam(M.t) * divt;
+    tzz1 = mu(c) * tzz1 - cm * lam(c) * divc;
     dum = u[c] - u[R.s]; dup = u[R.n] - u[c]; dvm = v[c] - v[R.w]; dvp = v[R.e] - v[c];
     dwm = w[c] - w[R.s]; dwp = w[R.n] - w[c];
     dupm1 = u[R.wn] - u[R.w]; dupm2 = u[R.wt] - u[R.w]; dvpm1 = v[R.es] - v[R.s];

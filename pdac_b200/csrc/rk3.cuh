@@ -369,13 +369,16 @@ __global__ void k_visc2d(Prm P, Fld F) {
     double vx = 0, vz = 0;
     if (ph == 0) {
         if (P.gas_viscosity) {
-            const double *mug = F.mug, *ep = F.ep;
-            stress2d_cell(P, R, M, i, k, [&](int q) { return mug[q]; }, [&](int q) { return ep[q]; }, F.ug, F.wg, vx, vz);
+            const double *mug = F.mug, *mut = P.iturb ? F.mugt : F.mug, *ep = F.ep;
+            stress2d_cell(P, R, M, i, k, [&](int q) { return mut[q]; }, [&](int q) { return mug[q]; },
+                          [&](int q) { return ep[q]; }, F.ug, F.wg, vx, vz);
         }
     } else if (P.part_viscosity) {
         const double cm = P.cmus[ph], ir = P.inrl[ph];
         const double *rl = F.rlk + off;
-        stress2d_cell(P, R, M, i, k, [&](int) { return cm; }, [&](int q) { return rl[q] * ir; }, F.us + off, F.ws + off,
+        const double *mst = P.iss ? F.must + off : nullptr;
+        stress2d_cell(P, R, M, i, k, [&](int q) { return mst ? mst[q] : cm; }, [&](int) { return cm; },
+                      [&](int q) { return rl[q] * ir; }, F.us + off, F.ws + off,
                       vx, vz);
         if (P.repulsive_model == 1) {
             const double a_rep = -8.76, b_rep = -0.27;

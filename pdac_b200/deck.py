@@ -343,10 +343,14 @@ class Deck:
     def check(self):
         """Options of the reference that this engine does not implement."""
         bad = []
-        if self["iturb"] != 0:
-            bad.append("iturb>0 (sub-grid turbulence)")
-        if self["iss"] != 0:
-            bad.append("iss>0")
+        if self["iturb"] not in (0, 1):
+            bad.append("iturb=2 (sub-grid model with ground roughness, needs topography)")
+        if self["iturb"] == 1 and self["modturbo"] == 2 and self.is3d:
+            bad.append("modturbo=2 (dynamic Smagorinsky model) in 3D")
+        if self["iturb"] == 1 and self["modturbo"] not in (1, 2):
+            bad.append("modturbo other than 1 or 2")
+        if self["iss"] not in (0, 1):
+            bad.append("iss>1")
         if self["ctu"] != 0:
             bad.append("ctu>0 (corner transport upwind)")
         if self["implicit_fluxes"] or self["implicit_enthalpy"]:

@@ -65,7 +65,7 @@ def lib():
 EXPORTED = (
     "pdac_gpu_create", "pdac_gpu_destroy", "pdac_gpu_last_error", "pdac_gpu_upload_state",
     "pdac_gpu_download_state", "pdac_gpu_boundary", "pdac_gpu_fieldn", "pdac_gpu_tilde", "pdac_gpu_iter",
-    "pdac_gpu_initialize_fieldn", "pdac_gpu_explicit_iter",
+    "pdac_gpu_initialize_fieldn", "pdac_gpu_explicit_iter", "pdac_gpu_sgsg", "pdac_gpu_sgss",
     "pdac_gpu_ygas", "pdac_gpu_htilde", "pdac_gpu_ftem", "pdac_gpu_step", "pdac_gpu_set_vent_factors",
     "pdac_gpu_get_array", "pdac_gpu_mass_totals", "pdac_gpu_phase_times", "pdac_gpu_stats",
     "pdac_gpu_reset_stats", "pdac_gpu_mark", "pdac_gpu_elapsed",
@@ -131,6 +131,14 @@ class Engine:
 
     def fieldn(self):
         self._chk(self.L.pdac_gpu_fieldn(self.h), "fieldn")
+
+    def sgsg(self):
+        """The sub-grid turbulence model after fieldn (prog.f:207)."""
+        self._chk(self.L.pdac_gpu_sgsg(self.h), "sgsg")
+
+    def sgss(self):
+        """The particle sub-grid stress after fieldn (prog.f:208)."""
+        self._chk(self.L.pdac_gpu_sgss(self.h), "sgss")
 
     def initialize_fieldn(self):
         self._chk(self.L.pdac_gpu_initialize_fieldn(self.h), "initialize_fieldn")

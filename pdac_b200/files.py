@@ -80,6 +80,8 @@ def run(engine, workdir, max_steps=None, log=None):
             engine.initialize_fieldn()
         else:
             engine.fieldn()
+        engine.sgsg()
+        engine.sgss()
         for r in range(1, rk + 1):
             dtr = dt / (rk + 1 - r)
             if explicit:

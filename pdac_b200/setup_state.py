@@ -410,6 +410,7 @@ class Case:
         c.gas_viscosity = int(bool(d["gas_viscosity"]))
         c.part_viscosity = int(bool(d["part_viscosity"]))
         c.repulsive_model = d["repulsive_model"]
+        c.iturb, c.modturbo, c.iss, c.cmut = int(d["iturb"]), int(d["modturbo"]), int(d["iss"]), float(d["cmut"])
         c.gravx, c.gravy, c.gravz = d["gravx"], d["gravy"], d["gravz"]
         for s in range(self.nsolid):
             c.dk[s] = d["diameter"][s] * 1.0e-6

@@ -5,7 +5,8 @@
 Runs the CPU oracle on the small 2D and 3D plume decks for three time steps
 in both sweep orders (lexicographic = the reference's order, colored = the
 CUDA engine's order), and on the same decks with the explicit SSP-RK3
-solver (time_integration = 1, which has no sweep order), and records, after every step, the outer-sweep count
+solver (time_integration = 1, which has no sweep order) and with the
+sub-grid turbulence model (iturb = 1, iss = 1), and records, after every step, the outer-sweep count
 and per-field summaries (sum, sum of |x|, max |x|) plus the values at a few
 fixed fluid cells.  The fixtures pin the oracle against unintended change;
 the GPU parity tests also compare the engine with the colored fixture.
@@ -64,8 +65,12 @@ def main():
         for name, order in (("lexicographic", pyoracle.ORDER_LEXICOGRAPHIC), ("colored", pyoracle.ORDER_COLORED)):
             data[f"{deck}/{name}"] = run(deck, order)
     # the explicit solver has no corrector, so its single fixture serves both orders
-    for deck in ("small_2d_rk3", "small_3d_rk3"):
+    for deck in ("small_2d_rk3", "small_3d_rk3", "small_2d_rk3_les"):
         data[f"{deck}/lexicographic"] = run(deck, pyoracle.ORDER_LEXICOGRAPHIC)
+    # the sub-grid turbulence model (iturb = 1, iss = 1)
+    for deck in ("small_2d_les", "small_3d_les"):
+        for name, order in (("lexicographic", pyoracle.ORDER_LEXICOGRAPHIC), ("colored", pyoracle.ORDER_COLORED)):
+            data[f"{deck}/{name}"] = run(deck, order)
     path = os.path.join(HERE, "oracle_small.json")
     with open(path, "w") as fh:
         json.dump(data, fh, indent=1)

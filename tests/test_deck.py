@@ -90,9 +90,20 @@ def test_plume_vent_and_flags():
 
 def test_unsupported_options_are_rejected():
     d = configs.plume_2d()
-    d.set("model", iturb=1)
+    d.set("model", iturb=2)
     with pytest.raises(ValueError, match="iturb"):
         Case(d)
+    d = configs.plume_3d(nx=8, ny=8, nz=8)
+    d.set("model", iturb=1, modturbo=2)
+    with pytest.raises(ValueError, match="modturbo"):
+        Case(d)
+
+
+def test_sub_grid_model_reaches_the_configuration():
+    d = configs.plume_2d()
+    d.set("model", iturb=1, iss=1, cmut=0.2)
+    cfg = Case(d).cfg()
+    assert (cfg.iturb, cfg.modturbo, cfg.iss, cfg.cmut) == (1, 1, 1, 0.2)
 
 
 def test_explicit_solver_selection():

@@ -15,7 +15,8 @@ GOLDEN = json.load(open(os.path.join(HERE, "golden", "oracle_small.json")))
 TOL = 1e-9
 
 
-@pytest.mark.parametrize("deck", ["small_2d", "small_3d", "small_2d_rk3", "small_3d_rk3"])
+@pytest.mark.parametrize("deck", ["small_2d", "small_3d", "small_2d_rk3", "small_3d_rk3", "small_2d_les", "small_3d_les",
+                                  "small_2d_rk3_les"])
 def test_engine_matches_colored_fixture(deck):
     """The explicit-solver decks (no corrector, no sweep order) have one
     fixture, stored under the lexicographic key."""
