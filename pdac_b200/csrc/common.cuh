@@ -15,6 +15,20 @@
 #define PDAC_MAXG 7
 #define TPB_RESID 256        // threads per block of the corrector's residual test
 
+// Register caps of the 128-thread stencil kernels, as the minimum number of
+// resident blocks per SM passed to __launch_bounds__.  Uncapped, the 3D
+// momentum and stress kernels take 150-200 registers a thread and run at
+// 2-3 blocks per SM, too few warps to cover their gathers' latency.  4 blocks
+// (128 registers) suits the momentum flux and stress kernels, 6 blocks (80
+// registers) the scalar flux kernels; a tighter cap makes the momentum
+// kernels spill.
+#ifndef PDAC_FLUX_MINB
+#define PDAC_FLUX_MINB 4
+#endif
+#ifndef PDAC_SCALAR_FLUX_MINB
+#define PDAC_SCALAR_FLUX_MINB 6
+#endif
+
 namespace pdac {
 
 // cell flags, grid.f:45-58

@@ -72,6 +72,15 @@ struct pdac_ctx {
     cudaEvent_t xev[9];
     double ex_ms[4] = {0, 0, 0, 0};
     long long ex_calls = 0;
+    // gas-enthalpy wavefront on hyperplane-ordered records: the cooperative
+    // grid (0 when the device cannot co-schedule one; the wavefront then
+    // runs as one launch per hyperplane) and whether it covers the widest
+    // hyperplane
+    pdac::Wave W{};
+    int *d_wave_idx = nullptr;    // order, src[3], start
+    double *d_wave_rec = nullptr; // records and pnew
+    int wave_grid_blocks = 0;
+    bool wave_one = false;
 };
 
 namespace {
@@ -184,6 +193,93 @@ int validate(const pdac_cfg *c, std::string &why) {
         return 1;
     }
     return 0;
+}
+
+// The records of the explicit solver's gas-enthalpy wavefront (fixed by the
+// cell flags): interior fluid cells in hyperplane order d = i + j + k (i + k
+// in 2D), cell order within a hyperplane; empty hyperplanes are dropped, as
+// no cell depends on one.  Also picks the cooperative grid.
+int setup_wave(pdac_ctx *ctx, const int *flag) {
+    const int nx = ctx->nx, ny = ctx->d3 ? ctx->ny : 1, nz = ctx->nz, n = ctx->ncell;
+    const int jlo = ctx->d3 ? 2 : 1, jhi = ctx->d3 ? ny - 1 : 1;
+    const int dmin = 2 + jlo + 2, dmax = (nx - 1) + jhi + (nz - 1);
+    const int nd = dmax - dmin + 1;
+    std::vector<int> count(nd + 1, 0), pos_of(n, -1);
+    auto each = [&](auto fn) {
+        for (int k = 2; k <= nz - 1; ++k)
+            for (int j = jlo; j <= jhi; ++j)
+                for (int i = 2; i <= nx - 1; ++i) {
+                    int c = (i - 1) + nx * ((j - 1) + ny * (k - 1));
+                    if (flag[c] & 1) fn(c, i + j + k - dmin);
+                }
+    };
+    each([&](int, int q) { count[q + 1]++; });
+    std::vector<int> first(nd + 1, 0);
+    for (int q = 0; q < nd; ++q) first[q + 1] = first[q] + count[q + 1];
+    const int np = first[nd];
+    std::vector<int> order(std::max(np, 1), 0), fill(first.begin(), first.end() - 1);
+    each([&](int c, int q) {
+        pos_of[c] = fill[q];
+        order[fill[q]++] = c;
+    });
+    std::vector<int> start;
+    int widest = 0;
+    for (int q = 0; q < nd; ++q)
+        if (first[q + 1] > first[q]) {
+            start.push_back(first[q]);
+            widest = std::max(widest, first[q + 1] - first[q]);
+        }
+    const int nplanes = (int)start.size();
+    start.push_back(np);
+    start.push_back(np);  // read one past the last hyperplane by the prefetch guard
+    std::vector<int> src(3 * (size_t)std::max(np, 1), -1);
+    for (int p = 0; p < np; ++p) {
+        const int c = order[p];
+        src[p] = pos_of[c - 1];
+        if (ctx->d3) src[(size_t)np + p] = pos_of[c - nx];
+        src[2 * (size_t)np + p] = pos_of[c - nx * ny];
+    }
+    const size_t ni = order.size() + src.size() + start.size();
+    CK(cudaMalloc(&ctx->d_wave_idx, ni * sizeof(int)));
+    int *o = ctx->d_wave_idx, *s = o + order.size(), *st = s + src.size();
+    CK(cudaMemcpy(o, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s, src.data(), src.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(st, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
+    const size_t nrec = (size_t)(pdac::WR_YG + ctx->ng) + 1;  // the fields and pnew
+    CK(cudaMalloc(&ctx->d_wave_rec, nrec * std::max(np, 1) * sizeof(double)));
+    pdac::Wave &W = ctx->W;
+    W.order = o;
+    W.src = s;
+    W.start = st;
+    W.rec = ctx->d_wave_rec;
+    W.pnew = ctx->d_wave_rec + (nrec - 1) * std::max(np, 1);
+    W.npos = np;
+    W.nplanes = nplanes;
+    W.dmin = dmin;
+    // a cooperative grid of co-resident blocks: one record per thread and
+    // hyperplane when the device holds enough blocks for the widest one
+    int dev = 0, coop = 0, nsm = 0, occ1 = 0, occn = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    ctx->wave_grid_blocks = 0;
+    ctx->wave_one = false;
+    if (!coop || np == 0) return PDAC_OK;
+    if (ctx->d3) {
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, pdac::k_rk3_wave_rec<3, true>, TPB, 0));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occn, pdac::k_rk3_wave_rec<3, false>, TPB, 0));
+    } else {
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, pdac::k_rk3_wave_rec<2, true>, TPB, 0));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occn, pdac::k_rk3_wave_rec<2, false>, TPB, 0));
+    }
+    const int need = blocks(widest);
+    if (need <= occ1 * nsm) {
+        ctx->wave_grid_blocks = need;
+        ctx->wave_one = true;
+    } else {
+        ctx->wave_grid_blocks = occn * nsm;
+    }
+    return PDAC_OK;
 }
 
 }  // namespace
@@ -385,6 +481,10 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     }
     int nq = 1 + ns + ng;
     CK(cudaMalloc(&ctx->d_partial, (size_t)nq * 1024 * sizeof(double)));
+    if (t1) {
+        int st = setup_wave(ctx, cfg->flag);
+        if (st) return st;
+    }
     *out = ctx;
     return PDAC_OK;
 }
@@ -410,6 +510,8 @@ int pdac_gpu_destroy(pdac_ctx *ctx) {
     cudaFreeHost(ctx->h_nit);
     cudaFree(ctx->d_cand);
     cudaFree(ctx->d_partial);
+    cudaFree(ctx->d_wave_idx);
+    cudaFree(ctx->d_wave_rec);
     cudaFreeHost(ctx->h_counters);
     for (auto &e : ctx->ev) cudaEventDestroy(e);
     for (auto &e : ctx->cev) cudaEventDestroy(e);
@@ -949,8 +1051,33 @@ static long long enqueue_explicit(pdac_ctx *ctx, double dt, cudaStream_t st, boo
         L++;
         mark();
         // gas-enthalpy wavefront over the hyperplanes i + j + k = d of the
-        // interior (2 <= i <= nx - 1 ...), in increasing d
-        if (ctx->d3) {
+        // interior (2 <= i <= nx - 1 ...), in increasing d: records, one
+        // cooperative launch over all hyperplanes, scatter of the results
+        if (ctx->wave_grid_blocks > 0) {
+            const pdac::Wave &W = ctx->W;
+            const int rb = blocks(W.npos);
+            cudaLaunchConfig_t lc = {};
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeCooperative;
+            at[0].val.cooperative = 1;
+            lc.gridDim = dim3(ctx->wave_grid_blocks);
+            lc.blockDim = dim3(TPB);
+            lc.stream = st;
+            lc.attrs = at;
+            lc.numAttrs = 1;
+            if (ctx->d3) {
+                pdac::k_rk3_wave_pre<3><<<rb, TPB, 0, st>>>(P, F, K, W, dt, stage);
+                if (ctx->wave_one) cudaLaunchKernelEx(&lc, pdac::k_rk3_wave_rec<3, true>, P, W, dt, stage);
+                else cudaLaunchKernelEx(&lc, pdac::k_rk3_wave_rec<3, false>, P, W, dt, stage);
+                pdac::k_rk3_wave_post<3><<<rb, TPB, 0, st>>>(P, F, K, W, stage);
+            } else {
+                pdac::k_rk3_wave_pre<2><<<rb, TPB, 0, st>>>(P, F, K, W, dt, stage);
+                if (ctx->wave_one) cudaLaunchKernelEx(&lc, pdac::k_rk3_wave_rec<2, true>, P, W, dt, stage);
+                else cudaLaunchKernelEx(&lc, pdac::k_rk3_wave_rec<2, false>, P, W, dt, stage);
+                pdac::k_rk3_wave_post<2><<<rb, TPB, 0, st>>>(P, F, K, W, stage);
+            }
+            L += 3;
+        } else if (ctx->d3) {
             const int nj = ny - 2, dmax = (nx - 1) + (ny - 1) + (nz - 1);
             for (int d = 6; d <= dmax; ++d) {
                 int kmin = std::max(2, d - (nx - 1) - (ny - 1)), kmax = std::min(nz - 1, d - 4);

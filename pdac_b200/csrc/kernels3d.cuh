@@ -242,7 +242,7 @@ __global__ void k_fieldn3d(Prm P, Fld F) {
 // one thread per (cell, phase) for one momentum component COMP (0 = x,
 // 1 = y, 2 = z): consecutive threads take consecutive cells of one phase
 template <int COMP>
-__global__ void k_tilde_flux3d(Prm P, Fld F) {
+__global__ void __launch_bounds__(128, PDAC_FLUX_MINB) k_tilde_flux3d(Prm P, Fld F) {
     unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (unsigned)P.ncell * (unsigned)(P.ns + 1)) return;
     int ph = (int)(t / (unsigned)P.ncell), c = (int)(t % (unsigned)P.ncell);
@@ -293,7 +293,7 @@ __global__ void k_tilde_flux3d(Prm P, Fld F) {
 // visc.f:150-291, stress3D visc.f:293-559) with the particle repulsion term
 // (tilde.f:362-416); one thread per (cell, phase), consecutive threads take
 // consecutive cells of one phase
-__global__ void k_visc3d(Prm P, Fld F) {
+__global__ void __launch_bounds__(128, PDAC_FLUX_MINB) k_visc3d(Prm P, Fld F) {
     unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (unsigned)P.ncell * (unsigned)(P.ns + 1)) return;
     int ph = (int)(t / (unsigned)P.ncell), c = (int)(t % (unsigned)P.ncell);
@@ -344,7 +344,7 @@ __global__ void k_visc3d(Prm P, Fld F) {
 }
 
 template <int NP>
-__global__ void k_tilde3d(Prm P, Fld F, double dt, const double *app0u, const double *app0v, const double *app0w) {
+__global__ void __launch_bounds__(128, PDAC_FLUX_MINB) k_tilde3d(Prm P, Fld F, double dt, const double *app0u, const double *app0v, const double *app0w) {
     constexpr int MP = Sys<NP>::M;  // phase capacity + 1
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.ncell || !fluid(P, c)) return;
@@ -624,7 +624,7 @@ __device__ __forceinline__ void calc_eps_3d(const Prm &P, const Fld &F, const Ra
 // ---------------------------------------------------------------------------
 // ygas, ygas.f:27-325 (3D)
 // ---------------------------------------------------------------------------
-__global__ void k_ygas_flux3d(Prm P, Fld F) {
+__global__ void __launch_bounds__(128, PDAC_SCALAR_FLUX_MINB) k_ygas_flux3d(Prm P, Fld F) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.ncell || !fluid(P, c)) return;
     int i, j, k;
@@ -692,7 +692,7 @@ __global__ void k_ygas3d(Prm P, Fld F, double dt) {
 // ---------------------------------------------------------------------------
 // GRAV as in k_htilde_flux2d
 template <bool GRAV>
-__global__ void k_htilde_flux3d(Prm P, Fld F) {
+__global__ void __launch_bounds__(128, PDAC_SCALAR_FLUX_MINB) k_htilde_flux3d(Prm P, Fld F) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.ncell || !fluid(P, c)) return;
     int i, j, k;

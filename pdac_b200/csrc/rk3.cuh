@@ -27,6 +27,7 @@
 //    solve (compute_physical_coeff :2105-2163, compute_linear_systems
 //    :822-994, solve_linear_systems :1347-1607) are parallel.
 #pragma once
+#include <cooperative_groups.h>
 #include "kernels3d.cuh"
 
 namespace pdac {
@@ -403,7 +404,7 @@ __global__ void k_visc2d(Prm P, Fld F) {
 // cell of the reference loop, so this thread writes its W/S/B faces always
 // and its E/N/T faces only towards non-fluid cells.
 template <int D>
-__global__ void k_rk3_mflux(Prm P, Fld F) {
+__global__ void __launch_bounds__(128, PDAC_FLUX_MINB) k_rk3_mflux(Prm P, Fld F) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.ncell || !fluid(P, c)) return;
     const size_t n = P.ncell;
@@ -609,6 +610,196 @@ __global__ void k_rk3_wave(Prm P, Fld F, RkF K, double dt, int stage, int d, int
     if (D == 3) F.vg[c] = K.xvg[c];
     F.wg[c] = K.xwg[c];
     for (int is = 1; is <= P.ns; ++is) F.rlk[(size_t)(is - 1) * n + c] = K.xrlk[(size_t)(is - 1) * n + c];
+}
+
+// ---- the wavefront on hyperplane-ordered records -----------------------------
+// Of a cell's gas-enthalpy update only the pressures of its west, south and
+// bottom neighbours come from the wavefront itself; everything else is known
+// once the stage kernel has run.  k_rk3_wave_pre computes those parts once
+// per stage in parallel and stores them as records ordered hyperplane by
+// hyperplane (interior fluid cells only), so that the wavefront reads them
+// coalesced and takes the three neighbour pressures from the previous
+// hyperplane's slice of pnew, which stays in L2.  The arithmetic and its
+// order are those of rhs_gas_enth and k_rk3_wave.
+struct Wave {
+    const int *order;   // record position -> cell
+    const int *src;     // [3][npos]: record of the W / S / B neighbour when it is a fluid cell, else -1
+    const int *start;   // hyperplane dmin + q holds records start[q] .. start[q + 1] - 1
+    double *rec;        // [WR_YG + ng][npos]
+    double *pnew;       // new pressure per record
+    int npos, nplanes, dmin;
+};
+// record fields; the wavefront's results (WR_O*) are stored in record order
+// too and scattered to the cell arrays by k_rk3_wave_post
+enum { WR_OR, WR_OSIEG, WR_OTG, WR_OCG, WR_AX, WR_AY, WR_AZ, WR_PE, WR_PN, WR_PT, WR_PW, WR_PS, WR_PB, WR_R0, WR_EP,
+       WR_SP, WR_INV, WR_TG, WR_ROG, WR_MG, WR_YG };
+
+// the non-recurrent part of every record, then the commit of the values
+// k_rk3_stage parked (nothing of this stage reads the old ones afterwards)
+template <int D>
+__global__ void k_rk3_wave_pre(Prm P, Fld F, RkF K, Wave W, double dt, int stage) {
+    int pos = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= W.npos) return;
+    const int c = W.order[pos];
+    Cell<D> q;
+    cell_of<D>(P, c, q);
+    const size_t n = P.ncell, np = W.npos;
+    const int i = q.i, j = q.j, k = q.k, e0 = (D == 3 ? 4 : 3) * P.nph;
+    auto R = [&](int f) -> double & { return W.rec[(size_t)f * np + pos]; };
+    const double *dx = P.dx, *dz = P.dz;
+    // lower-face gas velocities as the wavefront sees them: new (parked)
+    // where that neighbour is a record, committed one hyperplane earlier
+    const double ugw = W.src[pos] >= 0 ? K.xug[q.rw] : F.ug[q.rw];
+    const double wgb = W.src[2 * np + pos] >= 0 ? K.xwg[q.rb] : F.wg[q.rb];
+    double indxc = 1.0 / (dx[i] + (dx[i + 1] + dx[i - 1]) * 0.5);
+    double indyc = 0.0;
+    double indzc = 1.0 / (dz[k] + (dz[k + 1] + dz[k - 1]) * 0.5);
+    double ugc = 0.5 * (F.ug[c] + ugw);
+    double vgc = 0.0;
+    double wgc = 0.5 * (F.wg[c] + wgb);
+    if (D == 3) {
+        const double vgs = W.src[np + pos] >= 0 ? K.xvg[q.rs] : F.vg[q.rs];
+        indyc = 1.0 / (P.dy[j] + (P.dy[j + 1] + P.dy[j - 1]) * 0.5);
+        vgc = 0.5 * (F.vg[c] + vgs);
+    }
+    R(WR_AX) = indxc * ugc;
+    R(WR_AY) = indyc * vgc;
+    R(WR_AZ) = indzc * wgc;
+    // the old pressures: E / N / T are still old when the cell is reached,
+    // W / S / B are replaced by the wavefront where they are records
+    R(WR_PE) = F.p[q.me];
+    R(WR_PN) = D == 3 ? F.p[q.mn] : 0.0;
+    R(WR_PT) = F.p[q.mt];
+    R(WR_PW) = F.p[q.mw];
+    R(WR_PS) = D == 3 ? F.p[q.ms] : 0.0;
+    R(WR_PB) = F.p[q.mb];
+    double tmp = enth_div<D>(P, F, q, 0);
+    double r = 0.0;
+    r = r - tmp;
+    tmp = 1.0 / dt;
+    r = r + F.ep[c] * (F.p[c] - F.pn[c]) * tmp;
+    R(WR_R0) = r;
+    R(WR_EP) = F.ep[c];
+    double sp = F.rgpn[c] * F.siegn[c];
+    if (stage == 2) sp = sp + 0.25 * dt * K.k1[(size_t)e0 * n + c];
+    R(WR_SP) = sp;
+    R(WR_INV) = 1.0 / K.xrgp[c];
+    R(WR_TG) = F.tg[c];
+    R(WR_ROG) = F.rog[c];
+    double mg = 0.0;
+    for (int ig = 0; ig < P.ng; ++ig) mg = mg + GAS(F.xgc, c, ig) * P.gmw[P.gas_type[ig]];
+    R(WR_MG) = mg;
+    for (int ig = 0; ig < P.ng; ++ig) R(WR_YG + ig) = GAS(F.ygc, c, ig);
+    F.rgp[c] = K.xrgp[c];
+    F.ep[c] = K.xep[c];
+    F.ug[c] = K.xug[c];
+    if (D == 3) F.vg[c] = K.xvg[c];
+    F.wg[c] = K.xwg[c];
+    for (int is = 1; is <= P.ns; ++is) F.rlk[(size_t)(is - 1) * n + c] = K.xrlk[(size_t)(is - 1) * n + c];
+}
+
+// the inputs of one record
+struct WaveIn {
+    double ax, ay, az, pe, pn, pt, pw, ps, pb, r0, ep, sp, inv, tg, rog, mg, yg[PDAC_MAXG];
+    int sw, ss, sb;
+};
+
+template <int D>
+__device__ __forceinline__ void wave_load(const Prm &P, const Wave &W, int pos, WaveIn &v) {
+    const size_t np = W.npos;
+    auto R = [&](int f) { return W.rec[(size_t)f * np + pos]; };
+    v.ax = R(WR_AX); v.ay = D == 3 ? R(WR_AY) : 0.0; v.az = R(WR_AZ);
+    v.pe = R(WR_PE); v.pn = D == 3 ? R(WR_PN) : 0.0; v.pt = R(WR_PT);
+    v.pw = R(WR_PW); v.ps = D == 3 ? R(WR_PS) : 0.0; v.pb = R(WR_PB);
+    v.r0 = R(WR_R0); v.ep = R(WR_EP); v.sp = R(WR_SP); v.inv = R(WR_INV); v.tg = R(WR_TG); v.rog = R(WR_ROG);
+    v.mg = R(WR_MG);
+    for (int ig = 0; ig < P.ng; ++ig) v.yg[ig] = R(WR_YG + ig);
+    v.sw = W.src[pos]; v.ss = D == 3 ? W.src[np + pos] : -1; v.sb = W.src[2 * np + pos];
+}
+
+// the recurrent part: neighbour pressures, right-hand side, enthalpy,
+// temperature and pressure of one record; stores in record order only
+template <int D>
+__device__ __forceinline__ void wave_solve(const Prm &P, const Wave &W, const WaveIn &v, int pos, double a1dt,
+                                           double a2dt, int stage) {
+    const double pw = v.sw >= 0 ? __ldcg(W.pnew + v.sw) : v.pw;
+    const double pb = v.sb >= 0 ? __ldcg(W.pnew + v.sb) : v.pb;
+    double dpxyz = 0.0;
+    dpxyz = dpxyz + v.ax * (v.pe - pw);
+    if (D == 3) {
+        const double ps = v.ss >= 0 ? __ldcg(W.pnew + v.ss) : v.ps;
+        dpxyz = dpxyz + v.ay * (v.pn - ps);
+    } else {
+        dpxyz = dpxyz + 0.0;
+    }
+    dpxyz = dpxyz + v.az * (v.pt - pb);
+    const double r = v.r0 + v.ep * dpxyz;
+    const double siegtmp = stage == 1 ? v.sp + a1dt * r + a2dt * 0.0 : v.sp + a2dt * r;
+    const double sieg = siegtmp * v.inv;
+    double tg = v.tg, cg;
+    caloric_eosg(P, cg, tg, v.yg, sieg);
+    const double p = v.rog * tg * P.rgas / v.mg;
+    const size_t np = W.npos;
+    __stcg(W.pnew + pos, p);
+    W.rec[(size_t)WR_OR * np + pos] = r;
+    W.rec[(size_t)WR_OSIEG * np + pos] = sieg;
+    W.rec[(size_t)WR_OTG * np + pos] = tg;
+    W.rec[(size_t)WR_OCG * np + pos] = cg;
+}
+
+// every hyperplane of a stage in one cooperative launch over the records: a
+// grid-wide barrier separates the hyperplanes (all blocks are co-resident,
+// so it always completes) and the neighbour pressures of the previous
+// hyperplane are read past L1.  When the grid covers the widest hyperplane
+// (ONE) a thread holds at most one record per hyperplane and loads the next
+// one before the barrier, which leaves only the three neighbour pressures on
+// the critical path after it.
+template <int D, bool ONE>
+__global__ void __launch_bounds__(128) k_rk3_wave_rec(Prm P, Wave W, double dt, int stage) {
+    namespace cg = cooperative_groups;
+    cg::grid_group g = cg::this_grid();
+    const int nthr = gridDim.x * blockDim.x;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const double a1dt = (stage == 1 ? 1.0 : 0.25) * dt, a2dt = (stage == 1 ? 0.0 : 0.25) * dt;
+    if (ONE) {
+        WaveIn v;
+        int pos = W.start[0] + tid;
+        bool have = pos < W.start[1];
+        if (have) wave_load<D>(P, W, pos, v);
+        for (int q = 0; q < W.nplanes; ++q) {
+            if (have) wave_solve<D>(P, W, v, pos, a1dt, a2dt, stage);
+            if (q + 1 < W.nplanes) {
+                pos = W.start[q + 1] + tid;
+                have = pos < W.start[q + 2];
+                if (have) wave_load<D>(P, W, pos, v);
+            }
+            g.sync();
+        }
+    } else {
+        for (int q = 0; q < W.nplanes; ++q) {
+            const int end = W.start[q + 1];
+            for (int pos = W.start[q] + tid; pos < end; pos += nthr) {
+                WaveIn v;
+                wave_load<D>(P, W, pos, v);
+                wave_solve<D>(P, W, v, pos, a1dt, a2dt, stage);
+            }
+            g.sync();
+        }
+    }
+}
+
+// the wavefront's results to the cell arrays
+template <int D>
+__global__ void k_rk3_wave_post(Prm P, Fld F, RkF K, Wave W, int stage) {
+    int pos = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= W.npos) return;
+    const size_t np = W.npos, n = P.ncell;
+    const int c = W.order[pos], e0 = (D == 3 ? 4 : 3) * P.nph;
+    (stage == 1 ? K.k1 : K.k2)[(size_t)e0 * n + c] = W.rec[(size_t)WR_OR * np + pos];
+    F.sieg[c] = W.rec[(size_t)WR_OSIEG * np + pos];
+    F.tg[c] = W.rec[(size_t)WR_OTG * np + pos];
+    F.cg[c] = W.rec[(size_t)WR_OCG * np + pos];
+    F.p[c] = W.pnew[pos];
 }
 
 // stage 3 and the final combination rhs3 = init + dt (k1 + k2 + 4 k3) / 6
