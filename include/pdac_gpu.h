@@ -80,8 +80,8 @@ typedef struct pdac_cfg {
     double tref;
     int    gas_viscosity, part_viscosity, repulsive_model;
     int    iturb;               /* 0 none, 1 Smagorinsky sub-grid model      */
-    int    modturbo;            /* 1 static Smagorinsky (2 dynamic: 2D falls
-                                   back to 1, turbo.f:173-177)               */
+    int    modturbo;            /* 1 static Smagorinsky, 2 dynamic (Germano,
+                                   turbo.f:180-349; 2D falls back to 1)      */
     int    iss;                 /* 1 particle sub-grid stress (turbo.f:437)  */
     double cmut;                /* Smagorinsky constant                      */
     double gravx, gravy, gravz;
@@ -261,6 +261,29 @@ int pdac_gpu_sweep_log(pdac_ctx *ctx, double *out, long *n_inout);
 /* stream-ordered timing marks (slots 0..31) and the device time between two */
 int pdac_gpu_mark(pdac_ctx *ctx, int slot);
 int pdac_gpu_elapsed(pdac_ctx *ctx, int a, int b, double *ms);
+
+/* ---- ensembles of independent runs ------------------------------------ */
+/* No counterpart in the reference, which runs one domain per job (an
+ * ensemble there is many jobs).  A batch advances many contexts (members:
+ * any mix of grids, decks and time integrations, all on the current device)
+ * by one time step each, pdac_gpu_step(member, sweep, ...) on every member,
+ * with the members' kernels running concurrently on the device: a pool of
+ * nthreads host threads (<= 0: one per member) drives the members' own
+ * streams.  The batch does not own the members: create, upload and download
+ * them with the per-context calls, never while a batch step runs, and
+ * destroy the batch before them.  A member appears once.
+ * pdac_gpu_batch_step fills nit[m] and status[m] (either may be NULL) for
+ * every member, steps every member whatever the others return, and returns
+ * the first non-zero member status (its message in
+ * pdac_gpu_batch_last_error).  pdac_gpu_batch_elapsed gives the device time
+ * of the last batch step in ms, from its start on every member's stream to
+ * the end of the last member.                                            */
+typedef struct pdac_batch pdac_batch;
+int pdac_gpu_batch_create(pdac_ctx *const *members, int nmember, int nthreads, pdac_batch **out);
+int pdac_gpu_batch_step(pdac_batch *b, int sweep, int *nit, int *status);
+int pdac_gpu_batch_elapsed(pdac_batch *b, double *ms);
+const char *pdac_gpu_batch_last_error(const pdac_batch *b);
+int pdac_gpu_batch_destroy(pdac_batch *b);
 
 #ifdef __cplusplus
 }

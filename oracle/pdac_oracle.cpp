@@ -119,6 +119,7 @@ struct Oracle {
     vector<double> sink;
     vector<double> mf3, ef3, yfn;   // 3D momentum / enthalpy face fluxes, species y-fluxes
     vector<double> smag, mugt, kapgt, must;  // sub-grid model (turbo.f:10-14)
+    vector<double> scoeff;                   // dynamic coefficient cdyn of the last sgsg (modturbo = 2)
     vector<double> dgres;   // |dg|/conv at the last corrector visit (diagnostic)
     vector<double> vent_fact, vent_fact0;
     // padjust SAVE variables (iter.f:1005)
@@ -2135,7 +2136,7 @@ int pdac_oracle_get_array(void *h, const char *name, double *out, long *n_inout)
                {"rvgn", &o.rvgn}, {"rvsn", &o.rvsn}, {"rvg", &o.rvg}, {"rvs", &o.rvs}, {"appv", &o.appv},
                {"rgfn", &o.rgfn}, {"rsfn", &o.rsfn}, {"mf3", &o.mf3}, {"ef3", &o.ef3},
                {"gvisy", &o.gvisy}, {"pvisy", &o.pvisy}, {"hgfe", &o.hgfe}, {"hgft", &o.hgft},
-               {"hsfe", &o.hsfe}, {"hsft", &o.hsft}, {"smag", &o.smag}, {"mugt", &o.mugt}, {"kapgt", &o.kapgt},
+               {"hsfe", &o.hsfe}, {"hsft", &o.hsft}, {"smag", &o.smag}, {"scoeff", &o.scoeff}, {"mugt", &o.mugt}, {"kapgt", &o.kapgt},
                {"must", &o.must},
                // explicit-solver fields (explicit_solver.f:15-83)
                {"rgpstar", &o.rk.rgpS}, {"rlkstar", &o.rk.rlkS}, {"ugstar", &o.rk.ugS}, {"usstar", &o.rk.usS},

@@ -140,3 +140,19 @@ def small_3d_les(**kw):
 def small_2d_rk3_les(**kw):
     """small_2d_rk3 with the sub-grid models of small_2d_les."""
     return _les(small_2d_rk3(**kw))
+
+
+def _dynamic(deck):
+    deck.set("model", iturb=1, modturbo=2, iss=1)
+    return deck
+
+
+def small_3d_dyn(**kw):
+    """small_3d with the dynamic Smagorinsky model (modturbo = 2, turbo.f:180-349)
+    and the particle sub-grid stress."""
+    return _dynamic(small_3d(**kw))
+
+
+def small_3d_rk3_dyn(**kw):
+    """small_3d_rk3 with the sub-grid models of small_3d_dyn."""
+    return _dynamic(small_3d_rk3(**kw))

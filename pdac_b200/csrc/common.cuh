@@ -41,7 +41,7 @@ struct Prm {
     int d3;  // 1 for the 3D Cartesian path, 0 for 2D (x, z)
     int itc, muscl, lv, lm, pmodel, drag_model, icpc;
     int gas_viscosity, part_viscosity, repulsive_model, inmax;
-    int iturb, iss;  // sub-grid models (turbo.f)
+    int iturb, iss, modturbo;  // sub-grid models (turbo.f)
     int gas_type[PDAC_MAXG];
     double alpha, alphagrav, omega, delg, beta, flim, tref;
     double gravx, gravy, gravz, void_fraction;
@@ -73,6 +73,7 @@ struct Fld {
     double *yfe, *yfn, *yft;
     double *sink;
     double *smag, *mugt, *kapgt, *must;  // sub-grid model (turbo.f:10-14); must (ncell, ns)
+    double *dyn, *delt, *scoeff;         // dynamic model: per-cell work blocks, filter width, cdyn
     int *counters;  // [0] non-converged cells this sweep, [1] eos failures, [2] rls>1 cells, [3] boundary errors
 };
 

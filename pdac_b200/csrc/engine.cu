@@ -12,7 +12,9 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <condition_variable>
 #include <mutex>
+#include <thread>
 
 #include "../../include/pdac_gpu.h"
 #include "inner.cuh"
@@ -183,8 +185,8 @@ int validate(const pdac_cfg *c, std::string &why) {
     if (c->precision != PDAC_PREC_FP64) { why = "only PDAC_PREC_FP64 is built"; return 1; }
     if (c->time_integration != 0 && c->time_integration != 1) { why = "time_integration must be 0 or 1"; return 1; }
     if (c->iturb != 0 && c->iturb != 1) { why = "iturb must be 0 or 1 (iturb = 2 needs the topography's roughness)"; return 1; }
-    if (c->iturb == 1 && c->modturbo != 1 && !(c->modturbo == 2 && c->job_type == 2)) {
-        why = "modturbo must be 1 (the dynamic model, 2, is built only as its 2D fall-back to 1)";
+    if (c->iturb == 1 && c->modturbo != 1 && c->modturbo != 2) {
+        why = "modturbo must be 1 (static Smagorinsky) or 2 (dynamic; static in 2D, as turbo.f:180-185)";
         return 1;
     }
     if (c->iss != 0 && c->iss != 1) { why = "iss must be 0 or 1"; return 1; }
@@ -239,16 +241,18 @@ int setup_wave(pdac_ctx *ctx, const int *flag) {
         if (ctx->d3) src[(size_t)np + p] = pos_of[c - nx];
         src[2 * (size_t)np + p] = pos_of[c - nx * ny];
     }
-    const size_t ni = order.size() + src.size() + start.size();
+    const size_t ni = order.size() + src.size() + start.size() + pos_of.size();
     CK(cudaMalloc(&ctx->d_wave_idx, ni * sizeof(int)));
-    int *o = ctx->d_wave_idx, *s = o + order.size(), *st = s + src.size();
+    int *o = ctx->d_wave_idx, *s = o + order.size(), *st = s + src.size(), *po = st + start.size();
     CK(cudaMemcpy(o, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(s, src.data(), src.size() * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(st, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(po, pos_of.data(), pos_of.size() * sizeof(int), cudaMemcpyHostToDevice));
     const size_t nrec = (size_t)(pdac::WR_YG + ctx->ng) + 1;  // the fields and pnew
     CK(cudaMalloc(&ctx->d_wave_rec, nrec * std::max(np, 1) * sizeof(double)));
     pdac::Wave &W = ctx->W;
     W.order = o;
+    W.pos_of = po;
     W.src = s;
     W.start = st;
     W.rec = ctx->d_wave_rec;
@@ -309,7 +313,7 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     P.itc = cfg->itc; P.muscl = cfg->muscl; P.lv = cfg->lv; P.lm = cfg->lm; P.pmodel = cfg->pmodel;
     P.drag_model = cfg->drag_model; P.icpc = cfg->icpc; P.gas_viscosity = cfg->gas_viscosity;
     P.part_viscosity = cfg->part_viscosity; P.repulsive_model = cfg->repulsive_model; P.inmax = cfg->inmax;
-    P.iturb = cfg->iturb; P.iss = cfg->iss;
+    P.iturb = cfg->iturb; P.iss = cfg->iss; P.modturbo = cfg->modturbo;
     for (int ig = 0; ig < ng; ++ig) P.gas_type[ig] = cfg->gas_type[ig];
     P.alpha = cfg->alpha; P.alphagrav = cfg->alphagrav; P.omega = cfg->omega; P.delg = cfg->delg;
     P.beta = cfg->beta; P.flim = cfg->flim; P.tref = cfg->tref;
@@ -405,6 +409,7 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     // right-hand-side rows: mass, momentum per axis and enthalpy of each phase
     int t1 = ctx->ti == 1 ? 1 : 0, neq = (ctx->d3 ? 5 : 4) * ctx->nph;
     int lt = cfg->iturb >= 1 ? 1 : 0, ls = cfg->iss >= 1 ? 1 : 0;  // sub-grid model fields
+    int ld = lt && ctx->d3 && cfg->modturbo == 2 ? 1 : 0;              // the dynamic model's
     RkF &K = ctx->K;
     std::vector<Slot> slots = {
         {"p", &F.p, 1}, {"ep", &F.ep, 1}, {"rog", &F.rog, 1}, {"rgp", &F.rgp, 1}, {"tg", &F.tg, 1},
@@ -434,7 +439,8 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
         {"vsn", &K.vsn, ns * t1 * d3}, {"wsn", &K.wsn, ns * t1}, {"hv", &K.hv, ns * t1},
         {"k1", &K.k1, neq * t1}, {"k2", &K.k2, neq * t1}, {"xrgp", &K.xrgp, t1}, {"xrlk", &K.xrlk, ns * t1},
         {"xep", &K.xep, t1}, {"xug", &K.xug, t1}, {"xvg", &K.xvg, t1 * d3}, {"xwg", &K.xwg, t1},
-        {"smag", &F.smag, lt}, {"mugt", &F.mugt, lt}, {"kapgt", &F.kapgt, lt}, {"must", &F.must, ns * ls}};
+        {"smag", &F.smag, lt}, {"mugt", &F.mugt, lt}, {"kapgt", &F.kapgt, lt}, {"must", &F.must, ns * ls},
+        {"sgsdyn", &F.dyn, pdac::DY_N * ld}, {"delt", &F.delt, ld}, {"scoeff", &F.scoeff, ld}};
     // each field starts on a 256-byte boundary
     size_t stride = ((size_t)n + 31) / 32 * 32;
     size_t total = 0;
@@ -478,6 +484,15 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
             }
         }
         CK(cudaMemcpy(F.smag, smag.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    if (ld) {
+        // the dynamic model's filter width, (dz dy dx)^(1/3) (turbo.f:318)
+        std::vector<double> delt(n);
+        for (int c = 0; c < n; ++c) {
+            int i = c % nx + 1, j = (c / nx) % ny + 1, k = c / (nx * ny) + 1;
+            delt[c] = std::pow(dz[k] * dy[j] * dx[i], 1.0 / 3.0);
+        }
+        CK(cudaMemcpy(F.delt, delt.data(), n * sizeof(double), cudaMemcpyHostToDevice));
     }
     int nq = 1 + ns + ng;
     CK(cudaMalloc(&ctx->d_partial, (size_t)nq * 1024 * sizeof(double)));
@@ -991,9 +1006,15 @@ int pdac_gpu_initialize_fieldn(pdac_ctx *ctx) {
 int pdac_gpu_sgsg(pdac_ctx *ctx) {
     if (!ctx) return PDAC_ERR_ARG;
     if (!ctx->P.iturb) return PDAC_OK;
-    if (ctx->d3) pdac::k_sgsg<3><<<blocks(ctx->ncell), TPB, 0, ctx->stream>>>(ctx->P, ctx->F);
-    else pdac::k_sgsg<2><<<blocks(ctx->ncell), TPB, 0, ctx->stream>>>(ctx->P, ctx->F);
-    ctx->launches++;
+    if (ctx->F.dyn) {
+        pdac::k_sgsg_dyn1<<<blocks(ctx->ncell), TPB, 0, ctx->stream>>>(ctx->P, ctx->F);
+        pdac::k_sgsg_dyn2<<<blocks(ctx->ncell), TPB, 0, ctx->stream>>>(ctx->P, ctx->F);
+        ctx->launches += 2;
+    } else {
+        if (ctx->d3) pdac::k_sgsg<3><<<blocks(ctx->ncell), TPB, 0, ctx->stream>>>(ctx->P, ctx->F);
+        else pdac::k_sgsg<2><<<blocks(ctx->ncell), TPB, 0, ctx->stream>>>(ctx->P, ctx->F);
+        ctx->launches++;
+    }
     CK(cudaGetLastError());
     return PDAC_OK;
 }
@@ -1066,12 +1087,12 @@ static long long enqueue_explicit(pdac_ctx *ctx, double dt, cudaStream_t st, boo
             lc.attrs = at;
             lc.numAttrs = 1;
             if (ctx->d3) {
-                pdac::k_rk3_wave_pre<3><<<rb, TPB, 0, st>>>(P, F, K, W, dt, stage);
+                pdac::k_rk3_wave_pre<3><<<blocks(n), TPB, 0, st>>>(P, F, K, W, dt, stage);
                 if (ctx->wave_one) cudaLaunchKernelEx(&lc, pdac::k_rk3_wave_rec<3, true>, P, W, dt, stage);
                 else cudaLaunchKernelEx(&lc, pdac::k_rk3_wave_rec<3, false>, P, W, dt, stage);
                 pdac::k_rk3_wave_post<3><<<rb, TPB, 0, st>>>(P, F, K, W, stage);
             } else {
-                pdac::k_rk3_wave_pre<2><<<rb, TPB, 0, st>>>(P, F, K, W, dt, stage);
+                pdac::k_rk3_wave_pre<2><<<blocks(n), TPB, 0, st>>>(P, F, K, W, dt, stage);
                 if (ctx->wave_one) cudaLaunchKernelEx(&lc, pdac::k_rk3_wave_rec<2, true>, P, W, dt, stage);
                 else cudaLaunchKernelEx(&lc, pdac::k_rk3_wave_rec<2, false>, P, W, dt, stage);
                 pdac::k_rk3_wave_post<2><<<rb, TPB, 0, st>>>(P, F, K, W, stage);
@@ -1507,6 +1528,164 @@ int pdac_gpu_elapsed(pdac_ctx *ctx, int a, int b, double *ms) {
     float t = 0;
     CK(cudaEventElapsedTime(&t, ctx->user_ev[a], ctx->user_ev[b]));
     *ms = t;
+    return PDAC_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// ensembles: many independent contexts advanced together
+// ---------------------------------------------------------------------------
+// Each member keeps its own stream, graphs and host synchronisation points
+// (the sweep count of iter, the caloric-failure count of ftem); a pool of
+// host threads runs pdac_gpu_step on the members, so the members' kernels
+// run concurrently on the device while one member's host waits for its own
+// stream.  Small 2D members fill a few percent of the SMs each; run side by
+// side they fill the device.  Members are spread over the threads by the
+// longest-processing-time rule on their cell counts.
+struct pdac_batch {
+    std::vector<pdac_ctx *> m;
+    std::vector<std::vector<int>> work;  // members of each thread
+    std::vector<std::thread> th;
+    std::mutex mu;
+    std::condition_variable go, done;
+    long gen = 0;
+    int pending = 0, sweep = 0, dev = 0;
+    bool quit = false;
+    std::vector<int> nit, status;
+    cudaStream_t lead = nullptr;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    std::vector<cudaEvent_t> fin;
+    double last_ms = 0.0;
+    std::string err;
+};
+
+static void batch_worker(pdac_batch *b, int w) {
+    cudaSetDevice(b->dev);
+    long seen = 0;
+    for (;;) {
+        {
+            std::unique_lock<std::mutex> lk(b->mu);
+            b->go.wait(lk, [&] { return b->quit || b->gen != seen; });
+            if (b->quit) return;
+            seen = b->gen;
+        }
+        for (int i : b->work[w]) {
+            pdac_ctx *c = b->m[i];
+            int nit = 0, s = PDAC_OK;
+            if (cudaStreamWaitEvent(c->stream, b->t0, 0) != cudaSuccess) s = PDAC_ERR_CUDA;
+            if (!s) s = pdac_gpu_step(c, b->sweep, &nit);
+            // the completion mark is recorded whatever the status, so that
+            // the lead stream's wait below always refers to this step
+            cudaEventRecord(b->fin[i], c->stream);
+            b->nit[i] = nit;
+            b->status[i] = s;
+        }
+        std::lock_guard<std::mutex> lk(b->mu);
+        if (--b->pending == 0) b->done.notify_all();
+    }
+}
+
+static void batch_free(pdac_batch *b) {
+    {
+        std::lock_guard<std::mutex> lk(b->mu);
+        b->quit = true;
+    }
+    b->go.notify_all();
+    for (auto &t : b->th) t.join();
+    for (auto e : b->fin) if (e) cudaEventDestroy(e);
+    if (b->t0) cudaEventDestroy(b->t0);
+    if (b->t1) cudaEventDestroy(b->t1);
+    if (b->lead) cudaStreamDestroy(b->lead);
+    delete b;
+}
+
+extern "C" {
+
+int pdac_gpu_batch_create(pdac_ctx *const *members, int nmember, int nthreads, pdac_batch **out) {
+    if (!members || !out || nmember < 1) return PDAC_ERR_ARG;
+    *out = nullptr;
+    for (int i = 0; i < nmember; ++i) {
+        if (!members[i]) return PDAC_ERR_ARG;
+        for (int j = 0; j < i; ++j)
+            if (members[j] == members[i]) return PDAC_ERR_ARG;  // one context stepped twice at once would race
+    }
+    int nt = nthreads > 0 ? std::min(nthreads, nmember) : nmember;
+    pdac_batch *b = new pdac_batch();
+    b->m.assign(members, members + nmember);
+    b->nit.assign(nmember, 0);
+    b->status.assign(nmember, 0);
+    b->fin.assign(nmember, nullptr);
+    if (cudaGetDevice(&b->dev) != cudaSuccess || cudaStreamCreateWithFlags(&b->lead, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->t0) != cudaSuccess || cudaEventCreate(&b->t1) != cudaSuccess) {
+        batch_free(b);
+        return PDAC_ERR_CUDA;
+    }
+    for (auto &e : b->fin)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+            batch_free(b);
+            return PDAC_ERR_CUDA;
+        }
+    // longest processing time first: each member, largest first, to the
+    // thread with the fewest cells so far
+    std::vector<int> order(nmember);
+    for (int i = 0; i < nmember; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return b->m[a]->ncell > b->m[c]->ncell; });
+    std::vector<long> load(nt, 0);
+    b->work.assign(nt, {});
+    for (int i : order) {
+        int w = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        b->work[w].push_back(i);
+        load[w] += b->m[i]->ncell;
+    }
+    for (int w = 0; w < nt; ++w) b->th.emplace_back(batch_worker, b, w);
+    *out = b;
+    return PDAC_OK;
+}
+
+int pdac_gpu_batch_step(pdac_batch *b, int sweep, int *nit, int *status) {
+    if (!b) return PDAC_ERR_ARG;
+    if (cudaEventRecord(b->t0, b->lead) != cudaSuccess) return PDAC_ERR_CUDA;
+    {
+        std::lock_guard<std::mutex> lk(b->mu);
+        b->sweep = sweep;
+        b->pending = (int)b->th.size();
+        b->gen++;
+    }
+    b->go.notify_all();
+    {
+        std::unique_lock<std::mutex> lk(b->mu);
+        b->done.wait(lk, [&] { return b->pending == 0; });
+    }
+    for (auto e : b->fin)
+        if (cudaStreamWaitEvent(b->lead, e, 0) != cudaSuccess) return PDAC_ERR_CUDA;
+    if (cudaEventRecord(b->t1, b->lead) != cudaSuccess || cudaEventSynchronize(b->t1) != cudaSuccess) return PDAC_ERR_CUDA;
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, b->t0, b->t1) != cudaSuccess) return PDAC_ERR_CUDA;
+    b->last_ms = ms;
+    int first = PDAC_OK;
+    for (size_t i = 0; i < b->m.size(); ++i) {
+        if (nit) nit[i] = b->nit[i];
+        if (status) status[i] = b->status[i];
+        if (b->status[i] && !first) {
+            first = b->status[i];
+            b->err = "member " + std::to_string(i) + ": " + b->m[i]->err;
+        }
+    }
+    return first;
+}
+
+int pdac_gpu_batch_elapsed(pdac_batch *b, double *ms) {
+    if (!b || !ms) return PDAC_ERR_ARG;
+    *ms = b->last_ms;
+    return PDAC_OK;
+}
+
+const char *pdac_gpu_batch_last_error(const pdac_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+int pdac_gpu_batch_destroy(pdac_batch *b) {
+    if (!b) return PDAC_ERR_ARG;
+    batch_free(b);
     return PDAC_OK;
 }
 

@@ -1,5 +1,6 @@
 // les.cuh -- the sub-grid turbulence model of turbo.f on the device
-// (iturb = 1, static Smagorinsky; iss = 1 particle sub-grid stress).
+// (iturb = 1: static Smagorinsky, modturbo = 1, or the dynamic model in 3D,
+// modturbo = 2; iss = 1 particle sub-grid stress).
 //
 // smag = (cmut delta)^2 (x anis in 3D) is fixed per cell at set-up on the
 // host (turbulence_setup, turbo.f:42-108).  Each step k_sgsg sets the
@@ -39,9 +40,12 @@ __device__ __forceinline__ double strain2d(const Prm &P, const double *u, const 
     return sqrt(2.0 * (sr1 * sr1 + sr2 * sr2 + 2.0 * (sr12 * sr12) + d33 * d33));
 }
 
-// strain3d, turbo.f:519-621
-__device__ __forceinline__ double strain3d(const Prm &P, const double *u, const double *v, const double *w,
-                                           const Raw3 &R, int i, int j, int k) {
+// strain3d, turbo.f:519-621: the modulus and the six components
+struct Strain {
+    double mod, s11, s12, s22, s13, s23, s33;
+};
+__device__ __forceinline__ Strain strain3d_c(const Prm &P, const double *u, const double *v, const double *w,
+                                             const Raw3 &R, int i, int j, int k) {
     const double *dx = P.dx, *dy = P.dy, *dz = P.dz;
     const int c = R.c;
     double dxp = dx[i] + dx[i + 1], dxm = dx[i] + dx[i - 1];
@@ -59,8 +63,131 @@ __device__ __forceinline__ double strain3d(const Prm &P, const double *u, const 
     double sr12 = (uyp - uym) / (dyp + dym) + (vxp - vxm) / (dxp + dxm);
     double sr13 = (uzp - uzm) / (dzp + dzm) + (wxp - wxm) / (dxp + dxm);
     double sr23 = (vzp - vzm) / (dzp + dzm) + (wyp - wym) / (dyp + dym);
-    return sqrt(2.0 * (sr11 * sr11 + sr22 * sr22 + sr33 * sr33 + 2.0 * (sr12 * sr12) + 2.0 * (sr13 * sr13) +
-                       2.0 * (sr23 * sr23)));
+    double mod = sqrt(2.0 * (sr11 * sr11 + sr22 * sr22 + sr33 * sr33 + 2.0 * (sr12 * sr12) + 2.0 * (sr13 * sr13) +
+                             2.0 * (sr23 * sr23)));
+    return {mod, sr11, sr12, sr22, sr13, sr23, sr33};
+}
+__device__ __forceinline__ double strain3d(const Prm &P, const double *u, const double *v, const double *w,
+                                           const Raw3 &R, int i, int j, int k) {
+    return strain3d_c(P, u, v, w, R, i, j, k).mod;
+}
+
+// ---- dynamic model (modturbo = 2, 3D), turbo.f:180-349 ---------------------
+// Seven-point values of first_rnb (subscr.f:2259-2289): the centre from the
+// index given, the six neighbours from the current cell's raw indices.
+struct St7 {
+    double c, e, w, n, s, t, b;
+};
+__device__ __forceinline__ St7 first_rnb7(const double *a, int c0, const Raw3 &R) {
+    return {a[c0], a[R.e], a[R.w], a[R.n], a[R.s], a[R.t], a[R.b]};
+}
+__device__ __forceinline__ St7 st_half_sum(const St7 &p, const St7 &q) {
+    return {0.5 * (p.c + q.c), 0.5 * (p.e + q.e), 0.5 * (p.w + q.w), 0.5 * (p.n + q.n), 0.5 * (p.s + q.s),
+            0.5 * (p.t + q.t), 0.5 * (p.b + q.b)};
+}
+__device__ __forceinline__ St7 st_prod(const St7 &p, const St7 &q) {
+    return {p.c * q.c, p.e * q.e, p.w * q.w, p.n * q.n, p.s * q.s, p.t * q.t, p.b * q.b};
+}
+// filter_3d (turbo.f:436-474): the mean of the 1-2-1 filters along x, y, z
+__device__ __forceinline__ double filter_3d(const St7 &q) {
+    double fx = 0.25 * (q.w + 2.0 * q.c + q.e);
+    double fy = 0.25 * (q.s + 2.0 * q.c + q.n);
+    double fz = 0.25 * (q.b + 2.0 * q.c + q.t);
+    return 1.0 / 3.0 * (fx + fy + fz);
+}
+// the 16 per-cell blocks of F.dyn: |S|, |S| S_ij (6), the test-filtered
+// velocities (3) and their filtered products (uu, vv, ww, uv, uw, vw)
+enum { DY_MOD, DY_P11, DY_P12, DY_P22, DY_P13, DY_P23, DY_P33, DY_FU, DY_FV, DY_FW, DY_FUU, DY_FVV, DY_FWW,
+       DY_FUV, DY_FUW, DY_FVW, DY_N };
+
+// pass 1 (turbo.f:199-233, vel_hat turbo.f:385-433), every cell: fluid
+// cells get their strain products and filtered velocities, others zeros
+__global__ void k_sgsg_dyn1(Prm P, Fld F) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= P.ncell) return;
+    const size_t n = P.ncell;
+    double *d = F.dyn;
+    if (!fluid(P, c)) {
+        for (int q = 0; q < DY_N; ++q) d[q * n + c] = 0.0;
+        return;
+    }
+    int i, j, k;
+    ijk_of(P, c, i, j, k);
+    Raw3 R;
+    raw3(P, i, j, k, R);
+    Strain sr = strain3d_c(P, F.ug, F.vg, F.wg, R, i, j, k);
+    d[DY_MOD * n + c] = sr.mod;
+    d[DY_P11 * n + c] = sr.mod * sr.s11;
+    d[DY_P12 * n + c] = sr.mod * sr.s12;
+    d[DY_P22 * n + c] = sr.mod * sr.s22;
+    d[DY_P13 * n + c] = sr.mod * sr.s13;
+    d[DY_P23 * n + c] = sr.mod * sr.s23;
+    d[DY_P33 * n + c] = sr.mod * sr.s33;
+    const St7 u = st_half_sum(first_rnb7(F.ug, c, R), first_rnb7(F.ug, R.w, R));
+    const St7 v = st_half_sum(first_rnb7(F.vg, c, R), first_rnb7(F.vg, R.s, R));
+    const St7 w = st_half_sum(first_rnb7(F.wg, c, R), first_rnb7(F.wg, R.b, R));
+    d[DY_FU * n + c] = filter_3d(u);
+    d[DY_FV * n + c] = filter_3d(v);
+    d[DY_FW * n + c] = filter_3d(w);
+    d[DY_FUU * n + c] = filter_3d(st_prod(u, u));
+    d[DY_FVV * n + c] = filter_3d(st_prod(v, v));
+    d[DY_FWW * n + c] = filter_3d(st_prod(w, w));
+    d[DY_FUV * n + c] = filter_3d(st_prod(u, v));
+    d[DY_FUW * n + c] = filter_3d(st_prod(u, w));
+    d[DY_FVW * n + c] = filter_3d(st_prod(v, w));
+}
+
+// pass 2 (turbo.f:255-349), every cell: the Germano coefficient cdyn from
+// the Leonard stress L of the filtered velocities and M = 4 |S^| S^ - (|S| S)^,
+// smag = cdyn delta^2, then the viscosity and conductivity as the static
+// model; delta = (dx dy dz)^(1/3) per cell is set up on the host
+__global__ void k_sgsg_dyn2(Prm P, Fld F) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= P.ncell) return;
+    if (!fluid(P, c)) {
+        F.mugt[c] = 0.0;
+        F.kapgt[c] = 0.0;
+        return;
+    }
+    const size_t n = P.ncell;
+    const double *d = F.dyn;
+    int i, j, k;
+    ijk_of(P, c, i, j, k);
+    Raw3 R;
+    raw3(P, i, j, k, R);
+    const double fu = d[DY_FU * n + c], fv = d[DY_FV * n + c], fw = d[DY_FW * n + c];
+    Strain fs = strain3d_c(P, d + DY_FU * n, d + DY_FV * n, d + DY_FW * n, R, i, j, k);
+    double fp11 = filter_3d(first_rnb7(d + DY_P11 * n, c, R));
+    double fp12 = filter_3d(first_rnb7(d + DY_P12 * n, c, R));
+    double fp22 = filter_3d(first_rnb7(d + DY_P22 * n, c, R));
+    double fp13 = filter_3d(first_rnb7(d + DY_P13 * n, c, R));
+    double fp23 = filter_3d(first_rnb7(d + DY_P23 * n, c, R));
+    double fp33 = filter_3d(first_rnb7(d + DY_P33 * n, c, R));
+    double l11 = fu * fu - d[DY_FUU * n + c];
+    double l12 = fu * fv - d[DY_FUV * n + c];
+    double l22 = fv * fv - d[DY_FVV * n + c];
+    double l13 = fu * fw - d[DY_FUW * n + c];
+    double l23 = fv * fw - d[DY_FVW * n + c];
+    double l33 = fw * fw - d[DY_FWW * n + c];
+    double m11 = (4.0 * fs.mod * fs.s11 - fp11);
+    double m12 = (4.0 * fs.mod * fs.s12 - fp12);
+    double m22 = (4.0 * fs.mod * fs.s22 - fp22);
+    double m13 = (4.0 * fs.mod * fs.s13 - fp13);
+    double m23 = (4.0 * fs.mod * fs.s23 - fp23);
+    double m33 = (4.0 * fs.mod * fs.s33 - fp33);
+    const double delt = F.delt[c];
+    double num = l11 * m11 + l22 * m22 + l33 * m33 + 2.0 * l12 * m12 + 2.0 * l13 * m13 + 2.0 * l23 * m23;
+    double den = (delt * delt) * (m11 * m11 + m22 * m22 + m33 * m33 + 2.0 * (m12 * m12) + 2.0 * (m13 * m13) +
+                                  2.0 * (m23 * m23));
+    double cdyn = den == 0.0 ? 0.0 : 0.5 * num / den;
+    const double smag = cdyn * (delt * delt);
+    F.smag[c] = smag;
+    F.scoeff[c] = cdyn;
+    const double pranumt = 0.5;
+    double mugt = F.rog[c] * smag * d[DY_MOD * n + c];
+    if (mugt < 0.0) mugt = 0.0;
+    F.mugt[c] = mugt;
+    F.kapgt[c] = mugt * F.cg[c] / pranumt;
 }
 
 // sgsg (modturbo = 1, and the 2D fall-back of modturbo = 2), every cell

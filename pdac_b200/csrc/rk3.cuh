@@ -623,6 +623,7 @@ __global__ void k_rk3_wave(Prm P, Fld F, RkF K, double dt, int stage, int d, int
 // order are those of rhs_gas_enth and k_rk3_wave.
 struct Wave {
     const int *order;   // record position -> cell
+    const int *pos_of;  // cell -> record position, -1 for cells without a record
     const int *src;     // [3][npos]: record of the W / S / B neighbour when it is a fluid cell, else -1
     const int *start;   // hyperplane dmin + q holds records start[q] .. start[q + 1] - 1
     double *rec;        // [WR_YG + ng][npos]
@@ -635,12 +636,16 @@ enum { WR_OR, WR_OSIEG, WR_OTG, WR_OCG, WR_AX, WR_AY, WR_AZ, WR_PE, WR_PN, WR_PT
        WR_SP, WR_INV, WR_TG, WR_ROG, WR_MG, WR_YG };
 
 // the non-recurrent part of every record, then the commit of the values
-// k_rk3_stage parked (nothing of this stage reads the old ones afterwards)
+// k_rk3_stage parked (nothing of this stage reads the old ones afterwards).
+// One thread per cell in cell order, so that the reads coalesce; the record
+// stores scatter, but the records of one hyperplane's neighbouring cells
+// (i - 1, j + 1, k) are written a few rows apart in time and meet in L2.
 template <int D>
 __global__ void k_rk3_wave_pre(Prm P, Fld F, RkF K, Wave W, double dt, int stage) {
-    int pos = blockIdx.x * blockDim.x + threadIdx.x;
-    if (pos >= W.npos) return;
-    const int c = W.order[pos];
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= P.ncell) return;
+    const int pos = W.pos_of[c];
+    if (pos < 0) return;
     Cell<D> q;
     cell_of<D>(P, c, q);
     const size_t n = P.ncell, np = W.npos;

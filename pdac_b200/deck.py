@@ -345,8 +345,6 @@ class Deck:
         bad = []
         if self["iturb"] not in (0, 1):
             bad.append("iturb=2 (sub-grid model with ground roughness, needs topography)")
-        if self["iturb"] == 1 and self["modturbo"] == 2 and self.is3d:
-            bad.append("modturbo=2 (dynamic Smagorinsky model) in 3D")
         if self["iturb"] == 1 and self["modturbo"] not in (1, 2):
             bad.append("modturbo other than 1 or 2")
         if self["iss"] not in (0, 1):

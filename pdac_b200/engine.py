@@ -70,7 +70,8 @@ EXPORTED = (
     "pdac_gpu_get_array", "pdac_gpu_mass_totals", "pdac_gpu_phase_times", "pdac_gpu_stats",
     "pdac_gpu_reset_stats", "pdac_gpu_mark", "pdac_gpu_elapsed",
     "pdac_gpu_write_restart", "pdac_gpu_read_restart", "pdac_gpu_write_output", "pdac_gpu_mass_residuals",
-    "pdac_gpu_append_mass_check",
+    "pdac_gpu_append_mass_check", "pdac_gpu_batch_create", "pdac_gpu_batch_step", "pdac_gpu_batch_elapsed",
+    "pdac_gpu_batch_last_error", "pdac_gpu_batch_destroy",
 )
 
 

@@ -94,7 +94,7 @@ def test_unsupported_options_are_rejected():
     with pytest.raises(ValueError, match="iturb"):
         Case(d)
     d = configs.plume_3d(nx=8, ny=8, nz=8)
-    d.set("model", iturb=1, modturbo=2)
+    d.set("model", iturb=1, modturbo=3)
     with pytest.raises(ValueError, match="modturbo"):
         Case(d)
 
@@ -104,6 +104,9 @@ def test_sub_grid_model_reaches_the_configuration():
     d.set("model", iturb=1, iss=1, cmut=0.2)
     cfg = Case(d).cfg()
     assert (cfg.iturb, cfg.modturbo, cfg.iss, cfg.cmut) == (1, 1, 1, 0.2)
+    d = configs.plume_3d(nx=8, ny=8, nz=8)
+    d.set("model", iturb=1, modturbo=2)
+    assert Case(d).cfg().modturbo == 2
 
 
 def test_explicit_solver_selection():

@@ -1,6 +1,7 @@
 """Parity of the sub-grid turbulence model (turbo.f: iturb = 1 static
-Smagorinsky, iss = 1 particle sub-grid stress) on the GPU with the CPU
-oracle, with both time integrations.
+Smagorinsky, the dynamic model in 3D with modturbo = 2, iss = 1 particle
+sub-grid stress) on the GPU with the CPU oracle, with both time
+integrations.
 
 Tolerances as in the other parity tests: 1e-12 (relative L-infinity) for
 the explicit passes (sgsg / sgss, tilde), 1e-9 for iter and whole steps.
@@ -44,31 +45,39 @@ def _state(case, eng, ora, tol, where):
     assert not bad, f"{where}: {bad}"
 
 
-@pytest.mark.parametrize("builder", ["small_2d_les", "small_3d_les"])
+@pytest.mark.parametrize("builder", ["small_2d_les", "small_3d_les", "small_3d_dyn"])
 def test_calls_semi_implicit_les(builder):
     case, eng, ora = _pair(builder)
     dt = case.deck["dt"]
+    dynamic = case.deck["modturbo"] == 2
     _arrays(eng, ora, ["smag"], 0.0, "turbulence_setup")
     for sweep in (1, 2, 3):
         eng.boundary(sweep); ora.boundary(sweep)
         eng.fieldn(); ora.fieldn()
         eng.sgsg(); eng.sgss(); ora.sgs()
-        _arrays(eng, ora, ["mugt", "kapgt", "must"], TOL_EXPLICIT, f"sgsg/sgss {sweep}")
+        # the dynamic coefficient is a ratio of differences of filtered
+        # fields: after the first step it carries the corrector's round-off
+        # (within the step tolerance) amplified, so it is held to the step
+        # tolerance there and to the explicit one on identical inputs
+        tol = TOL_STEP if dynamic and sweep > 1 else TOL_EXPLICIT
+        _arrays(eng, ora, ["mugt", "kapgt", "must"] + (["smag", "scoeff"] if dynamic else []), tol,
+                f"sgsg/sgss {sweep}")
         eng.tilde(dt); ora.tilde(dt)
-        _arrays(eng, ora, ["mugt", "must", "appu", "appw"], TOL_EXPLICIT, f"tilde {sweep}")
-        _arrays(eng, ora, ["rug", "rwg", "rus", "rws"], TOL_EXPLICIT, f"tilde {sweep}")
+        _arrays(eng, ora, ["mugt", "must", "appu", "appw"], tol, f"tilde {sweep}")
+        _arrays(eng, ora, ["rug", "rwg", "rus", "rws"], tol, f"tilde {sweep}")
         n1 = eng.iter(dt); n2 = ora.iter(dt)
         assert n1 == n2, f"outer sweeps differ: gpu {n1} oracle {n2}"
         _state(case, eng, ora, TOL_STEP, f"iter {sweep}")
         eng.ygas(dt); ora.ygas(dt)
         eng.htilde(dt); ora.htilde(dt)
-        _arrays(eng, ora, ["kapgt"], TOL_EXPLICIT, f"htilde {sweep}")
+        _arrays(eng, ora, ["kapgt"], tol, f"htilde {sweep}")
         _arrays(eng, ora, ["rhg", "rhs"], TOL_STEP, f"htilde {sweep}")
         eng.ftem(dt); ora.ftem(dt)
         _state(case, eng, ora, TOL_STEP, f"ftem {sweep}")
 
 
-@pytest.mark.parametrize("builder", ["small_2d_les", "small_3d_les", "small_2d_rk3_les"])
+@pytest.mark.parametrize("builder", ["small_2d_les", "small_3d_les", "small_2d_rk3_les", "small_3d_dyn",
+                                     "small_3d_rk3_dyn"])
 def test_steps_les(builder):
     case, eng, ora = _pair(builder)
     for s in range(1, 7):
