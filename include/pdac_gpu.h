@@ -102,6 +102,15 @@ typedef struct pdac_cfg {
     /* &inlet: vent velocity fluctuations (vent.f:902-936) */
     int    irand;
 
+    /* &model isink, rprox, rdist and &mesh center_x, center_y: the particle
+     * sink at the ground (sink.f:46-121): with isink > 0 every fluid cell
+     * above a wall takes out the downward particle flux of its cell centre
+     * when rprox < distance from (center_x, center_y) < rdist, and the mass
+     * taken out accumulates per ground column (massl)                      */
+    int    isink;
+    double rprox, rdist;
+    double center_x, center_y;
+
     int    precision;               /* PDAC_PREC_FP64 / PDAC_PREC_MIXED      */
 
     /* mesh metric and flags (read at create) */
@@ -224,6 +233,13 @@ int pdac_gpu_mass_residuals(pdac_ctx *ctx, int nswp, double dt, double *out, int
 /* the same values appended to path as one pdac.chm line,
  * FORMAT(I8,15(G30.20E3)) (residuals.f:123-127)                           */
 int pdac_gpu_append_mass_check(pdac_ctx *ctx, const char *path, int nswp, double dt);
+/* print_mass_loss (sink.f:123-167, called at prog.f:355 before outp as
+ * massl.NNNN and at prog.f:386 after tapewr as massl.res): the mass each
+ * ground column has lost to the sink, formatted as the reference writes it;
+ * read_mass_loss (sink.f:168-207, setup.f:147): such a file's values, added
+ * back at each column's next sink update.  Both need isink > 0.           */
+int pdac_gpu_write_mass_loss(pdac_ctx *ctx, const char *path);
+int pdac_gpu_read_mass_loss(pdac_ctx *ctx, const char *path);
 
 /* vent fluctuation factors for the next boundary call, one per vent cell in
  * cfg->vent_ijk order (vent.f:824-873 random_switch draws them in 3D).     */

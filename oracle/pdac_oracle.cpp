@@ -117,6 +117,11 @@ struct Oracle {
     vector<double> rgfe, rgfn, rgft, rsfe, rsfn, rsft, conv, abeta;
     vector<double> egfe, egft, esfe, esft, hgfe, hgft, hsfe, hsft, yfe, yft;
     vector<double> sink;
+    // the ground sink (sink.f): cell-centre coordinates x(i), y(j) of
+    // grid.f:286-298 (1-based), the mass taken out per ground column and
+    // solid (massl, ntr x ns with ntr = nx in 2D, nx ny in 3D) and the
+    // values a restart adds back at each column's first update (mass_loss)
+    vector<double> xc, yc, massl, mass_loss;
     vector<double> mf3, ef3, yfn;   // 3D momentum / enthalpy face fluxes, species y-fluxes
     vector<double> smag, mugt, kapgt, must;  // sub-grid model (turbo.f:10-14)
     vector<double> scoeff;                   // dynamic coefficient cdyn of the last sgsg (modturbo = 2)
@@ -1725,9 +1730,55 @@ void zerograd(Oracle &o, int n2, int n1) {
     o.p[n2] = o.p[n1];
 }
 
+// ---------------------------------------------------------------------------
+// ground sink, sink.f:22-121
+// ---------------------------------------------------------------------------
+// allocate_sink (sink.f:22-43) and the cell-centre coordinates (grid.f:286-298)
+void sink_setup(Oracle &o) {
+    int ntr = o.d3 ? o.nx * o.ny : o.nx;
+    o.massl.assign((size_t)ntr * o.ns, 0.0);
+    o.mass_loss.assign((size_t)ntr * o.ns, 0.0);
+    o.xc.assign(o.nx + 1, 0.0);
+    o.yc.assign(o.ny + 1, 0.0);
+    double xb = 0.0;
+    o.xc[1] = -0.5 * o.dx[1] + xb;
+    for (int i = 2; i <= o.nx; ++i) {
+        xb = (xb + o.dx[i]);
+        o.xc[i] = (xb - 0.5 * o.dx[i]);
+    }
+    double yb = 0.0;
+    o.yc[1] = -0.5 * o.dy[1] + yb;  // dy = 0 in 2D: y(1) = 0
+    for (int j = 2; j <= o.ny; ++j) {
+        yb = yb + o.dy[j];
+        o.yc[j] = (yb - 0.5 * o.dy[j]);
+    }
+}
+
+// sink_update (sink.f:46-121) of fluid cell c above a wall or filled cell:
+// the downward flux rlk min(0, ws) / dz of the cell centre inside the ring
+// rprox < r < rdist, and its mass over the step into the column's massl
+void sink_update(Oracle &o, int c, int is) {
+    int i, j, k;
+    o.ijk_of(c, i, j, k);
+    double rsft_up = o.S(o.rlk, c, is);
+    double wst = std::min(0.0, o.S(o.ws, c, is));  // wsink, interp.f:811
+    double cx = o.xc[i] - o.cfg.center_x, cy = o.yc[j] - o.cfg.center_y;
+    double dist2 = cx * cx + cy * cy;
+    double rprox2 = o.cfg.rprox * o.cfg.rprox, rdist2 = o.cfg.rdist * o.cfg.rdist;
+    if (dist2 > rprox2 && dist2 < rdist2) o.S(o.sink, c, is) = rsft_up * wst * o.indz[k];
+    int ntr = o.d3 ? o.nx * o.ny : o.nx;
+    size_t b = (size_t)(is - 1) * ntr + (o.d3 ? (i - 1) + o.nx * (j - 1) : (i - 1));
+    double dt = o.cfg.dt;
+    if (!o.d3) o.massl[b] = o.massl[b] + o.S(o.sink, c, is) * o.dx[i] * o.dz[k] * dt;
+    else o.massl[b] = o.massl[b] + o.S(o.sink, c, is) * o.dx[i] * o.dy[j] * o.dz[k] * dt;
+    o.massl[b] = o.mass_loss[b] + o.massl[b];
+    o.mass_loss[b] = 0.0;
+}
+
 void boundary_2d(Oracle &o, int sweep) {
     (void)sweep;
     int n = o.ncell, ns = o.ns;
+    if (o.cfg.isink > 0) std::fill(o.sink.begin(), o.sink.end(), 0.0);  // bdry.f:73
     auto US = [&](vector<double> &a, int c, int is) -> double & { return a[(size_t)(is - 1) * n + c]; };
     auto copy_s = [&](vector<double> &a, int dst, int src, double f) { for (int is = 1; is <= ns; ++is) US(a, dst, is) = f * US(a, src, is); };
     auto set_s = [&](vector<double> &a, int dst, double v) { for (int is = 1; is <= ns; ++is) US(a, dst, is) = v; };
@@ -1838,9 +1889,13 @@ void boundary_2d(Oracle &o, int sweep) {
             if (f2 == SLIP) {
                 o.wg[n2] = 0; set_s(o.ws, n2, 0.0);
                 if (o.flag[ipjkm] == SLIP) { o.ug[n2] = o.ug[n1]; copy_s(o.us, n2, n1, 1.0); }
+                if (o.cfg.isink > 0) for (int is = 1; is <= ns; ++is) sink_update(o, n1, is);
             } else if (f2 == NOSLIP) {
                 o.wg[n2] = 0; set_s(o.ws, n2, 0.0);
                 if (o.flag[ipjkm] == NOSLIP) { o.ug[n2] = -o.ug[n1]; copy_s(o.us, n2, n1, -1.0); }
+                if (o.cfg.isink > 0) for (int is = 1; is <= ns; ++is) sink_update(o, n1, is);
+            } else if (f2 == FILLED1 || f2 == FILLED2) {
+                if (o.cfg.isink > 0) for (int is = 1; is <= ns; ++is) sink_update(o, n1, is);
             } else if (f2 == FREE_IO || f2 == ZERO_GRAD) {
                 o.wg[n2] = o.wg[n1]; copy_s(o.ws, n2, n1, 1.0);
                 o.ug[n2] = o.ug[n1]; copy_s(o.us, n2, n1, 1.0);
@@ -1966,6 +2021,7 @@ int pdac_oracle_create(const pdac_cfg *cfg, void **out) {
     if (o->d3) build_tables3(*o);
     alloc(*o);
     les_setup(*o);
+    sink_setup(*o);
     *out = o;
     return PDAC_OK;
 }
@@ -2131,12 +2187,12 @@ int pdac_oracle_get_array(void *h, const char *name, double *out, long *n_inout)
                {"wgfe", &o.wgfe}, {"wgft", &o.wgft}, {"usfe", &o.usfe}, {"usft", &o.usft},
                {"wsfe", &o.wsfe}, {"wsft", &o.wsft}, {"rgfe", &o.rgfe}, {"rgft", &o.rgft},
                {"rsfe", &o.rsfe}, {"rsft", &o.rsft}, {"conv", &o.conv}, {"abeta", &o.abeta},
-               {"rhg", &o.rhg}, {"rhs", &o.rhs}, {"egfe", &o.egfe}, {"egft", &o.egft},
+               {"rhg", &o.rhg}, {"rhs", &o.rhs}, {"sink", &o.sink}, {"egfe", &o.egfe}, {"egft", &o.egft},
                {"esfe", &o.esfe}, {"esft", &o.esft}, {"dgres", &o.dgres},
                {"rvgn", &o.rvgn}, {"rvsn", &o.rvsn}, {"rvg", &o.rvg}, {"rvs", &o.rvs}, {"appv", &o.appv},
                {"rgfn", &o.rgfn}, {"rsfn", &o.rsfn}, {"mf3", &o.mf3}, {"ef3", &o.ef3},
                {"gvisy", &o.gvisy}, {"pvisy", &o.pvisy}, {"hgfe", &o.hgfe}, {"hgft", &o.hgft},
-               {"hsfe", &o.hsfe}, {"hsft", &o.hsft}, {"smag", &o.smag}, {"scoeff", &o.scoeff}, {"mugt", &o.mugt}, {"kapgt", &o.kapgt},
+               {"hsfe", &o.hsfe}, {"hsft", &o.hsft}, {"smag", &o.smag}, {"scoeff", &o.scoeff}, {"massl", &o.massl}, {"mugt", &o.mugt}, {"kapgt", &o.kapgt},
                {"must", &o.must},
                // explicit-solver fields (explicit_solver.f:15-83)
                {"rgpstar", &o.rk.rgpS}, {"rlkstar", &o.rk.rlkS}, {"ugstar", &o.rk.ugS}, {"usstar", &o.rk.usS},

@@ -57,6 +57,8 @@ class PdacCfg(C.Structure):
         ("plim", C.c_double * MAX_NSOLID),
         ("void_fraction", C.c_double), ("atm_ygc", C.c_double * MAX_NGAS),
         ("irand", C.c_int),
+        ("isink", C.c_int), ("rprox", C.c_double), ("rdist", C.c_double),
+        ("center_x", C.c_double), ("center_y", C.c_double),
         ("precision", C.c_int),
         ("dx", _dp), ("dy", _dp), ("dz", _dp), ("flag", _ip),
         ("p_atm", _dp), ("t_atm", _dp),
@@ -129,6 +131,8 @@ def declare(lib, prefix, handle_type):
             "write_output": [h, C.c_char_p, C.c_double],
             "mass_residuals": [h, C.c_int, C.c_double, _dp, C.c_int],
             "append_mass_check": [h, C.c_char_p, C.c_int, C.c_double],
+            "write_mass_loss": [h, C.c_char_p],
+            "read_mass_loss": [h, C.c_char_p],
         })
     if prefix == "pdac_oracle":
         sigs["sgs"] = [h]

@@ -156,3 +156,20 @@ def small_3d_dyn(**kw):
 def small_3d_rk3_dyn(**kw):
     """small_3d_rk3 with the sub-grid models of small_3d_dyn."""
     return _dynamic(small_3d_rk3(**kw))
+
+
+def small_2d_sink(**kw):
+    """small_2d with the ground sink (isink = 1) on the ring 10 m < r < 60 m
+    around the axis."""
+    d = small_2d(**kw)
+    d.set("model", isink=1, rprox=10.0, rdist=60.0)
+    return d
+
+
+def small_3d_sink(**kw):
+    """small_3d with the ground sink on the ring 20 m < r < 70 m around the
+    domain centre (100 m, 80 m)."""
+    d = small_3d(**kw)
+    d.set("model", isink=1, rprox=20.0, rdist=70.0)
+    d.set("mesh", center_x=100.0, center_y=80.0)
+    return d

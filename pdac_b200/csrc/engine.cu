@@ -21,6 +21,7 @@
 #include "rk3.cuh"
 #include "io.cuh"
 #include "les.cuh"
+#include "sink.cuh"
 
 using namespace pdac;
 
@@ -78,6 +79,11 @@ struct pdac_ctx {
     // grid (0 when the device cannot co-schedule one; the wavefront then
     // runs as one launch per hyperplane) and whether it covers the widest
     // hyperplane
+    // ground sink (isink > 0): per-column mass taken out, restart values,
+    // ring mask
+    pdac::Sink S{};
+    double *d_sinkbuf = nullptr;
+    int *d_ring = nullptr;
     pdac::Wave W{};
     int *d_wave_idx = nullptr;    // order, src[3], start
     double *d_wave_rec = nullptr; // records and pnew
@@ -500,6 +506,40 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
         int st = setup_wave(ctx, cfg->flag);
         if (st) return st;
     }
+    if (cfg->isink > 0) {
+        // allocate_sink (sink.f:22-43); the ring test of sink_update
+        // (sink.f:95-96) per ground column from the cell-centre coordinates
+        // of grid.f:286-298 (dy = 0 in 2D, so y(1) = 0)
+        const int ntr = ctx->d3 ? nx * ny : nx;
+        std::vector<double> xc(nx + 1, 0.0), yc(ny + 1, 0.0);
+        double xb = 0.0;
+        xc[1] = -0.5 * dx[1] + xb;
+        for (int i = 2; i <= nx; ++i) { xb = (xb + dx[i]); xc[i] = (xb - 0.5 * dx[i]); }
+        if (ctx->d3) {
+            double yb = 0.0;
+            yc[1] = -0.5 * dy[1] + yb;
+            for (int j = 2; j <= ny; ++j) { yb = yb + dy[j]; yc[j] = (yb - 0.5 * dy[j]); }
+        }
+        std::vector<int> ring(ntr);
+        const double rprox2 = cfg->rprox * cfg->rprox, rdist2 = cfg->rdist * cfg->rdist;
+        for (int b = 0; b < ntr; ++b) {
+            int i = b % nx + 1, j = ctx->d3 ? b / nx + 1 : 1;
+            double cx = xc[i] - cfg->center_x, cy = yc[j] - cfg->center_y;
+            double dist2 = cx * cx + cy * cy;
+            ring[b] = (dist2 > rprox2 && dist2 < rdist2) ? 1 : 0;
+        }
+        const size_t nm = (size_t)ntr * ns;
+        CK(cudaMalloc(&ctx->d_sinkbuf, 2 * nm * sizeof(double)));
+        CK(cudaMemset(ctx->d_sinkbuf, 0, 2 * nm * sizeof(double)));
+        CK(cudaMalloc(&ctx->d_ring, ntr * sizeof(int)));
+        CK(cudaMemcpy(ctx->d_ring, ring.data(), ntr * sizeof(int), cudaMemcpyHostToDevice));
+        ctx->S.massl = ctx->d_sinkbuf;
+        ctx->S.mass_loss = ctx->d_sinkbuf + nm;
+        ctx->S.ring = ctx->d_ring;
+        ctx->S.ntr = ntr;
+        ctx->names.push_back({"massl", {ctx->S.massl, nm}});
+        ctx->names.push_back({"mass_loss", {ctx->S.mass_loss, nm}});
+    }
     *out = ctx;
     return PDAC_OK;
 }
@@ -525,6 +565,8 @@ int pdac_gpu_destroy(pdac_ctx *ctx) {
     cudaFreeHost(ctx->h_nit);
     cudaFree(ctx->d_cand);
     cudaFree(ctx->d_partial);
+    cudaFree(ctx->d_sinkbuf);
+    cudaFree(ctx->d_ring);
     cudaFree(ctx->d_wave_idx);
     cudaFree(ctx->d_wave_rec);
     cudaFreeHost(ctx->h_counters);
@@ -573,6 +615,12 @@ int pdac_gpu_boundary(pdac_ctx *ctx, int sweep) {
     if (ctx->d3) pdac::k_boundary3d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F);
     else pdac::k_boundary2d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F);
     ctx->launches++;
+    if (ctx->S.ntr > 0) {
+        const long nt = (long)ctx->S.ntr * ctx->ns;
+        if (ctx->d3) pdac::k_sink<3><<<blocks(nt), TPB, 0, st>>>(ctx->P, ctx->F, ctx->S, ctx->cfg.dt);
+        else pdac::k_sink<2><<<blocks(nt), TPB, 0, st>>>(ctx->P, ctx->F, ctx->S, ctx->cfg.dt);
+        ctx->launches++;
+    }
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[1], st));
     return PDAC_OK;
@@ -1459,6 +1507,98 @@ int pdac_gpu_append_mass_check(pdac_ctx *ctx, const char *path, int nswp, double
     bool ok = std::fputs(line.c_str(), f) >= 0;
     ok = (std::fclose(f) == 0) && ok;
     if (!ok) return fail(ctx, PDAC_ERR_ARG, std::string("append_mass_check: write error on ") + path);
+    return PDAC_OK;
+}
+
+// print_mass_loss (sink.f:123-167): the columns' accumulated mass in the
+// reference's formatted layout, FORMAT(10(1x,G14.6E3)): in 2D one line per
+// column i with the ns values and the running total over the columns, in
+// 3D per solid a header '(1x,//,1x,"ML",I1,"=",G14.6,/)' with that solid's
+// total and then the ntr column values, ten to a line
+int pdac_gpu_write_mass_loss(pdac_ctx *ctx, const char *path) {
+    if (!ctx || !path) return PDAC_ERR_ARG;
+    if (ctx->S.ntr == 0) return fail(ctx, PDAC_ERR_CONFIG, "write_mass_loss: the run has no sink (isink = 0)");
+    const int ntr = ctx->S.ntr, ns = ctx->ns;
+    std::vector<double> ml((size_t)ntr * ns);
+    CK(cudaMemcpyAsync(ml.data(), ctx->S.massl, ml.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    auto at = [&](int b, int is) { return ml[(size_t)(is - 1) * ntr + b]; };
+    std::string out;
+    auto group = [&](const std::vector<double> &v) {
+        for (size_t q = 0; q < v.size(); ++q) {
+            if (q > 0 && q % 10 == 0) out += "\n";
+            out += " " + pdac::io::fortran_g(v[q], 14, 6, 3);
+        }
+        out += "\n";
+    };
+    if (!ctx->d3) {
+        double masstotal = 0.0;
+        for (int b = 0; b < ntr; ++b) {
+            double sum = 0.0;
+            std::vector<double> v;
+            for (int is = 1; is <= ns; ++is) { sum = sum + at(b, is); v.push_back(at(b, is)); }
+            masstotal = masstotal + sum;
+            v.push_back(masstotal);
+            group(v);
+        }
+    } else {
+        for (int is = 1; is <= ns; ++is) {
+            double masstotal = 0.0;
+            std::vector<double> v(ntr);
+            for (int b = 0; b < ntr; ++b) { masstotal = masstotal + at(b, is); v[b] = at(b, is); }
+            char head[64];
+            std::snprintf(head, sizeof head, "\n\n ML%1d=", is);
+            out += head + pdac::io::fortran_g(masstotal, 14, 6, 2) + "\n\n";
+            group(v);
+        }
+    }
+    FILE *f = std::fopen(path, "w");
+    if (!f) return fail(ctx, PDAC_ERR_ARG, std::string("write_mass_loss: cannot open ") + path);
+    bool ok = std::fputs(out.c_str(), f) >= 0;
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) return fail(ctx, PDAC_ERR_ARG, std::string("write_mass_loss: write error on ") + path);
+    return PDAC_OK;
+}
+
+// read_mass_loss (sink.f:168-207): a file written by print_mass_loss into
+// the values that the next sink update of each column adds back
+int pdac_gpu_read_mass_loss(pdac_ctx *ctx, const char *path) {
+    if (!ctx || !path) return PDAC_ERR_ARG;
+    if (ctx->S.ntr == 0) return fail(ctx, PDAC_ERR_CONFIG, "read_mass_loss: the run has no sink (isink = 0)");
+    const int ntr = ctx->S.ntr, ns = ctx->ns;
+    FILE *f = std::fopen(path, "r");
+    if (!f) return fail(ctx, PDAC_ERR_ARG, std::string("read_mass_loss: cannot open ") + path);
+    std::vector<std::string> tok;
+    char word[256];
+    while (std::fscanf(f, "%255s", word) == 1) tok.push_back(word);
+    std::fclose(f);
+    std::vector<double> ml((size_t)ntr * ns);
+    size_t q = 0;
+    auto num = [&](double &x) {
+        if (q >= tok.size()) return false;
+        char *end = nullptr;
+        x = std::strtod(tok[q].c_str(), &end);
+        return end && *end == '\0' && tok[q++].size() > 0;
+    };
+    bool ok = true;
+    if (!ctx->d3) {
+        for (int b = 0; b < ntr && ok; ++b) {
+            double total;
+            for (int is = 1; is <= ns && ok; ++is) ok = num(ml[(size_t)(is - 1) * ntr + b]);
+            ok = ok && num(total);
+        }
+    } else {
+        for (int is = 1; is <= ns && ok; ++is) {
+            double total;
+            ok = q < tok.size() && tok[q].rfind("ML", 0) == 0;
+            if (ok) ++q;
+            ok = ok && num(total);
+            for (int b = 0; b < ntr && ok; ++b) ok = num(ml[(size_t)(is - 1) * ntr + b]);
+        }
+    }
+    if (!ok || q != tok.size()) return fail(ctx, PDAC_ERR_ARG, std::string("read_mass_loss: unexpected layout in ") + path);
+    CK(cudaMemcpyAsync(ctx->S.mass_loss, ml.data(), ml.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
     return PDAC_OK;
 }
 

@@ -363,8 +363,8 @@ class Deck:
             bad.append("irex>1 (reactions)")
         if self["immb"] != 0 or self["itp"] != 0:
             bad.append("immersed boundaries / topography")
-        if self["isink"] != 0:
-            bad.append("isink>0")
+        if self["isink"] < 0:
+            bad.append("isink<0")
         if self["idome"] != 0:
             bad.append("idome>0")
         if self["ibl"] != 0:

@@ -6,8 +6,11 @@ loop (or initialize_fieldn and explicit_iter with time_integration = 1),
 then the output dump every ``nprint`` steps (outp, output.NNNN), the
 mass-check line every step when ``imr >= 1`` (pdac.chm) and the restart
 file every ``ndump`` steps (tapewr, pdac.res), with nprint = NINT(tpr/dt)
-and ndump = NINT(tdump/dt) (prog.f:84-85).  ``restart_mode = 'restart'``
-starts from pdac.res (taperd, setup.f:147-150).  The files themselves are
+and ndump = NINT(tdump/dt) (prog.f:84-85); with the ground sink (isink > 0)
+also the columns' lost mass before each output (massl.NNNN, prog.f:355) and
+after each restart file (massl.res, prog.f:386).  ``restart_mode =
+'restart'`` starts from pdac.res (taperd, setup.f:147-150) and, with the
+sink, from massl.NNNN of the namelist's nfil.  The files themselves are
 written by the engine's C entry points in the reference's formats.
 """
 from __future__ import annotations
@@ -29,6 +32,11 @@ def lettera(k):
 def output_name(nfil):
     """outp.f:221: output.NNNN."""
     return "output." + lettera(nfil)
+
+
+def massl_name(nfil=None):
+    """sink.f:141-145: massl.NNNN, or massl.res without a counter."""
+    return "massl.res" if nfil is None else "massl." + lettera(nfil)
 
 
 def nint(x):
@@ -55,7 +63,11 @@ def run(engine, workdir, max_steps=None, log=None):
         raise ValueError(f"restart_mode {mode!r} is not supported by this driver")
     os.makedirs(workdir, exist_ok=True)
     path = lambda name: os.path.join(workdir, name)
+    sink = int(d["isink"]) > 0
     if mode == "restart":
+        if sink:
+            # setup.f:147: read_mass_loss(nfil) with the namelist's nfil
+            engine.read_mass_loss(path(massl_name(int(d["nfil"]))))
         t, nfil = engine.read_restart(path(RESTART_FILE))
     else:
         t, nfil = 0.0, 0
@@ -97,6 +109,8 @@ def run(engine, workdir, max_steps=None, log=None):
         if log:
             log.write(f"Iteration: {sweep:6d} nit: {0 if explicit else nit:5d}\n")
         if sweep % nprint == 0:
+            if sink:
+                engine.write_mass_loss(path(massl_name(nfil)))
             engine.write_output(path(output_name(nfil)), t)
             nfil += 1
         if int(d["imr"]) >= 1:
@@ -105,6 +119,8 @@ def run(engine, workdir, max_steps=None, log=None):
         stop_now = (_time.time() - w0) > float(d["max_seconds"])
         if sweep % ndump == 0 or stop_now:
             engine.write_restart(path(RESTART_FILE), t, nfil)
+            if sink:
+                engine.write_mass_loss(path(massl_name()))
         if t + 0.1 * dt >= d["tstop"] or stop_now or (max_steps is not None and steps >= max_steps):
             break
     return t, nfil, sweep

@@ -424,6 +424,9 @@ class Case:
         for g, v in enumerate(d.atm_ygc()):
             c.atm_ygc[g] = v
         c.irand = d["irand"]
+        c.isink = int(d["isink"])
+        c.rprox, c.rdist = float(d["rprox"]), float(d["rdist"])
+        c.center_x, c.center_y = float(d["center_x"]), float(d["center_y"])
         c.precision = self.precision
         keep = dict(dx=np.ascontiguousarray(self.dx), dy=np.ascontiguousarray(self.dy),
                     dz=np.ascontiguousarray(self.dz), flag=np.ascontiguousarray(self.flag, dtype=np.int32),
