@@ -74,6 +74,12 @@ typedef struct pdac_cfg {
     double beta;                /* beta-limiter parameter                    */
     double flim;                /* invdm decoupling threshold (ftem.f:221)   */
     int    update_eosg;
+    int    implicit_fluxes;     /* 1: tilde at the start of every outer sweep
+                                   of iter (iter.f:211-226), none before it */
+    int    implicit_enthalpy;   /* 1: ftem (after htilde when implicit_fluxes)
+                                   at the end of every outer sweep
+                                   (iter.f:362-379), htilde before iter
+                                   otherwise (prog.f:246-292)               */
 
     /* &model */
     int    pmodel, drag_model, icpc;

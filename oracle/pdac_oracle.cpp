@@ -1386,8 +1386,21 @@ void inner_loop_2d(Oracle &o, int c, int nit, double &d3, double &p3, double &ab
     }
 }
 
+void htilde_2d(Oracle &o, double dt);
+int ftem_2d(Oracle &o, double dt);
+
+// allocate_fluxes (tilde.f:56-102, prog.f:229): the tilde momenta,
+// interphase terms and enthalpy right-hand sides start every RK stage at
+// zero; with implicit_fluxes iter's predictor reads those zeros
+void zero_tilde_terms(Oracle &o) {
+    for (auto *v : {&o.rug, &o.rvg, &o.rwg, &o.rus, &o.rvs, &o.rws, &o.appu, &o.appv, &o.appw, &o.rhg, &o.rhs})
+        std::fill(v->begin(), v->end(), 0.0);
+}
+
 int iter_2d(Oracle &o, double dt, int *nit_out) {
     int n = o.ncell;
+    if (o.cfg.implicit_fluxes) zero_tilde_terms(o);
+    bool eos = false;
     std::fill(o.rgfe.begin(), o.rgfe.end(), 0.0); std::fill(o.rgft.begin(), o.rgft.end(), 0.0);
     std::fill(o.rsfe.begin(), o.rsfe.end(), 0.0); std::fill(o.rsft.begin(), o.rsft.end(), 0.0);
     std::fill(o.conv.begin(), o.conv.end(), 0.0); std::fill(o.abeta.begin(), o.abeta.end(), 0.0);
@@ -1420,6 +1433,7 @@ int iter_2d(Oracle &o, double dt, int *nit_out) {
     int nit;
     for (nit = 1; nit <= o.cfg.maxout; ++nit) {
         o.ierr = 0;
+        if (o.cfg.implicit_fluxes) tilde_2d(o, dt);  // iter.f:211-226
         bool all = true;
         for (int c : order) {
             if (!o.fluidbit(c)) continue;
@@ -1435,11 +1449,15 @@ int iter_2d(Oracle &o, double dt, int *nit_out) {
                 inner_loop_2d(o, c, nit, d3, p3, o.abeta[c], o.conv[c], dgorig, dt);
             }
         }
+        if (o.cfg.implicit_enthalpy) {  // iter.f:362-379
+            if (o.cfg.implicit_fluxes) htilde_2d(o, dt);
+            if (ftem_2d(o, dt) != PDAC_OK) eos = true;
+        }
         if (all) break;
     }
     o.last_nit = nit;
     if (nit_out) *nit_out = nit;
-    return PDAC_OK;
+    return eos ? PDAC_ERR_EOS : PDAC_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -2160,14 +2178,22 @@ int pdac_oracle_step(void *h, int sweep, int *nit) {
     }
     pdac_oracle_fieldn(h);
     pdac_oracle_sgs(h);
+    const bool ifx = o.cfg.implicit_fluxes != 0, ien = o.cfg.implicit_enthalpy != 0;
     for (int rk = 1; rk <= o.cfg.rungekut; ++rk) {
         double dt = dt0 / (o.cfg.rungekut + 1 - rk);
-        pdac_oracle_tilde(h, dt);
-        pdac_oracle_iter(h, dt, nit);
+        // prog.f:246-292
+        if (!ifx) {
+            pdac_oracle_tilde(h, dt);
+            if (ien) pdac_oracle_htilde(h, dt);
+        }
+        int s1 = pdac_oracle_iter(h, dt, nit);
+        if (s1 != PDAC_OK) st = s1;
         pdac_oracle_ygas(h, dt);
-        pdac_oracle_htilde(h, dt);
-        int s2 = pdac_oracle_ftem(h, dt);
-        if (s2 != PDAC_OK) st = s2;
+        if (!ien) {
+            pdac_oracle_htilde(h, dt);
+            int s2 = pdac_oracle_ftem(h, dt);
+            if (s2 != PDAC_OK) st = s2;
+        }
     }
     return st;
 }

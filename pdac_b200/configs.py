@@ -173,3 +173,19 @@ def small_3d_sink(**kw):
     d.set("model", isink=1, rprox=20.0, rdist=70.0)
     d.set("mesh", center_x=100.0, center_y=80.0)
     return d
+
+
+def _implicit(deck, fluxes, enthalpy):
+    deck.set("numeric", implicit_fluxes=fluxes, implicit_enthalpy=enthalpy)
+    return deck
+
+
+def small_2d_implicit(fluxes=True, enthalpy=True, **kw):
+    """small_2d with tilde (implicit_fluxes) and / or ftem (implicit_enthalpy)
+    inside the outer sweeps of iter (iter.f:211-226, 362-379)."""
+    return _implicit(small_2d(**kw), fluxes, enthalpy)
+
+
+def small_3d_implicit(fluxes=True, enthalpy=True, **kw):
+    """small_3d with the implicit modes of small_2d_implicit."""
+    return _implicit(small_3d(**kw), fluxes, enthalpy)

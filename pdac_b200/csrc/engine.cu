@@ -56,6 +56,7 @@ struct pdac_ctx {
     cudaGraph_t it_graph = nullptr;
     cudaGraphExec_t it_exec = nullptr;
     double it_dt = 0.0;
+    long long it_per_sweep = 10;  // kernels of one sweep of that graph
     std::vector<double> sweep_log;  // per colour phase when profiling: sweep, colour, worklist, tested, ms x2
     bool prof = false;
     cudaEvent_t cev[9];
@@ -196,6 +197,7 @@ int validate(const pdac_cfg *c, std::string &why) {
         return 1;
     }
     if (c->iss != 0 && c->iss != 1) { why = "iss must be 0 or 1"; return 1; }
+    if (c->implicit_fluxes && c->alpha != 1.0) { why = "implicit_fluxes needs alpha = 1"; return 1; }
     if (c->time_integration == 1 && c->pmodel != 1 && c->pmodel != 2) {
         why = "time_integration = 1 needs pmodel 1 or 2 (explicit_solver.f:632-642)";
         return 1;
@@ -673,12 +675,11 @@ static void accumulate_conductivity(pdac_ctx *ctx, cudaStream_t st) {
     ctx->launches++;
 }
 
-int pdac_gpu_tilde(pdac_ctx *ctx, double dt) {
-    if (!ctx) return PDAC_ERR_ARG;
-    cudaStream_t st = ctx->stream;
+// the kernels of tilde on stream st (also inside the sweep graph of iter
+// with implicit_fluxes)
+static int enqueue_tilde(pdac_ctx *ctx, double dt, cudaStream_t st) {
     size_t n = ctx->ncell, ns = ctx->ns;
     Fld &F = ctx->F;
-    CK(cudaEventRecord(ctx->ev[4], st));
     int s = accumulate_viscosities(ctx, st);
     if (s) return s;
     if (ctx->d3) {
@@ -703,15 +704,33 @@ int pdac_gpu_tilde(pdac_ctx *ctx, double dt) {
         if (ctx->d3) CK(cudaMemcpyAsync(ctx->d_app0v, F.appv, n * ctx->nap * sizeof(double), cudaMemcpyDeviceToDevice, st));
     }
     CK(cudaGetLastError());
+    return PDAC_OK;
+}
+
+int pdac_gpu_tilde(pdac_ctx *ctx, double dt) {
+    if (!ctx) return PDAC_ERR_ARG;
+    cudaStream_t st = ctx->stream;
+    CK(cudaEventRecord(ctx->ev[4], st));
+    int s = enqueue_tilde(ctx, dt, st);
+    if (s) return s;
     CK(cudaEventRecord(ctx->ev[5], st));
     return PDAC_OK;
 }
+
+static int enqueue_htilde(pdac_ctx *ctx, double dt, cudaStream_t st);
+static int enqueue_ftem(pdac_ctx *ctx, double dt, cudaStream_t st, bool in_sweep);
 
 // one outer sweep of the corrector (iter.f:241-410): three colour phases of
 // candidate collection, residual test and inner loop; the sweep number is
 // read on the device from d_nit
 static int enqueue_sweep(pdac_ctx *ctx, double dt, cudaStream_t st, bool prof) {
     Fld &F = ctx->F;
+    // implicit_fluxes: momentum fluxes, stresses and drag of the current
+    // velocities before the cells are visited (iter.f:211-226)
+    if (ctx->cfg.implicit_fluxes) {
+        int s = enqueue_tilde(ctx, dt, st);
+        if (s) return s;
+    }
     const int nph = ctx->nph;
     const size_t n = ctx->ncell, nwords = (n + 31) / 32;
     const long nthr = (long)((ctx->nx + 2) / 3) * ctx->ny * ctx->nz;
@@ -733,6 +752,15 @@ static int enqueue_sweep(pdac_ctx *ctx, double dt, cudaStream_t st, bool prof) {
         if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_inner_team, 3, g, TPB_TEAM, st, ctx->P, F, dt, ctx->d_nit, ctx->d_work, cnt, dirty);
         else PHASE_LAUNCH_D(nph, pdac::k_inner_team, 2, g, TPB_TEAM, st, ctx->P, F, dt, ctx->d_nit, ctx->d_work, cnt, dirty);
         if (prof) CK(cudaEventRecord(ctx->cev[3 * col + 2], st));
+    }
+    // implicit_enthalpy: the enthalpy fluxes (with implicit_fluxes) and the
+    // enthalpy / interphase solve after the cells (iter.f:362-379), before
+    // the convergence test, so also in the last sweep
+    if (ctx->cfg.implicit_enthalpy) {
+        int s = PDAC_OK;
+        if (ctx->cfg.implicit_fluxes) s = enqueue_htilde(ctx, dt, st);
+        if (!s) s = enqueue_ftem(ctx, dt, st, true);
+        if (s) return s;
     }
     CK(cudaGetLastError());
     return PDAC_OK;
@@ -760,7 +788,13 @@ static int build_iter_graph(pdac_ctx *ctx, double dt) {
     CK(cudaGraphAddNode(&node, ctx->it_graph, nullptr, 0, &cp));
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     CK(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    // kernels of one sweep: the nine of the colour phases, the check, and
+    // those the implicit modes add (counted by their enqueue functions,
+    // which run here only to record them)
+    const long long before = ctx->launches;
     int s = enqueue_sweep(ctx, dt, st, false);
+    ctx->it_per_sweep = 10 + (ctx->launches - before);
+    ctx->launches = before;
     if (!s) pdac::k_sweep_check<<<1, 1, 0, st>>>(ctx->d_wcount, ctx->d_nit, ctx->cfg.maxout, loop);
     cudaGraph_t captured = nullptr;
     cudaError_t e = cudaStreamEndCapture(st, &captured);
@@ -772,12 +806,33 @@ static int build_iter_graph(pdac_ctx *ctx, double dt) {
     return PDAC_OK;
 }
 
+// allocate_fluxes (tilde.f:56-102), run by prog.f:229 before every RK
+// stage, leaves the tilde momenta, interphase terms and enthalpy
+// right-hand sides at zero; with implicit_fluxes no tilde precedes iter, so
+// its predictor reads those zeros
+static int zero_tilde_terms(pdac_ctx *ctx, cudaStream_t st) {
+    Fld &F = ctx->F;
+    const size_t n = ctx->ncell, ns = ctx->ns, nap = ctx->nap;
+    for (double *a : {F.rug, F.rvg, F.rwg, F.rhg})
+        if (a) CK(cudaMemsetAsync(a, 0, n * sizeof(double), st));
+    for (double *a : {F.rus, F.rvs, F.rws, F.rhs})
+        if (a) CK(cudaMemsetAsync(a, 0, n * ns * sizeof(double), st));
+    for (double *a : {F.appu, F.appv, F.appw})
+        if (a) CK(cudaMemsetAsync(a, 0, n * nap * sizeof(double), st));
+    return PDAC_OK;
+}
+
 int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
     if (!ctx) return PDAC_ERR_ARG;
     cudaStream_t st = ctx->stream;
     size_t n = ctx->ncell, ns = ctx->ns;
     Fld &F = ctx->F;
     CK(cudaEventRecord(ctx->ev[6], st));
+    if (ctx->cfg.implicit_fluxes) {
+        int s = zero_tilde_terms(ctx, st);
+        if (s) return s;
+    }
+    CK(cudaMemsetAsync(ctx->d_counters + 5, 0, sizeof(int), st));  // caloric failures of in-sweep ftem calls
     for (double *a : {F.rgfe, F.rgfn, F.rgft, F.conv, F.abeta})
         if (a) CK(cudaMemsetAsync(a, 0, n * sizeof(double), st));
     for (double *a : {F.rsfe, F.rsfn, F.rsft})
@@ -805,11 +860,12 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
         CK(cudaMemcpyAsync(ctx->d_nit, ctx->h_nit, sizeof(int), cudaMemcpyHostToDevice, st));
         CK(cudaGraphLaunch(ctx->it_exec, st));
         CK(cudaMemcpyAsync(ctx->h_nit, ctx->d_nit, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(ctx->h_counters + 5, ctx->d_counters + 5, sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         nit = *ctx->h_nit;
         int done = std::min(nit, ctx->cfg.maxout);
         ctx->sweeps += done;
-        ctx->launches += 10L * done;
+        ctx->launches += ctx->it_per_sweep * done;
     } else {
         // host loop with per-colour-phase timing
         for (nit = 1; nit <= ctx->cfg.maxout; ++nit) {
@@ -821,6 +877,7 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
             CK(cudaMemcpyAsync(ctx->h_counters, ctx->d_wcount, 6 * sizeof(int), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             ctx->sweeps++;
+            ctx->launches += (long long)ctx->cfg.implicit_enthalpy;  // k_eos_sticky
             long unconverged = (long)ctx->h_counters[0] + ctx->h_counters[1] + ctx->h_counters[2];
             ctx->work_cells += unconverged;
             ctx->tested_cells += (long)ctx->h_counters[3] + ctx->h_counters[4] + ctx->h_counters[5];
@@ -842,6 +899,13 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[7], st));
     if (nit_out) *nit_out = nit;
+    if (ctx->cfg.implicit_enthalpy) {
+        if (ctx->prof) {
+            CK(cudaMemcpyAsync(ctx->h_counters + 5, ctx->d_counters + 5, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+        }
+        if (ctx->h_counters[5]) return fail(ctx, PDAC_ERR_EOS, "iter: caloric equation of state failed in a sweep's ftem");
+    }
     return PDAC_OK;
 }
 
@@ -885,6 +949,8 @@ int static_scratch(pdac_ctx *ctx, unsigned char **out) {
 
 int pdac_gpu_iter_static(pdac_ctx *ctx, double dt, int *nit_out) {
     if (!ctx) return PDAC_ERR_ARG;
+    if (ctx->cfg.implicit_fluxes || ctx->cfg.implicit_enthalpy)
+        return fail(ctx, PDAC_ERR_CONFIG, "iter_static: the implicit-flux modes run through pdac_gpu_iter only");
     int m = (ctx->nx + 2) / 3;
     long nthr = (long)m * ctx->ny * ctx->nz;
     size_t n = ctx->ncell, ns = ctx->ns;
@@ -975,12 +1041,10 @@ int pdac_gpu_ygas(pdac_ctx *ctx, double dt) {
     return PDAC_OK;
 }
 
-int pdac_gpu_htilde(pdac_ctx *ctx, double dt) {
-    if (!ctx) return PDAC_ERR_ARG;
-    cudaStream_t st = ctx->stream;
+// the kernels of htilde on stream st
+static int enqueue_htilde(pdac_ctx *ctx, double dt, cudaStream_t st) {
     size_t n = ctx->ncell, ns = ctx->ns;
     Fld &F = ctx->F;
-    CK(cudaEventRecord(ctx->ev[10], st));
     for (double *a : {F.egfe, F.egfn, F.egft})
         if (a) CK(cudaMemsetAsync(a, 0, n * sizeof(double), st));
     for (double *a : {F.esfe, F.esfn, F.esft})
@@ -994,7 +1058,34 @@ int pdac_gpu_htilde(pdac_ctx *ctx, double dt) {
         pdac::k_htilde2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt), ctx->launches++;
     }
     CK(cudaGetLastError());
+    return PDAC_OK;
+}
+
+int pdac_gpu_htilde(pdac_ctx *ctx, double dt) {
+    if (!ctx) return PDAC_ERR_ARG;
+    cudaStream_t st = ctx->stream;
+    CK(cudaEventRecord(ctx->ev[10], st));
+    int s = enqueue_htilde(ctx, dt, st);
+    if (s) return s;
     CK(cudaEventRecord(ctx->ev[11], st));
+    return PDAC_OK;
+}
+
+namespace pdac {
+// an ftem inside the sweeps of iter: more than one caloric failure
+// (ftem.f:191-193) is remembered in counters[5] until iter returns
+__global__ void k_eos_sticky(int *counters) {
+    if (counters[1] > 1) counters[5] = 1;
+}
+}  // namespace pdac
+
+static int enqueue_ftem(pdac_ctx *ctx, double dt, cudaStream_t st, bool in_sweep) {
+    CK(cudaMemsetAsync(ctx->d_counters + 1, 0, sizeof(int), st));
+    if (ctx->d3) pdac::k_ftem3d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F, dt);
+    else pdac::k_ftem2d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F, dt);
+    ctx->launches++;
+    if (in_sweep) pdac::k_eos_sticky<<<1, 1, 0, st>>>(ctx->d_counters);
+    CK(cudaGetLastError());
     return PDAC_OK;
 }
 
@@ -1002,11 +1093,8 @@ int pdac_gpu_ftem(pdac_ctx *ctx, double dt) {
     if (!ctx) return PDAC_ERR_ARG;
     cudaStream_t st = ctx->stream;
     CK(cudaEventRecord(ctx->ev[12], st));
-    CK(cudaMemsetAsync(ctx->d_counters + 1, 0, sizeof(int), st));
-    if (ctx->d3) pdac::k_ftem3d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F, dt);
-    else pdac::k_ftem2d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F, dt);
-    ctx->launches++;
-    CK(cudaGetLastError());
+    int s = enqueue_ftem(ctx, dt, st, false);
+    if (s) return s;
     CK(cudaEventRecord(ctx->ev[13], st));
     CK(cudaMemcpyAsync(ctx->h_counters + 1, ctx->d_counters + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -1254,15 +1342,26 @@ int pdac_gpu_step(pdac_ctx *ctx, int sweep, int *nit) {
     }
     if ((s = pdac_gpu_fieldn(ctx))) return s;
     if ((s = pdac_gpu_sgsg(ctx)) || (s = pdac_gpu_sgss(ctx))) return s;
+    const bool ifx = ctx->cfg.implicit_fluxes != 0, ien = ctx->cfg.implicit_enthalpy != 0;
     for (int rk = 1; rk <= ctx->cfg.rungekut; ++rk) {
         double dt = dt0 / (ctx->cfg.rungekut + 1 - rk);
-        if ((s = pdac_gpu_tilde(ctx, dt))) return s;
-        if ((s = pdac_gpu_iter(ctx, dt, nit))) return s;
-        if ((s = pdac_gpu_ygas(ctx, dt))) return s;
-        if ((s = pdac_gpu_htilde(ctx, dt))) return s;
-        s = pdac_gpu_ftem(ctx, dt);
+        // prog.f:246-292: tilde (and htilde with implicit_enthalpy) before
+        // iter unless implicit_fluxes moves them into the sweeps; htilde and
+        // ftem after ygas unless implicit_enthalpy moved them
+        if (!ifx) {
+            if ((s = pdac_gpu_tilde(ctx, dt))) return s;
+            if (ien && (s = pdac_gpu_htilde(ctx, dt))) return s;
+        }
+        s = pdac_gpu_iter(ctx, dt, nit);
         if (s == PDAC_ERR_EOS) status = s;
         else if (s) return s;
+        if ((s = pdac_gpu_ygas(ctx, dt))) return s;
+        if (!ien) {
+            if ((s = pdac_gpu_htilde(ctx, dt))) return s;
+            s = pdac_gpu_ftem(ctx, dt);
+            if (s == PDAC_ERR_EOS) status = s;
+            else if (s) return s;
+        }
     }
     return status;
 }

@@ -351,8 +351,10 @@ class Deck:
             bad.append("iss>1")
         if self["ctu"] != 0:
             bad.append("ctu>0 (corner transport upwind)")
-        if self["implicit_fluxes"] or self["implicit_enthalpy"]:
-            bad.append("implicit_fluxes/implicit_enthalpy")
+        if self["implicit_fluxes"] and self["alpha"] != 1.0:
+            # the previous-visit interphase terms of alpha < 1 are not
+            # defined when tilde runs inside the sweeps
+            bad.append("implicit_fluxes with alpha other than 1")
         if self["time_integration"] not in (0, 1):
             bad.append("time_integration other than 0 or 1")
         elif self["time_integration"] == 1 and self["pmodel"] not in (1, 2):

@@ -405,6 +405,8 @@ class Case:
         c.muscl, c.lv, c.lm = d["muscl"], d["vel_limiter"], d["mass_limiter"]
         c.beta, c.flim = d["beta"], d["flim"]
         c.update_eosg = int(bool(d["update_eosg"]))
+        c.implicit_fluxes = int(bool(d["implicit_fluxes"]))
+        c.implicit_enthalpy = int(bool(d["implicit_enthalpy"]))
         c.pmodel, c.drag_model, c.icpc = d["pmodel"], d["drag_model"], d["icpc"]
         c.tref = d["tref"]
         c.gas_viscosity = int(bool(d["gas_viscosity"]))

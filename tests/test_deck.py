@@ -124,3 +124,13 @@ def test_explicit_solver_selection():
     with pytest.raises(ValueError, match="time_integration"):
         Case(d)
     assert Case(configs.plume_2d()).cfg().time_integration == 0
+
+
+def test_implicit_flux_modes_reach_the_configuration():
+    d = configs.small_2d_implicit(fluxes=True, enthalpy=False)
+    cfg = Case(d).cfg()
+    assert (cfg.implicit_fluxes, cfg.implicit_enthalpy) == (1, 0)
+    d = configs.small_2d_implicit()
+    d.set("numeric", alpha=0.5)
+    with pytest.raises(ValueError, match="implicit_fluxes"):
+        Case(d)
