@@ -117,6 +117,13 @@ typedef struct pdac_cfg {
     double rprox, rdist;
     double center_x, center_y;
 
+    /* &model compute_mixture: the gas-particle mixture fields (mixture.f,
+     * derived.f:220-331) at the end of every step (prog.f:331) and in the
+     * output files; &control formatted_output: output files as text
+     * (outp.f:226-231, io_parallel.f:38-50) instead of unformatted records */
+    int    compute_mixture;
+    int    formatted_output;
+
     int    precision;               /* PDAC_PREC_FP64 / PDAC_PREC_MIXED      */
 
     /* mesh metric and flags (read at create) */
@@ -226,10 +233,19 @@ int pdac_gpu_write_restart(pdac_ctx *ctx, const char *path, double time, int nfi
  * pdac_gpu_last_error on a missing file, bad framing or a dimension that
  * differs from the context's.                                              */
 int pdac_gpu_read_restart(pdac_ctx *ctx, const char *path, double *time, int *nfil);
-/* outp (outp.f:194-384), unformatted form: REAL(time, 4), then REAL*4
- * records of p, ug, [vg], wg, tg, xgc per gas, and per class rlk / rl, us,
- * [vs], ws, ts.  The caller names the file output.NNNN (lettera, letter.f). */
+/* outp (outp.f:194-384): p, ug, [vg], wg, tg, xgc per gas, and per class
+ * rlk / rl, us, [vs], ws, ts, then with compute_mixture rhom, um, [vm], wm,
+ * tm and yd per gas and class.  Unformatted (the default): REAL(time, 4)
+ * and one REAL*4 record per field.  With cfg formatted_output: text, a
+ * time header and per field its name and the values of each k plane,
+ * FORMAT(1x,10(1x,G14.6E3)) (io_parallel.f:38-50).  The caller names the
+ * file output.NNNN (lettera, letter.f).                                    */
 int pdac_gpu_write_output(pdac_ctx *ctx, const char *path, double time);
+/* compute_mixture_fields (mixture.f:32-52, prog.f:331): mixture density,
+ * velocity, temperature and mass fractions of every cell (cfg
+ * compute_mixture = 1; readable as rhom, um, vm, wm, tm, yd through
+ * pdac_gpu_get_array)                                                     */
+int pdac_gpu_compute_mixture_fields(pdac_ctx *ctx);
 /* print_mass_residuals (residuals.f:15-136): out = [res_g, res_s(nsolid),
  * res_gc(ngas), mfr], masses in the fluid cells minus the mass that entered
  * through inlet and vent cells in nswp steps of dt, and the vent mass flow

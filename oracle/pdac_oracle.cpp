@@ -122,6 +122,7 @@ struct Oracle {
     // solid (massl, ntr x ns with ntr = nx in 2D, nx ny in 3D) and the
     // values a restart adds back at each column's first update (mass_loss)
     vector<double> xc, yc, massl, mass_loss;
+    vector<double> rhom, um, vm, wm, tm, yd;  // mixture fields (mixture.f), yd (ncell, ng + ns)
     vector<double> mf3, ef3, yfn;   // 3D momentum / enthalpy face fluxes, species y-fluxes
     vector<double> smag, mugt, kapgt, must;  // sub-grid model (turbo.f:10-14)
     vector<double> scoeff;                   // dynamic coefficient cdyn of the last sgsg (modturbo = 2)
@@ -2126,6 +2127,44 @@ int pdac_oracle_ftem(void *h, double dt) {
     return o.d3 ? ftem_3d(o, dt) : ftem_2d(o, dt);
 }
 
+// compute_mixture_fields (mixture.f:32-52): derived.f:220-331 over every cell
+int pdac_oracle_compute_mixture_fields(void *h) {
+    Oracle &o = *(Oracle *)h;
+    const int n = o.ncell, ns = o.ns, ng = o.ng;
+    for (auto *v : {&o.rhom, &o.um, &o.vm, &o.wm, &o.tm}) v->assign(n, 0.0);
+    o.yd.assign((size_t)n * (ng + ns), 0.0);
+    for (int c = 0; c < n; ++c) {
+        double srl = 0.0;
+        for (int is = 1; is <= ns; ++is) srl = srl + o.S(o.rlk, c, is);
+        o.rhom[c] = o.rgp[c] + srl;
+        double cpgc[8];
+        hcapg(o, cpgc, o.tg[c]);
+        double cgas = 0.0;
+        for (int ig = 0; ig < ng; ++ig) cgas = cpgc[o.gas_type[ig]] * o.ygc[(size_t)ig * n + c] + cgas;
+        double sts = 0.0, scp = 0.0;
+        for (int is = 1; is <= ns; ++is) {
+            sts = sts + o.S(o.rlk, c, is) * o.cps[is] * o.S(o.ts, c, is);
+            scp = scp + o.S(o.rlk, c, is) * o.cps[is];
+        }
+        double tm = o.rgp[c] * cgas * o.tg[c] + sts;
+        double den = o.rgp[c] * cgas + scp;
+        o.tm[c] = tm / den;
+        auto velm = [&](const vector<double> &ug, const vector<double> &us) {
+            double sv = 0.0;
+            for (int is = 1; is <= ns; ++is) sv = sv + o.S(o.rlk, c, is) * us[(size_t)(is - 1) * n + c];
+            double v = o.rgp[c] * ug[c] + sv;
+            return v / o.rhom[c];
+        };
+        o.um[c] = velm(o.ug, o.us);
+        if (o.d3) o.vm[c] = velm(o.vg, o.vs);
+        o.wm[c] = velm(o.wg, o.ws);
+        double inrhom = 1.0 / o.rhom[c];
+        for (int ig = 0; ig < ng; ++ig) o.yd[(size_t)ig * n + c] = o.ygc[(size_t)ig * n + c] * o.rgp[c] * inrhom;
+        for (int is = 1; is <= ns; ++is) o.yd[(size_t)(ng + is - 1) * n + c] = o.S(o.rlk, c, is) * inrhom;
+    }
+    return PDAC_OK;
+}
+
 // sgsg / sgss as prog.f:207-208 calls them after fieldn
 int pdac_oracle_sgs(void *h) {
     Oracle &o = *(Oracle *)h;
@@ -2174,6 +2213,7 @@ int pdac_oracle_step(void *h, int sweep, int *nit) {
             if (s2 != PDAC_OK) st = s2;
             pdac_oracle_ygas(h, dt);
         }
+        if (o.cfg.compute_mixture) pdac_oracle_compute_mixture_fields(h);  // prog.f:331
         return st;
     }
     pdac_oracle_fieldn(h);
@@ -2195,6 +2235,7 @@ int pdac_oracle_step(void *h, int sweep, int *nit) {
             if (s2 != PDAC_OK) st = s2;
         }
     }
+    if (o.cfg.compute_mixture) pdac_oracle_compute_mixture_fields(h);  // prog.f:331
     return st;
 }
 
@@ -2218,7 +2259,8 @@ int pdac_oracle_get_array(void *h, const char *name, double *out, long *n_inout)
                {"rvgn", &o.rvgn}, {"rvsn", &o.rvsn}, {"rvg", &o.rvg}, {"rvs", &o.rvs}, {"appv", &o.appv},
                {"rgfn", &o.rgfn}, {"rsfn", &o.rsfn}, {"mf3", &o.mf3}, {"ef3", &o.ef3},
                {"gvisy", &o.gvisy}, {"pvisy", &o.pvisy}, {"hgfe", &o.hgfe}, {"hgft", &o.hgft},
-               {"hsfe", &o.hsfe}, {"hsft", &o.hsft}, {"smag", &o.smag}, {"scoeff", &o.scoeff}, {"massl", &o.massl}, {"mugt", &o.mugt}, {"kapgt", &o.kapgt},
+               {"hsfe", &o.hsfe}, {"hsft", &o.hsft}, {"smag", &o.smag}, {"scoeff", &o.scoeff}, {"massl", &o.massl}, {"rhom", &o.rhom}, {"um", &o.um},
+               {"vm", &o.vm}, {"wm", &o.wm}, {"tm", &o.tm}, {"yd", &o.yd}, {"mugt", &o.mugt}, {"kapgt", &o.kapgt},
                {"must", &o.must},
                // explicit-solver fields (explicit_solver.f:15-83)
                {"rgpstar", &o.rk.rgpS}, {"rlkstar", &o.rk.rlkS}, {"ugstar", &o.rk.ugS}, {"usstar", &o.rk.usS},

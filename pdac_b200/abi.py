@@ -60,6 +60,7 @@ class PdacCfg(C.Structure):
         ("irand", C.c_int),
         ("isink", C.c_int), ("rprox", C.c_double), ("rdist", C.c_double),
         ("center_x", C.c_double), ("center_y", C.c_double),
+        ("compute_mixture", C.c_int), ("formatted_output", C.c_int),
         ("precision", C.c_int),
         ("dx", _dp), ("dy", _dp), ("dz", _dp), ("flag", _ip),
         ("p_atm", _dp), ("t_atm", _dp),
@@ -130,6 +131,7 @@ def declare(lib, prefix, handle_type):
             "write_restart": [h, C.c_char_p, C.c_double, C.c_int],
             "read_restart": [h, C.c_char_p, _dp, C.POINTER(C.c_int)],
             "write_output": [h, C.c_char_p, C.c_double],
+            "compute_mixture_fields": [h],
             "mass_residuals": [h, C.c_int, C.c_double, _dp, C.c_int],
             "append_mass_check": [h, C.c_char_p, C.c_int, C.c_double],
             "write_mass_loss": [h, C.c_char_p],

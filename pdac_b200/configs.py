@@ -189,3 +189,20 @@ def small_2d_implicit(fluxes=True, enthalpy=True, **kw):
 def small_3d_implicit(fluxes=True, enthalpy=True, **kw):
     """small_3d with the implicit modes of small_2d_implicit."""
     return _implicit(small_3d(**kw), fluxes, enthalpy)
+
+
+def small_2d_mixture(formatted=False, **kw):
+    """small_2d with the mixture fields (compute_mixture) and, optionally,
+    text output files (formatted_output)."""
+    d = small_2d(**kw)
+    d.set("model", compute_mixture=True)
+    d.set("control", formatted_output=formatted)
+    return d
+
+
+def small_3d_mixture(formatted=False, **kw):
+    """small_3d with the options of small_2d_mixture."""
+    d = small_3d(**kw)
+    d.set("model", compute_mixture=True)
+    d.set("control", formatted_output=formatted)
+    return d

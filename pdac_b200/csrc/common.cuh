@@ -74,6 +74,7 @@ struct Fld {
     double *sink;
     double *smag, *mugt, *kapgt, *must;  // sub-grid model (turbo.f:10-14); must (ncell, ns)
     double *dyn, *delt, *scoeff;         // dynamic model: per-cell work blocks, filter width, cdyn
+    double *rhom, *um, *vm, *wm, *tm, *yd;  // mixture fields (mixture.f); yd (ncell, ng + ns)
     int *counters;  // [0] non-converged cells this sweep, [1] eos failures, [2] rls>1 cells, [3] boundary errors
 };
 

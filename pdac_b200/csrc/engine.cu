@@ -22,6 +22,7 @@
 #include "io.cuh"
 #include "les.cuh"
 #include "sink.cuh"
+#include "mixture.cuh"
 
 using namespace pdac;
 
@@ -418,6 +419,7 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     int t1 = ctx->ti == 1 ? 1 : 0, neq = (ctx->d3 ? 5 : 4) * ctx->nph;
     int lt = cfg->iturb >= 1 ? 1 : 0, ls = cfg->iss >= 1 ? 1 : 0;  // sub-grid model fields
     int ld = lt && ctx->d3 && cfg->modturbo == 2 ? 1 : 0;              // the dynamic model's
+    int lmix = cfg->compute_mixture ? 1 : 0;                           // mixture fields
     RkF &K = ctx->K;
     std::vector<Slot> slots = {
         {"p", &F.p, 1}, {"ep", &F.ep, 1}, {"rog", &F.rog, 1}, {"rgp", &F.rgp, 1}, {"tg", &F.tg, 1},
@@ -448,7 +450,9 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
         {"k1", &K.k1, neq * t1}, {"k2", &K.k2, neq * t1}, {"xrgp", &K.xrgp, t1}, {"xrlk", &K.xrlk, ns * t1},
         {"xep", &K.xep, t1}, {"xug", &K.xug, t1}, {"xvg", &K.xvg, t1 * d3}, {"xwg", &K.xwg, t1},
         {"smag", &F.smag, lt}, {"mugt", &F.mugt, lt}, {"kapgt", &F.kapgt, lt}, {"must", &F.must, ns * ls},
-        {"sgsdyn", &F.dyn, pdac::DY_N * ld}, {"delt", &F.delt, ld}, {"scoeff", &F.scoeff, ld}};
+        {"sgsdyn", &F.dyn, pdac::DY_N * ld}, {"delt", &F.delt, ld}, {"scoeff", &F.scoeff, ld},
+        {"rhom", &F.rhom, lmix}, {"um", &F.um, lmix}, {"vm", &F.vm, lmix * d3}, {"wm", &F.wm, lmix},
+        {"tm", &F.tm, lmix}, {"yd", &F.yd, (ng + ns) * lmix}};
     // each field starts on a 256-byte boundary
     size_t stride = ((size_t)n + 31) / 32 * 32;
     size_t total = 0;
@@ -1338,6 +1342,7 @@ int pdac_gpu_step(pdac_ctx *ctx, int sweep, int *nit) {
             else if (s) return s;
             if ((s = pdac_gpu_ygas(ctx, dt))) return s;
         }
+        if (ctx->cfg.compute_mixture && (s = pdac_gpu_compute_mixture_fields(ctx))) return s;  // prog.f:331
         return status;
     }
     if ((s = pdac_gpu_fieldn(ctx))) return s;
@@ -1363,6 +1368,7 @@ int pdac_gpu_step(pdac_ctx *ctx, int sweep, int *nit) {
             else if (s) return s;
         }
     }
+    if (ctx->cfg.compute_mixture && (s = pdac_gpu_compute_mixture_fields(ctx))) return s;  // prog.f:331
     return status;
 }
 
@@ -1522,40 +1528,96 @@ int pdac_gpu_read_restart(pdac_ctx *ctx, const char *path, double *time, int *nf
 // outp (outp.f:194-384), unformatted: REAL(time, 4), then single-precision
 // records of p, gas velocity, tg, xgc per gas, and per class eps = rlk/rl,
 // particle velocity and ts
+// outp (outp.f:194-384): the output fields in the reference's order; the
+// mixture fields follow with compute_mixture.  Unformatted: REAL(time, 4)
+// and one REAL*4 record per field.  Formatted (formatted_output):
+// '(1x,///,1x,"@@@ TIME = ",g11.4)', then per field a header
+// '(1x,//,1x,<name>,/)' and the values of each k plane (nx, or nx ny in 3D,
+// cells) with FORMAT(1x,10(1x,G14.6E3)), ten to a line
+// (write_array, io_parallel.f:38-50).
 int pdac_gpu_write_output(pdac_ctx *ctx, const char *path, double time) {
     if (!ctx || !path) return PDAC_ERR_ARG;
     const size_t n = ctx->ncell;
+    const bool lform = ctx->cfg.formatted_output != 0;
     Fld &F = ctx->F;
-    pdac::io::Writer w(path);
-    if (!w.ok) return fail(ctx, PDAC_ERR_ARG, std::string("write_output: cannot open ") + path);
-    float t4 = (float)time;
-    w.record(&t4, 4);
+    pdac::io::Writer w(lform ? nullptr : path);
+    std::string text;
+    if (lform) {
+        text = "\n\n\n @@@ TIME = " + pdac::io::fortran_g(time, 11, 4, 2) + "\n";
+    } else {
+        if (!w.ok) return fail(ctx, PDAC_ERR_ARG, std::string("write_output: cannot open ") + path);
+        float t4 = (float)time;
+        w.record(&t4, 4);
+    }
     std::vector<double> buf(n);
     std::vector<float> sgl(n);
-    auto put = [&](const double *d, double scale, bool scaled) -> int {
+    const size_t ntr = (size_t)ctx->nx * (ctx->d3 ? ctx->ny : 1);
+    auto put = [&](const char *head, const double *d, double scale, bool scaled) -> int {
         CK(cudaMemcpyAsync(buf.data(), d, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
-        for (size_t c = 0; c < n; ++c) sgl[c] = (float)(scaled ? buf[c] * scale : buf[c]);
-        w.record(sgl.data(), n * sizeof(float));
+        if (scaled)
+            for (size_t c = 0; c < n; ++c) buf[c] = buf[c] * scale;
+        if (!lform) {
+            for (size_t c = 0; c < n; ++c) sgl[c] = (float)buf[c];
+            w.record(sgl.data(), n * sizeof(float));
+            return PDAC_OK;
+        }
+        text += std::string("\n\n ") + head + "\n\n";
+        for (size_t first = 0; first < n; first += ntr) {
+            text += " ";
+            for (size_t q = 0; q < ntr; ++q) {
+                if (q > 0 && q % 10 == 0) text += "\n";
+                text += " " + pdac::io::fortran_g(buf[first + q], 14, 6, 3);
+            }
+            text += "\n";
+        }
         return PDAC_OK;
     };
+    auto name1 = [](const char *pre, int q) { return std::string(pre) + std::to_string(q); };
     int s;
-    if ((s = put(F.p, 1.0, false))) return s;
-    if ((s = put(F.ug, 1.0, false))) return s;
-    if (ctx->d3 && (s = put(F.vg, 1.0, false))) return s;
-    if ((s = put(F.wg, 1.0, false))) return s;
-    if ((s = put(F.tg, 1.0, false))) return s;
+    if ((s = put("P   ", F.p, 1.0, false))) return s;
+    if ((s = put("UG  ", F.ug, 1.0, false))) return s;
+    if (ctx->d3 && (s = put("VG  ", F.vg, 1.0, false))) return s;
+    if ((s = put("WG  ", F.wg, 1.0, false))) return s;
+    if ((s = put("TG  ", F.tg, 1.0, false))) return s;
     for (int ig = 0; ig < ctx->ng; ++ig)
-        if ((s = put(F.xgc + ig * n, 1.0, false))) return s;
+        if ((s = put(name1("XGC", ig + 1).c_str(), F.xgc + ig * n, 1.0, false))) return s;
     for (int is = 1; is <= ctx->ns; ++is) {
         size_t off = (size_t)(is - 1) * n;
-        if ((s = put(F.rlk + off, ctx->P.inrl[is], true))) return s;
-        if ((s = put(F.us + off, 1.0, false))) return s;
-        if (ctx->d3 && (s = put(F.vs + off, 1.0, false))) return s;
-        if ((s = put(F.ws + off, 1.0, false))) return s;
-        if ((s = put(F.ts + off, 1.0, false))) return s;
+        if ((s = put(name1("EPS", is).c_str(), F.rlk + off, ctx->P.inrl[is], true))) return s;
+        if ((s = put(name1(" US", is).c_str(), F.us + off, 1.0, false))) return s;
+        if (ctx->d3 && (s = put(name1(" VS", is).c_str(), F.vs + off, 1.0, false))) return s;
+        if ((s = put(name1(" WS", is).c_str(), F.ws + off, 1.0, false))) return s;
+        if ((s = put(name1(" TS", is).c_str(), F.ts + off, 1.0, false))) return s;
+    }
+    if (ctx->cfg.compute_mixture) {
+        if ((s = put("RHOM", F.rhom, 1.0, false))) return s;
+        if ((s = put("UM  ", F.um, 1.0, false))) return s;
+        if (ctx->d3 && (s = put("VM  ", F.vm, 1.0, false))) return s;
+        if ((s = put("WM  ", F.wm, 1.0, false))) return s;
+        if ((s = put("TM  ", F.tm, 1.0, false))) return s;
+        for (int q = 1; q <= ctx->ng + ctx->ns; ++q)
+            if ((s = put(name1("YD", q).c_str(), F.yd + (size_t)(q - 1) * n, 1.0, false))) return s;
+    }
+    if (lform) {
+        FILE *f = std::fopen(path, "w");
+        if (!f) return fail(ctx, PDAC_ERR_ARG, std::string("write_output: cannot open ") + path);
+        bool ok = std::fputs(text.c_str(), f) >= 0;
+        ok = (std::fclose(f) == 0) && ok;
+        if (!ok) return fail(ctx, PDAC_ERR_ARG, std::string("write_output: write error on ") + path);
+        return PDAC_OK;
     }
     if (!w.close()) return fail(ctx, PDAC_ERR_ARG, std::string("write_output: write error on ") + path);
+    return PDAC_OK;
+}
+
+int pdac_gpu_compute_mixture_fields(pdac_ctx *ctx) {
+    if (!ctx) return PDAC_ERR_ARG;
+    if (!ctx->F.rhom) return fail(ctx, PDAC_ERR_CONFIG, "compute_mixture_fields: the run has compute_mixture = 0");
+    if (ctx->d3) pdac::k_mixture<3><<<blocks(ctx->ncell), TPB, 0, ctx->stream>>>(ctx->P, ctx->F);
+    else pdac::k_mixture<2><<<blocks(ctx->ncell), TPB, 0, ctx->stream>>>(ctx->P, ctx->F);
+    ctx->launches++;
+    CK(cudaGetLastError());
     return PDAC_OK;
 }
 

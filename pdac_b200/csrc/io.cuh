@@ -111,7 +111,7 @@ constexpr int64_t SUBREC_MAX = 2147483639;
 struct Writer {
     FILE *f = nullptr;
     bool ok = true;
-    explicit Writer(const char *path) { f = std::fopen(path, "wb"); ok = f != nullptr; }
+    explicit Writer(const char *path) { f = path ? std::fopen(path, "wb") : nullptr; ok = f != nullptr; }
     ~Writer() { if (f) std::fclose(f); }
     void raw(const void *p, size_t n) { if (ok && n && std::fwrite(p, 1, n, f) != n) ok = false; }
     void record(const void *data, size_t bytes) {

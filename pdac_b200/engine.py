@@ -70,7 +70,8 @@ EXPORTED = (
     "pdac_gpu_get_array", "pdac_gpu_mass_totals", "pdac_gpu_phase_times", "pdac_gpu_stats",
     "pdac_gpu_reset_stats", "pdac_gpu_mark", "pdac_gpu_elapsed",
     "pdac_gpu_write_restart", "pdac_gpu_read_restart", "pdac_gpu_write_output", "pdac_gpu_mass_residuals",
-    "pdac_gpu_append_mass_check", "pdac_gpu_write_mass_loss", "pdac_gpu_read_mass_loss", "pdac_gpu_batch_create", "pdac_gpu_batch_step", "pdac_gpu_batch_elapsed",
+    "pdac_gpu_append_mass_check", "pdac_gpu_write_mass_loss", "pdac_gpu_read_mass_loss",
+    "pdac_gpu_compute_mixture_fields", "pdac_gpu_batch_create", "pdac_gpu_batch_step", "pdac_gpu_batch_elapsed",
     "pdac_gpu_batch_last_error", "pdac_gpu_batch_destroy",
 )
 
@@ -201,6 +202,10 @@ class Engine:
         """Append the pdac.chm line of step nswp to path."""
         dt = self.case.deck["dt"] if dt is None else dt
         self._chk(self.L.pdac_gpu_append_mass_check(self.h, os.fsencode(path), int(nswp), float(dt)), "append_mass_check")
+
+    def compute_mixture_fields(self):
+        """compute_mixture_fields (prog.f:331): rhom, um, vm, wm, tm, yd."""
+        self._chk(self.L.pdac_gpu_compute_mixture_fields(self.h), "compute_mixture_fields")
 
     def write_mass_loss(self, path):
         """print_mass_loss: the ground columns' lost mass (massl.NNNN / massl.res)."""

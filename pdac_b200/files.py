@@ -105,6 +105,8 @@ def run(engine, workdir, max_steps=None, log=None):
                 engine.ygas(dtr)
                 engine.htilde(dtr)
                 engine.ftem(dtr)
+        if d["compute_mixture"]:
+            engine.compute_mixture_fields()  # prog.f:331
         t = t + dt
         if log:
             log.write(f"Iteration: {sweep:6d} nit: {0 if explicit else nit:5d}\n")

@@ -429,6 +429,8 @@ class Case:
         c.isink = int(d["isink"])
         c.rprox, c.rdist = float(d["rprox"]), float(d["rdist"])
         c.center_x, c.center_y = float(d["center_x"]), float(d["center_y"])
+        c.compute_mixture = int(bool(d["compute_mixture"]))
+        c.formatted_output = int(bool(d["formatted_output"]))
         c.precision = self.precision
         keep = dict(dx=np.ascontiguousarray(self.dx), dy=np.ascontiguousarray(self.dy),
                     dz=np.ascontiguousarray(self.dz), flag=np.ascontiguousarray(self.flag, dtype=np.int32),

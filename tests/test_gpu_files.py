@@ -216,3 +216,106 @@ def test_time_loop_driver_files(tmp_path):
     eng2 = Engine(Case(d))
     t2, nfil2, sweep2 = files.run(eng2, str(tmp_path), max_steps=2)
     assert sweep2 == 6 and nfil2 == 4
+
+
+@pytest.mark.parametrize("builder", ["small_2d_mixture", "small_3d_mixture"])
+def test_mixture_fields_match_oracle(builder):
+    """compute_mixture_fields after every step (prog.f:331): mixture
+    density, velocity, temperature and mass fractions against the oracle at
+    the step tolerance."""
+    import pyoracle
+    from pdac_b200 import configs
+    from pdac_b200.engine import Engine
+    from pdac_b200.setup_state import Case
+    case = Case(getattr(configs, builder)())
+    eng = Engine(case)
+    ora = pyoracle.Oracle(case, order=pyoracle.ORDER_COLORED)
+    names = ["rhom", "um", "wm", "tm", "yd"] + (["vm"] if case.is3d else [])
+    for s in (1, 2, 3):
+        assert eng.step(s) == ora.step(s)
+        for name in names:
+            assert rel_linf(eng.get(name), ora.get(name)) <= 1e-9, (s, name)
+    eng.close()
+
+
+def _formatted_blocks(text):
+    """Split a formatted output file into (time line, [(name, values)])."""
+    lines = text.split("\n")
+    assert lines[:3] == ["", "", ""] and lines[3].startswith(" @@@ TIME = ")
+    blocks, q = [], 4
+    while q < len(lines) and lines[q:q + 2] == ["", ""] and q + 3 < len(lines):
+        name = lines[q + 2]
+        assert lines[q + 3] == ""
+        q += 4
+        rows = []
+        while q < len(lines) and lines[q] != "":
+            rows.append(lines[q])
+            q += 1
+        blocks.append((name, rows))
+    assert q == len(lines) - 1 and lines[-1] == ""
+    return lines[3], blocks
+
+
+@pytest.mark.parametrize("builder", ["small_2d_mixture", "small_3d_mixture"])
+def test_formatted_output_layout(builder, tmp_path):
+    """outp with formatted_output: the time header, then per field its name
+    and the values plane by plane, FORMAT(1x,10(1x,G14.6E3)) (io_parallel.f:
+    38-50), the mixture fields last."""
+    from pdac_b200 import configs
+    from pdac_b200.engine import Engine
+    from pdac_b200.setup_state import Case
+    case = Case(getattr(configs, builder)(formatted=True))
+    eng = Engine(case)
+    eng.step(1)
+    path = str(tmp_path / "output.0001")
+    eng.write_output(path, 0.01)
+    head, blocks = _formatted_blocks(open(path).read())
+    assert head == " @@@ TIME = " + fortran_g(0.01, 11, 4, 2)
+    st = eng.download()
+    n, ns, ng = case.ncell, case.nsolid, case.ngas
+    blk = lambda a, q: a[q * n:(q + 1) * n]
+    want = [("P   ", st["p"]), ("UG  ", st["ug"])] + ([("VG  ", st["vg"])] if case.is3d else [])
+    want += [("WG  ", st["wg"]), ("TG  ", st["tg"])]
+    want += [(f"XGC{g + 1}", blk(st["xgc"], g)) for g in range(ng)]
+    for q in range(ns):
+        want += [(f"EPS{q + 1}", blk(st["rlk"], q) * (1.0 / case.deck["density"][q])),
+                 (f" US{q + 1}", blk(st["us"], q))]
+        want += [(f" VS{q + 1}", blk(st["vs"], q))] if case.is3d else []
+        want += [(f" WS{q + 1}", blk(st["ws"], q)), (f" TS{q + 1}", blk(st["ts"], q))]
+    mix = {k: eng.get(k) for k in ("rhom", "um", "vm", "wm", "tm", "yd") if k != "vm" or case.is3d}
+    want += [("RHOM", mix["rhom"]), ("UM  ", mix["um"])] + ([("VM  ", mix["vm"])] if case.is3d else [])
+    want += [("WM  ", mix["wm"]), ("TM  ", mix["tm"])]
+    want += [(f"YD{q + 1}", blk(mix["yd"], q)) for q in range(ng + ns)]
+    assert [b[0] for b in blocks] == [" " + w[0] for w in want]
+    ntr = case.nx * (case.ny if case.is3d else 1)
+    for (name, rows), (_, vals) in zip(blocks, want):
+        expect = []
+        for first in range(0, n, ntr):
+            plane = [" " + fortran_g(v, 14, 6, 3) for v in vals[first:first + ntr]]
+            chunks = ["".join(plane[r:r + 10]) for r in range(0, ntr, 10)]
+            chunks[0] = " " + chunks[0]
+            expect += chunks
+        assert rows == expect, name
+    eng.close()
+
+
+def test_unformatted_output_with_mixture_fields(tmp_path):
+    """The unformatted output ends with the mixture fields' REAL*4 records."""
+    from pdac_b200 import configs
+    from pdac_b200.engine import Engine
+    from pdac_b200.setup_state import Case
+    case = Case(configs.small_2d_mixture())
+    eng = Engine(case)
+    eng.step(1)
+    path = str(tmp_path / "output.0001")
+    eng.write_output(path, 0.01)
+    recs = fortran_records(path)
+    ns, ng = case.nsolid, case.ngas
+    assert len(recs) == 1 + 4 + ng + 4 * ns + 4 + ng + ns
+    n = case.ncell
+    tail = [eng.get("rhom"), eng.get("um"), eng.get("wm"), eng.get("tm")]
+    yd = eng.get("yd")
+    tail += [yd[q * n:(q + 1) * n] for q in range(ng + ns)]
+    for r, a in zip(recs[-len(tail):], tail):
+        np.testing.assert_array_equal(np.frombuffer(r, dtype="<f4"), a.astype(np.float32))
+    eng.close()
