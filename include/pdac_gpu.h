@@ -307,7 +307,10 @@ int pdac_gpu_elapsed(pdac_ctx *ctx, int a, int b, double *ms);
  * by one time step each, pdac_gpu_step(member, sweep, ...) on every member,
  * with the members' kernels running concurrently on the device: a pool of
  * nthreads host threads (<= 0: one per member) drives the members' own
- * streams.  The batch does not own the members: create, upload and download
+ * streams.  While in a batch, members run without cooperative launches
+ * (the small-domain sweep loop and the explicit solver's wavefront take
+ * their multi-launch forms, with the same results), so that no two
+ * cooperative grids share the device.  The batch does not own the members: create, upload and download
  * them with the per-context calls, never while a batch step runs, and
  * destroy the batch before them.  A member appears once.
  * pdac_gpu_batch_step fills nit[m] and status[m] (either may be NULL) for

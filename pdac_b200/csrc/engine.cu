@@ -58,6 +58,14 @@ struct pdac_ctx {
     cudaGraphExec_t it_exec = nullptr;
     double it_dt = 0.0;
     long long it_per_sweep = 10;  // kernels of one sweep of that graph
+    // small domains: the whole sweep loop as one cooperative launch of
+    // coop_blocks blocks (0: the graph)
+    int coop_blocks = 0;
+    // cooperative launches (the small-domain sweep loop, the explicit
+    // solver's wavefront) only when the context is not stepped alongside
+    // others: a batch turns them off in its members, so that no two
+    // cooperative grids are in flight on the device at once
+    bool allow_coop = true;
     std::vector<double> sweep_log;  // per colour phase when profiling: sweep, colour, worklist, tested, ms x2
     bool prof = false;
     cudaEvent_t cev[9];
@@ -297,6 +305,68 @@ int setup_wave(pdac_ctx *ctx, const int *flag) {
 
 }  // namespace
 
+// Domains of at most this many cells run iter's sweep loop as one
+// cooperative launch (k_iter_coop): their colour phases are a few
+// microseconds of work each, less than the launch of a graph node.
+#ifndef PDAC_COOP_MAX_CELLS
+#define PDAC_COOP_MAX_CELLS (1 << 18)
+#endif
+#ifndef PDAC_COOP_CELLS_PER_BLOCK
+#define PDAC_COOP_CELLS_PER_BLOCK 1024
+#endif
+
+template <int NP>
+static cudaError_t launch_iter_coop_np(pdac_ctx *ctx, double dt, cudaStream_t st, const pdac::SweepWork &W) {
+    cudaLaunchConfig_t lc = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    lc.gridDim = dim3(ctx->coop_blocks);
+    lc.blockDim = dim3(TPB_TEAM);
+    lc.stream = st;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    if (ctx->d3) return cudaLaunchKernelEx(&lc, pdac::k_iter_coop<NP, 3>, ctx->P, ctx->F, dt, W, ctx->cfg.maxout);
+    return cudaLaunchKernelEx(&lc, pdac::k_iter_coop<NP, 2>, ctx->P, ctx->F, dt, W, ctx->cfg.maxout);
+}
+
+static cudaError_t launch_iter_coop(pdac_ctx *ctx, double dt, cudaStream_t st, const pdac::SweepWork &W) {
+    switch (ctx->nph) {
+        case 2: return launch_iter_coop_np<2>(ctx, dt, st, W);
+        case 3: return launch_iter_coop_np<3>(ctx, dt, st, W);
+        case 4: return launch_iter_coop_np<4>(ctx, dt, st, W);
+        case 6: return launch_iter_coop_np<6>(ctx, dt, st, W);
+        default: return launch_iter_coop_np<0>(ctx, dt, st, W);
+    }
+}
+
+// the cooperative grid of a small domain: one block of 128 threads per
+// PDAC_COOP_CELLS_PER_BLOCK cells, within what the device holds at once
+// (measured on the 128 x 192 2D plume: 1024 and 256 cells per block run
+// the step in 6.43 ms, 4096 in 7.46 ms, 64 in 6.76 ms)
+static int setup_iter_coop(pdac_ctx *ctx) {
+    ctx->coop_blocks = 0;
+    if ((long)ctx->ncell > PDAC_COOP_MAX_CELLS) return PDAC_OK;
+    int dev = 0, coop = 0, nsm = 0, occ = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    if (!coop) return PDAC_OK;
+    auto occ_of = [&](auto kernel) { return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, TPB_TEAM, 0); };
+    cudaError_t e;
+    switch (ctx->nph) {
+        case 2: e = ctx->d3 ? occ_of(pdac::k_iter_coop<2, 3>) : occ_of(pdac::k_iter_coop<2, 2>); break;
+        case 3: e = ctx->d3 ? occ_of(pdac::k_iter_coop<3, 3>) : occ_of(pdac::k_iter_coop<3, 2>); break;
+        case 4: e = ctx->d3 ? occ_of(pdac::k_iter_coop<4, 3>) : occ_of(pdac::k_iter_coop<4, 2>); break;
+        case 6: e = ctx->d3 ? occ_of(pdac::k_iter_coop<6, 3>) : occ_of(pdac::k_iter_coop<6, 2>); break;
+        default: e = ctx->d3 ? occ_of(pdac::k_iter_coop<0, 3>) : occ_of(pdac::k_iter_coop<0, 2>); break;
+    }
+    CK(e);
+    const int want = std::max(1, (int)((ctx->ncell + PDAC_COOP_CELLS_PER_BLOCK - 1) / PDAC_COOP_CELLS_PER_BLOCK));
+    ctx->coop_blocks = std::min(want, occ * nsm);
+    return PDAC_OK;
+}
+
 extern "C" {
 
 const char *pdac_gpu_last_error(const pdac_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
@@ -510,6 +580,9 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     CK(cudaMalloc(&ctx->d_partial, (size_t)nq * 1024 * sizeof(double)));
     if (t1) {
         int st = setup_wave(ctx, cfg->flag);
+        if (st) return st;
+    } else {
+        int st = setup_iter_coop(ctx);
         if (st) return st;
     }
     if (cfg->isink > 0) {
@@ -854,7 +927,17 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
     // every cell is tested in the first sweep
     CK(cudaMemsetAsync(ctx->d_dirty, 0xff, (n + 31) / 32 * sizeof(unsigned), st));
     int nit;
-    if (!ctx->prof) {
+    const bool coop = ctx->coop_blocks > 0 && ctx->allow_coop && !ctx->cfg.implicit_fluxes && !ctx->cfg.implicit_enthalpy;
+    if (!ctx->prof && coop) {
+        // small domain: the sweep loop in one cooperative launch
+        pdac::SweepWork W{ctx->d_wcount, ctx->d_cand, ctx->d_work, ctx->d_dirty, ctx->d_nit};
+        CK(launch_iter_coop(ctx, dt, st, W));
+        CK(cudaMemcpyAsync(ctx->h_nit, ctx->d_nit, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        nit = *ctx->h_nit;
+        ctx->sweeps += std::min(nit, ctx->cfg.maxout);
+        ctx->launches++;
+    } else if (!ctx->prof) {
         // the sweep loop runs on the device; one read-back of its count
         if (!ctx->it_exec || ctx->it_dt != dt) {
             int s = build_iter_graph(ctx, dt);
@@ -1214,7 +1297,7 @@ static long long enqueue_explicit(pdac_ctx *ctx, double dt, cudaStream_t st, boo
         // gas-enthalpy wavefront over the hyperplanes i + j + k = d of the
         // interior (2 <= i <= nx - 1 ...), in increasing d: records, one
         // cooperative launch over all hyperplanes, scatter of the results
-        if (ctx->wave_grid_blocks > 0) {
+        if (ctx->wave_grid_blocks > 0 && ctx->allow_coop) {
             const pdac::Wave &W = ctx->W;
             const int rb = blocks(W.npos);
             cudaLaunchConfig_t lc = {};
@@ -1894,6 +1977,10 @@ static void batch_free(pdac_batch *b) {
     }
     b->go.notify_all();
     for (auto &t : b->th) t.join();
+    for (pdac_ctx *c : b->m) {
+        c->allow_coop = true;
+        c->ex_dt = -1.0;
+    }
     for (auto e : b->fin) if (e) cudaEventDestroy(e);
     if (b->t0) cudaEventDestroy(b->t0);
     if (b->t1) cudaEventDestroy(b->t1);
@@ -1914,6 +2001,12 @@ int pdac_gpu_batch_create(pdac_ctx *const *members, int nmember, int nthreads, p
     int nt = nthreads > 0 ? std::min(nthreads, nmember) : nmember;
     pdac_batch *b = new pdac_batch();
     b->m.assign(members, members + nmember);
+    // members take the non-cooperative paths while in the batch (the
+    // explicit_iter graph, built with the cooperative wavefront, is rebuilt)
+    for (pdac_ctx *c : b->m) {
+        c->allow_coop = false;
+        c->ex_dt = -1.0;
+    }
     b->nit.assign(nmember, 0);
     b->status.assign(nmember, 0);
     b->fin.assign(nmember, nullptr);

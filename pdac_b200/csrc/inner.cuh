@@ -13,9 +13,20 @@
 // fluxes stay in registers until the final store (nothing else touches the
 // cell's neighbourhood within a colour phase).
 #pragma once
+#include <cooperative_groups.h>
 #include "kernels3d.cuh"
 
 namespace pdac {
+
+// a load of a value that no thread of the current launch writes: through
+// the read-only cache in the one-launch-per-colour-phase form (RO); a plain
+// load in the persistent form, where other blocks write it between the
+// phases (separated by grid-wide barriers)
+template <bool RO>
+__device__ __forceinline__ double ldro(const double *p) {
+    if (RO) return __ldg(p);
+    return *p;
+}
 
 // mass flux through one face (masf + fmas, flux_m.f:47-324), written for a
 // face on the minus side (W/S/B) or the plus side (E/N/T) of the cell.
@@ -63,7 +74,7 @@ struct FaceK {
     double pnb, d0epnb, K1, K2, d1, inv;
 };
 
-template <int NP>
+template <int NP, bool RO>
 __device__ __forceinline__ void face_prepare(const Prm &P, const Fld &F, int c, int nb, int raw, int ii, int dir,
                                              int side, double dt, FaceK<NP> &K) {
     const int nph = nphases<NP>(P);
@@ -79,21 +90,21 @@ __device__ __forceinline__ void face_prepare(const Prm &P, const Fld &F, int c, 
     int rowc = side > 0 ? c : raw;
     K.d1 = d1;
     K.inv = inv;
-    K.pnb = __ldg(F.p + nb);
-    K.d0epnb = P.pmodel == 1 ? d0 * __ldg(F.ep + nb) : 0.0;
+    K.pnb = ldro<RO>(F.p + nb);
+    K.d0epnb = P.pmodel == 1 ? d0 * ldro<RO>(F.ep + nb) : 0.0;
     K.K1 = alpha * dt * inv * 2.0;
     K.K2 = dt * ag * inv * grav;
-    K.brow[0] = __ldg(rg + rowc);
-    K.d0rn[0] = d0 * __ldg(F.rgp + nb);
+    K.brow[0] = ldro<RO>(rg + rowc);
+    K.d0rn[0] = d0 * ldro<RO>(F.rgp + nb);
 #pragma unroll
     for (int l = 2; l <= nph; ++l) {
-        K.brow[l - 1] = __ldg(rs + (l - 2) * n + rowc);
-        K.d0rn[l - 1] = d0 * __ldg(F.rlk + (l - 2) * n + nb);
+        K.brow[l - 1] = ldro<RO>(rs + (l - 2) * n + rowc);
+        K.d0rn[l - 1] = d0 * ldro<RO>(F.rlk + (l - 2) * n + nb);
     }
     const int nap = nph * (nph + 1) / 2;
 #pragma unroll
     for (int ls = 1; ls <= nap; ++ls)
-        K.A[ls - 1] = alpha * (d0 * __ldg(app + (ls - 1) * n + nb) + d1 * __ldg(app + (ls - 1) * n + c)) * inv;
+        K.A[ls - 1] = alpha * (d0 * ldro<RO>(app + (ls - 1) * n + nb) + d1 * ldro<RO>(app + (ls - 1) * n + c)) * inv;
 }
 
 // the in-loop assembly and solution; side as in face_system
@@ -136,10 +147,11 @@ __device__ __forceinline__ void face_assemble(const Prm &P, const FaceK<NP> &K, 
 #define PDAC_INNER_MINB 2
 #endif
 
-template <int NP, int D>
-__global__ void __launch_bounds__(128, PDAC_INNER_MINB) k_inner_team(Prm P, Fld F, double dt, const int *nitp, const int *list,
-                                                                     const int *count, unsigned *dirty) {
-    const int nit = *nitp;  // outer sweep number, 1-based
+// the inner loop of the worklist's nwork cells (outer sweep nit, 1-based)
+// by the warps warp, warp + nwarps, ... of the launch; RO as in ldro
+template <int NP, int D, bool RO>
+__device__ __forceinline__ void inner_team_run(const Prm &P, const Fld &F, double dt, int nit, const int *list,
+                                               int nwork, unsigned *dirty, int warp, int nwarps) {
     constexpr int T = D == 3 ? 6 : 4;    // lanes per cell
     constexpr int TPW = 32 / T;          // teams per warp (3D: 5, lanes 30 and 31 idle)
     constexpr int NC = Sys<NP>::M - 1;   // phase capacity
@@ -149,8 +161,6 @@ __global__ void __launch_bounds__(128, PDAC_INNER_MINB) k_inner_team(Prm P, Fld 
     if (tw >= TPW) return;  // idle lanes take no part in any team
     const int q = lane - tw * T, tb = tw * T;
     const unsigned tmask = ((1u << T) - 1u) << tb;
-    const int nwork = *count;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
     for (int w = warp * TPW + tw; w < nwork; w += nwarps * TPW) {
         const int c = list[w];
         int i, j, k;
@@ -204,17 +214,17 @@ __global__ void __launch_bounds__(128, PDAC_INNER_MINB) k_inner_team(Prm P, Fld 
 #pragma unroll
         for (int l = 2; l <= nph; ++l) vel[l - 1] = svel[(l - 2) * n + fcell];
         FaceK<NP> K;
-        if (solved) face_prepare<NP>(P, F, c, minus ? rm : rp, rawnb, ii, dir, minus ? -1 : +1, dt, K);
+        if (solved) face_prepare<NP, RO>(P, F, c, minus ? rm : rp, rawnb, ii, dir, minus ? -1 : +1, dt, K);
         // mass-flux stencil of this face by phase (gas first): neighbour
         // values, or the cell's own current value where the slot is the cell
         const int rfar = minus ? rmm : rpp;
         const bool sm = rm == c, sp = rp == c, sfar = rfar == c;
         double cm[NC], cp[NC], cfar[NC];
-        cm[0] = __ldg(F.rgp + rm); cp[0] = __ldg(F.rgp + rp); cfar[0] = mus ? __ldg(F.rgp + rfar) : 0.0;
+        cm[0] = ldro<RO>(F.rgp + rm); cp[0] = ldro<RO>(F.rgp + rp); cfar[0] = mus ? ldro<RO>(F.rgp + rfar) : 0.0;
 #pragma unroll
         for (int l = 2; l <= nph; ++l) {
             const double *D_ = F.rlk + (size_t)(l - 2) * n;
-            cm[l - 1] = __ldg(D_ + rm); cp[l - 1] = __ldg(D_ + rp); cfar[l - 1] = mus ? __ldg(D_ + rfar) : 0.0;
+            cm[l - 1] = ldro<RO>(D_ + rm); cp[l - 1] = ldro<RO>(D_ + rp); cfar[l - 1] = mus ? ldro<RO>(D_ + rfar) : 0.0;
         }
         auto mflux = [&](int ph, double own) {
             double dm = sm ? own : cm[ph], dp = sp ? own : cp[ph], df = sfar ? own : cfar[ph];
@@ -330,6 +340,13 @@ __global__ void __launch_bounds__(128, PDAC_INNER_MINB) k_inner_team(Prm P, Fld 
     }
 }
 
+template <int NP, int D>
+__global__ void __launch_bounds__(128, PDAC_INNER_MINB) k_inner_team(Prm P, Fld F, double dt, const int *nitp, const int *list,
+                                                                     const int *count, unsigned *dirty) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    inner_team_run<NP, D, true>(P, F, dt, *nitp, list, *count, dirty, warp, nwarps);
+}
+
 // Residual test of one colour phase (iter.f:241-319) in two launches.
 // The active set is one bit per cell: the test of a cell reads only its own
 // p/rog/rgp and the mass fluxes of its faces, which change only when the
@@ -340,10 +357,14 @@ __global__ void __launch_bounds__(128, PDAC_INNER_MINB) k_inner_team(Prm P, Fld 
 // bits of non-fluid cells, which are never tested); k_resid_test tests each
 // candidate: a converged cell updates its volume fractions (calc_eps) and
 // rgp, an unconverged one goes to the worklist of k_inner_team.
-__global__ void __launch_bounds__(TPB_RESID) k_resid_collect(Prm P, int colour, unsigned *dirty, int *cand,
-                                                             int *ncand) {
+// candidates of one colour: the block's threads take consecutive words of
+// the bitmask, block-uniform rounds over the grid (one round when the grid
+// covers the words)
+template <int TPBK>
+__device__ __forceinline__ void collect_phase(const Prm &P, int colour, unsigned *dirty, int *cand, int *ncand) {
     const unsigned nwords = ((unsigned)P.ncell + 31u) / 32u;
-    unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    for (unsigned base = blockIdx.x * (unsigned)TPBK; base < nwords; base += gridDim.x * (unsigned)TPBK) {
+    unsigned t = base + threadIdx.x;
     int mine[32], nmine = 0;
     if (t < nwords) {
         unsigned w = dirty[t], keep = w;
@@ -360,14 +381,20 @@ __global__ void __launch_bounds__(TPB_RESID) k_resid_collect(Prm P, int colour, 
         }
         if (keep != dirty[t]) dirty[t] = keep;
     }
-    block_append_n<TPB_RESID, 32>(cand, ncand, mine, nmine, nullptr, 0);
+    block_append_n<TPBK, 32>(cand, ncand, mine, nmine, nullptr, 0);
+    }
 }
 
-template <int NP, int D>
-__global__ void __launch_bounds__(TPB_RESID) k_resid_test(Prm P, Fld F, double dt, const int *cand, const int *ncand,
-                                                          int *work, int *count) {
-    const int len = *ncand;
-    for (int base = blockIdx.x * TPB_RESID; base < len; base += gridDim.x * TPB_RESID) {
+__global__ void __launch_bounds__(TPB_RESID) k_resid_collect(Prm P, int colour, unsigned *dirty, int *cand,
+                                                             int *ncand) {
+    collect_phase<TPB_RESID>(P, colour, dirty, cand, ncand);
+}
+
+// the residual test of the len candidates, block-uniform rounds
+template <int TPBK, int NP, int D>
+__device__ __forceinline__ void test_phase(const Prm &P, const Fld &F, double dt, const int *cand, int len, int *work,
+                                           int *count) {
+    for (int base = blockIdx.x * TPBK; base < len; base += gridDim.x * TPBK) {
         int idx = base + threadIdx.x, c = -1, nmine = 0;
         if (idx < len) {
             c = cand[idx];
@@ -389,8 +416,55 @@ __global__ void __launch_bounds__(TPB_RESID) k_resid_test(Prm P, Fld F, double d
             if (fabs(dg) <= F.conv[c]) F.rgp[c] = F.ep[c] * F.rog[c];
             else nmine = 1;
         }
-        block_append_n<TPB_RESID, 1>(work, count, &c, nmine, count + 3, idx < len ? 1 : 0);
+        block_append_n<TPBK, 1>(work, count, &c, nmine, count + 3, idx < len ? 1 : 0);
     }
+}
+
+template <int NP, int D>
+__global__ void __launch_bounds__(TPB_RESID) k_resid_test(Prm P, Fld F, double dt, const int *cand, const int *ncand,
+                                                          int *work, int *count) {
+    test_phase<TPB_RESID, NP, D>(P, F, dt, cand, *ncand, work, count);
+}
+
+// The whole outer sweep loop of iter (iter.f:204-410) in one cooperative
+// launch, for small domains: the colour phases' collect, test and inner
+// loop follow each other across grid-wide barriers instead of launches.
+// Every thread of the grid takes every barrier the same number of times:
+// the loop ends on counters that all threads read after the same barrier.
+struct SweepWork {
+    int *wcount;      // [col] worklist length, [3 + col] cells tested, [6 + col] candidates
+    int *cand, *work; // candidate list and worklist of one colour phase
+    unsigned *dirty;  // active set, one bit per cell
+    int *nit;         // the sweep count on return, as the graph's k_sweep_check leaves it
+};
+
+template <int NP, int D>
+__global__ void __launch_bounds__(128, PDAC_INNER_MINB) k_iter_coop(Prm P, Fld F, double dt, SweepWork W, int maxout) {
+    namespace cg = cooperative_groups;
+    cg::grid_group g = cg::this_grid();
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    int nit = 1;
+    for (;;) {
+        if (blockIdx.x == 0 && threadIdx.x < 9) W.wcount[threadIdx.x] = 0;
+        g.sync();
+        for (int col = 0; col < 3; ++col) {
+            collect_phase<128>(P, col, W.dirty, W.cand, W.wcount + 6 + col);
+            g.sync();
+            test_phase<128, NP, D>(P, F, dt, W.cand, __ldcg(W.wcount + 6 + col), W.work, W.wcount + col);
+            g.sync();
+            inner_team_run<NP, D, false>(P, F, dt, nit, W.work, __ldcg(W.wcount + col), W.dirty, warp, nwarps);
+            g.sync();
+        }
+        const long unconverged = (long)__ldcg(W.wcount) + __ldcg(W.wcount + 1) + __ldcg(W.wcount + 2);
+        if (unconverged == 0) break;
+        if (nit >= maxout) {
+            nit = maxout + 1;
+            break;
+        }
+        ++nit;
+        g.sync();  // every thread has read the counters before they are cleared
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *W.nit = nit;
 }
 
 // End of one outer sweep on the device (iter.f:388-410): with no unconverged
