@@ -18,6 +18,10 @@ does not depend on how many members are drawn or on which rank draws it.
 
 :func:`split` partitions the members over ranks (one GPU each) by the
 longest-processing-time rule on cell counts; ranks exchange nothing.
+
+The CUDA runtime maps streams onto CUDA_DEVICE_MAX_CONNECTIONS hardware
+queues (8 by default, read when CUDA starts in the process): set it to 32
+before CUDA starts so that the members' streams do not share queues.
 """
 from __future__ import annotations
 
