@@ -3,9 +3,11 @@
 The reference runs one domain per job; an ensemble there is many jobs.  Here
 a batch (``pdac_gpu_batch_*`` in include/pdac_gpu.h) steps many engine
 contexts at once, each on its own stream, so that small 2D members, which
-fill a few percent of a B200 each, run side by side.  Every member follows
-exactly the single-context path, so a member of a batch produces the same
-bits as the same deck run alone.
+fill a few percent of a B200 each, run side by side.  A member computes
+exactly what it computes alone: in the batch its sweep loop and wavefront
+take their multi-launch forms instead of one cooperative launch, with the
+same arithmetic, so a member of a batch produces the same bits as the same
+deck run alone.
 
 :func:`member_decks` draws the members of the 2D cylindrical ensemble: the
 plume of :func:`pdac_b200.configs.plume_2d` (10 m cells, axis vent of radius
