@@ -80,6 +80,13 @@ typedef struct pdac_cfg {
                                    at the end of every outer sweep
                                    (iter.f:362-379), htilde before iter
                                    otherwise (prog.f:246-292)               */
+    int    optimization;        /* inner loop of the corrector: 1 inner_loop
+                                   (iter.f:480-580), 2 opt_inner_loop
+                                   (iter.f:1255-1547), whose density
+                                   stencils keep the loop-entry value of the
+                                   cell where a neighbour slot is the cell
+                                   itself; 3 is 2 outside 3D with two
+                                   classes (iter.f:160-161)                 */
 
     /* &model */
     int    pmodel, drag_model, icpc;

@@ -1231,22 +1231,40 @@ void tilde_2d(Oracle &o, double dt) {
 // ---------------------------------------------------------------------------
 // iter.f:38-1248 (2D)
 // ---------------------------------------------------------------------------
-void calc_gas_mass_flux_2d(Oracle &o, int c) {
+// opt_inner_loop's density stencils (iter.f:1330-1360): built at loop entry,
+// only the centre updated, so slots remapped to the cell hold its
+// loop-entry value v
+void stale_first2(const Oracle &o, Sten &s, int c, double v) {
+    if (o.nbrem(E, c) == c) s.e = v;
+    if (o.nbrem(T, c) == c) s.t = v;
+    if (o.nbrem(W, c) == c) s.w = v;
+    if (o.nbrem(B, c) == c) s.b = v;
+}
+void stale_third2(const Oracle &o, Sten &s, int c, double v) {
+    if (o.nbrem(EE, c) == c) s.ee = v;
+    if (o.nbrem(TT, c) == c) s.tt = v;
+    if (o.nbrem(WW, c) == c) s.ww = v;
+    if (o.nbrem(BB, c) == c) s.bb = v;
+}
+
+void calc_gas_mass_flux_2d(Oracle &o, int c, const double *own0 = nullptr) {
     int i, j, k;
     o.ijk_of(c, i, j, k);
     int imjk = o.nbraw(W, c), ijkm = o.nbraw(B, c);
     Sten dens, u, w;
     first_nb2(o, dens, o.rgp.data(), c);
+    if (own0) stale_first2(o, dens, c, *own0);
     first_rnb2(o, u, o.ug.data(), c);
     first_rnb2(o, w, o.wg.data(), c);
     masf_2d(o, o.rgfe[c], o.rgft[c], o.rgfe[imjk], o.rgft[ijkm], dens, u, w, i);
     if (o.cfg.muscl > 0 && o.flag[c] == FLUID) {
         third_nb2(o, dens, o.rgp.data(), c);
+        if (own0) stale_third2(o, dens, c, *own0);
         fmas_2d(o, o.rgfe[c], o.rgft[c], o.rgfe[imjk], o.rgft[ijkm], dens, u, w, c);
     }
 }
 
-void calc_part_mass_flux_2d(Oracle &o, int c) {
+void calc_part_mass_flux_2d(Oracle &o, int c, const double *own0 = nullptr) {
     int i, j, k;
     o.ijk_of(c, i, j, k);
     int n = o.ncell;
@@ -1255,12 +1273,14 @@ void calc_part_mass_flux_2d(Oracle &o, int c) {
         Sten dens, u, w;
         const double *R = &o.rlk[(size_t)(is - 1) * n];
         first_nb2(o, dens, R, c);
+        if (own0) stale_first2(o, dens, c, own0[is]);
         first_rnb2(o, u, &o.us[(size_t)(is - 1) * n], c);
         first_rnb2(o, w, &o.ws[(size_t)(is - 1) * n], c);
         double *fe = &o.rsfe[(size_t)(is - 1) * n], *ft = &o.rsft[(size_t)(is - 1) * n];
         masf_2d(o, fe[c], ft[c], fe[imjk], ft[ijkm], dens, u, w, i);
         if (o.cfg.muscl > 0 && o.flag[c] == FLUID) {
             third_nb2(o, dens, R, c);
+            if (own0) stale_third2(o, dens, c, own0[is]);
             fmas_2d(o, fe[c], ft[c], fe[imjk], ft[ijkm], dens, u, w, c);
         }
     }
@@ -1364,6 +1384,11 @@ void inner_loop_2d(Oracle &o, int c, int nit, double &d3, double &p3, double &ab
     int kros = -1;
     double xg[PDAC_MAX_NGAS];
     for (int ig = 0; ig < o.ng; ++ig) xg[ig] = o.xgc[(size_t)ig * o.ncell + c];
+    // optimization >= 2: opt_inner_loop (iter.f:1255-1547)
+    const bool opt = o.cfg.optimization >= 2;
+    double own0[PDAC_MAX_NSOLID + 1];
+    own0[0] = o.rgp[c];
+    for (int is = 1; is <= o.ns; ++is) own0[is] = o.S(o.rlk, c, is);
     for (int loop = 1; loop <= o.cfg.inmax; ++loop) {
         if (loop > 1 || nit > 1) padjust(o, o.p[c], kros, d3, p3, o.cfg.omega, abeta_);
         o.rog[c] = thermal_eosg(o, o.tg[c], o.p[c], xg);
@@ -1373,10 +1398,10 @@ void inner_loop_2d(Oracle &o, int c, int nit, double &d3, double &p3, double &ab
         assemble_wb_2d(o, c, dt, au1, bu1, aw1, bw1);
         assemble_et_2d(o, c, dt, au, bu, aw, bw);
         solve_all_2d(o, c, au1, bu1, aw1, bw1, au, bu, aw, bw);
-        calc_part_mass_flux_2d(o, c);
+        calc_part_mass_flux_2d(o, c, opt ? own0 : nullptr);
         calc_eps_2d(o, c, dt);
         o.rgp[c] = o.ep[c] * o.rog[c];
-        calc_gas_mass_flux_2d(o, c);
+        calc_gas_mass_flux_2d(o, c, opt ? own0 : nullptr);
         double dg = calc_res_2d(o, c, dt);
         if (std::fabs(dg) > conv_ || std::fabs(dg) >= std::fabs(dgorig)) {
             if (nit == 1 && loop == 1) dgorig = dg;

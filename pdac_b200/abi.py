@@ -46,7 +46,7 @@ class PdacCfg(C.Structure):
         ("inmax", C.c_int), ("maxout", C.c_int),
         ("muscl", C.c_int), ("lv", C.c_int), ("lm", C.c_int),
         ("beta", C.c_double), ("flim", C.c_double), ("update_eosg", C.c_int),
-        ("implicit_fluxes", C.c_int), ("implicit_enthalpy", C.c_int),
+        ("implicit_fluxes", C.c_int), ("implicit_enthalpy", C.c_int), ("optimization", C.c_int),
         ("pmodel", C.c_int), ("drag_model", C.c_int), ("icpc", C.c_int),
         ("tref", C.c_double),
         ("gas_viscosity", C.c_int), ("part_viscosity", C.c_int), ("repulsive_model", C.c_int),

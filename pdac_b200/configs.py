@@ -206,3 +206,18 @@ def small_3d_mixture(formatted=False, **kw):
     d.set("model", compute_mixture=True)
     d.set("control", formatted_output=formatted)
     return d
+
+
+def small_2d_opt(optimization=2, **kw):
+    """small_2d with the reference's optimized inner loop (optimization = 2,
+    opt_inner_loop, iter.f:1255-1547)."""
+    d = small_2d(**kw)
+    d.set("numeric", optimization=optimization)
+    return d
+
+
+def small_3d_opt(optimization=2, **kw):
+    """small_3d with the optimized inner loop of small_2d_opt."""
+    d = small_3d(**kw)
+    d.set("numeric", optimization=optimization)
+    return d

@@ -42,6 +42,7 @@ struct Prm {
     int itc, muscl, lv, lm, pmodel, drag_model, icpc;
     int gas_viscosity, part_viscosity, repulsive_model, inmax;
     int iturb, iss, modturbo;  // sub-grid models (turbo.f)
+    int opt;                   // 2: opt_inner_loop's loop-entry density in self-remapped stencil slots
     int gas_type[PDAC_MAXG];
     double alpha, alphagrav, omega, delg, beta, flim, tref;
     double gravx, gravy, gravz, void_fraction;

@@ -207,6 +207,11 @@ int validate(const pdac_cfg *c, std::string &why) {
     }
     if (c->iss != 0 && c->iss != 1) { why = "iss must be 0 or 1"; return 1; }
     if (c->implicit_fluxes && c->alpha != 1.0) { why = "implicit_fluxes needs alpha = 1"; return 1; }
+    if (c->optimization < 1 || c->optimization > 3) { why = "optimization must be 1, 2 or 3"; return 1; }
+    if (c->optimization == 3 && c->job_type == 3 && c->nsolid == 2) {
+        why = "optimization = 3 in 3D with two classes (opt3_inner_loop) is not built";
+        return 1;
+    }
     if (c->time_integration == 1 && c->pmodel != 1 && c->pmodel != 2) {
         why = "time_integration = 1 needs pmodel 1 or 2 (explicit_solver.f:632-642)";
         return 1;
@@ -393,6 +398,7 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     P.drag_model = cfg->drag_model; P.icpc = cfg->icpc; P.gas_viscosity = cfg->gas_viscosity;
     P.part_viscosity = cfg->part_viscosity; P.repulsive_model = cfg->repulsive_model; P.inmax = cfg->inmax;
     P.iturb = cfg->iturb; P.iss = cfg->iss; P.modturbo = cfg->modturbo;
+    P.opt = cfg->optimization >= 2 ? 2 : 1;  // 3 runs as 2 outside 3D with two classes (iter.f:160-161)
     for (int ig = 0; ig < ng; ++ig) P.gas_type[ig] = cfg->gas_type[ig];
     P.alpha = cfg->alpha; P.alphagrav = cfg->alphagrav; P.omega = cfg->omega; P.delg = cfg->delg;
     P.beta = cfg->beta; P.flim = cfg->flim; P.tref = cfg->tref;

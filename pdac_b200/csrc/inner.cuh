@@ -226,8 +226,17 @@ __device__ __forceinline__ void inner_team_run(const Prm &P, const Fld &F, doubl
             const double *D_ = F.rlk + (size_t)(l - 2) * n;
             cm[l - 1] = ldro<RO>(D_ + rm); cp[l - 1] = ldro<RO>(D_ + rp); cfar[l - 1] = mus ? ldro<RO>(D_ + rfar) : 0.0;
         }
+        // opt_inner_loop (iter.f:1255-1547) builds the density stencils once
+        // and updates only their centre: a neighbour slot remapped to the
+        // cell keeps the loop-entry value there
+        double own0[NC];
+        own0[0] = F.rgp[c];
+#pragma unroll
+        for (int l = 2; l <= nph; ++l) own0[l - 1] = F.rlk[(size_t)(l - 2) * n + c];
+        const bool stale = P.opt == 2;
         auto mflux = [&](int ph, double own) {
-            double dm = sm ? own : cm[ph], dp = sp ? own : cp[ph], df = sfar ? own : cfar[ph];
+            const double slot = stale ? own0[ph] : own;
+            double dm = sm ? slot : cm[ph], dp = sp ? slot : cp[ph], df = sfar ? slot : cfar[ph];
             return minus ? face_mflux(P, g, true, vel[ph], own, dm, df, dp, 0.0, mus)
                          : face_mflux(P, g, false, vel[ph], own, dm, 0.0, dp, df, mus);
         };

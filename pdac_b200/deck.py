@@ -373,6 +373,9 @@ class Deck:
             bad.append("ibl>0")
         if self["ipro"] != 0 or self["iali"] not in (0, 1, 2, 3, 4):
             bad.append("ipro>0 or iali=5")
-        if self["optimization"] not in (1,):
-            bad.append("optimization!=1")
+        if self["optimization"] not in (1, 2, 3):
+            bad.append("optimization other than 1, 2 or 3")
+        elif self["optimization"] == 3 and self.is3d and self["nsolid"] == 2:
+            # opt3_inner_loop, the matrix-precomputing variant of 3D with two classes
+            bad.append("optimization=3 in 3D with two particle classes")
         return bad

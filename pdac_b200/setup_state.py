@@ -407,6 +407,7 @@ class Case:
         c.update_eosg = int(bool(d["update_eosg"]))
         c.implicit_fluxes = int(bool(d["implicit_fluxes"]))
         c.implicit_enthalpy = int(bool(d["implicit_enthalpy"]))
+        c.optimization = int(d["optimization"])
         c.pmodel, c.drag_model, c.icpc = d["pmodel"], d["drag_model"], d["icpc"]
         c.tref = d["tref"]
         c.gas_viscosity = int(bool(d["gas_viscosity"]))

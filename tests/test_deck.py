@@ -134,3 +134,12 @@ def test_implicit_flux_modes_reach_the_configuration():
     d.set("numeric", alpha=0.5)
     with pytest.raises(ValueError, match="implicit_fluxes"):
         Case(d)
+
+
+def test_inner_loop_variants():
+    assert Case(configs.small_2d_opt()).cfg().optimization == 2
+    assert Case(configs.small_2d_opt(optimization=3)).cfg().optimization == 3  # runs as 2 in 2D
+    d = configs.small_3d(diameters=(30.0, 250.0), ep_solid=(0.005, 0.01))
+    d.set("numeric", optimization=3)
+    with pytest.raises(ValueError, match="optimization=3"):
+        Case(d)
