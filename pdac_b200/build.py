@@ -36,8 +36,28 @@ def needs_build():
     return any(os.path.getmtime(s) > t for s in deps)
 
 
+HOST_SRC = os.path.join(HERE, "host", "pdac_run.cpp")
+HOST_BIN = os.path.join(OUT_DIR, "pdac_run")
+
+
+def build_host(force=False):
+    """The compiled time-loop driver (pdac_b200/host/pdac_run.cpp), linked
+    against the engine library with the library's directory as its run path."""
+    if not force and os.path.exists(HOST_BIN) and os.path.getmtime(HOST_BIN) >= max(
+            os.path.getmtime(HOST_SRC), os.path.getmtime(LIB)):
+        return HOST_BIN
+    cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-Wall", "-I", os.path.join(HERE, "..", "include"),
+           HOST_SRC, "-L", OUT_DIR, "-lpdac_b200", "-Wl,-rpath,$ORIGIN", "-o", HOST_BIN]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("host driver build failed")
+    return HOST_BIN
+
+
 def build(force=False, verbose=False, extra=()):
     if not force and not needs_build():
+        build_host()
         return LIB
     os.makedirs(OUT_DIR, exist_ok=True)
     cmd = [NVCC, *FLAGS, *extra, "-o", LIB, os.path.join(CSRC, "engine.cu")]
@@ -49,6 +69,7 @@ def build(force=False, verbose=False, extra=()):
         raise RuntimeError("nvcc failed")
     if verbose and (r.stdout or r.stderr):
         print(r.stdout + r.stderr)
+    build_host(force=True)
     return LIB
 
 

@@ -94,17 +94,25 @@ def run(engine, workdir, max_steps=None, log=None):
             engine.fieldn()
         engine.sgsg()
         engine.sgss()
+        ifx, ien = bool(d["implicit_fluxes"]), bool(d["implicit_enthalpy"])
+        nit = 0
         for r in range(1, rk + 1):
             dtr = dt / (rk + 1 - r)
             if explicit:
                 engine.explicit_iter(dtr)
                 engine.ygas(dtr)
             else:
-                engine.tilde(dtr)
+                # prog.f:246-292: the implicit modes move tilde (and htilde)
+                # into iter's sweeps
+                if not ifx:
+                    engine.tilde(dtr)
+                    if ien:
+                        engine.htilde(dtr)
                 nit = engine.iter(dtr)
                 engine.ygas(dtr)
-                engine.htilde(dtr)
-                engine.ftem(dtr)
+                if not ien:
+                    engine.htilde(dtr)
+                    engine.ftem(dtr)
         if d["compute_mixture"]:
             engine.compute_mixture_fields()  # prog.f:331
         t = t + dt
