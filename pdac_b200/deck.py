@@ -131,6 +131,69 @@ def _split_values(s):
     return vals
 
 
+class _ListReader:
+    """Fortran list-directed input over the records (lines) after the
+    namelists: each read() is one READ statement."""
+
+    def __init__(self, lines):
+        self.lines = list(lines)
+        self.pos = 0
+
+    @staticmethod
+    def _items(line):
+        out, cur, q = [], "", None
+        for ch in line:
+            if q:
+                if ch == q:
+                    q = None
+                else:
+                    cur += ch
+            elif ch in "'\"":
+                q = ch
+            elif ch == "," or ch.isspace():
+                if cur:
+                    out.append(cur)
+                cur = ""
+            elif ch == "/":
+                if cur:
+                    out.append(cur)
+                out.append("/")
+                cur = ""
+                break
+            else:
+                cur += ch
+        if cur:
+            out.append(cur)
+        return out
+
+    def find_card(self, name):
+        """READ(unit,*) card until TRIM(card) == name; False at the end."""
+        while self.pos < len(self.lines):
+            items = self._items(self.lines[self.pos])
+            self.pos += 1
+            if items and items[0] == name:
+                return True
+        return False
+
+    def read(self, count):
+        vals = []
+        while len(vals) < count:
+            if self.pos >= len(self.lines):
+                raise ValueError("input ended inside a card")
+            items = self._items(self.lines[self.pos])
+            self.pos += 1
+            for it in items:
+                if it == "/" or len(vals) >= count:
+                    break
+                m = re.fullmatch(r"(\d+)\*(.*)", it)
+                rep, tok = (int(m.group(1)), m.group(2)) if m else (1, it)
+                v = float(tok.replace("d", "e").replace("D", "e"))
+                vals.extend([v] * rep)
+            if items and items[-1] == "/":
+                break
+        return vals[:count]
+
+
 class Deck:
     """All namelist groups plus the MESH and FIXED_FLOWS cards of one run."""
 
@@ -217,57 +280,48 @@ class Deck:
                 g[k] = v
 
     def _cards(self, lines):
+        """The MESH and FIXED_FLOWS cards (input.f:786-890), read as the
+        reference's list-directed READs do: every READ starts at a new
+        record (line), takes values separated by commas or blanks (r*v
+        repeats, '/' ends the READ), continues on the next records when the
+        current one runs out and drops the rest of its last record."""
         nx, ny, nz = self["nx"], self["ny"], self["nz"]
-        toks = []
-        it = iter(lines)
-        # MESH card
-        for ln in it:
-            if ln.upper() == "MESH":
-                break
-        else:
+        rd = _ListReader(lines)
+        # MESH card: READ(iunit,*) card until TRIM(card) == 'MESH'
+        if not rd.find_card("MESH"):
             raise ValueError("MESH card not found")
         if self["iuni"] == 0 and self["grigen"] == 0:
-            need = nx + (ny if self.is3d else 0) + nz
-            while len(toks) < need:
-                toks.extend(float(x.replace("d", "e").replace("D", "e")) for x in next(it).split())
-            self.delta_x = np.array(toks[:nx])
-            off = nx
+            self.delta_x = np.array(rd.read(nx), dtype=float)
             if self.is3d:
-                self.delta_y = np.array(toks[off:off + ny])
-                off += ny
-            self.delta_z = np.array(toks[off:off + nz])
-        for ln in it:
-            if ln.upper() == "FIXED_FLOWS":
-                break
-        else:
+                self.delta_y = np.array(rd.read(ny), dtype=float)
+            self.delta_z = np.array(rd.read(nz), dtype=float)
+        if not rd.find_card("FIXED_FLOWS"):
             raise ValueError("FIXED_FLOWS card not found")
-        rest = " ".join(it).split()
-        vals = [float(x.replace("d", "e").replace("D", "e")) for x in rest]
-        q = 0
-        nb = int(vals[q]); q += 1
+        nb = int(rd.read(1)[0])
         ns = self["nsolid"]
         for _ in range(nb):
             if self.is3d:
-                typ, x0, x1, y0, y1, z0, z1 = (int(v) for v in vals[q:q + 7]); q += 7
+                typ, x0, x1, y0, y1, z0, z1 = (int(v) for v in rd.read(7))
             else:
-                typ, x0, x1, z0, z1 = (int(v) for v in vals[q:q + 5]); q += 5
+                typ, x0, x1, z0, z1 = (int(v) for v in rd.read(5))
                 y0 = y1 = 0
             blk = dict(typ=typ, xlo=x0, xhi=x1, ylo=y0, yhi=y1, zlo=z0, zhi=z1)
             if typ in (1, 5, 8):
                 if self.is3d:
-                    ugv, vgv, wgv, pv, epv, tgv = vals[q:q + 6]; q += 6
+                    ugv, vgv, wgv, pv, epv, tgv = rd.read(6)
                 else:
-                    ugv, wgv, pv, epv, tgv = vals[q:q + 5]; q += 5
+                    ugv, wgv, pv, epv, tgv = rd.read(5)
                     vgv = 0.0
-                sol = []
                 per = 5 if self.is3d else 4
-                for _s in range(ns):
-                    sv = vals[q:q + per]; q += per
+                sv_all = rd.read(per * ns)
+                sol = []
+                for q in range(ns):
+                    sv = sv_all[q * per:(q + 1) * per]
                     if self.is3d:
                         sol.append(dict(u=sv[0], v=sv[1], w=sv[2], eps=sv[3], t=sv[4]))
                     else:
                         sol.append(dict(u=sv[0], v=0.0, w=sv[1], eps=sv[2], t=sv[3]))
-                conc = vals[q:q + MAX_NGAS]; q += MAX_NGAS
+                conc = rd.read(MAX_NGAS)
                 blk.update(ug=ugv, vg=vgv, wg=wgv, p=pv, ep=epv, tg=tgv, solids=sol, ygc=conc)
             self.blocks.append(blk)
 

@@ -371,6 +371,16 @@ class Case:
         # cnvert, setup.f:280-390 (itd <= 1)
         X = mole(Y, self.gas_type)
         st["xgc"][:] = X.reshape(-1)
+        if d["density_specified"]:
+            # setup.f:319-327: the temperature slot holds a density, turned
+            # into the temperature of the thermal equation of state
+            mass = np.zeros(n)
+            for ig, gt in enumerate(self.gas_type):
+                mass = mass + X[ig] * GMW[gt - 1]
+            tem = st["p"] * mass / RGAS / st["tg"]
+            st["tg"][:] = tem
+            for s in range(ns):
+                TS[s] = tem
         st["rog"][:] = thermal_eosg(st["tg"], st["p"], X, self.gas_type)
         st["rgp"][:] = st["rog"] * st["ep"]
         cp = hcapg(st["tg"], d["icpc"], d["tref"])
