@@ -60,6 +60,118 @@ def mole(ygc, gas_type):
     return np.stack([ygc[ig] / g[ig] * molinv for ig in range(ygc.shape[0])])
 
 
+def _powi(x, n):
+    """x**n for an integer n by repeated squaring, as Fortran evaluates an
+    integer power."""
+    r, b, e = 1.0, x, abs(n)
+    while e:
+        if e & 1:
+            r = r * b
+        b = b * b
+        e >>= 1
+    return r if n >= 0 else 1.0 / r
+
+
+def _fnint(x):
+    """Fortran NINT: nearest integer, halves away from zero."""
+    return int(math.floor(abs(x) + 0.5)) * (1 if x >= 0 else -1)
+
+
+def generate_grid(nd, domain_size, alpha, demin, demax, n0, maxbeta):
+    """generate_grid, grid.f:485-786: nd cell sizes between demin (a band
+    of n0 cells around the relative position alpha) and demax, growing at a
+    constant rate found by adjusting it until the cells fill domain_size,
+    rounded to 1e-4 of the length unit."""
+    if demin == demax:
+        return np.full(nd, float(demin))
+    if nd < domain_size / demax:
+        raise ValueError("grid_generator: insufficient number of cells")
+    if nd > domain_size / demin:
+        raise ValueError("grid_generator: number of cells is too big")
+    if domain_size * alpha < demin:
+        alpha = 0.0
+    if domain_size * (1.0 - alpha) < demin:
+        alpha = 1.0
+    if alpha == 0.0:
+        n01, n02 = 0, n0
+        l1, l2 = 0.0, domain_size - n02 * demin
+    elif alpha == 1.0:
+        n01, n02 = n0, 0
+        l1, l2 = domain_size - n01 * demin, 0.0
+    else:
+        n01 = _fnint(n0 / 2.0)
+        n02 = n0 - n01
+        l1 = (domain_size * alpha) - n01 * demin
+        l2 = (domain_size * (1.0 - alpha)) - n02 * demin
+    der = demax / demin
+    beta, dbeta, minbeta = 1.2, 0.99, 1.0 + 1.0e-5
+    print_mesh, already = False, False
+
+    def side(l, n0s, frac_alpha, m, lcomp):
+        if l < 0:
+            return int(frac_alpha * domain_size / demin), 0.0, 0, 0
+        if (l / demax) > (nd - n0s):
+            raise ValueError("grid: insufficient number of cells")
+        if lcomp < l:
+            return n0s, l, m, int((l - lcomp) / demax)
+        return n0s, l, int(math.log(1.0 + (beta - 1.0) * (l / demin + 1.0)) / math.log(beta) - 1), 0
+
+    while not print_mesh:
+        m = int(math.log(der) / math.log(beta))
+        frac = (_powi(beta, m + 1) - 1.0) / (beta - 1.0)
+        lcomp = demin * (frac - 1.0)
+        n01, l1, m1, n11 = side(l1, n01, alpha, m, lcomp)
+        n02, l2, m2, n12 = side(l2, n02, 1.0 - alpha, m, lcomp)
+        if (l2 + l1) / demax > nd - n01 - n02:
+            raise ValueError("grid: insufficient number of cells")
+        tot = (n01 + m1 + n11) + (n02 + m2 + n12)
+        if tot < nd:
+            if beta * dbeta < minbeta:
+                print_mesh = True
+            else:
+                if already:
+                    dbeta = dbeta + (1.0 - dbeta) / 2.0
+                    already = False
+                beta = beta * dbeta
+        elif tot > nd:
+            if not already:
+                dbeta = dbeta + (1.0 - dbeta) / 2.0
+                already = True
+            beta = beta / dbeta
+        else:
+            if (1.0 - dbeta) <= 1.0e-15:
+                print_mesh = True
+            else:
+                already = True
+                beta = beta / dbeta
+
+    def refit(l, n1, m1_, realexp):
+        while True:
+            ntilde = (l - n1 * demax) / demin + 1.0
+            b1 = beta
+            if ntilde > 1.0:
+                for _ in range(50):
+                    num = (m1_ * (math.pow(b1, m1_ + 1.0) if realexp else _powi(b1, m1_ + 1)) + 1.0) / ntilde
+                    b1 = (1.0 - num) / (1.0 - (m1_ + 1.0) * _powi(b1, m1_) / ntilde)
+            if demin * _powi(b1, m1_) > demax:
+                if m1_ == 0 or b1 > maxbeta:
+                    return n1, m1_, b1
+                n1, m1_ = n1 + 1, m1_ - 1
+            else:
+                return n1, m1_, b1
+
+    n11, m1, beta1 = refit(l1, n11, m1, False)
+    n12, m2, beta2 = refit(l2, n12, m2, True)   # the reference raises beta2 to the real m2 + 1.D0
+    center = n11 + m1 + n01
+    delta = np.full(nd, float(demax))
+    for i in range(1, m1 + 1):
+        delta[center - n01 - i] = demin * _powi(beta1, i)
+    delta[center - n01:center + n02] = demin
+    for i in range(1, m2 + 1):
+        delta[center + n02 + i - 1] = demin * _powi(beta2, i)
+    return np.array([_fnint(v * 10000.0) / 10000.0 for v in delta])
+
+
 def thermal_eosg(tg, p, xgc, gas_type):
     """Ideal-gas density, eosg.f:114-137."""
     mg = np.zeros_like(np.asarray(tg, dtype=np.float64))
@@ -161,7 +273,19 @@ class Case:
     # grid.f:206-345
     def _grid(self):
         d = self.deck
-        if d["iuni"] == 1:
+        if d["grigen"] == 1:
+            # grid_setup (grid.f:244-256): generated non-uniform mesh
+            if any(d[k] != 0 for k in ("npx", "nmx", "npy", "nmy", "npz", "nmz")):
+                raise ValueError("grigen=1 with added cells (npx, nmx, ...) is not supported")
+            self.dx = generate_grid(self.nx, d["domain_x"], d["alpha_x"], d["dxmin"], d["dxmax"], max(d["n0x"], 1),
+                                    d["maxbeta"])
+            self.dy = (generate_grid(self.ny, d["domain_y"], d["alpha_y"], d["dymin"], d["dymax"], max(d["n0y"], 1),
+                                     d["maxbeta"]) if self.is3d else np.zeros(1))
+            self.dz = generate_grid(self.nz, d["domain_z"], d["alpha_z"], d["dzmin"], d["dzmax"], max(d["n0z"], 1),
+                                    d["maxbeta"])
+        elif d["grigen"] != 0:
+            raise ValueError("grigen=2 (generate_nu_grid) is not supported")
+        elif d["iuni"] == 1:
             self.dx = np.full(self.nx, float(d["dx0"]))
             self.dy = np.full(self.ny, float(d["dy0"])) if self.is3d else np.zeros(1)
             self.dz = np.full(self.nz, float(d["dz0"]))
@@ -169,8 +293,6 @@ class Case:
             self.dx = np.asarray(d.delta_x, dtype=np.float64)
             self.dy = np.asarray(d.delta_y, dtype=np.float64) if self.is3d else np.zeros(1)
             self.dz = np.asarray(d.delta_z, dtype=np.float64)
-        else:
-            raise ValueError("grigen>0 (generated non-uniform mesh) is not supported")
         nx, nz = self.nx, self.nz
         self.xb = np.zeros(nx)
         self.x = np.zeros(nx)

@@ -143,3 +143,19 @@ def test_inner_loop_variants():
     d.set("numeric", optimization=3)
     with pytest.raises(ValueError, match="optimization=3"):
         Case(d)
+
+
+def test_generated_mesh():
+    """generate_grid (grid.f:485-786): a band of n0 cells of the minimum
+    size at the relative position alpha, sizes growing at one rate to the
+    maximum, the domain filled to the mesh's 1e-4 rounding."""
+    from pdac_b200.setup_state import generate_grid
+    dz = generate_grid(110, 1000.0, 0.0, 5.0, 40.0, 81, 1.2)
+    assert len(dz) == 110 and np.all(dz[:81] == 5.0) and dz.max() == 40.0
+    assert np.all(np.diff(dz) >= -1e-9)  # growing away from the band at the bottom
+    assert abs(dz.sum() - 1000.0) < 0.5
+    assert np.allclose(dz * 1e4, np.round(dz * 1e4), rtol=0, atol=1e-6)
+    dx = generate_grid(200, 4000.0, 0.5, 10.0, 40.0, 40, 1.2)
+    c = np.argmin(dx)
+    assert dx.min() == 10.0 and np.count_nonzero(dx == 10.0) == 40 and abs(dx.sum() - 4000.0) < 1.0
+    assert np.all(generate_grid(10, 100.0, 0.5, 10.0, 10.0, 1, 1.2) == 10.0)

@@ -43,6 +43,7 @@ def test_example_decks_set_up_or_name_what_is_missing():
         except ValueError as e:
             outcome[name] = str(e)
     assert outcome["shock_tube_1"] == "ok" and outcome["jet_Ladenburg"] == "ok" and outcome["jet_Lewis"] == "ok"
+    assert outcome["dam_break_1"] == "ok"  # generated mesh (grigen = 1)
     assert "ctu" in outcome["jet_NASA"] and "ctu" in outcome["jet_Sommerfeld"]
 
 
