@@ -45,9 +45,15 @@ extern "C" {
 #define PDAC_MAX_NSOLID   8
 #define PDAC_MAX_NGAS     7
 
-/* precision modes */
+/* precision modes.  PDAC_PREC_MIXED (3D runs only; 2D is rejected at
+ * create): the face-flux passes -- momentum (flux_u/v/w.f), mass (flux_m.f),
+ * species and enthalpy (flux_sc.f, hotc.f) -- compute in FP32 from the FP64
+ * state and store their fluxes in FP64; the state, every conservative update,
+ * the pressure correction and the equations of state stay in FP64.  A face
+ * flux is shared by its two cells in both modes, so the phase masses are
+ * conserved to FP64 round-off. */
 #define PDAC_PREC_FP64    0   /* every kernel in FP64                         */
-#define PDAC_PREC_MIXED   1   /* FP32 fluxes/tilde/drag/EOS, FP64 corrector   */
+#define PDAC_PREC_MIXED   1   /* FP32 face-flux passes, FP64 everything else  */
 
 /*
  * Run configuration: the subset of the reference namelists (input.f:159-209,

@@ -55,8 +55,29 @@ struct Prm {
     double dkf[PDAC_MAXP][PDAC_MAXP];
     // device metric, 1-based padded
     const double *dx, *dy, *dz, *indx, *indy, *indz, *r, *rb, *inr, *inrb;
+    const float *dxf, *dyf, *dzf, *indxf, *indyf, *indzf;  // FP32 copies (mixed precision), else null
+    int mixed;  // 1: the 3D flux passes compute in FP32 (PDAC_PREC_MIXED)
     const double *p_atm, *t_atm;
     const int *flag;
+};
+
+// The metric arrays in the arithmetic type of a flux pass.
+template <typename Real> struct Met;
+template <> struct Met<double> {
+    static __device__ __forceinline__ const double *dx(const Prm &P) { return P.dx; }
+    static __device__ __forceinline__ const double *dy(const Prm &P) { return P.dy; }
+    static __device__ __forceinline__ const double *dz(const Prm &P) { return P.dz; }
+    static __device__ __forceinline__ const double *indx(const Prm &P) { return P.indx; }
+    static __device__ __forceinline__ const double *indy(const Prm &P) { return P.indy; }
+    static __device__ __forceinline__ const double *indz(const Prm &P) { return P.indz; }
+};
+template <> struct Met<float> {
+    static __device__ __forceinline__ const float *dx(const Prm &P) { return P.dxf; }
+    static __device__ __forceinline__ const float *dy(const Prm &P) { return P.dyf; }
+    static __device__ __forceinline__ const float *dz(const Prm &P) { return P.dzf; }
+    static __device__ __forceinline__ const float *indx(const Prm &P) { return P.indxf; }
+    static __device__ __forceinline__ const float *indy(const Prm &P) { return P.indyf; }
+    static __device__ __forceinline__ const float *indz(const Prm &P) { return P.indzf; }
 };
 
 // Device pointers of every field (state, n-level, tilde, fluxes, solver).

@@ -36,6 +36,7 @@ struct pdac_ctx {
     double *arena = nullptr;
     size_t arena_doubles = 0;
     double *metric = nullptr;
+    float *metric_f = nullptr;  // FP32 dx, dy, dz, indx, indy, indz of the mixed-precision flux passes
     int *d_flag = nullptr, *d_vent = nullptr, *d_counters = nullptr, *h_counters = nullptr;
     double *d_vfact = nullptr, *d_vfact0 = nullptr;
     double *d_app0u = nullptr, *d_app0v = nullptr, *d_app0w = nullptr;
@@ -198,7 +199,11 @@ int validate(const pdac_cfg *c, std::string &why) {
     if (c->rungekut < 1) { why = "rungekut must be >= 1"; return 1; }
     if (!c->dx || !c->dz || !c->flag || !c->p_atm || !c->t_atm) { why = "metric, flag or atmosphere pointer is NULL"; return 1; }
     if (c->nvent > 0 && !c->vent_ijk) { why = "vent_ijk is NULL"; return 1; }
-    if (c->precision != PDAC_PREC_FP64) { why = "only PDAC_PREC_FP64 is built"; return 1; }
+    if (c->precision != PDAC_PREC_FP64 && c->precision != PDAC_PREC_MIXED) {
+        why = "precision must be PDAC_PREC_FP64 or PDAC_PREC_MIXED";
+        return 1;
+    }
+    if (c->precision == PDAC_PREC_MIXED && c->job_type != 3) { why = "PDAC_PREC_MIXED is built for 3D runs only"; return 1; }
     if (c->time_integration != 0 && c->time_integration != 1) { why = "time_integration must be 0 or 1"; return 1; }
     if (c->iturb != 0 && c->iturb != 1) { why = "iturb must be 0 or 1 (iturb = 2 needs the topography's roughness)"; return 1; }
     if (c->iturb == 1 && c->modturbo != 1 && c->modturbo != 2) {
@@ -451,6 +456,21 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     }
     P.dx = mp[0]; P.dy = mp[1]; P.dz = mp[2]; P.indx = mp[3]; P.indy = mp[4]; P.indz = mp[5];
     P.r = mp[6]; P.rb = mp[7]; P.inr = mp[8]; P.inrb = mp[9]; P.p_atm = mp[10]; P.t_atm = mp[11];
+    P.mixed = cfg->precision == PDAC_PREC_MIXED;
+    if (P.mixed) {  // the metric of the FP32 flux passes: each FP64 value rounded to nearest
+        size_t ftot = 0;
+        for (int q = 0; q < 6; ++q) ftot += mets[q]->size();
+        std::vector<float> hf;
+        hf.reserve(ftot);
+        for (int q = 0; q < 6; ++q)
+            for (double v : *mets[q]) hf.push_back((float)v);
+        CK(cudaMalloc(&ctx->metric_f, ftot * sizeof(float)));
+        CK(cudaMemcpy(ctx->metric_f, hf.data(), ftot * sizeof(float), cudaMemcpyHostToDevice));
+        const float *fp[6];
+        size_t fo = 0;
+        for (int q = 0; q < 6; ++q) { fp[q] = ctx->metric_f + fo; fo += mets[q]->size(); }
+        P.dxf = fp[0]; P.dyf = fp[1]; P.dzf = fp[2]; P.indxf = fp[3]; P.indyf = fp[4]; P.indzf = fp[5];
+    }
     CK(cudaMalloc(&ctx->d_flag, n * sizeof(int)));
     CK(cudaMemcpy(ctx->d_flag, cfg->flag, n * sizeof(int), cudaMemcpyHostToDevice));
     P.flag = ctx->d_flag;
@@ -634,6 +654,7 @@ int pdac_gpu_destroy(pdac_ctx *ctx) {
     cudaStreamSynchronize(ctx->stream);
     cudaFree(ctx->arena);
     cudaFree(ctx->metric);
+    cudaFree(ctx->metric_f);
     cudaFree(ctx->d_flag);
     cudaFree(ctx->d_vent);
     cudaFree(ctx->d_vfact);
@@ -769,9 +790,15 @@ static int enqueue_tilde(pdac_ctx *ctx, double dt, cudaStream_t st) {
         CK(cudaMemsetAsync(F.mf, 0, n * 9 * (ns + 1) * sizeof(double), st));
         pdac::k_visc3d<<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
         ctx->launches++;
-        pdac::k_tilde_flux3d<0><<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
-        pdac::k_tilde_flux3d<1><<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
-        pdac::k_tilde_flux3d<2><<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
+        if (ctx->P.mixed) {
+            pdac::k_tilde_flux3d<0, float><<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
+            pdac::k_tilde_flux3d<1, float><<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
+            pdac::k_tilde_flux3d<2, float><<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
+        } else {
+            pdac::k_tilde_flux3d<0><<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
+            pdac::k_tilde_flux3d<1><<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
+            pdac::k_tilde_flux3d<2><<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
+        }
         ctx->launches += 3;
         PHASE_LAUNCH(ctx->nph, pdac::k_tilde3d, blocks(n), TPB, st, ctx->P, F, dt, ctx->d_app0u, ctx->d_app0v, ctx->d_app0w);
         ctx->launches++;
@@ -1122,7 +1149,8 @@ int pdac_gpu_ygas(pdac_ctx *ctx, double dt) {
         for (double *a : {ctx->F.yfe, ctx->F.yfn, ctx->F.yft})
             if (a) CK(cudaMemsetAsync(a, 0, n * ctx->ng * sizeof(double), st));
         if (ctx->d3) {
-            pdac::k_ygas_flux3d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F), ctx->launches++;
+            (ctx->P.mixed ? pdac::k_ygas_flux3d<float> : pdac::k_ygas_flux3d<double>)<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F),
+                ctx->launches++;
             pdac::k_ygas3d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F, dt), ctx->launches++;
         } else {
             pdac::k_ygas_flux2d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F), ctx->launches++;
@@ -1144,7 +1172,9 @@ static int enqueue_htilde(pdac_ctx *ctx, double dt, cudaStream_t st) {
         if (a) CK(cudaMemsetAsync(a, 0, n * ns * sizeof(double), st));
     accumulate_conductivity(ctx, st);
     if (ctx->d3) {
-        pdac::k_htilde_flux3d<true><<<blocks(n), TPB, 0, st>>>(ctx->P, F), ctx->launches++;
+        (ctx->P.mixed ? pdac::k_htilde_flux3d<true, float> : pdac::k_htilde_flux3d<true, double>)<<<blocks(n), TPB, 0, st>>>(
+            ctx->P, F),
+            ctx->launches++;
         pdac::k_htilde3d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt), ctx->launches++;
     } else {
         pdac::k_htilde_flux2d<true><<<blocks(n), TPB, 0, st>>>(ctx->P, F), ctx->launches++;
@@ -1279,11 +1309,19 @@ static long long enqueue_explicit(pdac_ctx *ctx, double dt, cudaStream_t st, boo
             L++;
         }
         if (ctx->d3) {
-            pdac::k_rk3_mflux<3><<<blocks(n), TPB, 0, st>>>(P, F);
-            pdac::k_tilde_flux3d<0><<<blocks(nphc), TPB, 0, st>>>(P, F);
-            pdac::k_tilde_flux3d<1><<<blocks(nphc), TPB, 0, st>>>(P, F);
-            pdac::k_tilde_flux3d<2><<<blocks(nphc), TPB, 0, st>>>(P, F);
-            pdac::k_htilde_flux3d<false><<<blocks(n), TPB, 0, st>>>(P, F);
+            if (P.mixed) {
+                pdac::k_rk3_mflux<3, float><<<blocks(n), TPB, 0, st>>>(P, F);
+                pdac::k_tilde_flux3d<0, float><<<blocks(nphc), TPB, 0, st>>>(P, F);
+                pdac::k_tilde_flux3d<1, float><<<blocks(nphc), TPB, 0, st>>>(P, F);
+                pdac::k_tilde_flux3d<2, float><<<blocks(nphc), TPB, 0, st>>>(P, F);
+                pdac::k_htilde_flux3d<false, float><<<blocks(n), TPB, 0, st>>>(P, F);
+            } else {
+                pdac::k_rk3_mflux<3><<<blocks(n), TPB, 0, st>>>(P, F);
+                pdac::k_tilde_flux3d<0><<<blocks(nphc), TPB, 0, st>>>(P, F);
+                pdac::k_tilde_flux3d<1><<<blocks(nphc), TPB, 0, st>>>(P, F);
+                pdac::k_tilde_flux3d<2><<<blocks(nphc), TPB, 0, st>>>(P, F);
+                pdac::k_htilde_flux3d<false><<<blocks(n), TPB, 0, st>>>(P, F);
+            }
             L += 5;
         } else {
             pdac::k_rk3_mflux<2><<<blocks(n), TPB, 0, st>>>(P, F);

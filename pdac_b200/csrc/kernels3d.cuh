@@ -240,8 +240,10 @@ __global__ void k_fieldn3d(Prm P, Fld F) {
 // tilde momentum fluxes, compute_all_fluxes_tilde tilde.f:850-1326 (3D)
 // ---------------------------------------------------------------------------
 // one thread per (cell, phase) for one momentum component COMP (0 = x,
-// 1 = y, 2 = z): consecutive threads take consecutive cells of one phase
-template <int COMP>
+// 1 = y, 2 = z): consecutive threads take consecutive cells of one phase.
+// Real is the arithmetic type: double, or float in the mixed-precision mode
+// (the FP64 state is converted as it is read; fluxes are stored in FP64).
+template <int COMP, typename Real = double>
 __global__ void __launch_bounds__(128, PDAC_FLUX_MINB) k_tilde_flux3d(Prm P, Fld F) {
     unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (unsigned)P.ncell * (unsigned)(P.ns + 1)) return;
@@ -261,12 +263,12 @@ __global__ void __launch_bounds__(128, PDAC_FLUX_MINB) k_tilde_flux3d(Prm P, Fld
     const double *V = ph == 0 ? F.vg : F.vs + off;
     const double *W = ph == 0 ? F.wg : F.ws + off;
     const double *D = ph == 0 ? F.rgp : F.rlk + off;
-    S3 u, v, w, d, ds3;
+    S3T<Real> u, v, w, d, ds3;
     rnb3(u, U, R);
     rnb3(v, V, R);
     rnb3(w, W, R);
     nb3(d, D, R, M);
-    F6d f = {0, 0, 0, 0, 0, 0};
+    F6T<Real> f = {0, 0, 0, 0, 0, 0};
     if (COMP == 0) {  // x momentum
         interp_x3(P, d, i, ds3);
         flu_3d(P, f, dw, ds, db, ds3, u, v, w, i);
@@ -624,6 +626,7 @@ __device__ __forceinline__ void calc_eps_3d(const Prm &P, const Fld &F, const Ra
 // ---------------------------------------------------------------------------
 // ygas, ygas.f:27-325 (3D)
 // ---------------------------------------------------------------------------
+template <typename Real = double>
 __global__ void __launch_bounds__(128, PDAC_SCALAR_FLUX_MINB) k_ygas_flux3d(Prm P, Fld F) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.ncell || !fluid(P, c)) return;
@@ -635,15 +638,15 @@ __global__ void __launch_bounds__(128, PDAC_SCALAR_FLUX_MINB) k_ygas_flux3d(Prm 
     rem3(P, i, j, k, R, M);
     bool dw = !fluid(P, R.w), ds = !fluid(P, R.s), db = !fluid(P, R.b);
     bool mus = P.muscl > 0 && P.flag[c] == FLUID;
-    S3 d;
+    S3T<Real> d;
     first_nb3(d, F.rgp, R, M);
     if (mus) third_nb3(d, F.rgp, M);
-    double uw = F.ug[R.w], uc = F.ug[c], vs = F.vg[R.s], vc = F.vg[c], wb = F.wg[R.b], wc = F.wg[c];
+    Real uw = F.ug[R.w], uc = F.ug[c], vs = F.vg[R.s], vc = F.vg[c], wb = F.wg[R.b], wc = F.wg[c];
     for (int ig = 0; ig < P.ng; ++ig) {
         const double *Y = F.ygc + (size_t)ig * P.ncell;
-        S3 y;
+        S3T<Real> y;
         first_nb3(y, Y, R, M);
-        F6d f = {0, 0, 0, 0, 0, 0};
+        F6T<Real> f = {0, 0, 0, 0, 0, 0};
         fsc_3d(P, f, dw, ds, db, d, y, uw, uc, vs, vc, wb, wc);
         if (mus) {
             third_nb3(y, Y, M);
@@ -691,7 +694,7 @@ __global__ void k_ygas3d(Prm P, Fld F, double dt) {
 // htilde, htilde.f:25-575 (3D)
 // ---------------------------------------------------------------------------
 // GRAV as in k_htilde_flux2d
-template <bool GRAV>
+template <bool GRAV, typename Real = double>
 __global__ void __launch_bounds__(128, PDAC_SCALAR_FLUX_MINB) k_htilde_flux3d(Prm P, Fld F) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.ncell || !fluid(P, c)) return;
@@ -715,27 +718,27 @@ __global__ void __launch_bounds__(128, PDAC_SCALAR_FLUX_MINB) k_htilde_flux3d(Pr
         double *fE = ph == 0 ? F.egfe : F.esfe + off;
         double *fN = ph == 0 ? F.egfn : F.esfn + off;
         double *fT = ph == 0 ? F.egft : F.esft + off;
-        S3 en, de;
+        S3T<Real> en, de;
         first_nb3(en, EN, R, M);
         first_nb3(de, DE, R, M);
-        double uw = U[R.w], uc = U[c], vs = V[R.s], vc = V[c], wb = W[R.b], wc = W[c];
-        F6d f = {0, 0, 0, 0, 0, 0};
+        Real uw = U[R.w], uc = U[c], vs = V[R.s], vc = V[c], wb = W[R.b], wc = W[c];
+        F6T<Real> f = {0, 0, 0, 0, 0, 0};
         fsc_3d(P, f, dw, ds, db, en, de, uw, uc, vs, vc, wb, wc);
         if (mus) {
             third_nb3(en, EN, M);
             third_nb3(de, DE, M);
             muscl_fsc_3d(P, f, en, de, uc, vc, wc, i, j, k);
         }
-        F6d h = {0, 0, 0, 0, 0, 0};
+        F6T<Real> h = {0, 0, 0, 0, 0, 0};
         bool visc = ph == 0 ? P.gas_viscosity : P.part_viscosity;
         if (visc) {
-            S3 ka, ep, te;
+            S3T<Real> ka, ep, te;
             if (ph == 0) {
                 first_nb3(ka, P.iturb ? F.kapgt : F.kapg, R, M);
                 first_nb3(ep, F.ep, R, M);
                 first_nb3(te, F.tg, R, M);
             } else {
-                double kk = P.kap[ph], ir = P.inrl[ph];
+                Real kk = P.kap[ph], ir = P.inrl[ph];
                 ka.c = ka.e = ka.w = ka.n = ka.s = ka.t = ka.b = kk;
                 ep.c = ir * de.c; ep.e = ir * de.e; ep.w = ir * de.w; ep.n = ir * de.n; ep.s = ir * de.s;
                 ep.t = ir * de.t; ep.b = ir * de.b;

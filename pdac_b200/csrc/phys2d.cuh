@@ -105,14 +105,18 @@ __device__ __forceinline__ void third_nb2(St &s, const T *a, const Rem2 &M) {
 }
 
 // ---- limiters.f:14-56 --------------------------------------------------------
-__device__ __forceinline__ double limiter(int t, double erre, double beta) {
+// Real is the arithmetic type of the flux pass (double, or float in the
+// mixed-precision mode of the 3D flux kernels)
+template <typename Real>
+__device__ __forceinline__ Real limiter(int t, Real erre, double beta_) {
+    const Real beta = Real(beta_);
     switch (t) {
-    case 1: return fmax(0.0, 2.0 * erre / (1.0 + erre));
-    case 2: return fmax(0.0, fmin(erre, 1.0));
-    case 3: return fmax(fmax(0.0, fmin(2.0 * erre, 1.0)), fmin(erre, 2.0));
-    case 4: { double bu = (1.0 - beta) + beta * erre; return fmax(0.0, fmin(fmin(2.0 * erre, bu), 2.0)); }
-    case 0: return (1.0 - beta) + beta * erre;
-    default: return 0.0;
+    case 1: return fmax(Real(0.0), Real(2.0) * erre / (Real(1.0) + erre));
+    case 2: return fmax(Real(0.0), fmin(erre, Real(1.0)));
+    case 3: return fmax(fmax(Real(0.0), fmin(Real(2.0) * erre, Real(1.0))), fmin(erre, Real(2.0)));
+    case 4: { Real bu = (Real(1.0) - beta) + beta * erre; return fmax(Real(0.0), fmin(fmin(Real(2.0) * erre, bu), Real(2.0))); }
+    case 0: return (Real(1.0) - beta) + beta * erre;
+    default: return Real(0.0);
     }
 }
 

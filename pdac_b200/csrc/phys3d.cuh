@@ -80,12 +80,14 @@ __device__ __forceinline__ void rem3(const Prm &P, int i, int j, int k, const Ra
     if (j == P.ny - 2) M.nnn = M.nn;
 }
 
-struct S3 {
-    double c, e, w, n, s, t, b, ee, ww, nn, ss, tt, bb;
-    double en, et, es, eb, nt, wn, nb, wt, st, eee, nnn, ttt, een, eet, enn, nnt, ett, ntt;
+template <typename Real>
+struct S3T {
+    Real c, e, w, n, s, t, b, ee, ww, nn, ss, tt, bb;
+    Real en, et, es, eb, nt, wn, nb, wt, st, eee, nnn, ttt, een, eet, enn, nnt, ett, ntt;
 };
-template <typename T>
-__device__ __forceinline__ void nb3(S3 &s, const T *a, const Raw3 &R, const Rem3 &M) {
+using S3 = S3T<double>;
+template <typename T, typename Real>
+__device__ __forceinline__ void nb3(S3T<Real> &s, const T *a, const Raw3 &R, const Rem3 &M) {
     s.c = a[R.c]; s.e = a[M.e]; s.w = a[M.w]; s.n = a[M.n]; s.s = a[M.s]; s.t = a[M.t]; s.b = a[M.b];
     s.ee = a[M.ee]; s.nn = a[M.nn]; s.tt = a[M.tt];
     s.en = a[R.en]; s.et = a[R.et]; s.es = a[R.es]; s.eb = a[M.eb]; s.nt = a[R.nt]; s.wn = a[R.wn];
@@ -94,8 +96,8 @@ __device__ __forceinline__ void nb3(S3 &s, const T *a, const Raw3 &R, const Rem3
     s.een = a[M.een]; s.eet = a[M.eet]; s.enn = a[M.enn]; s.nnt = a[M.nnt]; s.ett = a[M.ett]; s.ntt = a[M.ntt];
     s.ww = s.ss = s.bb = 0;
 }
-template <typename T>
-__device__ __forceinline__ void rnb3(S3 &s, const T *a, const Raw3 &R) {
+template <typename T, typename Real>
+__device__ __forceinline__ void rnb3(S3T<Real> &s, const T *a, const Raw3 &R) {
     s.c = a[R.c]; s.e = a[R.e]; s.n = a[R.n]; s.t = a[R.t]; s.w = a[R.w]; s.s = a[R.s]; s.b = a[R.b];
     s.ee = a[R.ee]; s.nn = a[R.nn]; s.tt = a[R.tt];
     s.en = a[R.en]; s.et = a[R.et]; s.es = a[R.es]; s.eb = a[R.eb]; s.nt = a[R.nt]; s.wn = a[R.wn];
@@ -104,21 +106,22 @@ __device__ __forceinline__ void rnb3(S3 &s, const T *a, const Raw3 &R) {
     s.een = a[R.een]; s.eet = a[R.eet]; s.enn = a[R.enn]; s.nnt = a[R.nnt]; s.ett = a[R.ett]; s.ntt = a[R.ntt];
     s.ww = s.ss = s.bb = 0;
 }
-template <typename T>
-__device__ __forceinline__ void first_nb3(S3 &s, const T *a, const Raw3 &R, const Rem3 &M) {
+template <typename T, typename Real>
+__device__ __forceinline__ void first_nb3(S3T<Real> &s, const T *a, const Raw3 &R, const Rem3 &M) {
     s.c = a[R.c]; s.e = a[M.e]; s.w = a[M.w]; s.n = a[M.n]; s.s = a[M.s]; s.t = a[M.t]; s.b = a[M.b];
 }
-template <typename T>
-__device__ __forceinline__ void third_nb3(S3 &s, const T *a, const Rem3 &M) {
+template <typename T, typename Real>
+__device__ __forceinline__ void third_nb3(S3T<Real> &s, const T *a, const Rem3 &M) {
     s.ee = a[M.ee]; s.ww = a[M.ww]; s.nn = a[M.nn]; s.ss = a[M.ss]; s.tt = a[M.tt]; s.bb = a[M.bb];
 }
 
 // interp.f (3D members)
-__device__ __forceinline__ void interp_x3(const Prm &P, const S3 &f, int i, S3 &s) {
-    const double *dx = P.dx;
+template <typename Real>
+__device__ __forceinline__ void interp_x3(const Prm &P, const S3T<Real> &f, int i, S3T<Real> &s) {
+    const Real *dx = Met<Real>::dx(P);
     int ip2 = min(P.nx, i + 2), ip3 = min(P.nx, i + 3);
-    double indxm = 1.0 / (dx[i] + dx[i - 1]), indxp = 1.0 / (dx[i] + dx[i + 1]);
-    double indxpp = 1.0 / (dx[i + 1] + dx[ip2]), indxppp = 1.0 / (dx[ip2] + dx[ip3]);
+    Real indxm = Real(1.0) / (dx[i] + dx[i - 1]), indxp = Real(1.0) / (dx[i] + dx[i + 1]);
+    Real indxpp = Real(1.0) / (dx[i + 1] + dx[ip2]), indxppp = Real(1.0) / (dx[ip2] + dx[ip3]);
     s.c = (dx[i + 1] * f.c + dx[i] * f.e) * indxp;
     s.e = (dx[ip2] * f.e + dx[i + 1] * f.ee) * indxpp;
     s.n = (dx[i + 1] * f.n + dx[i] * f.en) * indxp;
@@ -130,11 +133,12 @@ __device__ __forceinline__ void interp_x3(const Prm &P, const S3 &f, int i, S3 &
     s.nn = (dx[i] * f.enn + dx[i + 1] * f.nn) * indxp;
     s.tt = (dx[i] * f.ett + dx[i + 1] * f.tt) * indxp;
 }
-__device__ __forceinline__ void interp_y3(const Prm &P, const S3 &f, int j, S3 &s) {
-    const double *dy = P.dy;
+template <typename Real>
+__device__ __forceinline__ void interp_y3(const Prm &P, const S3T<Real> &f, int j, S3T<Real> &s) {
+    const Real *dy = Met<Real>::dy(P);
     int jp2 = min(P.ny, j + 2), jp3 = min(P.ny, j + 3);
-    double indym = 1.0 / (dy[j] + dy[j - 1]), indyp = 1.0 / (dy[j] + dy[j + 1]);
-    double indypp = 1.0 / (dy[j + 1] + dy[jp2]), indyppp = 1.0 / (dy[jp2] + dy[jp3]);
+    Real indym = Real(1.0) / (dy[j] + dy[j - 1]), indyp = Real(1.0) / (dy[j] + dy[j + 1]);
+    Real indypp = Real(1.0) / (dy[j + 1] + dy[jp2]), indyppp = Real(1.0) / (dy[jp2] + dy[jp3]);
     s.c = (dy[j + 1] * f.c + dy[j] * f.n) * indyp;
     s.e = (dy[j + 1] * f.e + dy[j] * f.en) * indyp;
     s.n = (dy[jp2] * f.n + dy[j + 1] * f.nn) * indypp;
@@ -146,11 +150,12 @@ __device__ __forceinline__ void interp_y3(const Prm &P, const S3 &f, int j, S3 &
     s.nn = (dy[jp2] * f.nnn + dy[jp3] * f.nn) * indyppp;
     s.tt = (dy[j] * f.ntt + dy[j + 1] * f.tt) * indyp;
 }
-__device__ __forceinline__ void interp_z3(const Prm &P, const S3 &f, int k, S3 &s) {
-    const double *dz = P.dz;
+template <typename Real>
+__device__ __forceinline__ void interp_z3(const Prm &P, const S3T<Real> &f, int k, S3T<Real> &s) {
+    const Real *dz = Met<Real>::dz(P);
     int kp2 = min(P.nz, k + 2), kp3 = min(P.nz, k + 3);
-    double indzm = 1.0 / (dz[k] + dz[k - 1]), indzp = 1.0 / (dz[k] + dz[k + 1]);
-    double indzpp = 1.0 / (dz[k + 1] + dz[kp2]), indzppp = 1.0 / (dz[kp2] + dz[kp3]);
+    Real indzm = Real(1.0) / (dz[k] + dz[k - 1]), indzp = Real(1.0) / (dz[k] + dz[k + 1]);
+    Real indzpp = Real(1.0) / (dz[k + 1] + dz[kp2]), indzppp = Real(1.0) / (dz[kp2] + dz[kp3]);
     s.c = (dz[k + 1] * f.c + dz[k] * f.t) * indzp;
     s.e = (dz[k + 1] * f.e + dz[k] * f.et) * indzp;
     s.n = (dz[k + 1] * f.n + dz[k] * f.nt) * indzp;
@@ -163,216 +168,229 @@ __device__ __forceinline__ void interp_z3(const Prm &P, const S3 &f, int k, S3 &
     s.tt = (dz[kp2] * f.ttt + dz[kp3] * f.tt) * indzppp;
 }
 
-struct F6d { double e, n, t, w, s, b; };
+template <typename Real>
+struct F6T { Real e, n, t, w, s, b; };
+using F6d = F6T<double>;
 
 // one limited face correction: shared by the momentum, mass and scalar MUSCL
 // routines, which differ only in the gradients and increments they pass
-__device__ __forceinline__ void muscl_face(int lt, double beta, double &fx, double cs, double gradc, double gradm,
-                                           double gradp, double incr_p, double incr_m, bool lim_on) {
-    double erre = 0, incr = 0, lim = 0;
+template <typename Real>
+__device__ __forceinline__ void muscl_face(int lt, double beta, Real &fx, Real cs, Real gradc, Real gradm,
+                                           Real gradp, Real incr_p, Real incr_m, bool lim_on) {
+    Real erre = 0, incr = 0, lim = 0;
     if (cs >= 0) { if (gradc != 0) erre = gradm / gradc; incr = incr_p; }
     else if (cs < 0) { if (gradc != 0) erre = gradp / gradc; incr = incr_m; }
     if (lim_on) lim = limiter(lt, erre, beta);
-    double upwnd = lim * gradc * incr;
+    Real upwnd = lim * gradc * incr;
     fx = fx + upwnd * cs;
 }
 
-__device__ __forceinline__ void flu_3d(const Prm &P, F6d &f, bool dw, bool ds, bool db, const S3 &d, const S3 &u,
-                                       const S3 &v, const S3 &w, int i) {
-    const double *dx = P.dx;
-    double indxp = 1.0 / (dx[i] + dx[i + 1]), cs;
-    if (dw) { cs = 0.5 * (u.c + u.w); f.w = 0.5 * (cs - fabs(cs)) * d.c * u.c + 0.5 * (cs + fabs(cs)) * d.w * u.w; }
-    if (ds) { cs = (dx[i + 1] * v.s + dx[i] * v.es) * indxp; f.s = 0.5 * (cs - fabs(cs)) * d.c * u.c + 0.5 * (cs + fabs(cs)) * d.s * u.s; }
-    if (db) { cs = (dx[i + 1] * w.b + dx[i] * w.eb) * indxp; f.b = 0.5 * (cs - fabs(cs)) * d.c * u.c + 0.5 * (cs + fabs(cs)) * d.b * u.b; }
-    cs = 0.5 * (u.c + u.e);
-    f.e = 0.5 * (cs - fabs(cs)) * d.e * u.e + 0.5 * (cs + fabs(cs)) * d.c * u.c;
+template <typename Real>
+__device__ __forceinline__ void flu_3d(const Prm &P, F6T<Real> &f, bool dw, bool ds, bool db, const S3T<Real> &d, const S3T<Real> &u,
+                                       const S3T<Real> &v, const S3T<Real> &w, int i) {
+    const Real *dx = Met<Real>::dx(P);
+    Real indxp = Real(1.0) / (dx[i] + dx[i + 1]), cs;
+    if (dw) { cs = Real(0.5) * (u.c + u.w); f.w = Real(0.5) * (cs - fabs(cs)) * d.c * u.c + Real(0.5) * (cs + fabs(cs)) * d.w * u.w; }
+    if (ds) { cs = (dx[i + 1] * v.s + dx[i] * v.es) * indxp; f.s = Real(0.5) * (cs - fabs(cs)) * d.c * u.c + Real(0.5) * (cs + fabs(cs)) * d.s * u.s; }
+    if (db) { cs = (dx[i + 1] * w.b + dx[i] * w.eb) * indxp; f.b = Real(0.5) * (cs - fabs(cs)) * d.c * u.c + Real(0.5) * (cs + fabs(cs)) * d.b * u.b; }
+    cs = Real(0.5) * (u.c + u.e);
+    f.e = Real(0.5) * (cs - fabs(cs)) * d.e * u.e + Real(0.5) * (cs + fabs(cs)) * d.c * u.c;
     cs = (dx[i + 1] * v.c + dx[i] * v.e) * indxp;
-    f.n = 0.5 * (cs - fabs(cs)) * d.n * u.n + 0.5 * (cs + fabs(cs)) * d.c * u.c;
+    f.n = Real(0.5) * (cs - fabs(cs)) * d.n * u.n + Real(0.5) * (cs + fabs(cs)) * d.c * u.c;
     cs = (dx[i + 1] * w.c + dx[i] * w.e) * indxp;
-    f.t = 0.5 * (cs - fabs(cs)) * d.t * u.t + 0.5 * (cs + fabs(cs)) * d.c * u.c;
+    f.t = Real(0.5) * (cs - fabs(cs)) * d.t * u.t + Real(0.5) * (cs + fabs(cs)) * d.c * u.c;
 }
-__device__ __forceinline__ void muscl_flu_3d(const Prm &P, F6d &f, const S3 &d, const S3 &u, const S3 &v, const S3 &w,
+template <typename Real>
+__device__ __forceinline__ void muscl_flu_3d(const Prm &P, F6T<Real> &f, const S3T<Real> &d, const S3T<Real> &u, const S3T<Real> &v, const S3T<Real> &w,
                                              int i, int j, int k) {
-    const double *dx = P.dx, *dy = P.dy, *dz = P.dz, *indx = P.indx;
+    const Real *dx = Met<Real>::dx(P), *dy = Met<Real>::dy(P), *dz = Met<Real>::dz(P), *indx = Met<Real>::indx(P);
     int ip2 = min(P.nx, i + 2), jp2 = min(P.ny, j + 2), kp2 = min(P.nz, k + 2);
-    double indxp = 1.0 / (dx[i] + dx[i + 1]);
-    double indym = 1.0 / (dy[j] + dy[j - 1]), indyp = 1.0 / (dy[j] + dy[j + 1]), indypp = 1.0 / (dy[j + 1] + dy[jp2]);
-    double indzm = 1.0 / (dz[k] + dz[k - 1]), indzp = 1.0 / (dz[k] + dz[k + 1]), indzpp = 1.0 / (dz[k + 1] + dz[kp2]);
-    double gradw = indx[i] * (u.c * d.c - u.w * d.w);
-    double gradc = indx[i + 1] * (u.e * d.e - u.c * d.c);
-    double grade = indx[ip2] * (u.ee * d.ee - u.e * d.e);
-    muscl_face(P.lv, P.beta, f.e, 0.5 * (u.c + u.e), gradc, gradw, grade, 0.5 * dx[i + 1], -0.5 * dx[i + 1], true);
-    double grads = (u.c * d.c - u.s * d.s) * 2.0 * indym;
-    gradc = (u.n * d.n - u.c * d.c) * 2.0 * indyp;
-    double gradn = (u.nn * d.nn - u.n * d.n) * 2.0 * indypp;
-    muscl_face(P.lv, P.beta, f.n, (dx[i + 1] * v.c + dx[i] * v.e) * indxp, gradc, grads, gradn, 0.5 * dy[j], -0.5 * dy[j + 1], true);
-    double gradb = (u.c * d.c - u.b * d.b) * 2.0 * indzm;
-    gradc = (u.t * d.t - u.c * d.c) * 2.0 * indzp;
-    double gradt = (u.tt * d.tt - u.t * d.t) * 2.0 * indzpp;
-    muscl_face(P.lv, P.beta, f.t, (dx[i + 1] * w.c + dx[i] * w.e) * indxp, gradc, gradb, gradt, 0.5 * dz[k], -0.5 * dz[k + 1], true);
+    Real indxp = Real(1.0) / (dx[i] + dx[i + 1]);
+    Real indym = Real(1.0) / (dy[j] + dy[j - 1]), indyp = Real(1.0) / (dy[j] + dy[j + 1]), indypp = Real(1.0) / (dy[j + 1] + dy[jp2]);
+    Real indzm = Real(1.0) / (dz[k] + dz[k - 1]), indzp = Real(1.0) / (dz[k] + dz[k + 1]), indzpp = Real(1.0) / (dz[k + 1] + dz[kp2]);
+    Real gradw = indx[i] * (u.c * d.c - u.w * d.w);
+    Real gradc = indx[i + 1] * (u.e * d.e - u.c * d.c);
+    Real grade = indx[ip2] * (u.ee * d.ee - u.e * d.e);
+    muscl_face(P.lv, P.beta, f.e, Real(0.5) * (u.c + u.e), gradc, gradw, grade, Real(0.5) * dx[i + 1], -Real(0.5) * dx[i + 1], true);
+    Real grads = (u.c * d.c - u.s * d.s) * Real(2.0) * indym;
+    gradc = (u.n * d.n - u.c * d.c) * Real(2.0) * indyp;
+    Real gradn = (u.nn * d.nn - u.n * d.n) * Real(2.0) * indypp;
+    muscl_face(P.lv, P.beta, f.n, (dx[i + 1] * v.c + dx[i] * v.e) * indxp, gradc, grads, gradn, Real(0.5) * dy[j], -Real(0.5) * dy[j + 1], true);
+    Real gradb = (u.c * d.c - u.b * d.b) * Real(2.0) * indzm;
+    gradc = (u.t * d.t - u.c * d.c) * Real(2.0) * indzp;
+    Real gradt = (u.tt * d.tt - u.t * d.t) * Real(2.0) * indzpp;
+    muscl_face(P.lv, P.beta, f.t, (dx[i + 1] * w.c + dx[i] * w.e) * indxp, gradc, gradb, gradt, Real(0.5) * dz[k], -Real(0.5) * dz[k + 1], true);
 }
-__device__ __forceinline__ void flv_3d(const Prm &P, F6d &f, bool dw, bool ds, bool db, const S3 &d, const S3 &u,
-                                       const S3 &v, const S3 &w, int j) {
-    const double *dy = P.dy;
-    double indyp = 1.0 / (dy[j] + dy[j + 1]), cs;
-    if (dw) { cs = (u.wn * dy[j] + u.w * dy[j + 1]) * indyp; f.w = 0.5 * (cs - fabs(cs)) * d.c * v.c + 0.5 * (cs + fabs(cs)) * d.w * v.w; }
-    if (ds) { cs = 0.5 * (v.c + v.s); f.s = 0.5 * (cs - fabs(cs)) * d.c * v.c + 0.5 * (cs + fabs(cs)) * d.s * v.s; }
-    if (db) { cs = (w.nb * dy[j] + w.b * dy[j + 1]) * indyp; f.b = 0.5 * (cs - fabs(cs)) * d.c * v.c + 0.5 * (cs + fabs(cs)) * d.b * v.b; }
+template <typename Real>
+__device__ __forceinline__ void flv_3d(const Prm &P, F6T<Real> &f, bool dw, bool ds, bool db, const S3T<Real> &d, const S3T<Real> &u,
+                                       const S3T<Real> &v, const S3T<Real> &w, int j) {
+    const Real *dy = Met<Real>::dy(P);
+    Real indyp = Real(1.0) / (dy[j] + dy[j + 1]), cs;
+    if (dw) { cs = (u.wn * dy[j] + u.w * dy[j + 1]) * indyp; f.w = Real(0.5) * (cs - fabs(cs)) * d.c * v.c + Real(0.5) * (cs + fabs(cs)) * d.w * v.w; }
+    if (ds) { cs = Real(0.5) * (v.c + v.s); f.s = Real(0.5) * (cs - fabs(cs)) * d.c * v.c + Real(0.5) * (cs + fabs(cs)) * d.s * v.s; }
+    if (db) { cs = (w.nb * dy[j] + w.b * dy[j + 1]) * indyp; f.b = Real(0.5) * (cs - fabs(cs)) * d.c * v.c + Real(0.5) * (cs + fabs(cs)) * d.b * v.b; }
     cs = indyp * (u.c * dy[j + 1] + u.n * dy[j]);
-    f.e = 0.5 * (cs - fabs(cs)) * d.e * v.e + 0.5 * (cs + fabs(cs)) * d.c * v.c;
-    cs = 0.5 * (v.n + v.c);
-    f.n = 0.5 * (cs - fabs(cs)) * d.n * v.n + 0.5 * (cs + fabs(cs)) * d.c * v.c;
+    f.e = Real(0.5) * (cs - fabs(cs)) * d.e * v.e + Real(0.5) * (cs + fabs(cs)) * d.c * v.c;
+    cs = Real(0.5) * (v.n + v.c);
+    f.n = Real(0.5) * (cs - fabs(cs)) * d.n * v.n + Real(0.5) * (cs + fabs(cs)) * d.c * v.c;
     cs = indyp * (w.c * dy[j + 1] + w.n * dy[j]);
-    f.t = 0.5 * (cs - fabs(cs)) * d.t * v.t + 0.5 * (cs + fabs(cs)) * d.c * v.c;
+    f.t = Real(0.5) * (cs - fabs(cs)) * d.t * v.t + Real(0.5) * (cs + fabs(cs)) * d.c * v.c;
 }
-__device__ __forceinline__ void muscl_flv_3d(const Prm &P, F6d &f, const S3 &d, const S3 &u, const S3 &v, const S3 &w,
+template <typename Real>
+__device__ __forceinline__ void muscl_flv_3d(const Prm &P, F6T<Real> &f, const S3T<Real> &d, const S3T<Real> &u, const S3T<Real> &v, const S3T<Real> &w,
                                              int i, int j, int k) {
-    const double *dx = P.dx, *dy = P.dy, *dz = P.dz, *indy = P.indy;
+    const Real *dx = Met<Real>::dx(P), *dy = Met<Real>::dy(P), *dz = Met<Real>::dz(P), *indy = Met<Real>::indy(P);
     int ip2 = min(P.nx, i + 2), jp2 = min(P.ny, j + 2), kp2 = min(P.nz, k + 2);
-    double indyp = 1.0 / (dy[j] + dy[j + 1]);
-    double indxm = 1.0 / (dx[i] + dx[i - 1]), indxp = 1.0 / (dx[i] + dx[i + 1]), indxpp = 1.0 / (dx[i + 1] + dx[ip2]);
-    double indzm = 1.0 / (dz[k] + dz[k - 1]), indzp = 1.0 / (dz[k] + dz[k + 1]), indzpp = 1.0 / (dz[k + 1] + dz[kp2]);
-    double gradw = 2.0 * indxm * (v.c * d.c - v.w * d.w);
-    double gradc = 2.0 * indxp * (v.e * d.e - v.c * d.c);
-    double grade = 2.0 * indxpp * (v.ee * d.ee - v.e * d.e);
-    muscl_face(P.lv, P.beta, f.e, indyp * (u.c * dy[j + 1] + u.n * dy[j]), gradc, gradw, grade, 0.5 * dx[i], -0.5 * dx[i + 1], true);
-    double grads = (v.c * d.c - v.s * d.s) * indy[j];
+    Real indyp = Real(1.0) / (dy[j] + dy[j + 1]);
+    Real indxm = Real(1.0) / (dx[i] + dx[i - 1]), indxp = Real(1.0) / (dx[i] + dx[i + 1]), indxpp = Real(1.0) / (dx[i + 1] + dx[ip2]);
+    Real indzm = Real(1.0) / (dz[k] + dz[k - 1]), indzp = Real(1.0) / (dz[k] + dz[k + 1]), indzpp = Real(1.0) / (dz[k + 1] + dz[kp2]);
+    Real gradw = Real(2.0) * indxm * (v.c * d.c - v.w * d.w);
+    Real gradc = Real(2.0) * indxp * (v.e * d.e - v.c * d.c);
+    Real grade = Real(2.0) * indxpp * (v.ee * d.ee - v.e * d.e);
+    muscl_face(P.lv, P.beta, f.e, indyp * (u.c * dy[j + 1] + u.n * dy[j]), gradc, gradw, grade, Real(0.5) * dx[i], -Real(0.5) * dx[i + 1], true);
+    Real grads = (v.c * d.c - v.s * d.s) * indy[j];
     gradc = (v.n * d.n - v.c * d.c) * indy[j + 1];
-    double gradn = (v.nn * d.nn - v.n * d.n) * indy[jp2];
-    muscl_face(P.lv, P.beta, f.n, 0.5 * (v.n + v.c), gradc, grads, gradn, 0.5 * dy[j + 1], -0.5 * dy[j + 1], true);
-    double gradb = (v.c * d.c - v.b * d.b) * 2.0 * indzm;
-    gradc = (v.t * d.t - v.c * d.c) * 2.0 * indzp;
-    double gradt = (v.tt * d.tt - v.t * d.t) * 2.0 * indzpp;
-    muscl_face(P.lv, P.beta, f.t, (dy[j + 1] * w.c + dy[j] * w.n) * indyp, gradc, gradb, gradt, 0.5 * dz[k], -0.5 * dz[k + 1], true);
+    Real gradn = (v.nn * d.nn - v.n * d.n) * indy[jp2];
+    muscl_face(P.lv, P.beta, f.n, Real(0.5) * (v.n + v.c), gradc, grads, gradn, Real(0.5) * dy[j + 1], -Real(0.5) * dy[j + 1], true);
+    Real gradb = (v.c * d.c - v.b * d.b) * Real(2.0) * indzm;
+    gradc = (v.t * d.t - v.c * d.c) * Real(2.0) * indzp;
+    Real gradt = (v.tt * d.tt - v.t * d.t) * Real(2.0) * indzpp;
+    muscl_face(P.lv, P.beta, f.t, (dy[j + 1] * w.c + dy[j] * w.n) * indyp, gradc, gradb, gradt, Real(0.5) * dz[k], -Real(0.5) * dz[k + 1], true);
 }
-__device__ __forceinline__ void flw_3d(const Prm &P, F6d &f, bool dw, bool ds, bool db, const S3 &d, const S3 &u,
-                                       const S3 &v, const S3 &w, int k) {
-    const double *dz = P.dz;
-    double indzp = 1.0 / (dz[k] + dz[k + 1]), cs;
-    if (dw) { cs = (dz[k + 1] * u.w + dz[k] * u.wt) * indzp; f.w = 0.5 * d.w * w.w * (cs + fabs(cs)) + 0.5 * d.c * w.c * (cs - fabs(cs)); }
-    if (ds) { cs = (dz[k + 1] * v.s + dz[k] * v.st) * indzp; f.s = 0.5 * d.s * w.s * (cs + fabs(cs)) + 0.5 * d.c * w.c * (cs - fabs(cs)); }
-    if (db) { cs = 0.5 * (w.b + w.c); f.b = 0.5 * d.b * w.b * (cs + fabs(cs)) + 0.5 * d.c * w.c * (cs - fabs(cs)); }
+template <typename Real>
+__device__ __forceinline__ void flw_3d(const Prm &P, F6T<Real> &f, bool dw, bool ds, bool db, const S3T<Real> &d, const S3T<Real> &u,
+                                       const S3T<Real> &v, const S3T<Real> &w, int k) {
+    const Real *dz = Met<Real>::dz(P);
+    Real indzp = Real(1.0) / (dz[k] + dz[k + 1]), cs;
+    if (dw) { cs = (dz[k + 1] * u.w + dz[k] * u.wt) * indzp; f.w = Real(0.5) * d.w * w.w * (cs + fabs(cs)) + Real(0.5) * d.c * w.c * (cs - fabs(cs)); }
+    if (ds) { cs = (dz[k + 1] * v.s + dz[k] * v.st) * indzp; f.s = Real(0.5) * d.s * w.s * (cs + fabs(cs)) + Real(0.5) * d.c * w.c * (cs - fabs(cs)); }
+    if (db) { cs = Real(0.5) * (w.b + w.c); f.b = Real(0.5) * d.b * w.b * (cs + fabs(cs)) + Real(0.5) * d.c * w.c * (cs - fabs(cs)); }
     cs = (dz[k + 1] * u.c + dz[k] * u.t) * indzp;
-    f.e = 0.5 * d.c * w.c * (cs + fabs(cs)) + 0.5 * d.e * w.e * (cs - fabs(cs));
+    f.e = Real(0.5) * d.c * w.c * (cs + fabs(cs)) + Real(0.5) * d.e * w.e * (cs - fabs(cs));
     cs = (dz[k + 1] * v.c + dz[k] * v.t) * indzp;
-    f.n = 0.5 * d.c * w.c * (cs + fabs(cs)) + 0.5 * d.n * w.n * (cs - fabs(cs));
-    cs = 0.5 * (w.c + w.t);
-    f.t = 0.5 * d.c * w.c * (cs + fabs(cs)) + 0.5 * d.t * w.t * (cs - fabs(cs));
+    f.n = Real(0.5) * d.c * w.c * (cs + fabs(cs)) + Real(0.5) * d.n * w.n * (cs - fabs(cs));
+    cs = Real(0.5) * (w.c + w.t);
+    f.t = Real(0.5) * d.c * w.c * (cs + fabs(cs)) + Real(0.5) * d.t * w.t * (cs - fabs(cs));
 }
-__device__ __forceinline__ void muscl_flw_3d(const Prm &P, F6d &f, const S3 &d, const S3 &u, const S3 &v, const S3 &w,
+template <typename Real>
+__device__ __forceinline__ void muscl_flw_3d(const Prm &P, F6T<Real> &f, const S3T<Real> &d, const S3T<Real> &u, const S3T<Real> &v, const S3T<Real> &w,
                                              int i, int j, int k) {
-    const double *dx = P.dx, *dy = P.dy, *dz = P.dz, *indz = P.indz;
+    const Real *dx = Met<Real>::dx(P), *dy = Met<Real>::dy(P), *dz = Met<Real>::dz(P), *indz = Met<Real>::indz(P);
     int ip2 = min(P.nx, i + 2), jp2 = min(P.ny, j + 2), kp2 = min(P.nz, k + 2);
-    double indxm = 1.0 / (dx[i] + dx[i - 1]), indxp = 1.0 / (dx[i] + dx[i + 1]), indxpp = 1.0 / (dx[i + 1] + dx[ip2]);
-    double indym = 1.0 / (dy[j] + dy[j - 1]), indyp = 1.0 / (dy[j] + dy[j + 1]), indypp = 1.0 / (dy[j + 1] + dy[jp2]);
-    double indzp = 1.0 / (dz[k] + dz[k + 1]);
-    double gradw = 2.0 * indxm * (w.c * d.c - w.w * d.w);
-    double gradc = 2.0 * indxp * (w.e * d.e - w.c * d.c);
-    double grade = 2.0 * indxpp * (w.ee * d.ee - w.e * d.e);
-    muscl_face(P.lv, P.beta, f.e, (dz[k + 1] * u.c + dz[k] * u.t) * indzp, gradc, gradw, grade, 0.5 * dx[i], -0.5 * dx[i + 1], true);
-    double grads = 2.0 * indym * (w.c * d.c - w.s * d.s);
-    gradc = 2.0 * indyp * (w.n * d.n - w.c * d.c);
-    double gradn = 2.0 * indypp * (w.nn * d.nn - w.n * d.n);
-    muscl_face(P.lv, P.beta, f.n, (dz[k + 1] * v.c + dz[k] * v.t) * indzp, gradc, grads, gradn, 0.5 * dy[j], -0.5 * dy[j + 1], true);
-    double gradb = indz[k] * (w.c * d.c - w.b * d.b);
+    Real indxm = Real(1.0) / (dx[i] + dx[i - 1]), indxp = Real(1.0) / (dx[i] + dx[i + 1]), indxpp = Real(1.0) / (dx[i + 1] + dx[ip2]);
+    Real indym = Real(1.0) / (dy[j] + dy[j - 1]), indyp = Real(1.0) / (dy[j] + dy[j + 1]), indypp = Real(1.0) / (dy[j + 1] + dy[jp2]);
+    Real indzp = Real(1.0) / (dz[k] + dz[k + 1]);
+    Real gradw = Real(2.0) * indxm * (w.c * d.c - w.w * d.w);
+    Real gradc = Real(2.0) * indxp * (w.e * d.e - w.c * d.c);
+    Real grade = Real(2.0) * indxpp * (w.ee * d.ee - w.e * d.e);
+    muscl_face(P.lv, P.beta, f.e, (dz[k + 1] * u.c + dz[k] * u.t) * indzp, gradc, gradw, grade, Real(0.5) * dx[i], -Real(0.5) * dx[i + 1], true);
+    Real grads = Real(2.0) * indym * (w.c * d.c - w.s * d.s);
+    gradc = Real(2.0) * indyp * (w.n * d.n - w.c * d.c);
+    Real gradn = Real(2.0) * indypp * (w.nn * d.nn - w.n * d.n);
+    muscl_face(P.lv, P.beta, f.n, (dz[k + 1] * v.c + dz[k] * v.t) * indzp, gradc, grads, gradn, Real(0.5) * dy[j], -Real(0.5) * dy[j + 1], true);
+    Real gradb = indz[k] * (w.c * d.c - w.b * d.b);
     gradc = indz[k + 1] * (w.t * d.t - w.c * d.c);
-    double gradt = indz[kp2] * (w.tt * d.tt - w.t * d.t);
-    muscl_face(P.lv, P.beta, f.t, 0.5 * (w.c + w.t), gradc, gradb, gradt, 0.5 * dz[k + 1], -0.5 * dz[k + 1], true);
+    Real gradt = indz[kp2] * (w.tt * d.tt - w.t * d.t);
+    muscl_face(P.lv, P.beta, f.t, Real(0.5) * (w.c + w.t), gradc, gradb, gradt, Real(0.5) * dz[k + 1], -Real(0.5) * dz[k + 1], true);
 }
 
 // masf_3d + fmas_3d for one cell; face velocities given directly
-__device__ __forceinline__ void massflux_3d(const Prm &P, const S3 &d, double uw, double uc, double vs, double vc,
-                                            double wb, double wc, int i, int j, int k, bool muscl_on, int flw, int fle,
-                                            int fls, int fln, int flb, int flt, F6d &f) {
-    double cs;
-    cs = uw; f.w = 0.5 * (cs - fabs(cs)) * d.c + 0.5 * (cs + fabs(cs)) * d.w;
-    cs = vs; f.s = 0.5 * (cs - fabs(cs)) * d.c + 0.5 * (cs + fabs(cs)) * d.s;
-    cs = wb; f.b = 0.5 * (cs - fabs(cs)) * d.c + 0.5 * (cs + fabs(cs)) * d.b;
-    cs = uc; f.e = 0.5 * (cs - fabs(cs)) * d.e + 0.5 * (cs + fabs(cs)) * d.c;
-    cs = vc; f.n = 0.5 * (cs - fabs(cs)) * d.n + 0.5 * (cs + fabs(cs)) * d.c;
-    cs = wc; f.t = 0.5 * (cs - fabs(cs)) * d.t + 0.5 * (cs + fabs(cs)) * d.c;
+template <typename Real>
+__device__ __forceinline__ void massflux_3d(const Prm &P, const S3T<Real> &d, Real uw, Real uc, Real vs, Real vc,
+                                            Real wb, Real wc, int i, int j, int k, bool muscl_on, int flw, int fle,
+                                            int fls, int fln, int flb, int flt, F6T<Real> &f) {
+    Real cs;
+    cs = uw; f.w = Real(0.5) * (cs - fabs(cs)) * d.c + Real(0.5) * (cs + fabs(cs)) * d.w;
+    cs = vs; f.s = Real(0.5) * (cs - fabs(cs)) * d.c + Real(0.5) * (cs + fabs(cs)) * d.s;
+    cs = wb; f.b = Real(0.5) * (cs - fabs(cs)) * d.c + Real(0.5) * (cs + fabs(cs)) * d.b;
+    cs = uc; f.e = Real(0.5) * (cs - fabs(cs)) * d.e + Real(0.5) * (cs + fabs(cs)) * d.c;
+    cs = vc; f.n = Real(0.5) * (cs - fabs(cs)) * d.n + Real(0.5) * (cs + fabs(cs)) * d.c;
+    cs = wc; f.t = Real(0.5) * (cs - fabs(cs)) * d.t + Real(0.5) * (cs + fabs(cs)) * d.c;
     if (!muscl_on) return;
-    const double *dx = P.dx, *dy = P.dy, *dz = P.dz;
+    const Real *dx = Met<Real>::dx(P), *dy = Met<Real>::dy(P), *dz = Met<Real>::dz(P);
     int im2 = max(1, i - 2), ip2 = min(P.nx, i + 2), jm2 = max(1, j - 2), jp2 = min(P.ny, j + 2);
     int km2 = max(1, k - 2), kp2 = min(P.nz, k + 2);
-    double indxmm = 1.0 / (dx[i - 1] + dx[im2]), indxm = 1.0 / (dx[i] + dx[i - 1]), indxp = 1.0 / (dx[i] + dx[i + 1]), indxpp = 1.0 / (dx[i + 1] + dx[ip2]);
-    double indymm = 1.0 / (dy[j - 1] + dy[jm2]), indym = 1.0 / (dy[j] + dy[j - 1]), indyp = 1.0 / (dy[j] + dy[j + 1]), indypp = 1.0 / (dy[j + 1] + dy[jp2]);
-    double indzmm = 1.0 / (dz[k - 1] + dz[km2]), indzm = 1.0 / (dz[k] + dz[k - 1]), indzp = 1.0 / (dz[k] + dz[k + 1]), indzpp = 1.0 / (dz[k + 1] + dz[kp2]);
-    double gradc, gradw, grade, grads, gradn, gradb, gradt;
-    gradc = 2.0 * indxm * (d.c - d.w); gradw = 2.0 * indxmm * (d.w - d.ww); grade = 2.0 * indxp * (d.e - d.c);
-    muscl_face(P.lm, P.beta, f.w, uw, gradc, gradw, grade, 0.5 * dx[i - 1], -0.5 * dx[i], i != 2 && flw == FLUID);
-    gradw = gradc; gradc = grade; grade = 2.0 * indxpp * (d.ee - d.e);
-    muscl_face(P.lm, P.beta, f.e, uc, gradc, gradw, grade, 0.5 * dx[i], -0.5 * dx[i + 1], i != P.nx - 1 && fle == FLUID);
-    gradc = 2.0 * indym * (d.c - d.s); grads = 2.0 * indymm * (d.s - d.ss); gradn = 2.0 * indyp * (d.n - d.c);
-    muscl_face(P.lm, P.beta, f.s, vs, gradc, grads, gradn, 0.5 * dy[j - 1], -0.5 * dy[j], j != 2 && fls == FLUID);
-    grads = gradc; gradc = gradn; gradn = 2.0 * indypp * (d.nn - d.n);
-    muscl_face(P.lm, P.beta, f.n, vc, gradc, grads, gradn, 0.5 * dy[j], -0.5 * dy[j + 1], j != P.ny - 1 && fln == FLUID);
-    gradc = 2.0 * indzm * (d.c - d.b); gradb = 2.0 * indzmm * (d.b - d.bb); gradt = 2.0 * indzp * (d.t - d.c);
-    muscl_face(P.lm, P.beta, f.b, wb, gradc, gradb, gradt, 0.5 * dz[k - 1], -0.5 * dz[k], k != 2 && flb == FLUID);
-    gradb = gradc; gradc = gradt; gradt = 2.0 * indzpp * (d.tt - d.t);
-    muscl_face(P.lm, P.beta, f.t, wc, gradc, gradb, gradt, 0.5 * dz[k], -0.5 * dz[k + 1], k != P.nz - 1 && flt == FLUID);
+    Real indxmm = Real(1.0) / (dx[i - 1] + dx[im2]), indxm = Real(1.0) / (dx[i] + dx[i - 1]), indxp = Real(1.0) / (dx[i] + dx[i + 1]), indxpp = Real(1.0) / (dx[i + 1] + dx[ip2]);
+    Real indymm = Real(1.0) / (dy[j - 1] + dy[jm2]), indym = Real(1.0) / (dy[j] + dy[j - 1]), indyp = Real(1.0) / (dy[j] + dy[j + 1]), indypp = Real(1.0) / (dy[j + 1] + dy[jp2]);
+    Real indzmm = Real(1.0) / (dz[k - 1] + dz[km2]), indzm = Real(1.0) / (dz[k] + dz[k - 1]), indzp = Real(1.0) / (dz[k] + dz[k + 1]), indzpp = Real(1.0) / (dz[k + 1] + dz[kp2]);
+    Real gradc, gradw, grade, grads, gradn, gradb, gradt;
+    gradc = Real(2.0) * indxm * (d.c - d.w); gradw = Real(2.0) * indxmm * (d.w - d.ww); grade = Real(2.0) * indxp * (d.e - d.c);
+    muscl_face(P.lm, P.beta, f.w, uw, gradc, gradw, grade, Real(0.5) * dx[i - 1], -Real(0.5) * dx[i], i != 2 && flw == FLUID);
+    gradw = gradc; gradc = grade; grade = Real(2.0) * indxpp * (d.ee - d.e);
+    muscl_face(P.lm, P.beta, f.e, uc, gradc, gradw, grade, Real(0.5) * dx[i], -Real(0.5) * dx[i + 1], i != P.nx - 1 && fle == FLUID);
+    gradc = Real(2.0) * indym * (d.c - d.s); grads = Real(2.0) * indymm * (d.s - d.ss); gradn = Real(2.0) * indyp * (d.n - d.c);
+    muscl_face(P.lm, P.beta, f.s, vs, gradc, grads, gradn, Real(0.5) * dy[j - 1], -Real(0.5) * dy[j], j != 2 && fls == FLUID);
+    grads = gradc; gradc = gradn; gradn = Real(2.0) * indypp * (d.nn - d.n);
+    muscl_face(P.lm, P.beta, f.n, vc, gradc, grads, gradn, Real(0.5) * dy[j], -Real(0.5) * dy[j + 1], j != P.ny - 1 && fln == FLUID);
+    gradc = Real(2.0) * indzm * (d.c - d.b); gradb = Real(2.0) * indzmm * (d.b - d.bb); gradt = Real(2.0) * indzp * (d.t - d.c);
+    muscl_face(P.lm, P.beta, f.b, wb, gradc, gradb, gradt, Real(0.5) * dz[k - 1], -Real(0.5) * dz[k], k != 2 && flb == FLUID);
+    gradb = gradc; gradc = gradt; gradt = Real(2.0) * indzpp * (d.tt - d.t);
+    muscl_face(P.lm, P.beta, f.t, wc, gradc, gradb, gradt, Real(0.5) * dz[k], -Real(0.5) * dz[k + 1], k != P.nz - 1 && flt == FLUID);
 }
 
 // fsc_3d + muscl_fsc_3d; W/S/B only where that neighbour is not fluid
-__device__ __forceinline__ void fsc_3d(const Prm &P, F6d &f, bool dw, bool ds, bool db, const S3 &d, const S3 &fl,
-                                       double uw, double uc, double vs, double vc, double wb, double wc) {
-    double cs;
-    if (dw) { cs = uw; f.w = 0.5 * (cs - fabs(cs)) * d.c * fl.c + 0.5 * (cs + fabs(cs)) * d.w * fl.w; }
-    if (ds) { cs = vs; f.s = 0.5 * (cs - fabs(cs)) * d.c * fl.c + 0.5 * (cs + fabs(cs)) * d.s * fl.s; }
-    if (db) { cs = wb; f.b = 0.5 * (cs - fabs(cs)) * d.c * fl.c + 0.5 * (cs + fabs(cs)) * d.b * fl.b; }
-    cs = uc; f.e = 0.5 * (cs - fabs(cs)) * d.e * fl.e + 0.5 * (cs + fabs(cs)) * d.c * fl.c;
-    cs = vc; f.n = 0.5 * (cs - fabs(cs)) * d.n * fl.n + 0.5 * (cs + fabs(cs)) * d.c * fl.c;
-    cs = wc; f.t = 0.5 * (cs - fabs(cs)) * d.t * fl.t + 0.5 * (cs + fabs(cs)) * d.c * fl.c;
+template <typename Real>
+__device__ __forceinline__ void fsc_3d(const Prm &P, F6T<Real> &f, bool dw, bool ds, bool db, const S3T<Real> &d, const S3T<Real> &fl,
+                                       Real uw, Real uc, Real vs, Real vc, Real wb, Real wc) {
+    Real cs;
+    if (dw) { cs = uw; f.w = Real(0.5) * (cs - fabs(cs)) * d.c * fl.c + Real(0.5) * (cs + fabs(cs)) * d.w * fl.w; }
+    if (ds) { cs = vs; f.s = Real(0.5) * (cs - fabs(cs)) * d.c * fl.c + Real(0.5) * (cs + fabs(cs)) * d.s * fl.s; }
+    if (db) { cs = wb; f.b = Real(0.5) * (cs - fabs(cs)) * d.c * fl.c + Real(0.5) * (cs + fabs(cs)) * d.b * fl.b; }
+    cs = uc; f.e = Real(0.5) * (cs - fabs(cs)) * d.e * fl.e + Real(0.5) * (cs + fabs(cs)) * d.c * fl.c;
+    cs = vc; f.n = Real(0.5) * (cs - fabs(cs)) * d.n * fl.n + Real(0.5) * (cs + fabs(cs)) * d.c * fl.c;
+    cs = wc; f.t = Real(0.5) * (cs - fabs(cs)) * d.t * fl.t + Real(0.5) * (cs + fabs(cs)) * d.c * fl.c;
 }
-__device__ __forceinline__ void muscl_fsc_3d(const Prm &P, F6d &f, const S3 &d, const S3 &fl, double uc, double vc,
-                                             double wc, int i, int j, int k) {
-    const double *dx = P.dx, *dy = P.dy, *dz = P.dz;
+template <typename Real>
+__device__ __forceinline__ void muscl_fsc_3d(const Prm &P, F6T<Real> &f, const S3T<Real> &d, const S3T<Real> &fl, Real uc, Real vc,
+                                             Real wc, int i, int j, int k) {
+    const Real *dx = Met<Real>::dx(P), *dy = Met<Real>::dy(P), *dz = Met<Real>::dz(P);
     int ip2 = min(P.nx, i + 2), jp2 = min(P.ny, j + 2), kp2 = min(P.nz, k + 2);
-    double indxm = 1.0 / (dx[i] + dx[i - 1]), indxp = 1.0 / (dx[i] + dx[i + 1]), indxpp = 1.0 / (dx[i + 1] + dx[ip2]);
-    double indym = 1.0 / (dy[j] + dy[j - 1]), indyp = 1.0 / (dy[j] + dy[j + 1]), indypp = 1.0 / (dy[j + 1] + dy[jp2]);
-    double indzm = 1.0 / (dz[k] + dz[k - 1]), indzp = 1.0 / (dz[k] + dz[k + 1]), indzpp = 1.0 / (dz[k + 1] + dz[kp2]);
-    double gradc = 2.0 * indxp * (d.e * fl.e - d.c * fl.c);
-    double gradw = 2.0 * indxm * (d.c * fl.c - d.w * fl.w);
-    double grade = 2.0 * indxpp * (d.ee * fl.ee - d.e * fl.e);
-    muscl_face(P.lm, P.beta, f.e, uc, gradc, gradw, grade, 0.5 * dx[i], -0.5 * dx[i + 1], i != P.nx - 1);
-    gradc = 2.0 * indyp * (d.n * fl.n - d.c * fl.c);
-    double grads = 2.0 * indym * (d.c * fl.c - d.s * fl.s);
-    double gradn = 2.0 * indypp * (d.nn * fl.nn - d.n * fl.n);
-    muscl_face(P.lm, P.beta, f.n, vc, gradc, grads, gradn, 0.5 * dy[j], -0.5 * dy[j + 1], j != P.ny - 1);
-    gradc = 2.0 * indzp * (d.t * fl.t - d.c * fl.c);
-    double gradb = 2.0 * indzm * (d.c * fl.c - d.b * fl.b);
-    double gradt = 2.0 * indzpp * (d.tt * fl.tt - d.t * fl.t);
-    muscl_face(P.lm, P.beta, f.t, wc, gradc, gradb, gradt, 0.5 * dz[k], -0.5 * dz[k + 1], k != P.nz - 1);
+    Real indxm = Real(1.0) / (dx[i] + dx[i - 1]), indxp = Real(1.0) / (dx[i] + dx[i + 1]), indxpp = Real(1.0) / (dx[i + 1] + dx[ip2]);
+    Real indym = Real(1.0) / (dy[j] + dy[j - 1]), indyp = Real(1.0) / (dy[j] + dy[j + 1]), indypp = Real(1.0) / (dy[j + 1] + dy[jp2]);
+    Real indzm = Real(1.0) / (dz[k] + dz[k - 1]), indzp = Real(1.0) / (dz[k] + dz[k + 1]), indzpp = Real(1.0) / (dz[k + 1] + dz[kp2]);
+    Real gradc = Real(2.0) * indxp * (d.e * fl.e - d.c * fl.c);
+    Real gradw = Real(2.0) * indxm * (d.c * fl.c - d.w * fl.w);
+    Real grade = Real(2.0) * indxpp * (d.ee * fl.ee - d.e * fl.e);
+    muscl_face(P.lm, P.beta, f.e, uc, gradc, gradw, grade, Real(0.5) * dx[i], -Real(0.5) * dx[i + 1], i != P.nx - 1);
+    gradc = Real(2.0) * indyp * (d.n * fl.n - d.c * fl.c);
+    Real grads = Real(2.0) * indym * (d.c * fl.c - d.s * fl.s);
+    Real gradn = Real(2.0) * indypp * (d.nn * fl.nn - d.n * fl.n);
+    muscl_face(P.lm, P.beta, f.n, vc, gradc, grads, gradn, Real(0.5) * dy[j], -Real(0.5) * dy[j + 1], j != P.ny - 1);
+    gradc = Real(2.0) * indzp * (d.t * fl.t - d.c * fl.c);
+    Real gradb = Real(2.0) * indzm * (d.c * fl.c - d.b * fl.b);
+    Real gradt = Real(2.0) * indzpp * (d.tt * fl.tt - d.t * fl.t);
+    muscl_face(P.lm, P.beta, f.t, wc, gradc, gradb, gradt, Real(0.5) * dz[k], -Real(0.5) * dz[k + 1], k != P.nz - 1);
 }
 
 // hotc.f:12-82 (3D)
-__device__ __forceinline__ void hotc_3d(const Prm &P, F6d &h, bool hw, bool hs, bool hb, const S3 &ep, const S3 &tg,
-                                        const S3 &ka, int i, int j, int k) {
-    const double *dx = P.dx, *dy = P.dy, *dz = P.dz;
+template <typename Real>
+__device__ __forceinline__ void hotc_3d(const Prm &P, F6T<Real> &h, bool hw, bool hs, bool hb, const S3T<Real> &ep, const S3T<Real> &tg,
+                                        const S3T<Real> &ka, int i, int j, int k) {
+    const Real *dx = Met<Real>::dx(P), *dy = Met<Real>::dy(P), *dz = Met<Real>::dz(P);
     if (hw) {
-        double indxm = 1.0 / (dx[i] + dx[i - 1]);
-        double km = (dx[i - 1] * ka.c + dx[i] * ka.w) * indxm, em = (dx[i - 1] * ep.c + dx[i] * ep.w) * indxm;
-        h.w = km * em * (tg.c - tg.w) * indxm * 2.0;
+        Real indxm = Real(1.0) / (dx[i] + dx[i - 1]);
+        Real km = (dx[i - 1] * ka.c + dx[i] * ka.w) * indxm, em = (dx[i - 1] * ep.c + dx[i] * ep.w) * indxm;
+        h.w = km * em * (tg.c - tg.w) * indxm * Real(2.0);
     }
     if (hs) {
-        double indym = 1.0 / (dy[j] + dy[j - 1]);
-        double km = (dy[j - 1] * ka.c + dy[j] * ka.s) * indym, em = (dy[j - 1] * ep.c + dy[j] * ep.s) * indym;
-        h.s = km * em * (tg.c - tg.s) * indym * 2.0;
+        Real indym = Real(1.0) / (dy[j] + dy[j - 1]);
+        Real km = (dy[j - 1] * ka.c + dy[j] * ka.s) * indym, em = (dy[j - 1] * ep.c + dy[j] * ep.s) * indym;
+        h.s = km * em * (tg.c - tg.s) * indym * Real(2.0);
     }
     if (hb) {
-        double indzm = 1.0 / (dz[k] + dz[k - 1]);
-        double km = (dz[k - 1] * ka.c + dz[k] * ka.b) * indzm, em = (dz[k - 1] * ep.c + dz[k] * ep.b) * indzm;
-        h.b = km * em * (tg.c - tg.b) * indzm * 2.0;
+        Real indzm = Real(1.0) / (dz[k] + dz[k - 1]);
+        Real km = (dz[k - 1] * ka.c + dz[k] * ka.b) * indzm, em = (dz[k - 1] * ep.c + dz[k] * ep.b) * indzm;
+        h.b = km * em * (tg.c - tg.b) * indzm * Real(2.0);
     }
-    double indxp = 1.0 / (dx[i] + dx[i + 1]);
-    double kme = (dx[i + 1] * ka.c + dx[i] * ka.e) * indxp, epme = (dx[i + 1] * ep.c + dx[i] * ep.e) * indxp;
-    h.e = kme * epme * (tg.e - tg.c) * indxp * 2.0;
-    double indyp = 1.0 / (dy[j] + dy[j + 1]);
-    double kmn = (dy[j + 1] * ka.c + dy[j] * ka.n) * indyp, epmn = (dy[j + 1] * ep.c + dy[j] * ep.n) * indyp;
-    h.n = kmn * epmn * (tg.n - tg.c) * indyp * 2.0;
-    double indzp = 1.0 / (dz[k] + dz[k + 1]);
-    double kmt = (dz[k + 1] * ka.c + dz[k] * ka.t) * indzp, epmt = (dz[k + 1] * ep.c + dz[k] * ep.t) * indzp;
-    h.t = kmt * epmt * (tg.t - tg.c) * indzp * 2.0;
+    Real indxp = Real(1.0) / (dx[i] + dx[i + 1]);
+    Real kme = (dx[i + 1] * ka.c + dx[i] * ka.e) * indxp, epme = (dx[i + 1] * ep.c + dx[i] * ep.e) * indxp;
+    h.e = kme * epme * (tg.e - tg.c) * indxp * Real(2.0);
+    Real indyp = Real(1.0) / (dy[j] + dy[j + 1]);
+    Real kmn = (dy[j + 1] * ka.c + dy[j] * ka.n) * indyp, epmn = (dy[j + 1] * ep.c + dy[j] * ep.n) * indyp;
+    h.n = kmn * epmn * (tg.n - tg.c) * indyp * Real(2.0);
+    Real indzp = Real(1.0) / (dz[k] + dz[k + 1]);
+    Real kmt = (dz[k + 1] * ka.c + dz[k] * ka.t) * indzp, epmt = (dz[k + 1] * ep.c + dz[k] * ep.t) * indzp;
+    h.t = kmt * epmt * (tg.t - tg.c) * indzp * Real(2.0);
 }
 
 // stress3D (visc.f:293-559) for one cell; mu == lambda on this path

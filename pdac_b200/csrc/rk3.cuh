@@ -403,7 +403,8 @@ __global__ void k_visc2d(Prm P, Fld F) {
 // zero.  A face shared by two fluid cells ends with the value of the later
 // cell of the reference loop, so this thread writes its W/S/B faces always
 // and its E/N/T faces only towards non-fluid cells.
-template <int D>
+// Real as in k_tilde_flux3d (float only in 3D).
+template <int D, typename Real = double>
 __global__ void __launch_bounds__(128, PDAC_FLUX_MINB) k_rk3_mflux(Prm P, Fld F) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.ncell || !fluid(P, c)) return;
@@ -426,14 +427,14 @@ __global__ void __launch_bounds__(128, PDAC_FLUX_MINB) k_rk3_mflux(Prm P, Fld F)
             double *fe = ph == 0 ? F.rgfe : F.rsfe + off;
             double *fn = ph == 0 ? F.rgfn : F.rsfn + off;
             double *ft = ph == 0 ? F.rgft : F.rsft + off;
-            S3 d;
+            S3T<Real> d;
             first_nb3(d, Dn, R, M);
             if (mus) {
                 third_nb3(d, Dn, M);
                 d.ww = 0.0; d.ss = 0.0; d.bb = 0.0;
             }
-            F6d f;
-            massflux_3d(P, d, U[R.w], U[c], V[R.s], V[c], W[R.b], W[c], i, j, k, mus, fl[R.w], fl[R.e], fl[R.s], fl[R.n],
+            F6T<Real> f;
+            massflux_3d(P, d, Real(U[R.w]), Real(U[c]), Real(V[R.s]), Real(V[c]), Real(W[R.b]), Real(W[c]), i, j, k, mus, fl[R.w], fl[R.e], fl[R.s], fl[R.n],
                         fl[R.b], fl[R.t], f);
             fe[R.w] = f.w;
             fn[R.s] = f.s;
