@@ -55,7 +55,11 @@ struct Prm {
     double dkf[PDAC_MAXP][PDAC_MAXP];
     // device metric, 1-based padded
     const double *dx, *dy, *dz, *indx, *indy, *indz, *r, *rb, *inr, *inrb;
-    const float *dxf, *dyf, *dzf, *indxf, *indyf, *indzf;  // FP32 copies (mixed precision), else null
+    // hx[m] = 1 / (dx[m] + dx[m+1]) over the padded range (hy, hz alike): the
+    // reciprocal face spacings of interp.f and flux_*.f, divided once on the host
+    // (an IEEE division, so the same bits as dividing in the kernel)
+    const double *hx, *hy, *hz;
+    const float *dxf, *dyf, *dzf, *indxf, *indyf, *indzf, *hxf, *hyf, *hzf;  // FP32 copies (mixed precision), else null
     int mixed;  // 1: the 3D flux passes compute in FP32 (PDAC_PREC_MIXED)
     const double *p_atm, *t_atm;
     const int *flag;
@@ -70,6 +74,9 @@ template <> struct Met<double> {
     static __device__ __forceinline__ const double *indx(const Prm &P) { return P.indx; }
     static __device__ __forceinline__ const double *indy(const Prm &P) { return P.indy; }
     static __device__ __forceinline__ const double *indz(const Prm &P) { return P.indz; }
+    static __device__ __forceinline__ const double *hx(const Prm &P) { return P.hx; }
+    static __device__ __forceinline__ const double *hy(const Prm &P) { return P.hy; }
+    static __device__ __forceinline__ const double *hz(const Prm &P) { return P.hz; }
 };
 template <> struct Met<float> {
     static __device__ __forceinline__ const float *dx(const Prm &P) { return P.dxf; }
@@ -78,6 +85,9 @@ template <> struct Met<float> {
     static __device__ __forceinline__ const float *indx(const Prm &P) { return P.indxf; }
     static __device__ __forceinline__ const float *indy(const Prm &P) { return P.indyf; }
     static __device__ __forceinline__ const float *indz(const Prm &P) { return P.indzf; }
+    static __device__ __forceinline__ const float *hx(const Prm &P) { return P.hxf; }
+    static __device__ __forceinline__ const float *hy(const Prm &P) { return P.hyf; }
+    static __device__ __forceinline__ const float *hz(const Prm &P) { return P.hzf; }
 };
 
 // Device pointers of every field (state, n-level, tilde, fluxes, solver).

@@ -437,13 +437,22 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
         for (int i = 1; i <= nx; ++i) inr[i] = 1.0 / r[i];
     }
     for (int k = 1; k <= nz; ++k) { patm[k] = cfg->p_atm[k - 1]; tatm[k] = cfg->t_atm[k - 1]; }
+    // reciprocal face spacings; the last entry pairs the padding with itself
+    auto recip = [](const std::vector<double> &d, bool on) {
+        std::vector<double> h(d.size(), 0.0);
+        if (on)
+            for (size_t m = 0; m < d.size(); ++m) h[m] = 1.0 / (d[m] + d[std::min(m + 1, d.size() - 1)]);
+        return h;
+    };
+    std::vector<double> hx = recip(dx, true), hy = recip(dy, ctx->d3), hz = recip(dz, true);
 
     CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     for (auto &e : ctx->ev) CK(cudaEventCreate(&e));
     for (auto &e : ctx->cev) CK(cudaEventCreate(&e));
     for (auto &e : ctx->user_ev) CK(cudaEventCreate(&e));
     for (auto &e : ctx->xev) CK(cudaEventCreate(&e));
-    std::vector<std::vector<double> *> mets = {&dx, &dy, &dz, &indx, &indy, &indz, &r, &rb, &inr, &inrb, &patm, &tatm};
+    std::vector<std::vector<double> *> mets = {&dx, &dy, &dz, &indx, &indy, &indz, &r, &rb, &inr, &inrb, &patm, &tatm,
+                                               &hx, &hy, &hz};
     size_t mtot = 0;
     for (auto *v : mets) mtot += v->size();
     CK(cudaMalloc(&ctx->metric, mtot * sizeof(double)));
@@ -456,20 +465,23 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     }
     P.dx = mp[0]; P.dy = mp[1]; P.dz = mp[2]; P.indx = mp[3]; P.indy = mp[4]; P.indz = mp[5];
     P.r = mp[6]; P.rb = mp[7]; P.inr = mp[8]; P.inrb = mp[9]; P.p_atm = mp[10]; P.t_atm = mp[11];
+    P.hx = mp[12]; P.hy = mp[13]; P.hz = mp[14];
     P.mixed = cfg->precision == PDAC_PREC_MIXED;
     if (P.mixed) {  // the metric of the FP32 flux passes: each FP64 value rounded to nearest
+        const int qs[9] = {0, 1, 2, 3, 4, 5, 12, 13, 14};
         size_t ftot = 0;
-        for (int q = 0; q < 6; ++q) ftot += mets[q]->size();
+        for (int q : qs) ftot += mets[q]->size();
         std::vector<float> hf;
         hf.reserve(ftot);
-        for (int q = 0; q < 6; ++q)
+        for (int q : qs)
             for (double v : *mets[q]) hf.push_back((float)v);
         CK(cudaMalloc(&ctx->metric_f, ftot * sizeof(float)));
         CK(cudaMemcpy(ctx->metric_f, hf.data(), ftot * sizeof(float), cudaMemcpyHostToDevice));
-        const float *fp[6];
+        const float *fp[9];
         size_t fo = 0;
-        for (int q = 0; q < 6; ++q) { fp[q] = ctx->metric_f + fo; fo += mets[q]->size(); }
+        for (int q = 0; q < 9; ++q) { fp[q] = ctx->metric_f + fo; fo += mets[qs[q]]->size(); }
         P.dxf = fp[0]; P.dyf = fp[1]; P.dzf = fp[2]; P.indxf = fp[3]; P.indyf = fp[4]; P.indzf = fp[5];
+        P.hxf = fp[6]; P.hyf = fp[7]; P.hzf = fp[8];
     }
     CK(cudaMalloc(&ctx->d_flag, n * sizeof(int)));
     CK(cudaMemcpy(ctx->d_flag, cfg->flag, n * sizeof(int), cudaMemcpyHostToDevice));

@@ -243,7 +243,7 @@ __global__ void k_fieldn2d(Prm P, Fld F) {
         int ijke = is_wallf(P.flag[R.e]) ? c : R.e;
         int ijkt = is_wallf(P.flag[R.t]) ? c : R.t;
         const double *dx = P.dx, *dz = P.dz;
-        double indxp = 1.0 / (dx[i] + dx[i + 1]), indzp = 1.0 / (dz[k] + dz[k + 1]);
+        double indxp = P.hx[i], indzp = P.hz[k];
         double rgp_e = (dx[i + 1] * F.rgp[c] + dx[i] * F.rgp[ijke]) * indxp;
         double rgp_t = (dz[k + 1] * F.rgp[c] + dz[k] * F.rgp[ijkt]) * indzp;
         F.rugn[c] = rgp_e * F.ug[c];
@@ -322,8 +322,8 @@ __device__ __forceinline__ void stress2d_cell(const Prm &P, const Raw2 &R, const
     const double *dx = P.dx, *dz = P.dz, *indx = P.indx, *indz = P.indz, *r = P.r, *rb = P.rb, *inr = P.inr, *inrb = P.inrb;
     const double cm = 2.0 / 3.0;
     int c = R.c;
-    double indxp = 1.0 / (dx[i] + dx[i + 1]), indxm = 1.0 / (dx[i] + dx[i - 1]);
-    double indzp = 1.0 / (dz[k] + dz[k + 1]), indzm = 1.0 / (dz[k] + dz[k - 1]);
+    double indxp = P.hx[i], indxm = P.hx[i - 1];
+    double indzp = P.hz[k], indzm = P.hz[k - 1];
     double divr = ((rb[i + 1] * u[R.e] - rb[i] * u[c]) * inr[i + 1] * indx[i + 1] + (w[R.e] - w[R.eb]) * indz[k]);
     double divc = ((rb[i] * u[c] - rb[i - 1] * u[R.w]) * inr[i] * indx[i] + (w[c] - w[R.b]) * indz[k]);
     double divt = ((rb[i] * u[R.t] - rb[i - 1] * u[R.wt]) * inr[i] * indx[i] + (w[R.t] - w[c]) * indz[k + 1]);
@@ -397,7 +397,7 @@ __global__ void k_tilde2d(Prm P, Fld F, double dt, const double *app0u, const do
     }
     double alpha = P.alpha, ag = P.alphagrav;
     double dxi = dx[i], dxip1 = dx[i + 1], dzk = dz[k], dzkp1 = dz[k + 1];
-    double indxp = 1.0 / (dx[i] + dx[i + 1]), indzp = 1.0 / (dz[k] + dz[k + 1]);
+    double indxp = P.hx[i], indzp = P.hz[k];
     double ugfx = F.ugfe[c] - F.ugfe[imjk], ugfz = F.ugft[c] - F.ugft[ijkm];
     double wgfx = F.wgfe[c] - F.wgfe[imjk], wgfz = F.wgft[c] - F.wgft[ijkm];
     double epn_e = 1.0, epn_t = 1.0;
@@ -558,8 +558,8 @@ __device__ __forceinline__ void betas_2d(const Prm &P, const Fld &F, const Raw2 
                                          double &cnv, double &abt) {
     const double *dx = P.dx, *dz = P.dz;
     int c = R.c;
-    double indxp = 1.0 / (dx[i] + dx[i + 1]), indxm = 1.0 / (dx[i] + dx[i - 1]);
-    double indzp = 1.0 / (dz[k] + dz[k + 1]), indzm = 1.0 / (dz[k] + dz[k - 1]);
+    double indxp = P.hx[i], indxm = P.hx[i - 1];
+    double indzp = P.hz[k], indzm = P.hz[k - 1];
     auto open = [](int f) { return f == BL_CELL || f == FLUID || f == DOME || f == IMMB || f == FREE_IO || f == ZERO_GRAD; };
     double iep_e = open(P.flag[R.e]) ? (dx[i + 1] * F.ep[c] + dx[i] * F.ep[M.e]) * indxp * indxp * 2.0 : 0.0;
     double iep_w = open(P.flag[R.w]) ? (dx[i - 1] * F.ep[c] + dx[i] * F.ep[M.w]) * indxm * indxm * 2.0 : 0.0;

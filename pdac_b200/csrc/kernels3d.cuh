@@ -200,7 +200,7 @@ __global__ void k_fieldn3d(Prm P, Fld F) {
         int ijkn = is_wallf(P.flag[R.n]) ? c : R.n;
         int ijkt = is_wallf(P.flag[R.t]) ? c : R.t;
         const double *dx = P.dx, *dy = P.dy, *dz = P.dz;
-        double indxp = 1.0 / (dx[i] + dx[i + 1]), indyp = 1.0 / (dy[j] + dy[j + 1]), indzp = 1.0 / (dz[k] + dz[k + 1]);
+        double indxp = P.hx[i], indyp = P.hy[j], indzp = P.hz[k];
         double rgp_e = (dx[i + 1] * F.rgp[c] + dx[i] * F.rgp[ijke]) * indxp;
         double rgp_n = (dy[j + 1] * F.rgp[c] + dy[j] * F.rgp[ijkn]) * indyp;
         double rgp_t = (dz[k + 1] * F.rgp[c] + dz[k] * F.rgp[ijkt]) * indzp;
@@ -310,7 +310,7 @@ __global__ void __launch_bounds__(128, PDAC_FLUX_MINB) k_visc3d(Prm P, Fld F) {
     size_t n = P.ncell;
     size_t off = (size_t)(ph > 0 ? ph - 1 : 0) * n;
     int ijke = M.e, ijkn = M.n, ijkt = M.t;
-    double indxp = 1.0 / (dx[i] + dx[i + 1]), indyp = 1.0 / (dy[j] + dy[j + 1]), indzp = 1.0 / (dz[k] + dz[k + 1]);
+    double indxp = P.hx[i], indyp = P.hy[j], indzp = P.hz[k];
     const double a_rep = -8.76, b_rep = -0.27;
     double vx = 0, vy = 0, vz = 0;
     if (ph == 0) {
@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(128, PDAC_FLUX_MINB) k_tilde3d(Prm P, Fld F, d
     int imjk = R.w, ijmk = R.s, ijkm = R.b, ijke = M.e, ijkn = M.n, ijkt = M.t;
     double alpha = P.alpha, ag = P.alphagrav;
     double dxi = dx[i], dxip1 = dx[i + 1], dyj = dy[j], dyjp1 = dy[j + 1], dzk = dz[k], dzkp1 = dz[k + 1];
-    double indxp = 1.0 / (dx[i] + dx[i + 1]), indyp = 1.0 / (dy[j] + dy[j + 1]), indzp = 1.0 / (dz[k] + dz[k + 1]);
+    double indxp = P.hx[i], indyp = P.hy[j], indzp = P.hz[k];
     double rr[MP][3];
     double kpgv[MP];
 #pragma unroll
@@ -550,9 +550,9 @@ __device__ __forceinline__ void betas_3d(const Prm &P, const Fld &F, const Raw3 
                                          double dt, double &cnv, double &abt) {
     const double *dx = P.dx, *dy = P.dy, *dz = P.dz;
     int c = R.c;
-    double indxp = 1.0 / (dx[i] + dx[i + 1]), indxm = 1.0 / (dx[i] + dx[i - 1]);
-    double indzp = 1.0 / (dz[k] + dz[k + 1]), indzm = 1.0 / (dz[k] + dz[k - 1]);
-    double indyp = 1.0 / (dy[j] + dy[j + 1]), indym = 1.0 / (dy[j] + dy[j - 1]);
+    double indxp = P.hx[i], indxm = P.hx[i - 1];
+    double indzp = P.hz[k], indzm = P.hz[k - 1];
+    double indyp = P.hy[j], indym = P.hy[j - 1];
     auto open = [](int f) { return f == BL_CELL || f == FLUID || f == DOME || f == IMMB || f == FREE_IO || f == ZERO_GRAD; };
     const int *fl = P.flag;
     double iep_e = open(fl[R.e]) ? (dx[i + 1] * F.ep[c] + dx[i] * F.ep[M.e]) * indxp * indxp * 2.0 : 0.0;

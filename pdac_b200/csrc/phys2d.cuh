@@ -124,8 +124,8 @@ __device__ __forceinline__ Real limiter(int t, Real erre, double beta_) {
 __device__ __forceinline__ void interp_x2(const Prm &P, const St &f, int i, St &s) {
     const double *dx = P.dx;
     int ip2 = min(P.nx, i + 2), ip3 = min(P.nx, i + 3);
-    double indxm = 1.0 / (dx[i] + dx[i - 1]), indxp = 1.0 / (dx[i] + dx[i + 1]);
-    double indxpp = 1.0 / (dx[i + 1] + dx[ip2]), indxppp = 1.0 / (dx[ip2] + dx[ip3]);
+    double indxm = P.hx[i - 1], indxp = P.hx[i];
+    double indxpp = P.hx[i + 1], indxppp = P.hx[ip2];
     s.c = (dx[i + 1] * f.c + dx[i] * f.e) * indxp;
     s.e = (dx[ip2] * f.e + dx[i + 1] * f.ee) * indxpp;
     s.t = (dx[i + 1] * f.t + dx[i] * f.et) * indxp;
@@ -137,8 +137,8 @@ __device__ __forceinline__ void interp_x2(const Prm &P, const St &f, int i, St &
 __device__ __forceinline__ void interp_z2(const Prm &P, const St &f, int k, St &s) {
     const double *dz = P.dz;
     int kp2 = min(P.nz, k + 2), kp3 = min(P.nz, k + 3);
-    double indzm = 1.0 / (dz[k] + dz[k - 1]), indzp = 1.0 / (dz[k] + dz[k + 1]);
-    double indzpp = 1.0 / (dz[k + 1] + dz[kp2]), indzppp = 1.0 / (dz[kp2] + dz[kp3]);
+    double indzm = P.hz[k - 1], indzp = P.hz[k];
+    double indzpp = P.hz[k + 1], indzppp = P.hz[kp2];
     s.c = (dz[k + 1] * f.c + dz[k] * f.t) * indzp;
     s.e = (dz[k + 1] * f.e + dz[k] * f.et) * indzp;
     s.t = (dz[kp2] * f.t + dz[k + 1] * f.tt) * indzpp;
@@ -153,7 +153,7 @@ __device__ __forceinline__ void interp_z2(const Prm &P, const St &f, int k, St &
 __device__ __forceinline__ void flu_2d(const Prm &P, double &fe, double &ft, double &fw, double &fb, bool dow, bool dob,
                                        const St &d, const St &u, const St &w, int i) {
     const double *dx = P.dx;
-    double indxp = 1.0 / (dx[i] + dx[i + 1]), cs;
+    double indxp = P.hx[i], cs;
     if (dow) {
         cs = 0.5 * (u.c + u.w);
         fw = 0.5 * (cs - fabs(cs)) * d.c * u.c * P.r[i] + 0.5 * (cs + fabs(cs)) * d.w * u.w * P.r[i];
@@ -172,8 +172,8 @@ __device__ __forceinline__ void muscl_flu_2d(const Prm &P, double &fe, double &f
                                              int i, int k, bool doe, bool dot) {
     const double *dx = P.dx, *dz = P.dz, *indx = P.indx;
     int ip2 = min(P.nx, i + 2), kp2 = min(P.nz, k + 2);
-    double indxp = 1.0 / (dx[i] + dx[i + 1]), indzm = 1.0 / (dz[k] + dz[k - 1]);
-    double indzp = 1.0 / (dz[k] + dz[k + 1]), indzpp = 1.0 / (dz[k + 1] + dz[kp2]);
+    double indxp = P.hx[i], indzm = P.hz[k - 1];
+    double indzp = P.hz[k], indzpp = P.hz[k + 1];
     double erre, incr = 0, cs, lim, upwnd, gradc;
     if (doe) {
         gradc = indx[i + 1] * (d.e * u.e - d.c * u.c);
@@ -202,7 +202,7 @@ __device__ __forceinline__ void muscl_flu_2d(const Prm &P, double &fe, double &f
 __device__ __forceinline__ void flw_2d(const Prm &P, double &fe, double &ft, double &fw, double &fb, bool dow, bool dob,
                                        const St &d, const St &u, const St &w, int i, int k) {
     const double *dz = P.dz;
-    double indzp = 1.0 / (dz[k] + dz[k + 1]), cs;
+    double indzp = P.hz[k], cs;
     if (dow) {
         cs = (u.wt * dz[k] + u.w * dz[k + 1]) * indzp;
         fw = 0.5 * d.w * w.w * (cs + fabs(cs)) * P.rb[i - 1] + 0.5 * d.c * w.c * (cs - fabs(cs)) * P.rb[i - 1];
@@ -221,8 +221,8 @@ __device__ __forceinline__ void muscl_flw_2d(const Prm &P, double &fe, double &f
                                              int i, int k, bool doe, bool dot) {
     const double *dx = P.dx, *dz = P.dz, *indz = P.indz;
     int ip2 = min(P.nx, i + 2), kp2 = min(P.nz, k + 2);
-    double indxm = 1.0 / (dx[i] + dx[i - 1]), indxp = 1.0 / (dx[i] + dx[i + 1]);
-    double indxpp = 1.0 / (dx[i + 1] + dx[ip2]), indzp = 1.0 / (dz[k] + dz[k + 1]);
+    double indxm = P.hx[i - 1], indxp = P.hx[i];
+    double indxpp = P.hx[i + 1], indzp = P.hz[k];
     double erre, incr = 0, cs, lim, upwnd, gradc;
     if (doe) {
         gradc = 2.0 * indxp * (d.e * w.e - d.c * w.c);
@@ -264,10 +264,10 @@ __device__ __forceinline__ void massflux_2d(const Prm &P, const St &d, double uw
     cs = wc; f.t = 0.5 * (cs - fabs(cs)) * d.t + 0.5 * (cs + fabs(cs)) * d.c;
     if (!muscl_on) return;
     int im2 = max(1, i - 2), ip2 = min(P.nx, i + 2), km2 = max(1, k - 2), kp2 = min(P.nz, k + 2);
-    double indxmm = 1.0 / (dx[i - 1] + dx[im2]), indxm = 1.0 / (dx[i] + dx[i - 1]);
-    double indxp = 1.0 / (dx[i] + dx[i + 1]), indxpp = 1.0 / (dx[i + 1] + dx[ip2]);
-    double indzmm = 1.0 / (dz[k - 1] + dz[km2]), indzm = 1.0 / (dz[k] + dz[k - 1]);
-    double indzp = 1.0 / (dz[k] + dz[k + 1]), indzpp = 1.0 / (dz[k + 1] + dz[kp2]);
+    double indxmm = P.hx[max(i - 2, 0)], indxm = P.hx[i - 1];
+    double indxp = P.hx[i], indxpp = P.hx[i + 1];
+    double indzmm = P.hz[max(k - 2, 0)], indzm = P.hz[k - 1];
+    double indzp = P.hz[k], indzpp = P.hz[k + 1];
     double gradc, gradw, grade, gradb, gradt, erre, incr = 0, lim, upwnd;
     // West
     gradc = 2.0 * indxm * (d.c - d.w);
@@ -323,8 +323,8 @@ __device__ __forceinline__ void muscl_fsc_2d(const Prm &P, double &fe, double &f
                                              double wc, int i, int k) {
     const double *dx = P.dx, *dz = P.dz;
     int ip2 = min(P.nx, i + 2), kp2 = min(P.nz, k + 2);
-    double indxm = 1.0 / (dx[i] + dx[i - 1]), indxp = 1.0 / (dx[i] + dx[i + 1]), indxpp = 1.0 / (dx[i + 1] + dx[ip2]);
-    double indzm = 1.0 / (dz[k] + dz[k - 1]), indzp = 1.0 / (dz[k] + dz[k + 1]), indzpp = 1.0 / (dz[k + 1] + dz[kp2]);
+    double indxm = P.hx[i - 1], indxp = P.hx[i], indxpp = P.hx[i + 1];
+    double indzm = P.hz[k - 1], indzp = P.hz[k], indzpp = P.hz[k + 1];
     double gradc = 2.0 * indxp * (d.e * f.e - d.c * f.c);
     double gradw = 2.0 * indxm * (d.c * f.c - d.w * f.w);
     double grade = 2.0 * indxpp * (d.ee * f.ee - d.e * f.e);
@@ -350,22 +350,22 @@ __device__ __forceinline__ void hotc_2d(const Prm &P, double &hfe, double &hft, 
                                         const St &ep, const St &tg, const St &ka, int i, int k) {
     const double *dx = P.dx, *dz = P.dz;
     if (dow) {
-        double indxm = 1.0 / (dx[i] + dx[i - 1]);
+        double indxm = P.hx[i - 1];
         double kmw = (dx[i - 1] * ka.c + dx[i] * ka.w) * indxm;
         double epmw = (dx[i - 1] * ep.c + dx[i] * ep.w) * indxm;
         hfw = kmw * epmw * (tg.c - tg.w) * indxm * 2.0 * P.rb[i - 1];
     }
     if (dob) {
-        double indzm = 1.0 / (dz[k] + dz[k - 1]);
+        double indzm = P.hz[k - 1];
         double kmb = (dz[k - 1] * ka.c + dz[k] * ka.b) * indzm;
         double epmb = (dz[k - 1] * ep.c + dz[k] * ep.b) * indzm;
         hfb = kmb * epmb * (tg.c - tg.b) * indzm * 2.0;
     }
-    double indxp = 1.0 / (dx[i] + dx[i + 1]);
+    double indxp = P.hx[i];
     double kme = (dx[i + 1] * ka.c + dx[i] * ka.e) * indxp;
     double epme = (dx[i + 1] * ep.c + dx[i] * ep.e) * indxp;
     hfe = kme * epme * (tg.e - tg.c) * indxp * 2.0 * P.rb[i];
-    double indzp = 1.0 / (dz[k] + dz[k + 1]);
+    double indzp = P.hz[k];
     double kmt = (dz[k + 1] * ka.c + dz[k] * ka.t) * indzp;
     double epmt = (dz[k + 1] * ep.c + dz[k] * ep.t) * indzp;
     hft = kmt * epmt * (tg.t - tg.c) * indzp * 2.0;

@@ -120,8 +120,8 @@ template <typename Real>
 __device__ __forceinline__ void interp_x3(const Prm &P, const S3T<Real> &f, int i, S3T<Real> &s) {
     const Real *dx = Met<Real>::dx(P);
     int ip2 = min(P.nx, i + 2), ip3 = min(P.nx, i + 3);
-    Real indxm = Real(1.0) / (dx[i] + dx[i - 1]), indxp = Real(1.0) / (dx[i] + dx[i + 1]);
-    Real indxpp = Real(1.0) / (dx[i + 1] + dx[ip2]), indxppp = Real(1.0) / (dx[ip2] + dx[ip3]);
+    Real indxm = Met<Real>::hx(P)[i - 1], indxp = Met<Real>::hx(P)[i];
+    Real indxpp = Met<Real>::hx(P)[i + 1], indxppp = Met<Real>::hx(P)[ip2];
     s.c = (dx[i + 1] * f.c + dx[i] * f.e) * indxp;
     s.e = (dx[ip2] * f.e + dx[i + 1] * f.ee) * indxpp;
     s.n = (dx[i + 1] * f.n + dx[i] * f.en) * indxp;
@@ -137,8 +137,8 @@ template <typename Real>
 __device__ __forceinline__ void interp_y3(const Prm &P, const S3T<Real> &f, int j, S3T<Real> &s) {
     const Real *dy = Met<Real>::dy(P);
     int jp2 = min(P.ny, j + 2), jp3 = min(P.ny, j + 3);
-    Real indym = Real(1.0) / (dy[j] + dy[j - 1]), indyp = Real(1.0) / (dy[j] + dy[j + 1]);
-    Real indypp = Real(1.0) / (dy[j + 1] + dy[jp2]), indyppp = Real(1.0) / (dy[jp2] + dy[jp3]);
+    Real indym = Met<Real>::hy(P)[j - 1], indyp = Met<Real>::hy(P)[j];
+    Real indypp = Met<Real>::hy(P)[j + 1], indyppp = Met<Real>::hy(P)[jp2];
     s.c = (dy[j + 1] * f.c + dy[j] * f.n) * indyp;
     s.e = (dy[j + 1] * f.e + dy[j] * f.en) * indyp;
     s.n = (dy[jp2] * f.n + dy[j + 1] * f.nn) * indypp;
@@ -154,8 +154,8 @@ template <typename Real>
 __device__ __forceinline__ void interp_z3(const Prm &P, const S3T<Real> &f, int k, S3T<Real> &s) {
     const Real *dz = Met<Real>::dz(P);
     int kp2 = min(P.nz, k + 2), kp3 = min(P.nz, k + 3);
-    Real indzm = Real(1.0) / (dz[k] + dz[k - 1]), indzp = Real(1.0) / (dz[k] + dz[k + 1]);
-    Real indzpp = Real(1.0) / (dz[k + 1] + dz[kp2]), indzppp = Real(1.0) / (dz[kp2] + dz[kp3]);
+    Real indzm = Met<Real>::hz(P)[k - 1], indzp = Met<Real>::hz(P)[k];
+    Real indzpp = Met<Real>::hz(P)[k + 1], indzppp = Met<Real>::hz(P)[kp2];
     s.c = (dz[k + 1] * f.c + dz[k] * f.t) * indzp;
     s.e = (dz[k + 1] * f.e + dz[k] * f.et) * indzp;
     s.n = (dz[k + 1] * f.n + dz[k] * f.nt) * indzp;
@@ -189,7 +189,7 @@ template <typename Real>
 __device__ __forceinline__ void flu_3d(const Prm &P, F6T<Real> &f, bool dw, bool ds, bool db, const S3T<Real> &d, const S3T<Real> &u,
                                        const S3T<Real> &v, const S3T<Real> &w, int i) {
     const Real *dx = Met<Real>::dx(P);
-    Real indxp = Real(1.0) / (dx[i] + dx[i + 1]), cs;
+    Real indxp = Met<Real>::hx(P)[i], cs;
     if (dw) { cs = Real(0.5) * (u.c + u.w); f.w = Real(0.5) * (cs - fabs(cs)) * d.c * u.c + Real(0.5) * (cs + fabs(cs)) * d.w * u.w; }
     if (ds) { cs = (dx[i + 1] * v.s + dx[i] * v.es) * indxp; f.s = Real(0.5) * (cs - fabs(cs)) * d.c * u.c + Real(0.5) * (cs + fabs(cs)) * d.s * u.s; }
     if (db) { cs = (dx[i + 1] * w.b + dx[i] * w.eb) * indxp; f.b = Real(0.5) * (cs - fabs(cs)) * d.c * u.c + Real(0.5) * (cs + fabs(cs)) * d.b * u.b; }
@@ -205,9 +205,9 @@ __device__ __forceinline__ void muscl_flu_3d(const Prm &P, F6T<Real> &f, const S
                                              int i, int j, int k) {
     const Real *dx = Met<Real>::dx(P), *dy = Met<Real>::dy(P), *dz = Met<Real>::dz(P), *indx = Met<Real>::indx(P);
     int ip2 = min(P.nx, i + 2), jp2 = min(P.ny, j + 2), kp2 = min(P.nz, k + 2);
-    Real indxp = Real(1.0) / (dx[i] + dx[i + 1]);
-    Real indym = Real(1.0) / (dy[j] + dy[j - 1]), indyp = Real(1.0) / (dy[j] + dy[j + 1]), indypp = Real(1.0) / (dy[j + 1] + dy[jp2]);
-    Real indzm = Real(1.0) / (dz[k] + dz[k - 1]), indzp = Real(1.0) / (dz[k] + dz[k + 1]), indzpp = Real(1.0) / (dz[k + 1] + dz[kp2]);
+    Real indxp = Met<Real>::hx(P)[i];
+    Real indym = Met<Real>::hy(P)[j - 1], indyp = Met<Real>::hy(P)[j], indypp = Met<Real>::hy(P)[j + 1];
+    Real indzm = Met<Real>::hz(P)[k - 1], indzp = Met<Real>::hz(P)[k], indzpp = Met<Real>::hz(P)[k + 1];
     Real gradw = indx[i] * (u.c * d.c - u.w * d.w);
     Real gradc = indx[i + 1] * (u.e * d.e - u.c * d.c);
     Real grade = indx[ip2] * (u.ee * d.ee - u.e * d.e);
@@ -225,7 +225,7 @@ template <typename Real>
 __device__ __forceinline__ void flv_3d(const Prm &P, F6T<Real> &f, bool dw, bool ds, bool db, const S3T<Real> &d, const S3T<Real> &u,
                                        const S3T<Real> &v, const S3T<Real> &w, int j) {
     const Real *dy = Met<Real>::dy(P);
-    Real indyp = Real(1.0) / (dy[j] + dy[j + 1]), cs;
+    Real indyp = Met<Real>::hy(P)[j], cs;
     if (dw) { cs = (u.wn * dy[j] + u.w * dy[j + 1]) * indyp; f.w = Real(0.5) * (cs - fabs(cs)) * d.c * v.c + Real(0.5) * (cs + fabs(cs)) * d.w * v.w; }
     if (ds) { cs = Real(0.5) * (v.c + v.s); f.s = Real(0.5) * (cs - fabs(cs)) * d.c * v.c + Real(0.5) * (cs + fabs(cs)) * d.s * v.s; }
     if (db) { cs = (w.nb * dy[j] + w.b * dy[j + 1]) * indyp; f.b = Real(0.5) * (cs - fabs(cs)) * d.c * v.c + Real(0.5) * (cs + fabs(cs)) * d.b * v.b; }
@@ -241,9 +241,9 @@ __device__ __forceinline__ void muscl_flv_3d(const Prm &P, F6T<Real> &f, const S
                                              int i, int j, int k) {
     const Real *dx = Met<Real>::dx(P), *dy = Met<Real>::dy(P), *dz = Met<Real>::dz(P), *indy = Met<Real>::indy(P);
     int ip2 = min(P.nx, i + 2), jp2 = min(P.ny, j + 2), kp2 = min(P.nz, k + 2);
-    Real indyp = Real(1.0) / (dy[j] + dy[j + 1]);
-    Real indxm = Real(1.0) / (dx[i] + dx[i - 1]), indxp = Real(1.0) / (dx[i] + dx[i + 1]), indxpp = Real(1.0) / (dx[i + 1] + dx[ip2]);
-    Real indzm = Real(1.0) / (dz[k] + dz[k - 1]), indzp = Real(1.0) / (dz[k] + dz[k + 1]), indzpp = Real(1.0) / (dz[k + 1] + dz[kp2]);
+    Real indyp = Met<Real>::hy(P)[j];
+    Real indxm = Met<Real>::hx(P)[i - 1], indxp = Met<Real>::hx(P)[i], indxpp = Met<Real>::hx(P)[i + 1];
+    Real indzm = Met<Real>::hz(P)[k - 1], indzp = Met<Real>::hz(P)[k], indzpp = Met<Real>::hz(P)[k + 1];
     Real gradw = Real(2.0) * indxm * (v.c * d.c - v.w * d.w);
     Real gradc = Real(2.0) * indxp * (v.e * d.e - v.c * d.c);
     Real grade = Real(2.0) * indxpp * (v.ee * d.ee - v.e * d.e);
@@ -261,7 +261,7 @@ template <typename Real>
 __device__ __forceinline__ void flw_3d(const Prm &P, F6T<Real> &f, bool dw, bool ds, bool db, const S3T<Real> &d, const S3T<Real> &u,
                                        const S3T<Real> &v, const S3T<Real> &w, int k) {
     const Real *dz = Met<Real>::dz(P);
-    Real indzp = Real(1.0) / (dz[k] + dz[k + 1]), cs;
+    Real indzp = Met<Real>::hz(P)[k], cs;
     if (dw) { cs = (dz[k + 1] * u.w + dz[k] * u.wt) * indzp; f.w = Real(0.5) * d.w * w.w * (cs + fabs(cs)) + Real(0.5) * d.c * w.c * (cs - fabs(cs)); }
     if (ds) { cs = (dz[k + 1] * v.s + dz[k] * v.st) * indzp; f.s = Real(0.5) * d.s * w.s * (cs + fabs(cs)) + Real(0.5) * d.c * w.c * (cs - fabs(cs)); }
     if (db) { cs = Real(0.5) * (w.b + w.c); f.b = Real(0.5) * d.b * w.b * (cs + fabs(cs)) + Real(0.5) * d.c * w.c * (cs - fabs(cs)); }
@@ -277,9 +277,9 @@ __device__ __forceinline__ void muscl_flw_3d(const Prm &P, F6T<Real> &f, const S
                                              int i, int j, int k) {
     const Real *dx = Met<Real>::dx(P), *dy = Met<Real>::dy(P), *dz = Met<Real>::dz(P), *indz = Met<Real>::indz(P);
     int ip2 = min(P.nx, i + 2), jp2 = min(P.ny, j + 2), kp2 = min(P.nz, k + 2);
-    Real indxm = Real(1.0) / (dx[i] + dx[i - 1]), indxp = Real(1.0) / (dx[i] + dx[i + 1]), indxpp = Real(1.0) / (dx[i + 1] + dx[ip2]);
-    Real indym = Real(1.0) / (dy[j] + dy[j - 1]), indyp = Real(1.0) / (dy[j] + dy[j + 1]), indypp = Real(1.0) / (dy[j + 1] + dy[jp2]);
-    Real indzp = Real(1.0) / (dz[k] + dz[k + 1]);
+    Real indxm = Met<Real>::hx(P)[i - 1], indxp = Met<Real>::hx(P)[i], indxpp = Met<Real>::hx(P)[i + 1];
+    Real indym = Met<Real>::hy(P)[j - 1], indyp = Met<Real>::hy(P)[j], indypp = Met<Real>::hy(P)[j + 1];
+    Real indzp = Met<Real>::hz(P)[k];
     Real gradw = Real(2.0) * indxm * (w.c * d.c - w.w * d.w);
     Real gradc = Real(2.0) * indxp * (w.e * d.e - w.c * d.c);
     Real grade = Real(2.0) * indxpp * (w.ee * d.ee - w.e * d.e);
@@ -310,9 +310,9 @@ __device__ __forceinline__ void massflux_3d(const Prm &P, const S3T<Real> &d, Re
     const Real *dx = Met<Real>::dx(P), *dy = Met<Real>::dy(P), *dz = Met<Real>::dz(P);
     int im2 = max(1, i - 2), ip2 = min(P.nx, i + 2), jm2 = max(1, j - 2), jp2 = min(P.ny, j + 2);
     int km2 = max(1, k - 2), kp2 = min(P.nz, k + 2);
-    Real indxmm = Real(1.0) / (dx[i - 1] + dx[im2]), indxm = Real(1.0) / (dx[i] + dx[i - 1]), indxp = Real(1.0) / (dx[i] + dx[i + 1]), indxpp = Real(1.0) / (dx[i + 1] + dx[ip2]);
-    Real indymm = Real(1.0) / (dy[j - 1] + dy[jm2]), indym = Real(1.0) / (dy[j] + dy[j - 1]), indyp = Real(1.0) / (dy[j] + dy[j + 1]), indypp = Real(1.0) / (dy[j + 1] + dy[jp2]);
-    Real indzmm = Real(1.0) / (dz[k - 1] + dz[km2]), indzm = Real(1.0) / (dz[k] + dz[k - 1]), indzp = Real(1.0) / (dz[k] + dz[k + 1]), indzpp = Real(1.0) / (dz[k + 1] + dz[kp2]);
+    Real indxmm = Met<Real>::hx(P)[max(i - 2, 0)], indxm = Met<Real>::hx(P)[i - 1], indxp = Met<Real>::hx(P)[i], indxpp = Met<Real>::hx(P)[i + 1];
+    Real indymm = Met<Real>::hy(P)[max(j - 2, 0)], indym = Met<Real>::hy(P)[j - 1], indyp = Met<Real>::hy(P)[j], indypp = Met<Real>::hy(P)[j + 1];
+    Real indzmm = Met<Real>::hz(P)[max(k - 2, 0)], indzm = Met<Real>::hz(P)[k - 1], indzp = Met<Real>::hz(P)[k], indzpp = Met<Real>::hz(P)[k + 1];
     Real gradc, gradw, grade, grads, gradn, gradb, gradt;
     gradc = Real(2.0) * indxm * (d.c - d.w); gradw = Real(2.0) * indxmm * (d.w - d.ww); grade = Real(2.0) * indxp * (d.e - d.c);
     muscl_face(P.lm, P.beta, f.w, uw, gradc, gradw, grade, Real(0.5) * dx[i - 1], -Real(0.5) * dx[i], i != 2 && flw == FLUID);
@@ -345,9 +345,9 @@ __device__ __forceinline__ void muscl_fsc_3d(const Prm &P, F6T<Real> &f, const S
                                              Real wc, int i, int j, int k) {
     const Real *dx = Met<Real>::dx(P), *dy = Met<Real>::dy(P), *dz = Met<Real>::dz(P);
     int ip2 = min(P.nx, i + 2), jp2 = min(P.ny, j + 2), kp2 = min(P.nz, k + 2);
-    Real indxm = Real(1.0) / (dx[i] + dx[i - 1]), indxp = Real(1.0) / (dx[i] + dx[i + 1]), indxpp = Real(1.0) / (dx[i + 1] + dx[ip2]);
-    Real indym = Real(1.0) / (dy[j] + dy[j - 1]), indyp = Real(1.0) / (dy[j] + dy[j + 1]), indypp = Real(1.0) / (dy[j + 1] + dy[jp2]);
-    Real indzm = Real(1.0) / (dz[k] + dz[k - 1]), indzp = Real(1.0) / (dz[k] + dz[k + 1]), indzpp = Real(1.0) / (dz[k + 1] + dz[kp2]);
+    Real indxm = Met<Real>::hx(P)[i - 1], indxp = Met<Real>::hx(P)[i], indxpp = Met<Real>::hx(P)[i + 1];
+    Real indym = Met<Real>::hy(P)[j - 1], indyp = Met<Real>::hy(P)[j], indypp = Met<Real>::hy(P)[j + 1];
+    Real indzm = Met<Real>::hz(P)[k - 1], indzp = Met<Real>::hz(P)[k], indzpp = Met<Real>::hz(P)[k + 1];
     Real gradc = Real(2.0) * indxp * (d.e * fl.e - d.c * fl.c);
     Real gradw = Real(2.0) * indxm * (d.c * fl.c - d.w * fl.w);
     Real grade = Real(2.0) * indxpp * (d.ee * fl.ee - d.e * fl.e);
@@ -368,27 +368,27 @@ __device__ __forceinline__ void hotc_3d(const Prm &P, F6T<Real> &h, bool hw, boo
                                         const S3T<Real> &ka, int i, int j, int k) {
     const Real *dx = Met<Real>::dx(P), *dy = Met<Real>::dy(P), *dz = Met<Real>::dz(P);
     if (hw) {
-        Real indxm = Real(1.0) / (dx[i] + dx[i - 1]);
+        Real indxm = Met<Real>::hx(P)[i - 1];
         Real km = (dx[i - 1] * ka.c + dx[i] * ka.w) * indxm, em = (dx[i - 1] * ep.c + dx[i] * ep.w) * indxm;
         h.w = km * em * (tg.c - tg.w) * indxm * Real(2.0);
     }
     if (hs) {
-        Real indym = Real(1.0) / (dy[j] + dy[j - 1]);
+        Real indym = Met<Real>::hy(P)[j - 1];
         Real km = (dy[j - 1] * ka.c + dy[j] * ka.s) * indym, em = (dy[j - 1] * ep.c + dy[j] * ep.s) * indym;
         h.s = km * em * (tg.c - tg.s) * indym * Real(2.0);
     }
     if (hb) {
-        Real indzm = Real(1.0) / (dz[k] + dz[k - 1]);
+        Real indzm = Met<Real>::hz(P)[k - 1];
         Real km = (dz[k - 1] * ka.c + dz[k] * ka.b) * indzm, em = (dz[k - 1] * ep.c + dz[k] * ep.b) * indzm;
         h.b = km * em * (tg.c - tg.b) * indzm * Real(2.0);
     }
-    Real indxp = Real(1.0) / (dx[i] + dx[i + 1]);
+    Real indxp = Met<Real>::hx(P)[i];
     Real kme = (dx[i + 1] * ka.c + dx[i] * ka.e) * indxp, epme = (dx[i + 1] * ep.c + dx[i] * ep.e) * indxp;
     h.e = kme * epme * (tg.e - tg.c) * indxp * Real(2.0);
-    Real indyp = Real(1.0) / (dy[j] + dy[j + 1]);
+    Real indyp = Met<Real>::hy(P)[j];
     Real kmn = (dy[j + 1] * ka.c + dy[j] * ka.n) * indyp, epmn = (dy[j + 1] * ep.c + dy[j] * ep.n) * indyp;
     h.n = kmn * epmn * (tg.n - tg.c) * indyp * Real(2.0);
-    Real indzp = Real(1.0) / (dz[k] + dz[k + 1]);
+    Real indzp = Met<Real>::hz(P)[k];
     Real kmt = (dz[k + 1] * ka.c + dz[k] * ka.t) * indzp, epmt = (dz[k + 1] * ep.c + dz[k] * ep.t) * indzp;
     h.t = kmt * epmt * (tg.t - tg.c) * indzp * Real(2.0);
 }
@@ -401,9 +401,9 @@ __device__ __forceinline__ void stress3d_cell(const Prm &P, const Raw3 &R, const
     const double *dx = P.dx, *dy = P.dy, *dz = P.dz, *indx = P.indx, *indy = P.indy, *indz = P.indz;
     const double cm = 2.0 / 3.0;
     int c = R.c;
-    double indxp = 1.0 / (dx[i] + dx[i + 1]), indxm = 1.0 / (dx[i] + dx[i - 1]);
-    double indyp = 1.0 / (dy[j] + dy[j + 1]), indym = 1.0 / (dy[j] + dy[j - 1]);
-    double indzp = 1.0 / (dz[k] + dz[k + 1]), indzm = 1.0 / (dz[k] + dz[k - 1]);
+    double indxp = P.hx[i], indxm = P.hx[i - 1];
+    double indyp = P.hy[j], indym = P.hy[j - 1];
+    double indzp = P.hz[k], indzm = P.hz[k - 1];
     double indxp2 = indxp * 2.0, indxm2 = indxm * 2.0, indyp2 = indyp * 2.0, indym2 = indym * 2.0;
     double indzp2 = indzp * 2.0, indzm2 = indzm * 2.0;
     double dum = u[c] - u[R.w], dup = u[R.e] - u[c], dvm = v[c] - v[R.s], dvp = v[R.n] - v[c];

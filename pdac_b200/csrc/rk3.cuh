@@ -383,7 +383,7 @@ __global__ void k_visc2d(Prm P, Fld F) {
                       vx, vz);
         if (P.repulsive_model == 1) {
             const double a_rep = -8.76, b_rep = -0.27;
-            double indxp = 1.0 / (dx[i] + dx[i + 1]), indzp = 1.0 / (dz[k] + dz[k + 1]);
+            double indxp = P.hx[i], indzp = P.hz[k];
             double rc = rl[c], re = rl[M.e], rt = rl[M.t];
             double epsx = (dx[i + 1] * rc + dx[i] * re) * indxp * ir;
             double gepx = pow(10.0, -a_rep * epsx + b_rep);
