@@ -64,19 +64,48 @@ __device__ __forceinline__ double face_mflux(const Prm &P, const FaceGeo &g, boo
 // Loop-invariant part of one face's phase system (matrix.f:38-328) for the
 // cell's inner loop: everything that does not depend on the cell's own p,
 // ep, rgp and rlk, evaluated once with the operations of face_system so that
-// the in-loop assembly (face_assemble) reproduces face_system bit for bit.
+// the in-loop assembly (face_assemble) reproduces face_system bit for bit:
+// A(ls) = alpha (d0 app(nb) + d1 app(c)) / (d0 + d1) by interphase index,
+// brow(l) the tilde momenta of the face (gas first), d0rn(l) = d0 x the
+// neighbour bulk densities (l = 0: d0 rgp(nb)), and six scalars.  Two
+// storage forms with one interface: SH = true keeps them in this lane's
+// column of a shared [N][KS] array (blocks of KS threads), which frees ~50
+// registers of the inner loop for a third resident block per SM; SH = false
+// (the generic phase count, whose array would not fit) keeps them in
+// registers.
+constexpr int KS = 128;  // threads per block of every kernel running the inner loop
+
+template <int NP, bool SH>
+struct FaceK;
+
 template <int NP>
-struct FaceK {
-    static constexpr int NA = Sys<NP>::M * (Sys<NP>::M - 1) / 2;
-    double A[NA];               // alpha (d0 app(nb) + d1 app(c)) / (d0 + d1), by interphase index
-    double brow[Sys<NP>::M - 1];  // tilde momenta of the face, gas first
-    double d0rn[Sys<NP>::M - 1];  // d0 x neighbour particle bulk densities (index 0 = gas: d0 rgp(nb))
-    double pnb, d0epnb, K1, K2, d1, inv;
+struct FaceK<NP, false> {
+    static constexpr int M = Sys<NP>::M, NA = M * (M - 1) / 2;
+    double A_[NA], brow_[M - 1], d0rn_[M - 1], sc_[6];
+    __device__ __forceinline__ explicit FaceK(double *) {}
+    __device__ __forceinline__ double &A(int i) { return A_[i]; }
+    __device__ __forceinline__ double &brow(int l) { return brow_[l]; }
+    __device__ __forceinline__ double &d0rn(int l) { return d0rn_[l]; }
+    __device__ __forceinline__ double &sc(int q) { return sc_[q]; }
 };
 
-template <int NP, bool RO>
+template <int NP>
+struct FaceK<NP, true> {
+    static constexpr int M = Sys<NP>::M, NA = M * (M - 1) / 2, N = NA + 2 * (M - 1) + 6;
+    double *s;  // this lane's column: element q at s[q * KS]
+    __device__ __forceinline__ explicit FaceK(double *col) : s(col) {}
+    __device__ __forceinline__ double &A(int i) { return s[i * KS]; }
+    __device__ __forceinline__ double &brow(int l) { return s[(NA + l) * KS]; }
+    __device__ __forceinline__ double &d0rn(int l) { return s[(NA + M - 1 + l) * KS]; }
+    __device__ __forceinline__ double &sc(int q) { return s[(NA + 2 * (M - 1) + q) * KS]; }
+};
+
+// the six scalars of FaceK
+enum { FK_PNB = 0, FK_D0EPNB, FK_K1, FK_K2, FK_D1, FK_INV };
+
+template <int NP, bool RO, class KT>
 __device__ __forceinline__ void face_prepare(const Prm &P, const Fld &F, int c, int nb, int raw, int ii, int dir,
-                                             int side, double dt, FaceK<NP> &K) {
+                                             int side, double dt, KT &K) {
     const int nph = nphases<NP>(P);
     const size_t n = P.ncell;
     const double *dd = dir == 0 ? P.dx : (dir == 1 ? P.dy : P.dz);
@@ -88,64 +117,67 @@ __device__ __forceinline__ void face_prepare(const Prm &P, const Fld &F, int c, 
     double d0 = dd[ii], d1 = side > 0 ? dd[ii + 1] : dd[ii - 1];
     double inv = 1.0 / (d0 + d1);
     int rowc = side > 0 ? c : raw;
-    K.d1 = d1;
-    K.inv = inv;
-    K.pnb = ldro<RO>(F.p + nb);
-    K.d0epnb = P.pmodel == 1 ? d0 * ldro<RO>(F.ep + nb) : 0.0;
-    K.K1 = alpha * dt * inv * 2.0;
-    K.K2 = dt * ag * inv * grav;
-    K.brow[0] = ldro<RO>(rg + rowc);
-    K.d0rn[0] = d0 * ldro<RO>(F.rgp + nb);
+    K.sc(FK_D1) = d1;
+    K.sc(FK_INV) = inv;
+    K.sc(FK_PNB) = ldro<RO>(F.p + nb);
+    K.sc(FK_D0EPNB) = P.pmodel == 1 ? d0 * ldro<RO>(F.ep + nb) : 0.0;
+    K.sc(FK_K1) = alpha * dt * inv * 2.0;
+    K.sc(FK_K2) = dt * ag * inv * grav;
+    K.brow(0) = ldro<RO>(rg + rowc);
+    K.d0rn(0) = d0 * ldro<RO>(F.rgp + nb);
 #pragma unroll
     for (int l = 2; l <= nph; ++l) {
-        K.brow[l - 1] = ldro<RO>(rs + (l - 2) * n + rowc);
-        K.d0rn[l - 1] = d0 * ldro<RO>(F.rlk + (l - 2) * n + nb);
+        K.brow(l - 1) = ldro<RO>(rs + (l - 2) * n + rowc);
+        K.d0rn(l - 1) = d0 * ldro<RO>(F.rlk + (l - 2) * n + nb);
     }
     const int nap = nph * (nph + 1) / 2;
 #pragma unroll
     for (int ls = 1; ls <= nap; ++ls)
-        K.A[ls - 1] = alpha * (d0 * ldro<RO>(app + (ls - 1) * n + nb) + d1 * ldro<RO>(app + (ls - 1) * n + c)) * inv;
+        K.A(ls - 1) = alpha * (d0 * ldro<RO>(app + (ls - 1) * n + nb) + d1 * ldro<RO>(app + (ls - 1) * n + c)) * inv;
 }
 
 // the in-loop assembly and solution; side as in face_system
-template <int NP>
-__device__ __forceinline__ void face_assemble(const Prm &P, const FaceK<NP> &K, int side, double pc, double epc,
+template <int NP, class KT>
+__device__ __forceinline__ void face_assemble(const Prm &P, KT &K, int side, double pc, double epc,
                                               double rgpc, const double *rlkc, double *v) {
     constexpr int M = Sys<NP>::M;
     const int nph = nphases<NP>(P);
     double a[M][M], b[M];
-    double d1 = K.d1, inv = K.inv;
-    double dp = side > 0 ? pc - K.pnb : K.pnb - pc;
+    double d1 = K.sc(FK_D1), inv = K.sc(FK_INV), pnb = K.sc(FK_PNB), K1 = K.sc(FK_K1), K2 = K.sc(FK_K2);
+    double dp = side > 0 ? pc - pnb : pnb - pc;
     double ep_f = 1.0;
-    if (P.pmodel == 1) ep_f = (K.d0epnb + d1 * epc) * inv;
-    b[1] = K.brow[0] + K.K1 * ep_f * dp;
-    b[1] = b[1] + K.K2 * (K.d0rn[0] + d1 * rgpc);
-    a[1][1] = K.A[0] + (K.d0rn[0] + d1 * rgpc) * inv;
+    if (P.pmodel == 1) ep_f = (K.sc(FK_D0EPNB) + d1 * epc) * inv;
+    b[1] = K.brow(0) + K1 * ep_f * dp;
+    b[1] = b[1] + K2 * (K.d0rn(0) + d1 * rgpc);
+    a[1][1] = K.A(0) + (K.d0rn(0) + d1 * rgpc) * inv;
 #pragma unroll
     for (int l = 2; l <= nph; ++l) {
         double rc = rlkc[l - 2];
         double eps_f = 0.0;
-        if (P.pmodel == 1) eps_f = (K.d0rn[l - 1] + d1 * rc) * inv * P.inrl[l - 1];
-        b[l] = K.brow[l - 1] + K.K1 * eps_f * dp;
-        b[l] = b[l] + K.K2 * (K.d0rn[l - 1] + d1 * rc);
+        if (P.pmodel == 1) eps_f = (K.d0rn(l - 1) + d1 * rc) * inv * P.inrl[l - 1];
+        b[l] = K.brow(l - 1) + K1 * eps_f * dp;
+        b[l] = b[l] + K2 * (K.d0rn(l - 1) + d1 * rc);
         int ls1 = l * (l - 1) / 2;
 #pragma unroll
         for (int ll = 1; ll <= l; ++ll) {
-            double val = K.A[ls1 + ll - 1];
+            double val = K.A(ls1 + ll - 1);
             a[l][ll] = val;
             a[ll][l] = val;
         }
-        a[l][l] = a[l][l] + (K.d0rn[l - 1] + d1 * rc) * inv;
+        a[l][l] = a[l][l] + (K.d0rn(l - 1) + d1 * rc) * inv;
     }
     gauss_jordan_t<NP>(P, a, b);
 #pragma unroll
     for (int l = 1; l <= nph; ++l) v[l - 1] = b[l];
 }
 
-// minimum resident blocks per SM the register allocation must allow
-#ifndef PDAC_INNER_MINB
-#define PDAC_INNER_MINB 2
+// minimum resident blocks per SM the register allocation must allow: with
+// the face terms in shared memory, up to four phases fit 168 registers and
+// three blocks per SM without spilling; more phases take two blocks
+#ifndef PDAC_INNER_MINB_SMALL
+#define PDAC_INNER_MINB_SMALL 3
 #endif
+#define PDAC_INNER_MINB(NP) ((NP) > 0 && (NP) <= 4 ? PDAC_INNER_MINB_SMALL : 2)
 
 // the inner loop of the worklist's nwork cells (outer sweep nit, 1-based)
 // by the warps warp, warp + nwarps, ... of the launch; RO as in ldro
@@ -161,6 +193,8 @@ __device__ __forceinline__ void inner_team_run(const Prm &P, const Fld &F, doubl
     if (tw >= TPW) return;  // idle lanes take no part in any team
     const int q = lane - tw * T, tb = tw * T;
     const unsigned tmask = ((1u << T) - 1u) << tb;
+    constexpr bool SH = NP > 0 && NP <= 6;  // FaceK in shared memory (40 KB per block at NP = 6)
+    __shared__ double kcols[SH ? FaceK<NP, true>::N : 1][SH ? KS : 1];
     for (int w = warp * TPW + tw; w < nwork; w += nwarps * TPW) {
         const int c = list[w];
         int i, j, k;
@@ -213,7 +247,7 @@ __device__ __forceinline__ void inner_team_run(const Prm &P, const Fld &F, doubl
         vel[0] = gvel[fcell];
 #pragma unroll
         for (int l = 2; l <= nph; ++l) vel[l - 1] = svel[(l - 2) * n + fcell];
-        FaceK<NP> K;
+        FaceK<NP, SH> K(&kcols[0][SH ? threadIdx.x : 0]);
         if (solved) face_prepare<NP, RO>(P, F, c, minus ? rm : rp, rawnb, ii, dir, minus ? -1 : +1, dt, K);
         // mass-flux stencil of this face by phase (gas first): neighbour
         // values, or the cell's own current value where the slot is the cell
@@ -350,7 +384,7 @@ __device__ __forceinline__ void inner_team_run(const Prm &P, const Fld &F, doubl
 }
 
 template <int NP, int D>
-__global__ void __launch_bounds__(128, PDAC_INNER_MINB) k_inner_team(Prm P, Fld F, double dt, const int *nitp, const int *list,
+__global__ void __launch_bounds__(128, PDAC_INNER_MINB(NP)) k_inner_team(Prm P, Fld F, double dt, const int *nitp, const int *list,
                                                                      const int *count, unsigned *dirty) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
     inner_team_run<NP, D, true>(P, F, dt, *nitp, list, *count, dirty, warp, nwarps);
@@ -448,7 +482,7 @@ struct SweepWork {
 };
 
 template <int NP, int D>
-__global__ void __launch_bounds__(128, PDAC_INNER_MINB) k_iter_coop(Prm P, Fld F, double dt, SweepWork W, int maxout) {
+__global__ void __launch_bounds__(128, PDAC_INNER_MINB(NP)) k_iter_coop(Prm P, Fld F, double dt, SweepWork W, int maxout) {
     namespace cg = cooperative_groups;
     cg::grid_group g = cg::this_grid();
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
