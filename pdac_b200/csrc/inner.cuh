@@ -295,9 +295,12 @@ __device__ __forceinline__ void inner_team_run(const Prm &P, const Fld &F, doubl
         double dgorig = dg;
         const double conv = F.conv[c];
         double d3 = dg, p3 = F.p[c], abeta = F.abeta[c];
-        double xg[PDAC_MAXG];
-        for (int ig = 0; ig < P.ng; ++ig) xg[ig] = GAS(F.xgc, c, ig);
+        // the mixture molecular weight of thermal_eosg (eosg.f:114-137), which
+        // does not change within the loop: summed once, in thermal_eosg's order
+        double mg = 0;
+        for (int ig = 0; ig < P.ng; ++ig) mg = mg + GAS(F.xgc, c, ig) * P.gmw[P.gas_type[ig]];
         const double tgc = F.tg[c];
+        const double rgas_tg = P.rgas * tgc;
         int kros = -1;
         PAdj s = {0, 0, 0, 0, 0, 0};
         double p = F.p[c], ep = F.ep[c], rog = F.rog[c], rgp = F.rgp[c];
@@ -316,7 +319,7 @@ __device__ __forceinline__ void inner_team_run(const Prm &P, const Fld &F, doubl
         const int lS = tb + 1, lN = tb + 4;
         for (int loop = 1; loop <= P.inmax; ++loop) {
             if (loop > 1 || nit > 1) padjust(s, p, kros, d3, p3, P.omega, abeta);
-            rog = thermal_eosg(P, tgc, p, xg);
+            rog = p / rgas_tg * mg;  // thermal_eosg
             rgp = ep * rog;
             // this lane's face system (matrix.f:351-630)
             if (solved) face_assemble<NP>(P, K, minus ? -1 : +1, p, ep, rgp, rlk, vel);
