@@ -61,6 +61,9 @@ struct Prm {
     const double *hx, *hy, *hz;
     const float *dxf, *dyf, *dzf, *indxf, *indyf, *indzf, *hxf, *hyf, *hzf;  // FP32 copies (mixed precision), else null
     int mixed;  // 1: the 3D flux passes compute in FP32 (PDAC_PREC_MIXED)
+    // c / nx and c / (nx ny) as a 64-bit multiply-high: mnx = ceil(2^64 / nx)
+    // (mny likewise for ny), exact for every c < 2^32; 0 = divide instead
+    unsigned long long mnx, mny;
     const double *p_atm, *t_atm;
     const int *flag;
 };

@@ -404,6 +404,18 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     P.part_viscosity = cfg->part_viscosity; P.repulsive_model = cfg->repulsive_model; P.inmax = cfg->inmax;
     P.iturb = cfg->iturb; P.iss = cfg->iss; P.modturbo = cfg->modturbo;
     P.opt = cfg->optimization >= 2 ? 2 : 1;  // 3 runs as 2 outside 3D with two classes (iter.f:160-161)
+    {  // the multipliers of ijk_of, checked on every cell index of this mesh
+        auto magic = [&](unsigned d) -> unsigned long long {
+            if (d < 2) return 0ull;
+            unsigned long long m = ~0ull / d + 1ull;
+            const unsigned nmax = (unsigned)n;
+            for (unsigned c = 0; c < nmax; ++c)
+                if ((unsigned)(((unsigned __int128)c * m) >> 64) != c / d) return 0ull;
+            return m;
+        };
+        P.mnx = ctx->d3 ? magic((unsigned)ctx->nx) : 0ull;
+        P.mny = ctx->d3 ? magic((unsigned)ctx->ny) : 0ull;
+    }
     for (int ig = 0; ig < ng; ++ig) P.gas_type[ig] = cfg->gas_type[ig];
     P.alpha = cfg->alpha; P.alphagrav = cfg->alphagrav; P.omega = cfg->omega; P.delg = cfg->delg;
     P.beta = cfg->beta; P.flim = cfg->flim; P.tref = cfg->tref;

@@ -15,9 +15,12 @@
 namespace pdac {
 
 __device__ __forceinline__ void ijk_of(const Prm &P, int c, int &i, int &j, int &k) {
-    i = c % P.nx + 1;
-    j = (c / P.nx) % P.ny + 1;
-    k = c / (P.nx * P.ny) + 1;
+    const unsigned long long u = (unsigned)c;
+    const unsigned q1 = P.mnx ? (unsigned)__umul64hi(u, P.mnx) : (unsigned)c / (unsigned)P.nx;  // c / nx
+    const unsigned q2 = P.mny ? (unsigned)__umul64hi(q1, P.mny) : q1 / (unsigned)P.ny;           // c / (nx ny)
+    i = (int)((unsigned)c - q1 * (unsigned)P.nx) + 1;
+    j = (int)(q1 - q2 * (unsigned)P.ny) + 1;
+    k = (int)q2 + 1;
 }
 #define MFX(ph, comp, face) (F.mf + ((size_t)((ph) * 3 + (comp)) * 3 + (face)) * P.ncell)
 
