@@ -1,5 +1,5 @@
-"""Whole runs on the GPU against the oracle, judged as the reference's runs
-are judged: phase-mass totals (the fluid-cell sums of residuals.f:14-130)
+"""Whole runs on the GPU against the oracle, checked the way the reference's runs
+are checked: phase-mass totals (the fluid-cell sums of residuals.f:14-130)
 to 1e-12 relative after every step, and for a run with the ground sink the
 deposited mass per class (the columns' massl, sink.f) to 1e-6 relative and
 the runout, the largest distance from the vent axis at which the particle

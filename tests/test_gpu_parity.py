@@ -6,7 +6,7 @@ against each field's scale):
   * explicit phases (boundary, fieldn, tilde, ygas, htilde, ftem): 1e-12;
     the only differences are last-ulp differences of pow/exp/sqrt between
     the CUDA and glibc math libraries;
-  * iter and whole steps: 1e-9, the north-star bound for FP64 fields.
+  * iter and whole steps: 1e-9, the per-step bound for FP64 fields.
 """
 import numpy as np
 import pytest
