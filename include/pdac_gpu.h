@@ -26,12 +26,15 @@ extern "C" {
 #define PDAC_OK                 0
 #define PDAC_ERR_CONFIG         1   /* unsupported or inconsistent cfg        */
 #define PDAC_ERR_CUDA           2   /* CUDA runtime error                     */
-#define PDAC_ERR_MAXOUT         3   /* iter.f:428-450: maxout sweeps reached  */
+#define PDAC_ERR_MAXOUT         3   /* iter.f:428-450: maxout sweeps reached
+                                       with cfg cstop set                    */
 #define PDAC_ERR_EOS            4   /* ftem.f:191-193: caloric EOS failures   */
-#define PDAC_ERR_NONFINITE      5   /* non-finite value detected              */
+#define PDAC_ERR_NONFINITE      5   /* NaN or Inf in an uploaded field or in
+                                       the state after a step                */
 #define PDAC_ERR_ARG            6   /* bad argument (NULL, size, name)        */
 #define PDAC_ERR_BOUNDARY       7   /* inoutflow.f:99,143: rls >= 1 on a BC   */
-#define PDAC_ERR_TIMEOUT        8   /* a bounded device wait gave up          */
+#define PDAC_ERR_TIMEOUT        8   /* reserved: no kernel of this build waits
+                                       on a flag, so none can time out       */
 
 /* ---- cell flags, grid.f:45-58 ----------------------------------------- */
 #define PDAC_FLUID        1
@@ -76,6 +79,14 @@ typedef struct pdac_cfg {
     double alpha, alphagrav;
     double omega, delg;
     int    inmax, maxout;
+    int    cstop;               /* &control cstop (input.f:239): 1 = a call of
+                                   iter that ends without convergence after
+                                   maxout sweeps returns PDAC_ERR_MAXOUT, as
+                                   the reference stops the run there
+                                   (iter.f:449); 0 (the default) = it returns
+                                   PDAC_OK with *nit = maxout + 1, and
+                                   pdac_gpu_unconverged_cells lists the cells
+                                   the reference reports (iter.f:428-447)    */
     int    muscl, lv, lm;       /* limiter types (limiters.f:14-56)          */
     double beta;                /* beta-limiter parameter                    */
     double flim;                /* invdm decoupling threshold (ftem.f:221)   */
@@ -180,18 +191,29 @@ int pdac_gpu_boundary(pdac_ctx *ctx, int sweep);
 int pdac_gpu_fieldn(pdac_ctx *ctx);
 /* tilde (tilde.f:276-848): fluxes, stresses, drag, interphase matrix      */
 int pdac_gpu_tilde(pdac_ctx *ctx, double dt);
-/* iter (iter.f:38-477); *nit receives the number of outer sweeps          */
+/* iter (iter.f:38-477); *nit receives the number of outer sweeps, which is
+ * maxout + 1 when the sweeps did not converge (the reference's DO-loop
+ * count); then the call returns PDAC_ERR_MAXOUT if cfg cstop is set, else
+ * PDAC_OK                                                                 */
 int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit);
+/* the cells of the last outer sweep of the last pdac_gpu_iter that were not
+ * converged (|dg| > conv at their residual test, so they ran the inner
+ * loop): the report the reference writes to pdac.tst when iter ends at
+ * maxout (iter.f:428-447).  Flat 0-based indices in increasing order;
+ * *n_inout holds the capacity of ijk on entry and the count on return
+ * (PDAC_ERR_ARG with the count when ijk is NULL or too small).  Empty after
+ * a converged iter, whose last sweep had no such cell.                    */
+int pdac_gpu_unconverged_cells(pdac_ctx *ctx, int *ijk, long *n_inout);
 /* Variant of pdac_gpu_iter with no counterpart in the reference: the same
  * computation and results, but the corrector's scratch (per-colour
  * counters, worklist, active-set flags) lives in one fixed static device
  * array of PDAC_ITER_STATIC_SCRATCH_BYTES instead of the context's buffers,
- * and the call allocates no memory of any kind.  It serves hosts that fix
+ * and the call makes no device allocation.  It serves hosts that fix
  * their device footprint themselves -- e.g. a driver that reserves all
  * device memory for its own pool at start-up and must not see later
  * allocations, or whose memory accounting admits only the buffers it
  * created.  Limits and rules:
- *  - the mesh must fit: 256 + 2 * (4 * ceil((nx + 2) / 3) * ny * nz rounded
+ *  - the mesh must fit: 256 + 2 * (4 * ceil(nx / 3) * ny * nz rounded
  *    up to 256) + 4 * ceil(nx * ny * nz / 32) bytes
  *    <= PDAC_ITER_STATIC_SCRATCH_BYTES, else the
  *    call returns PDAC_ERR_ARG with the sizes in pdac_gpu_last_error;
@@ -203,7 +225,14 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit);
  *    active-set bits before the first one;
  *  - one array per device is shared by every context on it, so calls that
  *    overlap in time on one device (other threads or streams) race and are
- *    not allowed.                                                          */
+ *    not allowed;
+ *  - the array is part of the library's device image: every device that
+ *    loads the library holds its 8 MiB until the process exits, whether or
+ *    not the entry point is called;
+ *  - it reports the same sweep count and status as pdac_gpu_iter (also
+ *    PDAC_ERR_MAXOUT under cfg cstop) and times itself for
+ *    pdac_gpu_phase_times, but it keeps no list for
+ *    pdac_gpu_unconverged_cells.                                           */
 #define PDAC_ITER_STATIC_SCRATCH_BYTES (8 * 1024 * 1024)
 int pdac_gpu_iter_static(pdac_ctx *ctx, double dt, int *nit);
 /* sub-grid turbulence model (cfg iturb = 1, iss = 1), called after fieldn

@@ -39,6 +39,62 @@
 
 #include "../include/pdac_gpu.h"
 
+// The 3D passes run their cell loops on several host threads: every such
+// loop writes each value from exactly one cell -- the cell that writes it
+// last in the reference's serial cell order -- and reads only values that no
+// iteration of the loop writes, so the results are the same bits on any
+// number of threads.  The corrector runs the cells of one colour in parallel
+// (they share no stencil); the lexicographic order stays serial.  Threads:
+// PDAC_ORACLE_THREADS, else every hardware thread; pdac_oracle_set_threads.
+#include <atomic>
+#include <thread>
+
+static int g_oracle_threads = 0;  // 0: not yet chosen
+
+static int oracle_threads() {
+    if (g_oracle_threads <= 0) {
+        const char *e = std::getenv("PDAC_ORACLE_THREADS");
+        int n = e ? std::atoi(e) : (int)std::thread::hardware_concurrency();
+        g_oracle_threads = n > 0 ? n : 1;
+    }
+    return g_oracle_threads;
+}
+
+// f(lo, hi) over [0, n) in one contiguous range per thread
+template <class Fn>
+static void par_range(int n, Fn f) {
+    const int T = oracle_threads();
+    if (T <= 1 || n < 4096) { f(0, n); return; }
+    const int chunk = (n + T - 1) / T;
+    std::vector<std::thread> th;
+    for (int t = 1; t < T; ++t) {
+        const int lo = t * chunk, hi = std::min(n, lo + chunk);
+        if (lo < hi) th.emplace_back(f, lo, hi);
+    }
+    f(0, std::min(n, chunk));
+    for (auto &x : th) x.join();
+}
+
+// f(lo, hi) over [lo0, hi0) in chunks of 256 taken from a shared counter
+// (for loops whose iterations differ in cost)
+template <class Fn>
+static void par_dynamic(int lo0, int hi0, Fn f) {
+    const int T = oracle_threads();
+    if (T <= 1 || hi0 - lo0 < 512) { f(lo0, hi0); return; }
+    std::atomic<int> next(lo0);
+    auto work = [&]() {
+        for (;;) {
+            const int lo = next.fetch_add(256);
+            if (lo >= hi0) return;
+            f(lo, std::min(hi0, lo + 256));
+        }
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < T; ++t) th.emplace_back(work);
+    work();
+    for (auto &x : th) x.join();
+}
+
 namespace {
 
 using std::vector;
@@ -127,9 +183,9 @@ struct Oracle {
     vector<double> smag, mugt, kapgt, must;  // sub-grid model (turbo.f:10-14)
     vector<double> scoeff;                   // dynamic coefficient cdyn of the last sgsg (modturbo = 2)
     vector<double> dgres;   // |dg|/conv at the last corrector visit (diagnostic)
+    vector<int> unconv;     // cells of the last outer sweep that ran the inner loop (iter.f:428-447)
+    vector<double> app0;    // 3D tilde on several threads: the interphase terms of the previous call
     vector<double> vent_fact, vent_fact0;
-    // padjust SAVE variables (iter.f:1005)
-    double pa_dp = 0, pa_d1 = 0, pa_d2 = 0, pa_p1 = 0, pa_p2 = 0, pa_d12 = 0;
     int last_nit = 0, eos_fail = 0, ierr = 0;
 
     // ---- indexing ------------------------------------------------------
@@ -1314,8 +1370,19 @@ void calc_eps_2d(Oracle &o, int c, double dt) {
     if (rls > 1.0) o.ierr++;
 }
 
-// iter.f:997-1072 (SAVE state kept in the oracle, as in the reference)
-void padjust(Oracle &o, double &p, int &kros, double d3, double &p3, double omega, double &abeta) {
+// padjust's SAVE variables (iter.f:1005).  The reference keeps one copy per
+// process; here each thread keeps its own, so that cells of one colour can
+// run on several threads.  The values a cell reads are always the ones that
+// cell wrote: kros starts at -1 in every cell, the secant (kros = 2) needs
+// both sides set in that cell, and newp (kros = 3) follows it.
+struct PadjustSave {
+    double pa_dp = 0, pa_d1 = 0, pa_d2 = 0, pa_p1 = 0, pa_p2 = 0, pa_d12 = 0;
+};
+thread_local PadjustSave g_padjust_save;
+
+// iter.f:997-1072
+void padjust(Oracle &, double &p, int &kros, double d3, double &p3, double omega, double &abeta) {
+    PadjustSave &o = g_padjust_save;
     if (kros != 3) {
         if (d3 > 0.0) {
             o.pa_d1 = d3; o.pa_p1 = p3;
@@ -1459,6 +1526,7 @@ int iter_2d(Oracle &o, double dt, int *nit_out) {
     int nit;
     for (nit = 1; nit <= o.cfg.maxout; ++nit) {
         o.ierr = 0;
+        o.unconv.clear();
         if (o.cfg.implicit_fluxes) tilde_2d(o, dt);  // iter.f:211-226
         bool all = true;
         for (int c : order) {
@@ -1471,6 +1539,7 @@ int iter_2d(Oracle &o, double dt, int *nit_out) {
                 o.rgp[c] = o.ep[c] * o.rog[c];
             } else {
                 all = false;
+                o.unconv.push_back(c);
                 double d3 = dg, p3 = o.p[c];
                 inner_loop_2d(o, c, nit, d3, p3, o.abeta[c], o.conv[c], dgorig, dt);
             }
@@ -1483,7 +1552,8 @@ int iter_2d(Oracle &o, double dt, int *nit_out) {
     }
     o.last_nit = nit;
     if (nit_out) *nit_out = nit;
-    return eos ? PDAC_ERR_EOS : PDAC_OK;
+    if (eos) return PDAC_ERR_EOS;
+    return nit > o.cfg.maxout && o.cfg.cstop ? PDAC_ERR_MAXOUT : PDAC_OK;  // iter.f:449
 }
 
 // ---------------------------------------------------------------------------
@@ -2252,6 +2322,7 @@ int pdac_oracle_step(void *h, int sweep, int *nit) {
             if (ien) pdac_oracle_htilde(h, dt);
         }
         int s1 = pdac_oracle_iter(h, dt, nit);
+        if (s1 == PDAC_ERR_MAXOUT) return s1;  // error() stops the run (iter.f:449)
         if (s1 != PDAC_OK) st = s1;
         pdac_oracle_ygas(h, dt);
         if (!ien) {
@@ -2333,6 +2404,22 @@ int pdac_oracle_mass_totals(void *h, double *out, int nout) {
 }
 
 int pdac_oracle_last_nit(void *h) { return ((Oracle *)h)->last_nit; }
+// threads of the 3D cell loops (n <= 0 keeps the current count); returns
+// the number in use afterwards
+int pdac_oracle_set_threads(int n) {
+    if (n > 0) g_oracle_threads = n;
+    return oracle_threads();
+}
+// the cells of the last outer sweep that ran the inner loop, increasing
+int pdac_oracle_unconverged_cells(void *h, int *ijk, long *n_inout) {
+    Oracle &o = *(Oracle *)h;
+    vector<int> v = o.unconv;
+    std::sort(v.begin(), v.end());
+    if (!ijk || *n_inout < (long)v.size()) { *n_inout = (long)v.size(); return v.empty() ? PDAC_OK : PDAC_ERR_ARG; }
+    std::copy(v.begin(), v.end(), ijk);
+    *n_inout = (long)v.size();
+    return PDAC_OK;
+}
 int pdac_oracle_eos_fail(void *h) { return ((Oracle *)h)->eos_fail; }
 
 // known-answer helpers (pure functions of the reference formulas)

@@ -137,11 +137,32 @@ class Oracle:
         self._chk(self.L.pdac_oracle_step(self.h, sweep, C.byref(nit)), "step")
         return nit.value
 
+    def unconverged_cells(self):
+        """Cells of the last iter's last sweep that ran the inner loop."""
+        L = self.L
+        L.pdac_oracle_unconverged_cells.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_long)]
+        L.pdac_oracle_unconverged_cells.restype = C.c_int
+        n = C.c_long(0)
+        L.pdac_oracle_unconverged_cells(self.h, None, C.byref(n))
+        buf = np.zeros(max(n.value, 1), dtype=np.int32)
+        self._chk(L.pdac_oracle_unconverged_cells(self.h, buf.ctypes.data_as(C.POINTER(C.c_int)), C.byref(n)),
+                  "unconverged_cells")
+        return buf[:n.value].copy()
+
     def mass_totals(self):
         n = 1 + self.case.nsolid + self.case.ngas
         out = np.zeros(n)
         self._chk(self.L.pdac_oracle_mass_totals(self.h, abi.dptr(out), n), "mass_totals")
         return out
+
+
+def set_threads(n):
+    """Threads of the oracle's 3D cell loops in this process; returns the
+    count in use (the results are the same bits on any count)."""
+    L = lib()
+    L.pdac_oracle_set_threads.argtypes = [C.c_int]
+    L.pdac_oracle_set_threads.restype = C.c_int
+    return L.pdac_oracle_set_threads(int(n))
 
 
 def limiter(lim_type, erre, beta=0.25):

@@ -43,7 +43,7 @@ class PdacCfg(C.Structure):
         ("dt", C.c_double), ("rungekut", C.c_int), ("time_integration", C.c_int),
         ("alpha", C.c_double), ("alphagrav", C.c_double),
         ("omega", C.c_double), ("delg", C.c_double),
-        ("inmax", C.c_int), ("maxout", C.c_int),
+        ("inmax", C.c_int), ("maxout", C.c_int), ("cstop", C.c_int),
         ("muscl", C.c_int), ("lv", C.c_int), ("lm", C.c_int),
         ("beta", C.c_double), ("flim", C.c_double), ("update_eosg", C.c_int),
         ("implicit_fluxes", C.c_int), ("implicit_enthalpy", C.c_int), ("optimization", C.c_int),

@@ -48,7 +48,13 @@ struct pdac_ctx {
     // statistics: kernel launches, corrector launch timing (when profiling)
     long long launches = 0, sweeps = 0, corr_launches = 0, work_cells = 0, tested_cells = 0;
     double corr_ms = 0.0, resid_ms = 0.0, inner_ms = 0.0;
-    int *d_work = nullptr, *d_wcount = nullptr;  // corrector worklist and its per-colour lengths
+    // corrector worklists, one per colour (colour col at d_work + col *
+    // work_stride, so the last sweep's lists remain for
+    // pdac_gpu_unconverged_cells), and their per-colour lengths
+    int *d_work = nullptr, *d_wcount = nullptr;
+    long work_stride = 0;
+    int last_nit = 0;                             // sweep count of the last pdac_gpu_iter
+    int *d_nonfinite = nullptr, *h_nonfinite = nullptr;  // non-finite flag of the state checks
     unsigned *d_dirty = nullptr;                 // corrector active set, one bit per cell
     int *d_cand = nullptr;                       // candidate cells of one colour phase
     int inner_grid = 0;
@@ -511,7 +517,12 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
         CK(cudaMemcpy(ctx->d_vfact, one.data(), cfg->nvent * sizeof(double), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(ctx->d_vfact0, zero.data(), cfg->nvent * sizeof(double), cudaMemcpyHostToDevice));
     }
-    CK(cudaMalloc(&ctx->d_work, (size_t)n * sizeof(int)));
+    // a colour phase holds at most ceil(nx / 3) * ny * nz cells: for fixed
+    // (j, k), (i + j + k) mod 3 takes one value on every third i
+    ctx->work_stride = ((long)((ctx->nx + 2) / 3) * ctx->ny * ctx->nz + 63) / 64 * 64;
+    CK(cudaMalloc(&ctx->d_work, (size_t)3 * ctx->work_stride * sizeof(int)));
+    CK(cudaMalloc(&ctx->d_nonfinite, sizeof(int)));
+    CK(cudaMallocHost(&ctx->h_nonfinite, sizeof(int)));
     CK(cudaMalloc(&ctx->d_wcount, 16 * sizeof(int)));
     CK(cudaMalloc(&ctx->d_dirty, ((size_t)n + 31) / 32 * sizeof(unsigned)));
     CK(cudaMalloc(&ctx->d_cand, (size_t)n * sizeof(int)));
@@ -685,6 +696,8 @@ int pdac_gpu_destroy(pdac_ctx *ctx) {
     cudaFree(ctx->d_vfact0);
     cudaFree(ctx->d_counters);
     cudaFree(ctx->d_work);
+    cudaFree(ctx->d_nonfinite);
+    cudaFreeHost(ctx->h_nonfinite);
     cudaFree(ctx->d_wcount);
     cudaFree(ctx->d_dirty);
     if (ctx->it_exec) cudaGraphExecDestroy(ctx->it_exec);
@@ -709,27 +722,112 @@ int pdac_gpu_destroy(pdac_ctx *ctx) {
     return PDAC_OK;
 }
 
+namespace pdac {
+// up to 24 device arrays of doubles to scan for NaN / Inf
+struct FinList {
+    const double *a[24];
+    long long n[24];
+    int m;
+};
+
+// sets *flag when any value of the listed arrays is not finite; 16-byte
+// loads over each array's even-length body (every arena slot starts on a
+// 256-byte boundary), one scalar load for an odd tail
+__global__ void __launch_bounds__(256) k_nonfinite(FinList L, int *flag) {
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nthr = (long long)gridDim.x * blockDim.x;
+    bool bad = false;
+    for (int q = 0; q < L.m; ++q) {
+        const double2 *v = reinterpret_cast<const double2 *>(L.a[q]);
+        const long long half = L.n[q] / 2;
+        for (long long t = tid; t < half; t += nthr) {
+            double2 x = __ldg(v + t);
+            bad |= !isfinite(x.x) || !isfinite(x.y);
+        }
+        if ((L.n[q] & 1) && tid == 0) bad |= !isfinite(__ldg(L.a[q] + L.n[q] - 1));
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+}  // namespace pdac
+
+// scan arrays on the context's stream; PDAC_ERR_NONFINITE names the first
+// listed array that holds a NaN or Inf
+static int check_finite(pdac_ctx *ctx, const std::vector<std::pair<const double *, size_t>> &arrs,
+                        const std::vector<std::string> &names, const char *where) {
+    cudaStream_t st = ctx->stream;
+    CK(cudaMemsetAsync(ctx->d_nonfinite, 0, sizeof(int), st));
+    int dev = 0, nsm = 148;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    for (size_t b = 0; b < arrs.size(); b += 24) {
+        pdac::FinList L{};
+        L.m = (int)std::min<size_t>(24, arrs.size() - b);
+        for (int q = 0; q < L.m; ++q) { L.a[q] = arrs[b + q].first; L.n[q] = (long long)arrs[b + q].second; }
+        pdac::k_nonfinite<<<nsm * 8, 256, 0, st>>>(L, ctx->d_nonfinite);
+        ctx->launches++;
+    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(ctx->h_nonfinite, ctx->d_nonfinite, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (!*ctx->h_nonfinite) return PDAC_OK;
+    // name the field: one array at a time (only on this error path)
+    std::string which = "?";
+    for (size_t q = 0; q < arrs.size(); ++q) {
+        pdac::FinList L{};
+        L.m = 1;
+        L.a[0] = arrs[q].first;
+        L.n[0] = (long long)arrs[q].second;
+        CK(cudaMemsetAsync(ctx->d_nonfinite, 0, sizeof(int), st));
+        pdac::k_nonfinite<<<nsm * 8, 256, 0, st>>>(L, ctx->d_nonfinite);
+        CK(cudaMemcpyAsync(ctx->h_nonfinite, ctx->d_nonfinite, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (*ctx->h_nonfinite) { which = names[q]; break; }
+    }
+    return fail(ctx, PDAC_ERR_NONFINITE, std::string(where) + ": non-finite value in " + which);
+}
+
 static int xfer_state(pdac_ctx *ctx, pdac_state_view *s, bool up) {
     if (!ctx || !s) return PDAC_ERR_ARG;
     size_t n = ctx->ncell, ns = ctx->ns, ng = ctx->ng;
     Fld &F = ctx->F;
-    struct X { double *h; double *d; size_t cnt; bool need; };
-    X xs[] = {{s->p, F.p, n, true}, {s->ep, F.ep, n, true}, {s->rog, F.rog, n, true}, {s->rgp, F.rgp, n, true},
-              {s->tg, F.tg, n, true}, {s->sieg, F.sieg, n, true}, {s->cg, F.cg, n, true},
-              {s->ug, F.ug, n, true}, {s->vg, F.vg, n, ctx->d3}, {s->wg, F.wg, n, true},
-              {s->rlk, F.rlk, n * ns, true}, {s->ts, F.ts, n * ns, true}, {s->sies, F.sies, n * ns, true},
-              {s->us, F.us, n * ns, true}, {s->vs, F.vs, n * ns, ctx->d3}, {s->ws, F.ws, n * ns, true},
-              {s->ygc, F.ygc, n * ng, true}, {s->xgc, F.xgc, n * ng, true}};
+    struct X { double *h; double *d; size_t cnt; bool need; const char *name; };
+    X xs[] = {{s->p, F.p, n, true, "p"}, {s->ep, F.ep, n, true, "ep"}, {s->rog, F.rog, n, true, "rog"},
+              {s->rgp, F.rgp, n, true, "rgp"}, {s->tg, F.tg, n, true, "tg"}, {s->sieg, F.sieg, n, true, "sieg"},
+              {s->cg, F.cg, n, true, "cg"}, {s->ug, F.ug, n, true, "ug"}, {s->vg, F.vg, n, ctx->d3, "vg"},
+              {s->wg, F.wg, n, true, "wg"}, {s->rlk, F.rlk, n * ns, true, "rlk"}, {s->ts, F.ts, n * ns, true, "ts"},
+              {s->sies, F.sies, n * ns, true, "sies"}, {s->us, F.us, n * ns, true, "us"},
+              {s->vs, F.vs, n * ns, ctx->d3, "vs"}, {s->ws, F.ws, n * ns, true, "ws"},
+              {s->ygc, F.ygc, n * ng, true, "ygc"}, {s->xgc, F.xgc, n * ng, true, "xgc"}};
+    std::vector<std::pair<const double *, size_t>> sent;
+    std::vector<std::string> names;
     for (auto &x : xs) {
         if (!x.h) {
             if (up && x.need) return fail(ctx, PDAC_ERR_ARG, "upload: a required state field is NULL");
             continue;
         }
-        if (up) CK(cudaMemcpyAsync(x.d, x.h, x.cnt * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-        else CK(cudaMemcpyAsync(x.h, x.d, x.cnt * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        if (up) {
+            CK(cudaMemcpyAsync(x.d, x.h, x.cnt * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+            if (x.cnt) { sent.push_back({x.d, x.cnt}); names.push_back(x.name); }
+        } else {
+            CK(cudaMemcpyAsync(x.h, x.d, x.cnt * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        }
     }
+    // an uploaded NaN or Inf would spread through the corrector's
+    // neighbourhoods within a sweep: refuse it at the boundary
+    if (up) return check_finite(ctx, sent, names, "upload");
     CK(cudaStreamSynchronize(ctx->stream));
     return PDAC_OK;
+}
+
+// the state after a step: pressure, void fraction, gas bulk density,
+// temperature, enthalpy and the particle bulk densities, through which every
+// cell's update passes (a non-finite value anywhere in the stencil of a
+// fluid cell reaches them within the step)
+static int check_step_state(pdac_ctx *ctx) {
+    const Fld &F = ctx->F;
+    const size_t n = ctx->ncell;
+    return check_finite(ctx, {{F.p, n}, {F.ep, n}, {F.rgp, n}, {F.tg, n}, {F.sieg, n}, {F.rlk, n * ctx->ns}},
+                        {"p", "ep", "rgp", "tg", "sieg", "rlk"}, "step");
 }
 
 int pdac_gpu_upload_state(pdac_ctx *ctx, const pdac_state_view *s) { return xfer_state(ctx, const_cast<pdac_state_view *>(s), true); }
@@ -880,11 +978,12 @@ static int enqueue_sweep(pdac_ctx *ctx, double dt, cudaStream_t st, bool prof) {
         int *cnt = ctx->d_wcount + col, *ncand = ctx->d_wcount + 6 + col;
         if (prof) CK(cudaEventRecord(ctx->cev[3 * col], st));
         pdac::k_resid_collect<<<blocks((long)nwords, TPB_RESID), TPB_RESID, 0, st>>>(ctx->P, col, dirty, ctx->d_cand, ncand);
-        if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_resid_test, 3, test_grid, TPB_RESID, st, ctx->P, F, dt, ctx->d_cand, ncand, ctx->d_work, cnt);
-        else PHASE_LAUNCH_D(nph, pdac::k_resid_test, 2, test_grid, TPB_RESID, st, ctx->P, F, dt, ctx->d_cand, ncand, ctx->d_work, cnt);
+        int *wl = ctx->d_work + col * ctx->work_stride;
+        if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_resid_test, 3, test_grid, TPB_RESID, st, ctx->P, F, dt, ctx->d_cand, ncand, wl, cnt);
+        else PHASE_LAUNCH_D(nph, pdac::k_resid_test, 2, test_grid, TPB_RESID, st, ctx->P, F, dt, ctx->d_cand, ncand, wl, cnt);
         if (prof) CK(cudaEventRecord(ctx->cev[3 * col + 1], st));
-        if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_inner_team, 3, g, TPB_TEAM, st, ctx->P, F, dt, ctx->d_nit, ctx->d_work, cnt, dirty);
-        else PHASE_LAUNCH_D(nph, pdac::k_inner_team, 2, g, TPB_TEAM, st, ctx->P, F, dt, ctx->d_nit, ctx->d_work, cnt, dirty);
+        if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_inner_team, 3, g, TPB_TEAM, st, ctx->P, F, dt, ctx->d_nit, wl, cnt, dirty);
+        else PHASE_LAUNCH_D(nph, pdac::k_inner_team, 2, g, TPB_TEAM, st, ctx->P, F, dt, ctx->d_nit, wl, cnt, dirty);
         if (prof) CK(cudaEventRecord(ctx->cev[3 * col + 2], st));
     }
     // implicit_enthalpy: the enthalpy fluxes (with implicit_fluxes) and the
@@ -956,6 +1055,8 @@ static int zero_tilde_terms(pdac_ctx *ctx, cudaStream_t st) {
     return PDAC_OK;
 }
 
+static int maxout_status(pdac_ctx *ctx, int nit);
+
 int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
     if (!ctx) return PDAC_ERR_ARG;
     cudaStream_t st = ctx->stream;
@@ -987,7 +1088,7 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
     const bool coop = ctx->coop_blocks > 0 && ctx->allow_coop && !ctx->cfg.implicit_fluxes && !ctx->cfg.implicit_enthalpy;
     if (!ctx->prof && coop) {
         // small domain: the sweep loop in one cooperative launch
-        pdac::SweepWork W{ctx->d_wcount, ctx->d_cand, ctx->d_work, ctx->d_dirty, ctx->d_nit};
+        pdac::SweepWork W{ctx->d_wcount, ctx->d_cand, ctx->d_work, ctx->d_dirty, ctx->d_nit, ctx->work_stride};
         CK(launch_iter_coop(ctx, dt, st, W));
         CK(cudaMemcpyAsync(ctx->h_nit, ctx->d_nit, sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
@@ -1043,6 +1144,7 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[7], st));
     if (nit_out) *nit_out = nit;
+    ctx->last_nit = nit;
     if (ctx->cfg.implicit_enthalpy) {
         if (ctx->prof) {
             CK(cudaMemcpyAsync(ctx->h_counters + 5, ctx->d_counters + 5, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1050,6 +1152,39 @@ int pdac_gpu_iter(pdac_ctx *ctx, double dt, int *nit_out) {
         }
         if (ctx->h_counters[5]) return fail(ctx, PDAC_ERR_EOS, "iter: caloric equation of state failed in a sweep's ftem");
     }
+    return maxout_status(ctx, nit);
+}
+
+// the end of iter without convergence (iter.f:428-450): the reference
+// reports the unconverged cells and stops the run only with cstop
+static int maxout_status(pdac_ctx *ctx, int nit) {
+    if (nit <= ctx->cfg.maxout || !ctx->cfg.cstop) return PDAC_OK;
+    return fail(ctx, PDAC_ERR_MAXOUT, "iter: max number of iters exceeded (" + std::to_string(ctx->cfg.maxout) +
+                                          " outer sweeps without convergence)");
+}
+
+int pdac_gpu_unconverged_cells(pdac_ctx *ctx, int *ijk, long *n_inout) {
+    if (!ctx || !n_inout) return PDAC_ERR_ARG;
+    cudaStream_t st = ctx->stream;
+    int cnt[3] = {0, 0, 0};
+    if (ctx->last_nit > 0) {
+        CK(cudaMemcpyAsync(ctx->h_counters, ctx->d_wcount, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (int c = 0; c < 3; ++c) cnt[c] = ctx->h_counters[c];
+    }
+    const long total = (long)cnt[0] + cnt[1] + cnt[2];
+    if (!ijk || *n_inout < total) {
+        *n_inout = total;
+        return total ? fail(ctx, PDAC_ERR_ARG, "unconverged_cells: the list holds " + std::to_string(total) + " cells")
+                     : PDAC_OK;
+    }
+    long at = 0;
+    for (int c = 0; c < 3; ++c) {
+        if (cnt[c]) CK(cudaMemcpy(ijk + at, ctx->d_work + c * ctx->work_stride, cnt[c] * sizeof(int), cudaMemcpyDeviceToHost));
+        at += cnt[c];
+    }
+    std::sort(ijk, ijk + total);
+    *n_inout = total;
     return PDAC_OK;
 }
 
@@ -1115,6 +1250,7 @@ int pdac_gpu_iter_static(pdac_ctx *ctx, double dt, int *nit_out) {
     unsigned *dirty = reinterpret_cast<unsigned *>(base + 256 + 2 * work_bytes);
     cudaStream_t st = ctx->stream;
     Fld &F = ctx->F;
+    CK(cudaEventRecord(ctx->ev[6], st));
     for (double *a : {F.rgfe, F.rgfn, F.rgft, F.conv, F.abeta})
         if (a) CK(cudaMemsetAsync(a, 0, n * sizeof(double), st));
     for (double *a : {F.rsfe, F.rsfn, F.rsft})
@@ -1130,6 +1266,8 @@ int pdac_gpu_iter_static(pdac_ctx *ctx, double dt, int *nit_out) {
     ctx->launches += 2;
     CK(cudaGetLastError());
     CK(cudaMemsetAsync(dirty, 0xff, nwords * sizeof(unsigned), st));
+    // the context's own worklist lengths describe an earlier pdac_gpu_iter
+    ctx->last_nit = 0;
     const int test_grid = std::max(1, ctx->inner_grid / 2);
     int nit;
     for (nit = 1; nit <= ctx->cfg.maxout; ++nit) {
@@ -1148,15 +1286,20 @@ int pdac_gpu_iter_static(pdac_ctx *ctx, double dt, int *nit_out) {
             else PHASE_LAUNCH_D(nph, pdac::k_inner_team, 2, g, TPB_TEAM, st, ctx->P, F, dt, dnit, work, cnt, dirty);
             ctx->launches += 2;
         }
-        CK(cudaMemcpyAsync(ctx->h_counters, wcount, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(ctx->h_counters, wcount, 6 * sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         ctx->sweeps++;
         long unconverged = (long)ctx->h_counters[0] + ctx->h_counters[1] + ctx->h_counters[2];
+        if (ctx->prof) {
+            ctx->work_cells += unconverged;
+            ctx->tested_cells += (long)ctx->h_counters[3] + ctx->h_counters[4] + ctx->h_counters[5];
+        }
         if (unconverged == 0) break;
     }
     CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev[7], st));
     if (nit_out) *nit_out = nit;
-    return PDAC_OK;
+    return maxout_status(ctx, nit);
 }
 
 int pdac_gpu_ygas(pdac_ctx *ctx, double dt) {
@@ -1494,6 +1637,7 @@ int pdac_gpu_step(pdac_ctx *ctx, int sweep, int *nit) {
             if ((s = pdac_gpu_ygas(ctx, dt))) return s;
         }
         if (ctx->cfg.compute_mixture && (s = pdac_gpu_compute_mixture_fields(ctx))) return s;  // prog.f:331
+        if ((s = check_step_state(ctx))) return s;
         return status;
     }
     if ((s = pdac_gpu_fieldn(ctx))) return s;
@@ -1510,7 +1654,7 @@ int pdac_gpu_step(pdac_ctx *ctx, int sweep, int *nit) {
         }
         s = pdac_gpu_iter(ctx, dt, nit);
         if (s == PDAC_ERR_EOS) status = s;
-        else if (s) return s;
+        else if (s) return s;  // PDAC_ERR_MAXOUT under cstop stops here, as error() does (iter.f:449)
         if ((s = pdac_gpu_ygas(ctx, dt))) return s;
         if (!ien) {
             if ((s = pdac_gpu_htilde(ctx, dt))) return s;
@@ -1520,6 +1664,7 @@ int pdac_gpu_step(pdac_ctx *ctx, int sweep, int *nit) {
         }
     }
     if (ctx->cfg.compute_mixture && (s = pdac_gpu_compute_mixture_fields(ctx))) return s;  // prog.f:331
+    if ((s = check_step_state(ctx))) return s;
     return status;
 }
 

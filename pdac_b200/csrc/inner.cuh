@@ -479,9 +479,10 @@ __global__ void __launch_bounds__(TPB_RESID) k_resid_test(Prm P, Fld F, double d
 // the loop ends on counters that all threads read after the same barrier.
 struct SweepWork {
     int *wcount;      // [col] worklist length, [3 + col] cells tested, [6 + col] candidates
-    int *cand, *work; // candidate list and worklist of one colour phase
+    int *cand, *work; // candidate list of one colour phase; worklists, colour col at work + col * wstride
     unsigned *dirty;  // active set, one bit per cell
     int *nit;         // the sweep count on return, as the graph's k_sweep_check leaves it
+    long wstride;     // ints per colour's worklist
 };
 
 template <int NP, int D>
@@ -496,9 +497,10 @@ __global__ void __launch_bounds__(128, PDAC_INNER_MINB(NP)) k_iter_coop(Prm P, F
         for (int col = 0; col < 3; ++col) {
             collect_phase<128>(P, col, W.dirty, W.cand, W.wcount + 6 + col);
             g.sync();
-            test_phase<128, NP, D>(P, F, dt, W.cand, __ldcg(W.wcount + 6 + col), W.work, W.wcount + col);
+            int *wl = W.work + col * W.wstride;
+            test_phase<128, NP, D>(P, F, dt, W.cand, __ldcg(W.wcount + 6 + col), wl, W.wcount + col);
             g.sync();
-            inner_team_run<NP, D, false>(P, F, dt, nit, W.work, __ldcg(W.wcount + col), W.dirty, warp, nwarps);
+            inner_team_run<NP, D, false>(P, F, dt, nit, wl, __ldcg(W.wcount + col), W.dirty, warp, nwarps);
             g.sync();
         }
         const long unconverged = (long)__ldcg(W.wcount) + __ldcg(W.wcount + 1) + __ldcg(W.wcount + 2);

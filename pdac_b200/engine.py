@@ -72,7 +72,7 @@ EXPORTED = (
     "pdac_gpu_write_restart", "pdac_gpu_read_restart", "pdac_gpu_write_output", "pdac_gpu_mass_residuals",
     "pdac_gpu_append_mass_check", "pdac_gpu_write_mass_loss", "pdac_gpu_read_mass_loss",
     "pdac_gpu_compute_mixture_fields", "pdac_gpu_batch_create", "pdac_gpu_batch_step", "pdac_gpu_batch_elapsed",
-    "pdac_gpu_batch_last_error", "pdac_gpu_batch_destroy",
+    "pdac_gpu_batch_last_error", "pdac_gpu_batch_destroy", "pdac_gpu_unconverged_cells",
 )
 
 
@@ -155,6 +155,19 @@ class Engine:
         nit = C.c_int(0)
         self._chk(self.L.pdac_gpu_iter(self.h, dt, C.byref(nit)), "iter")
         return nit.value
+
+    def unconverged_cells(self):
+        """Flat indices of the cells the last iter's last sweep did not
+        converge (the reference's report at maxout, iter.f:428-447)."""
+        L = self.L
+        L.pdac_gpu_unconverged_cells.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_long)]
+        L.pdac_gpu_unconverged_cells.restype = C.c_int
+        n = C.c_long(0)
+        L.pdac_gpu_unconverged_cells(self.h, None, C.byref(n))
+        buf = np.zeros(max(n.value, 1), dtype=np.int32)
+        self._chk(L.pdac_gpu_unconverged_cells(self.h, buf.ctypes.data_as(C.POINTER(C.c_int)), C.byref(n)),
+                  "unconverged_cells")
+        return buf[:n.value].copy()
 
     def ygas(self, dt):
         self._chk(self.L.pdac_gpu_ygas(self.h, dt), "ygas")

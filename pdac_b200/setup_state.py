@@ -534,6 +534,7 @@ class Case:
         c.alpha, c.alphagrav = d["alpha"], d["alphagrav"]
         c.omega, c.delg = d["omega"], d["delg"]
         c.inmax, c.maxout = d["inmax"], d["maxout"]
+        c.cstop = int(bool(d["cstop"]))
         c.muscl, c.lv, c.lm = d["muscl"], d["vel_limiter"], d["mass_limiter"]
         c.beta, c.flim = d["beta"], d["flim"]
         c.update_eosg = int(bool(d["update_eosg"]))

@@ -70,3 +70,17 @@ def test_mixed_precision_is_rejected_in_2d_without_touching_the_gpu():
     assert L.pdac_gpu_create(C.byref(cfg), C.byref(h)) == abi.PDAC_ERR_CONFIG
     cfg.precision = 7
     assert L.pdac_gpu_create(C.byref(cfg), C.byref(h)) == abi.PDAC_ERR_CONFIG
+
+
+@pytest.mark.parametrize("nx", [9, 10, 11])
+def test_colour_phase_fits_the_worklist_bound(nx):
+    """A colour phase of the corrector ((i + j + k) mod 3, 1-based) holds at
+    most ceil(nx / 3) * ny * nz cells: the per-colour worklists of
+    pdac_gpu_iter and the static scratch of pdac_gpu_iter_static are sized
+    by that bound."""
+    import numpy as np
+    ny, nz = 7, 8
+    i, j, k = np.meshgrid(np.arange(1, nx + 1), np.arange(1, ny + 1), np.arange(1, nz + 1), indexing="ij")
+    col = (i + j + k) % 3
+    most = max(int(np.count_nonzero(col == c)) for c in range(3))
+    assert most <= (nx + 2) // 3 * ny * nz
