@@ -18,6 +18,7 @@
 
 #include "../../include/pdac_gpu.h"
 #include "inner.cuh"
+#include "tiles3d.cuh"
 #include "rk3.cuh"
 #include "io.cuh"
 #include "les.cuh"
@@ -102,6 +103,9 @@ struct pdac_ctx {
     double *d_sinkbuf = nullptr;
     int *d_ring = nullptr;
     pdac::Wave W{};
+    // shared-memory tiled 3D stencil passes: tile shape (index into
+    // TILE_SHAPES) and planes per block of the march up k
+    int tile_shape = 0, tile_kchunk = 32;
     int *d_wave_idx = nullptr;    // order, src[3], start
     double *d_wave_rec = nullptr; // records and pnew
     int wave_grid_blocks = 0;
@@ -109,6 +113,44 @@ struct pdac_ctx {
 };
 
 namespace {
+
+// tile shapes (TX cells along i, TY along j) of the tiled 3D stencil passes
+struct TileShape { int tx, ty; };
+const TileShape TILE_SHAPES[] = {{32, 4}, {32, 8}, {16, 8}, {64, 2}};
+const int N_TILE_SHAPES = 4;
+
+// set_attr: raise the kernel's dynamic shared-memory limit (done once per
+// context at create, outside any stream capture); else launch it
+template <int TX, int TY, typename Real>
+cudaError_t launch_mom_tile_t(const pdac::Prm &P, const pdac::Fld &F, int nph, int kchunk, cudaStream_t st,
+                              bool set_attr) {
+    const int sm = pdac::tile_smem_bytes<TX, TY, Real>(4);
+    if (set_attr)
+        return cudaFuncSetAttribute(pdac::k_mom_flux3d_tile<TX, TY, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    dim3 grid((P.nx + TX - 1) / TX, (P.ny + TY - 1) / TY, nph * ((P.nz + kchunk - 1) / kchunk));
+    pdac::k_mom_flux3d_tile<TX, TY, Real><<<grid, TX * TY, sm, st>>>(P, F, kchunk);
+    return cudaGetLastError();
+}
+
+template <typename Real>
+cudaError_t launch_mom_tile(const pdac::Prm &P, const pdac::Fld &F, int nph, int shape, int kchunk, cudaStream_t st,
+                            bool set_attr = false) {
+    switch (shape) {
+        case 1: return launch_mom_tile_t<32, 8, Real>(P, F, nph, kchunk, st, set_attr);
+        case 2: return launch_mom_tile_t<16, 8, Real>(P, F, nph, kchunk, st, set_attr);
+        case 3: return launch_mom_tile_t<64, 2, Real>(P, F, nph, kchunk, st, set_attr);
+        default: return launch_mom_tile_t<32, 4, Real>(P, F, nph, kchunk, st, set_attr);
+    }
+}
+
+cudaError_t set_tile_attrs(const pdac::Prm &P, const pdac::Fld &F) {
+    for (int s = 0; s < N_TILE_SHAPES; ++s) {
+        cudaError_t e = launch_mom_tile<double>(P, F, 1, s, 1, nullptr, true);
+        if (e == cudaSuccess) e = launch_mom_tile<float>(P, F, 1, s, 1, nullptr, true);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
 
 const int TPB = 128;
 const int TPB_TEAM = 128;
@@ -639,6 +681,7 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     }
     int nq = 1 + ns + ng;
     CK(cudaMalloc(&ctx->d_partial, (size_t)nq * 1024 * sizeof(double)));
+    if (ctx->d3) CK(set_tile_attrs(ctx->P, ctx->F));
     if (t1) {
         int st = setup_wave(ctx, cfg->flag);
         if (st) return st;
@@ -912,16 +955,9 @@ static int enqueue_tilde(pdac_ctx *ctx, double dt, cudaStream_t st) {
         CK(cudaMemsetAsync(F.mf, 0, n * 9 * (ns + 1) * sizeof(double), st));
         pdac::k_visc3d<<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
         ctx->launches++;
-        if (ctx->P.mixed) {
-            pdac::k_tilde_flux3d<0, float><<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
-            pdac::k_tilde_flux3d<1, float><<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
-            pdac::k_tilde_flux3d<2, float><<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
-        } else {
-            pdac::k_tilde_flux3d<0><<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
-            pdac::k_tilde_flux3d<1><<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
-            pdac::k_tilde_flux3d<2><<<blocks((long)n * (ns + 1)), TPB, 0, st>>>(ctx->P, F);
-        }
-        ctx->launches += 3;
+        if (ctx->P.mixed) CK(launch_mom_tile<float>(ctx->P, F, ctx->nph, ctx->tile_shape, ctx->tile_kchunk, st));
+        else CK(launch_mom_tile<double>(ctx->P, F, ctx->nph, ctx->tile_shape, ctx->tile_kchunk, st));
+        ctx->launches += 1;
         PHASE_LAUNCH(ctx->nph, pdac::k_tilde3d, blocks(n), TPB, st, ctx->P, F, dt, ctx->d_app0u, ctx->d_app0v, ctx->d_app0w);
         ctx->launches++;
     } else {
@@ -1466,7 +1502,7 @@ static long long enqueue_explicit(pdac_ctx *ctx, double dt, cudaStream_t st, boo
     const Prm &P = ctx->P;
     const Fld &F = ctx->F;
     const RkF &K = ctx->K;
-    const long n = ctx->ncell, nphc = (long)n * (ctx->ns + 1);
+    const long n = ctx->ncell;
     const int nph = ctx->nph, nx = ctx->nx, ny = ctx->ny, nz = ctx->nz;
     long long L = 0;
     // compute_fluxes: mass, momentum and enthalpy face fluxes of the state
@@ -1478,18 +1514,14 @@ static long long enqueue_explicit(pdac_ctx *ctx, double dt, cudaStream_t st, boo
         if (ctx->d3) {
             if (P.mixed) {
                 pdac::k_rk3_mflux<3, float><<<blocks(n), TPB, 0, st>>>(P, F);
-                pdac::k_tilde_flux3d<0, float><<<blocks(nphc), TPB, 0, st>>>(P, F);
-                pdac::k_tilde_flux3d<1, float><<<blocks(nphc), TPB, 0, st>>>(P, F);
-                pdac::k_tilde_flux3d<2, float><<<blocks(nphc), TPB, 0, st>>>(P, F);
+                (void)launch_mom_tile<float>(P, F, nph, ctx->tile_shape, ctx->tile_kchunk, st);
                 pdac::k_htilde_flux3d<false, float><<<blocks(n), TPB, 0, st>>>(P, F);
             } else {
                 pdac::k_rk3_mflux<3><<<blocks(n), TPB, 0, st>>>(P, F);
-                pdac::k_tilde_flux3d<0><<<blocks(nphc), TPB, 0, st>>>(P, F);
-                pdac::k_tilde_flux3d<1><<<blocks(nphc), TPB, 0, st>>>(P, F);
-                pdac::k_tilde_flux3d<2><<<blocks(nphc), TPB, 0, st>>>(P, F);
+                (void)launch_mom_tile<double>(P, F, nph, ctx->tile_shape, ctx->tile_kchunk, st);
                 pdac::k_htilde_flux3d<false><<<blocks(n), TPB, 0, st>>>(P, F);
             }
-            L += 5;
+            L += 3;
         } else {
             pdac::k_rk3_mflux<2><<<blocks(n), TPB, 0, st>>>(P, F);
             pdac::k_tilde_flux2d<<<blocks(n), TPB, 0, st>>>(P, F);

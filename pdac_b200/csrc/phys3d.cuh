@@ -38,8 +38,11 @@ __device__ __forceinline__ void raw3(const Prm &P, int i, int j, int k, Raw3 &R)
     R.eee = f(3, 0, 0); R.nnn = f(0, 3, 0); R.ttt = f(0, 0, 3);
 }
 
-__device__ __forceinline__ void rem3(const Prm &P, int i, int j, int k, const Raw3 &R, Rem3 &M) {
-    const int *fl = P.flag;
+// the remapped neighbours (ghost.f:963-989 and the fall-backs of
+// ghost.f:1417-2476) from the flags fl at the raw indices R: global indices
+// with the flag array, or the indices of a shared-memory tile with the
+// tile's copy of the flags
+__device__ __forceinline__ void rem3_fl(const Prm &P, const int *fl, int i, int j, int k, const Raw3 &R, Rem3 &M) {
     int c = R.c;
     M.e = is_wallf(fl[R.e]) ? c : R.e;
     M.w = is_wallf(fl[R.w]) ? c : R.w;
@@ -78,6 +81,10 @@ __device__ __forceinline__ void rem3(const Prm &P, int i, int j, int k, const Ra
     M.nnn = is_wallf(fl[R.nnn]) ? R.nn : R.nnn;
     if (j == P.ny - 1) M.nnn = M.n;
     if (j == P.ny - 2) M.nnn = M.nn;
+}
+
+__device__ __forceinline__ void rem3(const Prm &P, int i, int j, int k, const Raw3 &R, Rem3 &M) {
+    rem3_fl(P, P.flag, i, j, k, R, M);
 }
 
 template <typename Real>
