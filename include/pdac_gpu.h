@@ -342,6 +342,33 @@ int pdac_gpu_sweep_log(pdac_ctx *ctx, double *out, long *n_inout);
 int pdac_gpu_mark(pdac_ctx *ctx, int slot);
 int pdac_gpu_elapsed(pdac_ctx *ctx, int a, int b, double *ms);
 
+/* ---- launch-shape autotuner (no counterpart in the reference) ---------- */
+/* The launch shapes of the engine's tunable kernels, as five ints:
+ *   [0] form of the 3D momentum-flux pass: 0 = one thread per (cell,
+ *       phase) and component (three launches), 1..4 = the shared-memory
+ *       tiled pass with 32 x 4, 32 x 8, 16 x 8 or 64 x 2 cells (i x j) per
+ *       block;
+ *   [1] planes of a tiled block's march up k;
+ *   [2] blocks of the corrector's inner-loop kernel;
+ *   [3] blocks of its residual-test kernel;
+ *   [4] cells per block of the one-launch sweep loop of small domains.
+ * None of them changes a result: only the speed.
+ * pdac_gpu_autotune times candidates on the context's current state and
+ * installs the fastest: the momentum-flux pass directly (it rewrites the
+ * same face fluxes), the corrector's shapes as whole time steps on a device
+ * copy of the state that is restored afterwards (skipped if the copy does
+ * not fit in device memory; contexts with time_integration = 1 tune the
+ * flux pass only).  The state, statistics and sweep count the caller sees
+ * are unchanged.  Call it after a step or two, when the state is typical of
+ * the run.  With cache_path (may be NULL) the result is looked up first and
+ * appended after tuning, one text line per key (device name, grid, nsolid,
+ * ngas, precision, time integration, implicit modes); a cached entry is
+ * installed without timing.  out (may be NULL) receives the five values.
+ * pdac_gpu_set_tuning installs five given values (PDAC_ERR_ARG if out of
+ * range).                                                                  */
+int pdac_gpu_autotune(pdac_ctx *ctx, const char *cache_path, int *out, int nout);
+int pdac_gpu_set_tuning(pdac_ctx *ctx, const int *in, int nin);
+
 /* ---- ensembles of independent runs ------------------------------------ */
 /* No counterpart in the reference, which runs one domain per job (an
  * ensemble there is many jobs).  A batch advances many contexts (members:

@@ -67,8 +67,11 @@ struct pdac_ctx {
     double it_dt = 0.0;
     long long it_per_sweep = 10;  // kernels of one sweep of that graph
     // small domains: the whole sweep loop as one cooperative launch of
-    // coop_blocks blocks (0: the graph)
-    int coop_blocks = 0;
+    // coop_blocks blocks (0: the graph), coop_cpb cells per block, at most
+    // coop_max_blocks blocks resident at once
+    int coop_blocks = 0, coop_cpb = 1024, coop_max_blocks = 0;
+    // grid of the residual-test kernels (0: half the inner-loop grid)
+    int test_grid = 0;
     // cooperative launches (the small-domain sweep loop, the explicit
     // solver's wavefront) only when the context is not stepped alongside
     // others: a batch turns them off in its members, so that no two
@@ -114,10 +117,14 @@ struct pdac_ctx {
 
 namespace {
 
-// tile shapes (TX cells along i, TY along j) of the tiled 3D stencil passes
-struct TileShape { int tx, ty; };
-const TileShape TILE_SHAPES[] = {{32, 4}, {32, 8}, {16, 8}, {64, 2}};
-const int N_TILE_SHAPES = 4;
+// forms of the 3D momentum-flux pass (launch_mom_tile): 0 = one thread per
+// (cell, phase) and component, three launches (k_tilde_flux3d<0|1|2>, the
+// stencils gathered through L1); 1..4 = the shared-memory tiled pass
+// k_mom_flux3d_tile with 32 x 4, 32 x 8, 16 x 8 or 64 x 2 cells (i x j) per
+// block.  Measured on the 256 x 256 x 192 plume (the autotuner picks per
+// run): form 0 took 8.2 ms per tilde, the 32 x 4 tile ~9 ms -- its threads
+// run all three components between two barriers at 12 warps per SM
+const int N_TILE_SHAPES = 5;
 
 // set_attr: raise the kernel's dynamic shared-memory limit (done once per
 // context at create, outside any stream capture); else launch it
@@ -136,12 +143,24 @@ template <typename Real>
 cudaError_t launch_mom_tile(const pdac::Prm &P, const pdac::Fld &F, int nph, int shape, int kchunk, cudaStream_t st,
                             bool set_attr = false) {
     switch (shape) {
-        case 1: return launch_mom_tile_t<32, 8, Real>(P, F, nph, kchunk, st, set_attr);
-        case 2: return launch_mom_tile_t<16, 8, Real>(P, F, nph, kchunk, st, set_attr);
-        case 3: return launch_mom_tile_t<64, 2, Real>(P, F, nph, kchunk, st, set_attr);
-        default: return launch_mom_tile_t<32, 4, Real>(P, F, nph, kchunk, st, set_attr);
+        case 1: return launch_mom_tile_t<32, 4, Real>(P, F, nph, kchunk, st, set_attr);
+        case 2: return launch_mom_tile_t<32, 8, Real>(P, F, nph, kchunk, st, set_attr);
+        case 3: return launch_mom_tile_t<16, 8, Real>(P, F, nph, kchunk, st, set_attr);
+        case 4: return launch_mom_tile_t<64, 2, Real>(P, F, nph, kchunk, st, set_attr);
+        default: {
+            if (set_attr) return cudaSuccess;
+            const long nt = (long)P.ncell * nph;
+            const int g = (int)((nt + 127) / 128);
+            pdac::k_tilde_flux3d<0, Real><<<g, 128, 0, st>>>(P, F);
+            pdac::k_tilde_flux3d<1, Real><<<g, 128, 0, st>>>(P, F);
+            pdac::k_tilde_flux3d<2, Real><<<g, 128, 0, st>>>(P, F);
+            return cudaGetLastError();
+        }
     }
 }
+
+// kernel launches of one momentum-flux pass of form shape
+inline int mom_launches(int shape) { return shape == 0 ? 3 : 1; }
 
 cudaError_t set_tile_attrs(const pdac::Prm &P, const pdac::Fld &F) {
     for (int s = 0; s < N_TILE_SHAPES; ++s) {
@@ -420,8 +439,10 @@ static int setup_iter_coop(pdac_ctx *ctx) {
         default: e = ctx->d3 ? occ_of(pdac::k_iter_coop<0, 3>) : occ_of(pdac::k_iter_coop<0, 2>); break;
     }
     CK(e);
-    const int want = std::max(1, (int)((ctx->ncell + PDAC_COOP_CELLS_PER_BLOCK - 1) / PDAC_COOP_CELLS_PER_BLOCK));
-    ctx->coop_blocks = std::min(want, occ * nsm);
+    ctx->coop_cpb = PDAC_COOP_CELLS_PER_BLOCK;
+    ctx->coop_max_blocks = occ * nsm;
+    const int want = std::max(1, (int)((ctx->ncell + ctx->coop_cpb - 1) / ctx->coop_cpb));
+    ctx->coop_blocks = std::min(want, ctx->coop_max_blocks);
     return PDAC_OK;
 }
 
@@ -957,7 +978,7 @@ static int enqueue_tilde(pdac_ctx *ctx, double dt, cudaStream_t st) {
         ctx->launches++;
         if (ctx->P.mixed) CK(launch_mom_tile<float>(ctx->P, F, ctx->nph, ctx->tile_shape, ctx->tile_kchunk, st));
         else CK(launch_mom_tile<double>(ctx->P, F, ctx->nph, ctx->tile_shape, ctx->tile_kchunk, st));
-        ctx->launches += 1;
+        ctx->launches += mom_launches(ctx->tile_shape);
         PHASE_LAUNCH(ctx->nph, pdac::k_tilde3d, blocks(n), TPB, st, ctx->P, F, dt, ctx->d_app0u, ctx->d_app0v, ctx->d_app0w);
         ctx->launches++;
     } else {
@@ -1002,7 +1023,7 @@ static int enqueue_sweep(pdac_ctx *ctx, double dt, cudaStream_t st, bool prof) {
     const int nph = ctx->nph;
     const size_t n = ctx->ncell, nwords = (n + 31) / 32;
     const long nthr = (long)((ctx->nx + 2) / 3) * ctx->ny * ctx->nz;
-    const int test_grid = std::max(1, ctx->inner_grid / 2);
+    const int test_grid = ctx->test_grid > 0 ? ctx->test_grid : std::max(1, ctx->inner_grid / 2);
     // one team of lanes per worklist cell (5 teams of 6 lanes per warp in
     // 3D, 8 of 4 in 2D)
     const long team_threads = (nthr + (ctx->d3 ? 4 : 7)) / (ctx->d3 ? 5 : 8) * 32;
@@ -1521,7 +1542,7 @@ static long long enqueue_explicit(pdac_ctx *ctx, double dt, cudaStream_t st, boo
                 (void)launch_mom_tile<double>(P, F, nph, ctx->tile_shape, ctx->tile_kchunk, st);
                 pdac::k_htilde_flux3d<false><<<blocks(n), TPB, 0, st>>>(P, F);
             }
-            L += 3;
+            L += 2 + mom_launches(ctx->tile_shape);
         } else {
             pdac::k_rk3_mflux<2><<<blocks(n), TPB, 0, st>>>(P, F);
             pdac::k_tilde_flux2d<<<blocks(n), TPB, 0, st>>>(P, F);
@@ -1743,6 +1764,245 @@ int pdac_gpu_phase_times(pdac_ctx *ctx, double *ms7) {
         ms7[q] = t;
     }
     cudaGetLastError();
+    return PDAC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// autotuner of the launch shapes (no counterpart in the reference)
+// ---------------------------------------------------------------------------
+namespace {
+struct Tuning {
+    int tile_shape, tile_kchunk, inner_grid, test_grid, coop_cpb;
+};
+constexpr int N_TUNE = 5;
+
+Tuning get_tuning(const pdac_ctx *ctx) {
+    return {ctx->tile_shape, ctx->tile_kchunk, ctx->inner_grid,
+            ctx->test_grid > 0 ? ctx->test_grid : std::max(1, ctx->inner_grid / 2), ctx->coop_cpb};
+}
+
+// install t; the captured graphs hold the old launch shapes, so they are
+// rebuilt at their next use
+void put_tuning(pdac_ctx *ctx, const Tuning &t) {
+    ctx->tile_shape = t.tile_shape;
+    ctx->tile_kchunk = t.tile_kchunk;
+    ctx->inner_grid = t.inner_grid;
+    ctx->test_grid = t.test_grid;
+    ctx->coop_cpb = t.coop_cpb;
+    if (ctx->coop_max_blocks > 0)
+        ctx->coop_blocks = std::min(std::max(1, (int)((ctx->ncell + t.coop_cpb - 1) / t.coop_cpb)), ctx->coop_max_blocks);
+    if (ctx->it_exec) { cudaGraphExecDestroy(ctx->it_exec); ctx->it_exec = nullptr; }
+    if (ctx->it_graph) { cudaGraphDestroy(ctx->it_graph); ctx->it_graph = nullptr; }
+    if (ctx->ex_exec) { cudaGraphExecDestroy(ctx->ex_exec); ctx->ex_exec = nullptr; }
+    if (ctx->ex_graph) { cudaGraphDestroy(ctx->ex_graph); ctx->ex_graph = nullptr; }
+}
+
+bool tuning_valid(const pdac_ctx *ctx, const Tuning &t) {
+    return t.tile_shape >= 0 && t.tile_shape < N_TILE_SHAPES && t.tile_kchunk >= 1 && t.inner_grid >= 1 &&
+           t.test_grid >= 1 && t.coop_cpb >= 32 && t.tile_kchunk <= std::max(ctx->nz, 1);
+}
+
+// the cache key: what the best shapes depend on
+std::string tuning_key(const pdac_ctx *ctx) {
+    int dev = 0;
+    cudaDeviceProp prop{};
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+        cudaGetLastError();
+        std::snprintf(prop.name, sizeof prop.name, "unknown");
+    }
+    std::string name(prop.name);
+    for (char &ch : name)
+        if (ch == ' ' || ch == '\t') ch = '_';
+    char buf[256];
+    std::snprintf(buf, sizeof buf, "%s grid=%dx%dx%d nsolid=%d ngas=%d precision=%d time_integration=%d implicit=%d%d",
+                  name.c_str(), ctx->nx, ctx->ny, ctx->nz, ctx->ns, ctx->ng, ctx->cfg.precision, ctx->ti,
+                  ctx->cfg.implicit_fluxes, ctx->cfg.implicit_enthalpy);
+    return buf;
+}
+
+// cache file: one line per key, "<key> | t0 t1 t2 t3 t4"; the last line of a
+// key wins
+bool cache_find(const char *path, const std::string &key, Tuning &t) {
+    FILE *f = path ? std::fopen(path, "r") : nullptr;
+    if (!f) return false;
+    bool found = false;
+    char line[512];
+    while (std::fgets(line, sizeof line, f)) {
+        std::string l(line);
+        size_t bar = l.find(" | ");
+        if (bar == std::string::npos || l.compare(0, bar, key) != 0 || bar != key.size()) continue;
+        Tuning u{};
+        if (std::sscanf(l.c_str() + bar + 3, "%d %d %d %d %d", &u.tile_shape, &u.tile_kchunk, &u.inner_grid,
+                        &u.test_grid, &u.coop_cpb) == N_TUNE) {
+            t = u;
+            found = true;
+        }
+    }
+    std::fclose(f);
+    return found;
+}
+
+bool cache_add(const char *path, const std::string &key, const Tuning &t) {
+    FILE *f = path ? std::fopen(path, "a") : nullptr;
+    if (!f) return false;
+    bool ok = std::fprintf(f, "%s | %d %d %d %d %d\n", key.c_str(), t.tile_shape, t.tile_kchunk, t.inner_grid,
+                           t.test_grid, t.coop_cpb) > 0;
+    return std::fclose(f) == 0 && ok;
+}
+
+void tuning_out(const Tuning &t, int *out, int nout) {
+    const int v[N_TUNE] = {t.tile_shape, t.tile_kchunk, t.inner_grid, t.test_grid, t.coop_cpb};
+    for (int q = 0; q < nout && q < N_TUNE; ++q) out[q] = v[q];
+}
+}  // namespace
+
+int pdac_gpu_set_tuning(pdac_ctx *ctx, const int *in, int nin) {
+    if (!ctx || !in || nin < N_TUNE) return PDAC_ERR_ARG;
+    Tuning t{in[0], in[1], in[2], in[3], in[4]};
+    if (!tuning_valid(ctx, t)) return fail(ctx, PDAC_ERR_ARG, "set_tuning: a value is out of range");
+    put_tuning(ctx, t);
+    return PDAC_OK;
+}
+
+int pdac_gpu_autotune(pdac_ctx *ctx, const char *cache_path, int *out, int nout) {
+    if (!ctx || (out && nout < 0)) return PDAC_ERR_ARG;
+    const std::string key = tuning_key(ctx);
+    Tuning best = get_tuning(ctx);
+    if (cache_find(cache_path, key, best) && tuning_valid(ctx, best)) {
+        put_tuning(ctx, best);
+        if (out) tuning_out(best, out, nout);
+        return PDAC_OK;
+    }
+    cudaStream_t st = ctx->stream;
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    auto elapsed = [&](float &ms) -> int {
+        CK(cudaEventSynchronize(b));
+        CK(cudaEventElapsedTime(&ms, a, b));
+        return PDAC_OK;
+    };
+    int status = PDAC_OK;
+    // 1. tile shape and chunk of the 3D momentum-flux pass: a pure function
+    // of the state (it rewrites the same face fluxes), timed on it directly
+    if (ctx->d3 && status == PDAC_OK) {
+        float best_ms = 1e30f;
+        const int chunks[] = {16, 32, 64, ctx->nz};
+        for (int shape = 0; shape < N_TILE_SHAPES && status == PDAC_OK; ++shape)
+            for (int kc : chunks) {
+                if (kc < 1 || kc > ctx->nz || (shape == 0 && kc != chunks[1])) continue;  // form 0 has no chunks
+                auto launch = [&]() {
+                    return ctx->P.mixed ? launch_mom_tile<float>(ctx->P, ctx->F, ctx->nph, shape, kc, st)
+                                        : launch_mom_tile<double>(ctx->P, ctx->F, ctx->nph, shape, kc, st);
+                };
+                cudaError_t e = launch();
+                if (e == cudaSuccess) e = cudaEventRecord(a, st);
+                for (int r = 0; r < 3 && e == cudaSuccess; ++r) e = launch();
+                if (e == cudaSuccess) e = cudaEventRecord(b, st);
+                float ms = 0;
+                if (e != cudaSuccess) { status = fail(ctx, PDAC_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e)); break; }
+                if ((status = elapsed(ms))) break;
+                if (ms < best_ms) { best_ms = ms; best.tile_shape = shape; best.tile_kchunk = kc; }
+            }
+    }
+    // 2. the corrector's grids (and the cells per block of the one-launch
+    // sweep loop of small domains): whole time steps on the current state,
+    // restored after each candidate from a device copy; skipped when the
+    // copy does not fit in device memory
+    const bool semi = ctx->ti == 0;
+    double *snap = nullptr;
+    size_t nv = std::max(ctx->nvent, 1), nm = ctx->S.ntr > 0 ? (size_t)2 * ctx->S.ntr * ctx->ns : 0;
+    const size_t snap_doubles = ctx->arena_doubles + 2 * nv + nm;
+    if (status == PDAC_OK && semi && cudaMalloc(&snap, snap_doubles * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        snap = nullptr;
+    }
+    if (snap) {
+        auto copy_state = [&](bool save) -> int {
+            double *s0 = snap, *s1 = snap + ctx->arena_doubles, *s2 = s1 + nv, *s3 = s2 + nv;
+            auto cp = [&](double *dev, double *keep, size_t cnt) {
+                return cudaMemcpyAsync(save ? keep : dev, save ? dev : keep, cnt * sizeof(double),
+                                       cudaMemcpyDeviceToDevice, st);
+            };
+            CK(cp(ctx->arena, s0, ctx->arena_doubles));
+            CK(cp(ctx->d_vfact, s1, nv));
+            CK(cp(ctx->d_vfact0, s2, nv));
+            if (nm) CK(cp(ctx->d_sinkbuf, s3, nm));
+            return PDAC_OK;
+        };
+        // statistics and the last iter's count are the caller's, not the tuner's
+        const long long launches = ctx->launches, sweeps = ctx->sweeps, corr_launches = ctx->corr_launches,
+                        work_cells = ctx->work_cells, tested_cells = ctx->tested_cells, ex_calls = ctx->ex_calls;
+        const double corr_ms = ctx->corr_ms, resid_ms = ctx->resid_ms, inner_ms = ctx->inner_ms;
+        const int last_nit = ctx->last_nit;
+        const bool prof = ctx->prof;
+        const std::vector<double> sweep_log = ctx->sweep_log;
+        ctx->prof = false;
+        status = copy_state(true);
+        auto time_step = [&](const Tuning &t, float &ms) -> int {
+            put_tuning(ctx, t);
+            int nit = 0, s2;
+            // the first step builds the graphs for the shapes; the second is timed
+            for (int rep = 0; rep < 2; ++rep) {
+                if ((s2 = copy_state(false))) return s2;
+                CK(cudaEventRecord(a, st));
+                s2 = pdac_gpu_step(ctx, 1, &nit);
+                if (s2 == PDAC_ERR_CUDA) return s2;
+                CK(cudaEventRecord(b, st));
+                if ((s2 = elapsed(ms))) return s2;
+            }
+            return PDAC_OK;
+        };
+        int dev = 0, nsm = 148;
+        if (!status) status = cudaGetDevice(&dev) == cudaSuccess &&
+                                      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess
+                                  ? PDAC_OK
+                                  : fail(ctx, PDAC_ERR_CUDA, "autotune: device query");
+        const bool coop = ctx->coop_max_blocks > 0 && ctx->allow_coop && !ctx->cfg.implicit_fluxes &&
+                          !ctx->cfg.implicit_enthalpy;
+        float best_ms = 1e30f;
+        if (!status && coop) {
+            for (int cpb : {256, 512, 1024, 2048}) {
+                Tuning t = best;
+                t.coop_cpb = cpb;
+                float ms = 0;
+                if ((status = time_step(t, ms))) break;
+                if (ms < best_ms) { best_ms = ms; best = t; }
+            }
+        } else if (!status) {
+            for (int mult : {4, 8, 16, 32}) {
+                Tuning t = best;
+                t.inner_grid = nsm * mult;
+                t.test_grid = std::max(1, t.inner_grid / 2);
+                float ms = 0;
+                if ((status = time_step(t, ms))) break;
+                if (ms < best_ms) { best_ms = ms; best = t; }
+            }
+            for (int mult : {2, 4, 16}) {
+                if (status) break;
+                Tuning t = best;
+                t.test_grid = nsm * mult;
+                float ms = 0;
+                if ((status = time_step(t, ms))) break;
+                if (ms < best_ms) { best_ms = ms; best = t; }
+            }
+        }
+        int s3 = copy_state(false);
+        if (!status) status = s3;
+        if (!status) status = cudaStreamSynchronize(st) == cudaSuccess ? PDAC_OK : fail(ctx, PDAC_ERR_CUDA, "autotune: restore");
+        cudaFree(snap);
+        ctx->launches = launches; ctx->sweeps = sweeps; ctx->corr_launches = corr_launches;
+        ctx->work_cells = work_cells; ctx->tested_cells = tested_cells; ctx->ex_calls = ex_calls;
+        ctx->corr_ms = corr_ms; ctx->resid_ms = resid_ms; ctx->inner_ms = inner_ms;
+        ctx->last_nit = last_nit; ctx->prof = prof; ctx->sweep_log = sweep_log;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (status) return status;
+    put_tuning(ctx, best);
+    if (cache_path && !cache_add(cache_path, key, best))
+        return fail(ctx, PDAC_ERR_ARG, std::string("autotune: cannot append to ") + cache_path);
+    if (out) tuning_out(best, out, nout);
     return PDAC_OK;
 }
 

@@ -73,7 +73,11 @@ EXPORTED = (
     "pdac_gpu_append_mass_check", "pdac_gpu_write_mass_loss", "pdac_gpu_read_mass_loss",
     "pdac_gpu_compute_mixture_fields", "pdac_gpu_batch_create", "pdac_gpu_batch_step", "pdac_gpu_batch_elapsed",
     "pdac_gpu_batch_last_error", "pdac_gpu_batch_destroy", "pdac_gpu_unconverged_cells",
+    "pdac_gpu_autotune", "pdac_gpu_set_tuning",
 )
+
+# the launch shapes pdac_gpu_autotune / pdac_gpu_set_tuning exchange, in order
+TUNING_KEYS = ("tile_shape", "tile_kchunk", "inner_grid", "test_grid", "coop_cells_per_block")
 
 
 class Engine:
@@ -168,6 +172,25 @@ class Engine:
         self._chk(L.pdac_gpu_unconverged_cells(self.h, buf.ctypes.data_as(C.POINTER(C.c_int)), C.byref(n)),
                   "unconverged_cells")
         return buf[:n.value].copy()
+
+    def autotune(self, cache_path=None):
+        """Time the tunable launch shapes on the current state and keep the
+        fastest (pdac_gpu_autotune); returns them as a dict."""
+        L = self.L
+        L.pdac_gpu_autotune.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_int), C.c_int]
+        L.pdac_gpu_autotune.restype = C.c_int
+        out = (C.c_int * len(TUNING_KEYS))()
+        path = os.fsencode(cache_path) if cache_path is not None else None
+        self._chk(L.pdac_gpu_autotune(self.h, path, out, len(TUNING_KEYS)), "autotune")
+        return dict(zip(TUNING_KEYS, list(out)))
+
+    def set_tuning(self, tuning):
+        """Install launch shapes (a dict with TUNING_KEYS)."""
+        L = self.L
+        L.pdac_gpu_set_tuning.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.c_int]
+        L.pdac_gpu_set_tuning.restype = C.c_int
+        arr = (C.c_int * len(TUNING_KEYS))(*[int(tuning[k]) for k in TUNING_KEYS])
+        self._chk(L.pdac_gpu_set_tuning(self.h, arr, len(TUNING_KEYS)), "set_tuning")
 
     def ygas(self, dt):
         self._chk(self.L.pdac_gpu_ygas(self.h, dt), "ygas")

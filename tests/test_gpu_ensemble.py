@@ -83,3 +83,32 @@ def test_drawn_members_step_in_a_batch():
     b.close()
     for e in engines:
         e.close()
+
+
+def test_drawn_members_match_the_oracle():
+    """Two members of the 2D ensemble as drawn (grid, vent velocity and
+    temperature, class volume fractions), stepped in a batch, against the
+    oracle run on each member's deck: same outer sweeps, fields to 1e-9
+    (relative L-infinity over the fluid cells) after every step."""
+    import pyoracle
+    from helpers import STEP_FIELDS, compare_state
+    from pdac_b200.engine import Engine
+    from pdac_b200.ensemble import Batch, member_decks, split
+    from pdac_b200.setup_state import Case
+    decks = member_decks(64)
+    cells = [d["nx"] * d["nz"] for d in decks]
+    pick = [min(range(64), key=lambda m: cells[m]), sorted(range(64), key=lambda m: cells[m])[32]]
+    cases = [Case(decks[m]) for m in pick]
+    engines = [Engine(c) for c in cases]
+    oracles = [pyoracle.Oracle(c, order=pyoracle.ORDER_COLORED) for c in cases]
+    b = Batch(engines)
+    for s in range(1, 6):
+        nit = b.step(s)
+        for q, (c, e, o) in enumerate(zip(cases, engines, oracles)):
+            assert nit[q] == o.step(s), f"member {pick[q]} step {s}"
+            fluid = (c.flag & 1) == 1
+            errs, bad = compare_state(e.download(), o.get_state(), STEP_FIELDS, 1e-9, c.nsolid, c.ncell, cells=fluid)
+            assert not bad, f"member {pick[q]} step {s}: {bad}"
+    b.close()
+    for e in engines:
+        e.close()
