@@ -38,6 +38,10 @@
 #include <algorithm>
 
 #include "../include/pdac_gpu.h"
+// exp and pow of the per-cell physics: the engine's own routines (the same
+// bits on the host and the device; the C library's may differ from CUDA's in
+// the last bit)
+#include "../pdac_b200/csrc/fpmath.h"
 
 // The 3D passes run their cell loops on several host threads: every such
 // loop writes each value from exactly one cell -- the cell that writes it
@@ -648,7 +652,7 @@ void viscon(const Oracle &o, double &mu, double &kap, const double *xgc, double 
     for (int ig = 0; ig < o.ng; ++ig) {
         int igg = o.gas_type[ig];
         double tst = tg / o.mmugek[igg];
-        double om = 1.16145 * std::pow(tst, -0.14874) + 0.52487 * std::exp(-0.77320 * tst) + 2.16178 * std::exp(-2.43787 * tst);
+        double om = 1.16145 * pdac_fp::pow(tst, -0.14874) + 0.52487 * pdac_fp::exp(-0.77320 * tst) + 2.16178 * pdac_fp::exp(-2.43787 * tst);
         double m = 1.0e3 * o.gmw[igg];
         mmug[igg] = 26.69 * std::sqrt(m * tg) / (o.mmugs[igg] * o.mmugs[igg] * om);
         mmug[igg] = mmug[igg] * 1.0e-7;
@@ -670,7 +674,7 @@ void viscon(const Oracle &o, double &mu, double &kap, const double *xgc, double 
             int jgg = o.gas_type[jg];
             double aa = o.gmw[igg] / o.gmw[jgg];
             double bb = mmug[igg] / mmug[jgg];
-            double cc = 1.0 + std::sqrt(bb) * std::pow(aa, -0.25);
+            double cc = 1.0 + std::sqrt(bb) * pdac_fp::pow(aa, -0.25);
             phij[igg][jgg] = cc * cc / std::sqrt(8.0 * (1.0 + aa));
         }
     }
@@ -743,11 +747,11 @@ double kdrags(const Oracle &o, double du, double dv, double dw, double ep, doubl
         double eps = rlk * o.inrl[is];
         double reynum = rgp * o.dk[is] * o.phis[is] * vrel / mug;
         double dc;
-        if (reynum <= 1000.0) dc = (24.0 / reynum) * (1.0 + (double)0.15f * std::pow(reynum, (double)0.687f));
+        if (reynum <= 1000.0) dc = (24.0 / reynum) * (1.0 + (double)0.15f * pdac_fp::pow(reynum, (double)0.687f));
         else dc = (double)0.43828814f;
         dc = std::min(dc, 1.0e4);
         drag = 0.75 * dc * eps / (o.dk[is] * o.phis[is]) * rgp * vrel;
-        drag = drag * std::pow(ep, (double)(-2.65f));
+        drag = drag * pdac_fp::pow(ep, (double)(-2.65f));
     }
     return drag;
 }
@@ -757,9 +761,9 @@ double sdrag(const Oracle &o, double du, double dv, double dw, double ep, double
     double vrel = std::sqrt(du * du + dv * dv + dw * dw);
     double eps = rlk * o.inrl[is];
     double reynum = rgp * o.dk[is] * o.phis[is] * vrel / mug;
-    double a = std::pow(ep, (double)4.14f), b;
-    if (ep <= (double)0.85f) b = (double)0.8f * std::pow(ep, (double)1.28f);
-    else b = std::pow(ep, (double)2.65f);
+    double a = pdac_fp::pow(ep, (double)4.14f), b;
+    if (ep <= (double)0.85f) b = (double)0.8f * pdac_fp::pow(ep, (double)1.28f);
+    else b = pdac_fp::pow(ep, (double)2.65f);
     double vr = 0.5 * (a - (double)0.06f * reynum +
                        std::sqrt((double)0.0036f * reynum * reynum + (double)0.12f * reynum * (2.0 * b - a) + a * a));
     double dc = (0.63 + 4.8 / std::sqrt(reynum));
@@ -780,7 +784,7 @@ double ppdrag(const Oracle &o, const double *rlkc, int k, int kk) {  // rlkc 1-b
         if (xbar <= o.philim[k - 1][kk - 1]) epkl = o.epsl[k - 1][kk - 1] * xbar + o.phi[k2];
         else epkl = o.epsu[k - 1][kk - 1] * (1.0 - xbar) + o.phi[k1];
         double espo = 1.0 / 3.0;
-        double m1 = std::pow(epkl, espo), m2 = std::pow(epsum, espo);
+        double m1 = pdac_fp::pow(epkl, espo), m2 = pdac_fp::pow(epsum, espo);
         double effe = (3.0 * m1 + m2) / (2.0 * (m1 - m2));
         return 1.0 * (1.0 + 1.0) * rlkc[k - 1] * rlkc[kk - 1] * o.dkf[k - 1][kk - 1] * effe;
     }
@@ -798,9 +802,9 @@ double hvs(const Oracle &o, double rlk, double rog, double ep, double du, double
     double vrel = std::sqrt(du * du + dv * dv + dw * dw);
     double reynum = o.dk[k] * vrel * rog / mug;
     double pranum = cg * mug / kapg;
-    double pranumexp = std::pow(pranum, 1.0 / 3.0);
-    double nusselt = (2.0 + 5.0 * eps2) * (1.0 + 0.7 * std::pow(reynum, 0.2) * pranumexp);
-    nusselt = nusselt + (0.13 + 1.2 * eps2) * std::pow(reynum, 0.7) * pranumexp;
+    double pranumexp = pdac_fp::pow(pranum, 1.0 / 3.0);
+    double nusselt = (2.0 + 5.0 * eps2) * (1.0 + 0.7 * pdac_fp::pow(reynum, 0.2) * pranumexp);
+    nusselt = nusselt + (0.13 + 1.2 * eps2) * pdac_fp::pow(reynum, 0.7) * pranumexp;
     return nusselt * asurf;
 }
 
@@ -1130,10 +1134,10 @@ void repulsive_2d(Oracle &o) {
         for (int is = 1; is <= o.ns; ++is) {
             double rc = o.S(o.rlk, c, is), re = o.S(o.rlk, ijke, is), rt = o.S(o.rlk, ijkt, is);
             double epsx = (dx[i + 1] * rc + dx[i] * re) * indxp * o.inrl[is];
-            double gepx = std::pow(10.0, -a * epsx + b);
+            double gepx = pdac_fp::pow(10.0, -a * epsx + b);
             o.S(o.pvisx, c, is) = o.S(o.pvisx, c, is) - gepx * indxp * 2.0 * (re - rc) * o.inrl[is];
             double epsz = (dz[k + 1] * rc + dz[k] * rt) * indzp * o.inrl[is];
-            double gepz = std::pow(10.0, -a * epsz + b);
+            double gepz = pdac_fp::pow(10.0, -a * epsz + b);
             o.S(o.pvisz, c, is) = o.S(o.pvisz, c, is) - gepz * indzp * 2.0 * (rt - rc) * o.inrl[is];
         }
     }
@@ -2404,6 +2408,9 @@ int pdac_oracle_mass_totals(void *h, double *out, int nout) {
 }
 
 int pdac_oracle_last_nit(void *h) { return ((Oracle *)h)->last_nit; }
+// the shared exp and pow (for their accuracy tests)
+double pdac_oracle_fp_pow(double x, double y) { return pdac_fp::pow(x, y); }
+double pdac_oracle_fp_exp(double x) { return pdac_fp::exp(x); }
 // threads of the 3D cell loops (n <= 0 keeps the current count); returns
 // the number in use afterwards
 int pdac_oracle_set_threads(int n) {

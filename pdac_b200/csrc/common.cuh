@@ -10,6 +10,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "fpmath.h"  // exp and pow with the same bits as the host's (the oracle's)
+
 #define PDAC_MAXS 8          // max solid classes
 #define PDAC_MAXP (PDAC_MAXS + 1)
 #define PDAC_MAXG 7

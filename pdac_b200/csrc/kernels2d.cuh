@@ -431,10 +431,10 @@ __global__ void k_tilde2d(Prm P, Fld F, double dt, const double *app0u, const do
             if (P.repulsive_model == 1) {
                 double rc = rl[c], re = rl[ijke], rt = rl[ijkt];
                 double epsx = (dx[i + 1] * rc + dx[i] * re) * indxp * ir;
-                double gepx = pow(10.0, -a_rep * epsx + b_rep);
+                double gepx = pdac_fp::pow(10.0, -a_rep * epsx + b_rep);
                 pvx = pvx - gepx * indxp * 2.0 * (re - rc) * ir;
                 double epsz = (dz[k + 1] * rc + dz[k] * rt) * indzp * ir;
-                double gepz = pow(10.0, -a_rep * epsz + b_rep);
+                double gepz = pdac_fp::pow(10.0, -a_rep * epsz + b_rep);
                 pvz = pvz - gepz * indzp * 2.0 * (rt - rc) * ir;
             }
         }

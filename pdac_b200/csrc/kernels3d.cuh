@@ -333,13 +333,13 @@ __global__ void __launch_bounds__(128, PDAC_FLUX_MINB) k_visc3d(Prm P, Fld F) {
         if (P.repulsive_model == 1) {
             double rc = rl[c], re = rl[ijke], rn = rl[ijkn], rt = rl[ijkt];
             double epsx = (dx[i + 1] * rc + dx[i] * re) * indxp * ir;
-            double gepx = pow(10.0, -a_rep * epsx + b_rep);
+            double gepx = pdac_fp::pow(10.0, -a_rep * epsx + b_rep);
             vx = vx - gepx * indxp * 2.0 * (re - rc) * ir;
             double epsz = (dz[k + 1] * rc + dz[k] * rt) * indzp * ir;
-            double gepz = pow(10.0, -a_rep * epsz + b_rep);
+            double gepz = pdac_fp::pow(10.0, -a_rep * epsz + b_rep);
             vz = vz - gepz * indzp * 2.0 * (rt - rc) * ir;
             double epsy = (dy[j + 1] * rc + dy[j] * rn) * indyp * ir;
-            double gepy = pow(10.0, -a_rep * epsy + b_rep);
+            double gepy = pdac_fp::pow(10.0, -a_rep * epsy + b_rep);
             vy = vy - gepy * indyp * 2.0 * (rn - rc) * ir;
         }
     }

@@ -237,7 +237,7 @@ __global__ void k_sgss(Prm P, Fld F) {
     }
     const double cst = 0.5 * sqrt(2.0);
     double ex = (3.98 * F.rlk[off + c] * P.inrl[is] - 1.69);
-    double fact = pow(10.0, ex);
+    double fact = pdac_fp::pow(10.0, ex);
     F.must[off + c] = cst * P.cmus[is] * P.rl[is] * (P.dk[is] * P.dk[is]) * fact * modsr;
 }
 

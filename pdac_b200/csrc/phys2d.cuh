@@ -378,7 +378,7 @@ __device__ __forceinline__ void viscon(const Prm &P, double &mu, double &kap, co
     for (int ig = 0; ig < P.ng; ++ig) {
         int g = P.gas_type[ig];
         double tst = tg / P.mmugek[g];
-        double om = 1.16145 * pow(tst, -0.14874) + 0.52487 * exp(-0.77320 * tst) + 2.16178 * exp(-2.43787 * tst);
+        double om = 1.16145 * pdac_fp::pow(tst, -0.14874) + 0.52487 * pdac_fp::exp(-0.77320 * tst) + 2.16178 * pdac_fp::exp(-2.43787 * tst);
         double m = 1.0e3 * P.gmw[g];
         double v = 26.69 * sqrt(m * tg) / (P.mmugs[g] * P.mmugs[g] * om);
         mmug[ig] = v * 1.0e-7;
@@ -406,7 +406,7 @@ __device__ __forceinline__ void viscon(const Prm &P, double &mu, double &kap, co
             int h = P.gas_type[jg];
             double aa = P.gmw[g] / P.gmw[h];
             double bb = mmug[ig] / mmug[jg];
-            double cc = 1.0 + sqrt(bb) * pow(aa, -0.25);
+            double cc = 1.0 + sqrt(bb) * pdac_fp::pow(aa, -0.25);
             double phij = cc * cc / sqrt(8.0 * (1.0 + aa));
             sum = sum + xg[jg] * phij;
         }
@@ -476,11 +476,11 @@ __device__ __forceinline__ double kdrags(const Prm &P, double du, double dv, dou
             double eps = rlk * P.inrl[is];
             double reynum = rgp * P.dk[is] * P.phis[is] * vrel / mug;
             double dc;
-            if (reynum <= 1000.0) dc = (24.0 / reynum) * (1.0 + (double)0.15f * pow(reynum, (double)0.687f));
+            if (reynum <= 1000.0) dc = (24.0 / reynum) * (1.0 + (double)0.15f * pdac_fp::pow(reynum, (double)0.687f));
             else dc = (double)0.43828814f;
             dc = fmin(dc, 1.0e4);
             drag = 0.75 * dc * eps / (P.dk[is] * P.phis[is]) * rgp * vrel;
-            drag = drag * pow(ep, (double)(-2.65f));
+            drag = drag * pdac_fp::pow(ep, (double)(-2.65f));
         }
     }
     return drag;
@@ -494,9 +494,9 @@ __device__ __forceinline__ double sdrag(const Prm &P, double du, double dv, doub
     {
         double eps = rlk * P.inrl[is];
         double reynum = rgp * P.dk[is] * P.phis[is] * vrel / mug;
-        double a = pow(ep, (double)4.14f), b;
-        if (ep <= (double)0.85f) b = (double)0.8f * pow(ep, (double)1.28f);
-        else b = pow(ep, (double)2.65f);
+        double a = pdac_fp::pow(ep, (double)4.14f), b;
+        if (ep <= (double)0.85f) b = (double)0.8f * pdac_fp::pow(ep, (double)1.28f);
+        else b = pdac_fp::pow(ep, (double)2.65f);
         double vr = 0.5 * (a - (double)0.06f * reynum +
                            sqrt((double)0.0036f * reynum * reynum + (double)0.12f * reynum * (2.0 * b - a) + a * a));
         double dc = (0.63 + 4.8 / sqrt(reynum));
@@ -525,7 +525,7 @@ __device__ __forceinline__ double ppdrag(const Prm &P, const double *rlkc, int k
         if (xbar <= P.philim[k - 1][kk - 1]) epkl = P.epsl[k - 1][kk - 1] * xbar + P.phi[k2];
         else epkl = P.epsu[k - 1][kk - 1] * (1.0 - xbar) + P.phi[k1];
         double espo = 1.0 / 3.0;
-        double m1 = pow(epkl, espo), m2 = pow(epsum, espo);
+        double m1 = pdac_fp::pow(epkl, espo), m2 = pdac_fp::pow(epsum, espo);
         double effe = (3.0 * m1 + m2) / (2.0 * (m1 - m2));
         return 1.0 * (1.0 + 1.0) * rlkc[k - 1] * rlkc[kk - 1] * P.dkf[k - 1][kk - 1] * effe;
     }
@@ -542,9 +542,9 @@ __device__ __forceinline__ double hvs(const Prm &P, double rlk, double rog, doub
     double vrel = sqrt(du * du + dv * dv + dw * dw);
     double reynum = P.dk[k] * vrel * rog / mug;
     double pranum = cg * mug / kapg;
-    double pranumexp = pow(pranum, 1.0 / 3.0);
-    double nusselt = (2.0 + 5.0 * eps2) * (1.0 + 0.7 * pow(reynum, 0.2) * pranumexp);
-    nusselt = nusselt + (0.13 + 1.2 * eps2) * pow(reynum, 0.7) * pranumexp;
+    double pranumexp = pdac_fp::pow(pranum, 1.0 / 3.0);
+    double nusselt = (2.0 + 5.0 * eps2) * (1.0 + 0.7 * pdac_fp::pow(reynum, 0.2) * pranumexp);
+    nusselt = nusselt + (0.13 + 1.2 * eps2) * pdac_fp::pow(reynum, 0.7) * pranumexp;
     return nusselt * asurf;
 }
 

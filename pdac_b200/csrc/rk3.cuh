@@ -386,10 +386,10 @@ __global__ void k_visc2d(Prm P, Fld F) {
             double indxp = P.hx[i], indzp = P.hz[k];
             double rc = rl[c], re = rl[M.e], rt = rl[M.t];
             double epsx = (dx[i + 1] * rc + dx[i] * re) * indxp * ir;
-            double gepx = pow(10.0, -a_rep * epsx + b_rep);
+            double gepx = pdac_fp::pow(10.0, -a_rep * epsx + b_rep);
             vx = vx - gepx * indxp * 2.0 * (re - rc) * ir;
             double epsz = (dz[k + 1] * rc + dz[k] * rt) * indzp * ir;
-            double gepz = pow(10.0, -a_rep * epsz + b_rep);
+            double gepz = pdac_fp::pow(10.0, -a_rep * epsz + b_rep);
             vz = vz - gepz * indzp * 2.0 * (rt - rc) * ir;
         }
     }
