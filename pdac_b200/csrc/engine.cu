@@ -56,6 +56,13 @@ struct pdac_ctx {
     long work_stride = 0;
     int last_nit = 0;                             // sweep count of the last pdac_gpu_iter
     int *d_nonfinite = nullptr, *h_nonfinite = nullptr;  // non-finite flag of the state checks
+    // the whole semi-implicit time step as one graph (members of a batch):
+    // its kernels outside the sweep loop, and the step's outcome [nit, caloric
+    // failures of ftem, non-finite flag] read back once per step
+    cudaGraph_t step_graph = nullptr;
+    cudaGraphExec_t step_exec = nullptr;
+    long long step_launches = 0;
+    int *d_status = nullptr, *h_status = nullptr;
     unsigned *d_dirty = nullptr;                 // corrector active set, one bit per cell
     int *d_cand = nullptr;                       // candidate cells of one colour phase
     int inner_grid = 0;
@@ -586,6 +593,8 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     CK(cudaMalloc(&ctx->d_work, (size_t)3 * ctx->work_stride * sizeof(int)));
     CK(cudaMalloc(&ctx->d_nonfinite, sizeof(int)));
     CK(cudaMallocHost(&ctx->h_nonfinite, sizeof(int)));
+    CK(cudaMalloc(&ctx->d_status, 4 * sizeof(int)));
+    CK(cudaMallocHost(&ctx->h_status, 4 * sizeof(int)));
     CK(cudaMalloc(&ctx->d_wcount, 16 * sizeof(int)));
     CK(cudaMalloc(&ctx->d_dirty, ((size_t)n + 31) / 32 * sizeof(unsigned)));
     CK(cudaMalloc(&ctx->d_cand, (size_t)n * sizeof(int)));
@@ -762,6 +771,10 @@ int pdac_gpu_destroy(pdac_ctx *ctx) {
     cudaFree(ctx->d_work);
     cudaFree(ctx->d_nonfinite);
     cudaFreeHost(ctx->h_nonfinite);
+    if (ctx->step_exec) cudaGraphExecDestroy(ctx->step_exec);
+    if (ctx->step_graph) cudaGraphDestroy(ctx->step_graph);
+    cudaFree(ctx->d_status);
+    cudaFreeHost(ctx->h_status);
     cudaFree(ctx->d_wcount);
     cudaFree(ctx->d_dirty);
     if (ctx->it_exec) cudaGraphExecDestroy(ctx->it_exec);
@@ -897,11 +910,8 @@ static int check_step_state(pdac_ctx *ctx) {
 int pdac_gpu_upload_state(pdac_ctx *ctx, const pdac_state_view *s) { return xfer_state(ctx, const_cast<pdac_state_view *>(s), true); }
 int pdac_gpu_download_state(pdac_ctx *ctx, pdac_state_view *s) { return xfer_state(ctx, s, false); }
 
-int pdac_gpu_boundary(pdac_ctx *ctx, int sweep) {
-    if (!ctx) return PDAC_ERR_ARG;
-    (void)sweep;
-    cudaStream_t st = ctx->stream;
-    CK(cudaEventRecord(ctx->ev[0], st));
+// the kernels of boundary on stream st (also inside a whole-step graph)
+static int enqueue_boundary(pdac_ctx *ctx, cudaStream_t st) {
     if (ctx->nvent > 0 && ctx->cfg.irand >= 1)
         pdac::k_vent<<<blocks(ctx->nvent), TPB, 0, st>>>(ctx->P, ctx->F, ctx->d_vent, ctx->nvent, ctx->d_vfact, ctx->d_vfact0), ctx->launches++;
     if (ctx->d3) pdac::k_boundary3d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F);
@@ -914,14 +924,21 @@ int pdac_gpu_boundary(pdac_ctx *ctx, int sweep) {
         ctx->launches++;
     }
     CK(cudaGetLastError());
-    CK(cudaEventRecord(ctx->ev[1], st));
     return PDAC_OK;
 }
 
-int pdac_gpu_fieldn(pdac_ctx *ctx) {
+int pdac_gpu_boundary(pdac_ctx *ctx, int sweep) {
     if (!ctx) return PDAC_ERR_ARG;
-    cudaStream_t st = ctx->stream;
-    CK(cudaEventRecord(ctx->ev[2], st));
+    (void)sweep;
+    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    int s = enqueue_boundary(ctx, ctx->stream);
+    if (s) return s;
+    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    return PDAC_OK;
+}
+
+// the kernels of fieldn on stream st
+static int enqueue_fieldn(pdac_ctx *ctx, cudaStream_t st) {
     if (ctx->d3) pdac::k_fieldn3d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F);
     else pdac::k_fieldn2d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F);
     ctx->launches++;
@@ -936,7 +953,15 @@ int pdac_gpu_fieldn(pdac_ctx *ctx) {
     for (double *a : {F.appu, F.appv, F.appw, ctx->d_app0u, ctx->d_app0v, ctx->d_app0w})
         if (a) CK(cudaMemsetAsync(a, 0, n * ctx->nap * sizeof(double), st));
     CK(cudaGetLastError());
-    CK(cudaEventRecord(ctx->ev[3], st));
+    return PDAC_OK;
+}
+
+int pdac_gpu_fieldn(pdac_ctx *ctx) {
+    if (!ctx) return PDAC_ERR_ARG;
+    CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    int s = enqueue_fieldn(ctx, ctx->stream);
+    if (s) return s;
+    CK(cudaEventRecord(ctx->ev[3], ctx->stream));
     return PDAC_OK;
 }
 
@@ -1359,6 +1384,23 @@ int pdac_gpu_iter_static(pdac_ctx *ctx, double dt, int *nit_out) {
     return maxout_status(ctx, nit);
 }
 
+// the kernels of ygas with more than one gas, on stream st
+static int enqueue_ygas(pdac_ctx *ctx, double dt, cudaStream_t st) {
+    const size_t n = ctx->ncell;
+    for (double *a : {ctx->F.yfe, ctx->F.yfn, ctx->F.yft})
+        if (a) CK(cudaMemsetAsync(a, 0, n * ctx->ng * sizeof(double), st));
+    if (ctx->d3) {
+        (ctx->P.mixed ? pdac::k_ygas_flux3d<float> : pdac::k_ygas_flux3d<double>)<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F),
+            ctx->launches++;
+        pdac::k_ygas3d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F, dt), ctx->launches++;
+    } else {
+        pdac::k_ygas_flux2d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F), ctx->launches++;
+        pdac::k_ygas2d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F, dt), ctx->launches++;
+    }
+    CK(cudaGetLastError());
+    return PDAC_OK;
+}
+
 int pdac_gpu_ygas(pdac_ctx *ctx, double dt) {
     if (!ctx) return PDAC_ERR_ARG;
     cudaStream_t st = ctx->stream;
@@ -1370,18 +1412,9 @@ int pdac_gpu_ygas(pdac_ctx *ctx, double dt) {
         CK(cudaMemcpyAsync(ctx->F.xgc, one.data(), n * sizeof(double), cudaMemcpyHostToDevice, st));
         CK(cudaStreamSynchronize(st));
     } else {
-        for (double *a : {ctx->F.yfe, ctx->F.yfn, ctx->F.yft})
-            if (a) CK(cudaMemsetAsync(a, 0, n * ctx->ng * sizeof(double), st));
-        if (ctx->d3) {
-            (ctx->P.mixed ? pdac::k_ygas_flux3d<float> : pdac::k_ygas_flux3d<double>)<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F),
-                ctx->launches++;
-            pdac::k_ygas3d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F, dt), ctx->launches++;
-        } else {
-            pdac::k_ygas_flux2d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F), ctx->launches++;
-            pdac::k_ygas2d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F, dt), ctx->launches++;
-        }
+        int s = enqueue_ygas(ctx, dt, st);
+        if (s) return s;
     }
-    CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[9], st));
     return PDAC_OK;
 }
@@ -1795,6 +1828,8 @@ void put_tuning(pdac_ctx *ctx, const Tuning &t) {
     if (ctx->it_graph) { cudaGraphDestroy(ctx->it_graph); ctx->it_graph = nullptr; }
     if (ctx->ex_exec) { cudaGraphExecDestroy(ctx->ex_exec); ctx->ex_exec = nullptr; }
     if (ctx->ex_graph) { cudaGraphDestroy(ctx->ex_graph); ctx->ex_graph = nullptr; }
+    if (ctx->step_exec) { cudaGraphExecDestroy(ctx->step_exec); ctx->step_exec = nullptr; }
+    if (ctx->step_graph) { cudaGraphDestroy(ctx->step_graph); ctx->step_graph = nullptr; }
 }
 
 bool tuning_valid(const pdac_ctx *ctx, const Tuning &t) {
@@ -2432,9 +2467,157 @@ int pdac_gpu_elapsed(pdac_ctx *ctx, int a, int b, double *ms) {
 // stream.  Small 2D members fill a few percent of the SMs each; run side by
 // side they fill the device.  Members are spread over the threads by the
 // longest-processing-time rule on their cell counts.
+// ---------------------------------------------------------------------------
+// the whole semi-implicit time step as one CUDA graph (prog.f:162-331 with
+// rungekut = 1): boundary, fieldn, the sub-grid models, tilde and iter's
+// set-up as one child graph, the outer sweep loop as a conditional WHILE node
+// (the body of pdac_gpu_iter's graph), then ygas, htilde, ftem, the mixture
+// fields, the non-finite check and the copy of the step's outcome to pinned
+// host memory as a second child graph.  The same kernels in the same order
+// as pdac_gpu_step, so the same results; a batch launches it for each of its
+// members from one host thread.
+// ---------------------------------------------------------------------------
+namespace pdac {
+__global__ void k_set_int(int *p, int v) { *p = v; }
+__global__ void k_step_status(const int *nit, const int *counters, const int *nonfinite, int *out) {
+    out[0] = *nit;
+    out[1] = counters[1];
+    out[2] = *nonfinite;
+}
+}  // namespace pdac
+
+static bool step_graph_eligible(const pdac_ctx *ctx) {
+    const pdac_cfg &c = ctx->cfg;
+    return ctx->ti == 0 && c.rungekut == 1 && !c.implicit_fluxes && !c.implicit_enthalpy && !c.cstop &&
+           !c.update_eosg && ctx->ng > 1;
+}
+
+static int enqueue_step_pre(pdac_ctx *ctx, double dt, cudaStream_t st) {
+    int s;
+    if ((s = enqueue_boundary(ctx, st)) || (s = enqueue_fieldn(ctx, st))) return s;
+    if ((s = pdac_gpu_sgsg(ctx)) || (s = pdac_gpu_sgss(ctx))) return s;
+    if ((s = enqueue_tilde(ctx, dt, st))) return s;
+    // iter's set-up, as in pdac_gpu_iter
+    Fld &F = ctx->F;
+    const size_t n = ctx->ncell, ns = ctx->ns;
+    CK(cudaMemsetAsync(ctx->d_counters + 5, 0, sizeof(int), st));
+    for (double *a : {F.rgfe, F.rgfn, F.rgft, F.conv, F.abeta})
+        if (a) CK(cudaMemsetAsync(a, 0, n * sizeof(double), st));
+    for (double *a : {F.rsfe, F.rsfn, F.rsft})
+        if (a) CK(cudaMemsetAsync(a, 0, n * ns * sizeof(double), st));
+    const int nph = ctx->nph;
+    if (ctx->d3) {
+        PHASE_LAUNCH(nph, pdac::k_predictor3d, blocks(n), TPB, st, ctx->P, F, dt);
+        pdac::k_mflux_init3d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt);
+    } else {
+        PHASE_LAUNCH(nph, pdac::k_predictor2d, blocks(n), TPB, st, ctx->P, F, dt);
+        pdac::k_mflux_init2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt);
+    }
+    CK(cudaMemsetAsync(ctx->d_dirty, 0xff, (n + 31) / 32 * sizeof(unsigned), st));
+    pdac::k_set_int<<<1, 1, 0, st>>>(ctx->d_nit, 1);
+    ctx->launches += 3;
+    CK(cudaGetLastError());
+    return PDAC_OK;
+}
+
+static int enqueue_step_post(pdac_ctx *ctx, double dt, cudaStream_t st) {
+    int s;
+    if ((s = enqueue_ygas(ctx, dt, st)) || (s = enqueue_htilde(ctx, dt, st)) || (s = enqueue_ftem(ctx, dt, st, false)))
+        return s;
+    if (ctx->cfg.compute_mixture) {
+        if (ctx->d3) pdac::k_mixture<3><<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F);
+        else pdac::k_mixture<2><<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F);
+        ctx->launches++;
+    }
+    // check_step_state's fields, without its host read
+    const Fld &F = ctx->F;
+    const size_t n = ctx->ncell;
+    pdac::FinList L{};
+    const double *arr[6] = {F.p, F.ep, F.rgp, F.tg, F.sieg, F.rlk};
+    for (int q = 0; q < 6; ++q) { L.a[q] = arr[q]; L.n[q] = (long long)(q == 5 ? n * ctx->ns : n); }
+    L.m = 6;
+    int dev = 0, nsm = 148;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaMemsetAsync(ctx->d_nonfinite, 0, sizeof(int), st));
+    pdac::k_nonfinite<<<nsm * 8, 256, 0, st>>>(L, ctx->d_nonfinite);
+    pdac::k_step_status<<<1, 1, 0, st>>>(ctx->d_nit, ctx->d_counters, ctx->d_nonfinite, ctx->d_status);
+    CK(cudaMemcpyAsync(ctx->h_status, ctx->d_status, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    ctx->launches += 2;
+    CK(cudaGetLastError());
+    return PDAC_OK;
+}
+
+static int build_step_graph(pdac_ctx *ctx) {
+    if (ctx->step_exec) { cudaGraphExecDestroy(ctx->step_exec); ctx->step_exec = nullptr; }
+    if (ctx->step_graph) { cudaGraphDestroy(ctx->step_graph); ctx->step_graph = nullptr; }
+    const double dt = ctx->cfg.dt;
+    cudaStream_t st = ctx->stream;
+    const long long before = ctx->launches;
+    CK(cudaGraphCreate(&ctx->step_graph, 0));
+    cudaGraph_t part = nullptr;
+    // the kernels before the sweep loop
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+    int s = enqueue_step_pre(ctx, dt, st);
+    cudaError_t e = cudaStreamEndCapture(st, &part);
+    if (s) { ctx->launches = before; return s; }
+    CK(e);
+    cudaGraphNode_t pre, loop_node, post;
+    e = cudaGraphAddChildGraphNode(&pre, ctx->step_graph, nullptr, 0, part);
+    cudaGraphDestroy(part);
+    CK(e);
+    // the sweep loop
+    cudaGraphConditionalHandle loop;
+    CK(cudaGraphConditionalHandleCreate(&loop, ctx->step_graph, 1, cudaGraphCondAssignDefault));
+    alignas(cudaGraphNodeParams) unsigned char cp_storage[sizeof(cudaGraphNodeParams)] = {};
+    cudaGraphNodeParams &cp = *reinterpret_cast<cudaGraphNodeParams *>(cp_storage);
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = loop;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    CK(cudaGraphAddNode(&loop_node, ctx->step_graph, &pre, 1, &cp));
+    CK(cudaStreamBeginCaptureToGraph(st, cp.conditional.phGraph_out[0], nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    const long long mid = ctx->launches;
+    s = enqueue_sweep(ctx, dt, st, false);
+    ctx->it_per_sweep = 10 + (ctx->launches - mid);
+    ctx->launches = mid;
+    if (!s) pdac::k_sweep_check<<<1, 1, 0, st>>>(ctx->d_wcount, ctx->d_nit, ctx->cfg.maxout, loop);
+    cudaGraph_t body = nullptr;
+    e = cudaStreamEndCapture(st, &body);
+    if (s) { ctx->launches = before; return s; }
+    CK(e);
+    // the kernels after it
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+    s = enqueue_step_post(ctx, dt, st);
+    e = cudaStreamEndCapture(st, &part);
+    ctx->step_launches = ctx->launches - before;
+    ctx->launches = before;
+    if (s) return s;
+    CK(e);
+    e = cudaGraphAddChildGraphNode(&post, ctx->step_graph, &loop_node, 1, part);
+    cudaGraphDestroy(part);
+    CK(e);
+    CK(cudaGraphInstantiate(&ctx->step_exec, ctx->step_graph, 0));
+    return PDAC_OK;
+}
+
+// after a graph step has completed: its sweep count and status
+static int step_graph_outcome(pdac_ctx *ctx, int *nit) {
+    const int *h = ctx->h_status;
+    const int done = std::min(h[0], ctx->cfg.maxout);
+    ctx->sweeps += done;
+    ctx->launches += ctx->step_launches + ctx->it_per_sweep * done;
+    ctx->last_nit = h[0];
+    if (nit) *nit = h[0];
+    if (h[2]) return fail(ctx, PDAC_ERR_NONFINITE, "step: non-finite value in p, ep, rgp, tg, sieg or rlk");
+    if (h[1] > 1) return fail(ctx, PDAC_ERR_EOS, "ftem: caloric equation of state failed");
+    return PDAC_OK;
+}
+
 struct pdac_batch {
     std::vector<pdac_ctx *> m;
-    std::vector<std::vector<int>> work;  // members of each thread
+    std::vector<char> graph;             // member i steps as one CUDA graph launched by the caller's thread
+    std::vector<std::vector<int>> work;  // the other members, by thread
     std::vector<std::thread> th;
     std::mutex mu;
     std::condition_variable go, done;
@@ -2503,9 +2686,18 @@ int pdac_gpu_batch_create(pdac_ctx *const *members, int nmember, int nthreads, p
         for (int j = 0; j < i; ++j)
             if (members[j] == members[i]) return PDAC_ERR_ARG;  // one context stepped twice at once would race
     }
-    int nt = nthreads > 0 ? std::min(nthreads, nmember) : nmember;
     pdac_batch *b = new pdac_batch();
     b->m.assign(members, members + nmember);
+    // semi-implicit members step as whole-step graphs; the others (explicit
+    // solver, implicit-flux modes, cstop, one gas ...) through pdac_gpu_step
+    // on the thread pool
+    b->graph.assign(nmember, 0);
+    int nthread_members = 0;
+    for (int i = 0; i < nmember; ++i) {
+        b->graph[i] = step_graph_eligible(members[i]) ? 1 : 0;
+        nthread_members += b->graph[i] ? 0 : 1;
+    }
+    int nt = nthreads > 0 ? std::min(nthreads, nthread_members) : nthread_members;
     // members take the non-cooperative paths while in the batch (the
     // explicit_iter graph, built with the cooperative wavefront, is rebuilt)
     for (pdac_ctx *c : b->m) {
@@ -2533,6 +2725,7 @@ int pdac_gpu_batch_create(pdac_ctx *const *members, int nmember, int nthreads, p
     std::vector<long> load(nt, 0);
     b->work.assign(nt, {});
     for (int i : order) {
+        if (b->graph[i]) continue;
         int w = (int)(std::min_element(load.begin(), load.end()) - load.begin());
         b->work[w].push_back(i);
         load[w] += b->m[i]->ncell;
@@ -2545,6 +2738,21 @@ int pdac_gpu_batch_create(pdac_ctx *const *members, int nmember, int nthreads, p
 int pdac_gpu_batch_step(pdac_batch *b, int sweep, int *nit, int *status) {
     if (!b) return PDAC_ERR_ARG;
     if (cudaEventRecord(b->t0, b->lead) != cudaSuccess) return PDAC_ERR_CUDA;
+    // the graph members: one launch each from this thread (a member's graph
+    // is built at its first batch step, with its streams idle)
+    std::vector<char> launched(b->m.size(), 0);
+    for (size_t i = 0; i < b->m.size(); ++i) {
+        if (!b->graph[i]) continue;
+        pdac_ctx *c = b->m[i];
+        int s = c->step_exec ? PDAC_OK : build_step_graph(c);
+        if (!s && (cudaStreamWaitEvent(c->stream, b->t0, 0) != cudaSuccess ||
+                   cudaGraphLaunch(c->step_exec, c->stream) != cudaSuccess))
+            s = fail(c, PDAC_ERR_CUDA, "batch: step graph launch failed");
+        cudaEventRecord(b->fin[i], c->stream);
+        b->status[i] = s;
+        b->nit[i] = 0;
+        launched[i] = s == PDAC_OK;
+    }
     {
         std::lock_guard<std::mutex> lk(b->mu);
         b->sweep = sweep;
@@ -2562,6 +2770,8 @@ int pdac_gpu_batch_step(pdac_batch *b, int sweep, int *nit, int *status) {
     float ms = 0;
     if (cudaEventElapsedTime(&ms, b->t0, b->t1) != cudaSuccess) return PDAC_ERR_CUDA;
     b->last_ms = ms;
+    for (size_t i = 0; i < b->m.size(); ++i)
+        if (launched[i]) b->status[i] = step_graph_outcome(b->m[i], &b->nit[i]);
     int first = PDAC_OK;
     for (size_t i = 0; i < b->m.size(); ++i) {
         if (nit) nit[i] = b->nit[i];

@@ -117,7 +117,8 @@ PDAC_FP_FN void log_dd(double x, double &hi, double &lo) {
     double y = frexp_(x, &e);  // y in [0.5, 1)
     y = y * 2.0;
     e = e - 1;  // x = 2^e y, y in [1, 2)
-    const int j = (int)rint_((y - 1.0) * 128.0);
+    int j = (int)rint_((y - 1.0) * 128.0);
+    j = j < 0 ? 0 : (j > 128 ? 128 : j);  // y in [1, 2) gives 0 .. 128; the table has 129 entries
     const double F = 1.0 + (double)j * 0x1.0p-7;
     const double f = y - F;                    // exact: |f| <= 1/256
     const double g = f / F;                    // f/F = g + gl
@@ -139,22 +140,29 @@ PDAC_FP_FN void log_dd(double x, double &hi, double &lo) {
 }
 
 // x^y for the path's arguments: x >= 0 (x < 0 gives NaN unless y is an
-// integer), with the IEEE special cases the path can meet
+// integer), with the IEEE special cases the path can meet.  Written without
+// recursion: a recursive device function leaves the kernel's stack size to
+// the runtime's default limit instead of the size the compiler computes.
 PDAC_FP_FN double pow(double x, double y) {
     if (y == 0.0 || x == 1.0) return 1.0;
     if (x != x || y != y) return x + y;
+    bool negate = false;
     if (x < 0.0) {
         if (y != rint_(y)) return std::numeric_limits<double>::quiet_NaN();
-        const double r = pow(-x, y);
-        return rint_(y * 0.5) * 2.0 == y ? r : -r;
+        negate = rint_(y * 0.5) * 2.0 != y;  // an odd integer power keeps the sign
+        x = -x;
     }
-    if (x == 0.0) return y > 0.0 ? 0.0 : std::numeric_limits<double>::infinity();
-    if (x == std::numeric_limits<double>::infinity()) return y > 0.0 ? x : 0.0;
-    double lh, ll;
-    log_dd(x, lh, ll);
-    const double zh = y * lh;
-    const double zl = fma_(y, lh, -zh) + y * ll;
-    return exp_dd(zh, zl);
+    double r;
+    if (x == 0.0) r = y > 0.0 ? 0.0 : std::numeric_limits<double>::infinity();
+    else if (x == std::numeric_limits<double>::infinity()) r = y > 0.0 ? x : 0.0;
+    else {
+        double lh, ll;
+        log_dd(x, lh, ll);
+        const double zh = y * lh;
+        const double zl = fma_(y, lh, -zh) + y * ll;
+        r = exp_dd(zh, zl);
+    }
+    return negate ? -r : r;
 }
 
 }  // namespace pdac_fp
