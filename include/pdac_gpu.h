@@ -374,9 +374,15 @@ int pdac_gpu_set_tuning(pdac_ctx *ctx, const int *in, int nin);
  * ensemble there is many jobs).  A batch advances many contexts (members:
  * any mix of grids, decks and time integrations, all on the current device)
  * by one time step each, pdac_gpu_step(member, sweep, ...) on every member,
- * with the members' kernels running concurrently on the device: a pool of
- * nthreads host threads (<= 0: one per member) drives the members' own
- * streams.  While in a batch, members run without cooperative launches
+ * with the members' kernels running concurrently on the device.  A member on
+ * the semi-implicit path (time_integration = 0, rungekut = 1, no implicit-
+ * flux modes, cstop unset, more than one gas) takes its whole step as one
+ * CUDA graph -- boundary to ftem, the outer sweep loop as a conditional
+ * node, its outcome copied back once -- launched on its stream by the
+ * calling thread; the other members are driven by a pool of nthreads host
+ * threads (<= 0: one per such member).  Both give the member's results of
+ * pdac_gpu_step, bit for bit; pdac_gpu_phase_times is not updated by a
+ * graph step.  While in a batch, members run without cooperative launches
  * (the small-domain sweep loop and the explicit solver's wavefront take
  * their multi-launch forms, with the same results), so that no two
  * cooperative grids share the device.  The batch does not own the members: create, upload and download
