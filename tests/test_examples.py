@@ -1,5 +1,6 @@
 """The reference's own input decks (its examples/ directory, read in place
-when the reference tree is present; skipped otherwise): every run deck
+from the directory PDAC_REFERENCE_EXAMPLES names; skipped when it is not
+set or does not exist): every run deck
 parses with the reference's namelist and card syntax (list-directed
 records, quoted card names, r*v repeats), the decks whose options are built
 set up, the others are rejected naming the option, and the shock-tube deck
@@ -13,8 +14,9 @@ import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-EXAMPLES = "/root/reference/examples"
-pytestmark = pytest.mark.skipif(not os.path.isdir(EXAMPLES), reason="reference examples not present")
+EXAMPLES = os.environ.get("PDAC_REFERENCE_EXAMPLES", "")
+pytestmark = pytest.mark.skipif(not EXAMPLES or not os.path.isdir(EXAMPLES),
+                                reason="set PDAC_REFERENCE_EXAMPLES to the reference's examples directory")
 
 RUN_DECKS = ["dam_break_1", "jet_Ladenburg", "jet_Lewis", "jet_NASA", "jet_Sommerfeld", "shock_tube_1"]
 
