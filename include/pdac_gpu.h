@@ -156,6 +156,29 @@ typedef struct pdac_cfg {
     const double *p_atm, *t_atm;    /* nz hydrostatic profile (atmosphere.f:160-230) */
     int           nvent;            /* number of vent cells                  */
     const int    *vent_ijk;         /* nvent flat indices of vent cells      */
+
+    /* immersed boundaries over topography (&boundaries immb = 1 with
+     * &topography itp = 1; immb.f, interp.f:321-919, ghost.f:2888-3345).
+     * Built on the host from the topography (the reference's set_forcing,
+     * local_forcing, fill_cells and face_fractions); the arrays are read at
+     * create.  immb = 0 leaves every pointer unused (NULL allowed).         */
+    int           immb;
+    const int    *ib_faces;         /* ncell: the cell's face factors b_e_ ..
+                                       b_s_ as bits (1 E, 2 W, 4 T, 8 B,
+                                       16 N, 32 S; set = 1)                   */
+    const double *ib_ivf;           /* ncell: ivf_, 1 / fluid volume fraction */
+    const int    *ib_num[3];        /* ncell each (x, y, z): numx/numy/numz,
+                                       the cell's 1-based forcing point, 0 none */
+    int           ib_nfp[3];        /* forcing points per axis                */
+    const int    *ib_fp[3];         /* nfp x 6 per axis: i, j, k (1-based),
+                                       interpolation type, and the flat 0-based
+                                       indices of the first and second 3D
+                                       interpolation neighbours (index_q,
+                                       index_qq; -1 where not used)          */
+    const double *ib_nsl[3];        /* nfp x 3 per axis: the no-slip point    */
+    const double *x, *xb, *y, *yb, *z, *zb; /* cell-centre and face coordinates
+                                       (nx, nx, ny, ny, nz, nz), as the
+                                       topography translated them            */
 } pdac_cfg;
 
 /*

@@ -192,6 +192,18 @@ struct Oracle {
     vector<double> vent_fact, vent_fact0;
     int last_nit = 0, eos_fail = 0, ierr = 0;
 
+    // immersed boundaries (immb.f, interp.f:321-919, ghost.f:2888-3345):
+    // the cut-cell face factors and forcing-point tables of pdac_cfg, the
+    // forcing-point velocities of the last boundary pass (nfp x nph per
+    // axis, fptx/y/z(:)%vel) and the filled_cell_2 toggles (fc2)
+    int immb = 0;
+    vector<int> ib_faces;
+    vector<double> ib_ivf;
+    vector<int> ib_num[3], ib_fp[3];
+    vector<double> ib_nsl[3], ib_vel[3];
+    vector<char> fc2;
+    vector<double> xm, xbm, ym, ybm, zm, zbm;  // mesh coordinates, 1-based
+
     // ---- indexing ------------------------------------------------------
     int idx(int i, int j, int k) const {  // 1-based -> flat 0-based
         return (i - 1) + nx * ((j - 1) + ny * (k - 1));
@@ -334,6 +346,8 @@ void rnb2(const Oracle &o, Sten &s, const double *a, int c) {
     s.ee = a[o.nbraw(EE, c)]; s.tt = a[o.nbraw(TT, c)]; s.eet = a[o.nbraw(EET, c)];
     s.ett = a[o.nbraw(ETT, c)]; s.eee = a[o.nbraw(EEE, c)]; s.ttt = a[o.nbraw(TTT, c)];
 }
+#include "pdac_oracle_ib.inc"
+
 void first_nb2(const Oracle &o, Sten &s, const double *a, int c) {
     s.c = a[c]; s.e = a[o.nbrem(E, c)]; s.t = a[o.nbrem(T, c)]; s.w = a[o.nbrem(W, c)]; s.b = a[o.nbrem(B, c)];
 }
@@ -1184,6 +1198,8 @@ void tilde_2d(Oracle &o, double dt) {
             double *fwt = ph == 0 ? o.wgft.data() : &o.wsft[(size_t)(ph - 1) * n];
             rnb2(o, u, U, c);
             rnb2(o, w, Wv, c);
+            ib_mask(o, u, c, 1);  // b_e_ (tilde.f:896-945)
+            ib_mask(o, w, c, 4);  // b_t_
             nb2(o, dens, D, c);
             Sten dsx = interp_x2(o, dens, i);
             Sten dsz = interp_z2(o, dens, k);
@@ -1226,6 +1242,7 @@ void tilde_2d(Oracle &o, double dt) {
         t_ = t_ + (1.0 - alpha) * indzp * 2.0 * epn_t * (o.pn[c] - o.pn[ijkt]);
         o.rwg[c] = o.rwgn[c] + dt * t_;
         double kpgv[PDAC_MAX_NSOLID + 1] = {0};
+        double dugs_c[PDAC_MAX_NSOLID + 1] = {0}, dvgs_c[PDAC_MAX_NSOLID + 1] = {0}, dwgs_c[PDAC_MAX_NSOLID + 1] = {0};
         for (int is = 1; is <= ns; ++is) {
             double usfx = o.S(o.usfe, c, is) - o.S(o.usfe, imjk, is), usfz = o.S(o.usft, c, is) - o.S(o.usft, ijkm, is);
             double wsfx = o.S(o.wsfe, c, is) - o.S(o.wsfe, imjk, is), wsfz = o.S(o.wsft, c, is) - o.S(o.wsft, ijkm, is);
@@ -1254,6 +1271,8 @@ void tilde_2d(Oracle &o, double dt) {
                 kpgv[is] = kdrags(o, dugs, 0.0, dwgs, o.ep[c], o.rgp[c], o.S(o.rlk, c, is), o.mug[c], is);
             else
                 kpgv[is] = sdrag(o, dugs, 0.0, dwgs, o.ep[c], o.rgp[c], o.S(o.rlk, c, is), o.mug[c], is);
+            dugs_c[is] = dugs;
+            dwgs_c[is] = dwgs;
         }
         inter_2d(o, c, kpgv, dt);
         // (1 - alpha) explicit interphase part, tilde.f:597-680; app of the
@@ -1285,6 +1304,7 @@ void tilde_2d(Oracle &o, double dt) {
                 }
             }
         }
+        ib_tilde_forcing(o, c, dt, kpgv, dugs_c, dvgs_c, dwgs_c);  // tilde.f:708-801
     }
 }
 
@@ -1350,23 +1370,25 @@ double calc_res_2d(Oracle &o, int c, double dt) {
     int i, j, k;
     o.ijk_of(c, i, j, k);
     int imjk = o.nbraw(W, c), ijkm = o.nbraw(B, c);
-    double resx = (1.0 * o.rgfe[c] - 1.0 * o.rgfe[imjk]) * o.indx[i] * o.inr[i];
-    double resz = (1.0 * o.rgft[c] - 1.0 * o.rgft[ijkm]) * o.indz[k];
+    const CellFaces b = cell_faces(o, c);
+    double resx = (b.e * o.rgfe[c] - b.w * o.rgfe[imjk]) * o.indx[i] * o.inr[i];
+    double resz = (b.t * o.rgft[c] - b.b * o.rgft[ijkm]) * o.indz[k];
     double resy = 0.0;
-    return o.rgp[c] - o.rgpn[c] + dt * 1.0 * (resx + resy + resz);
+    return o.rgp[c] - o.rgpn[c] + dt * b.ivf * (resx + resy + resz);
 }
 
 void calc_eps_2d(Oracle &o, int c, double dt) {
     int i, j, k;
     o.ijk_of(c, i, j, k);
     int imjk = o.nbraw(W, c), ijkm = o.nbraw(B, c);
+    const CellFaces b = cell_faces(o, c);
     double rls = 0;
     for (int is = 1; is <= o.ns; ++is) {
-        double rlkx = (1.0 * o.S(o.rsfe, c, is) - 1.0 * o.S(o.rsfe, imjk, is)) * o.indx[i] * o.inr[i];
-        double rlkz = (1.0 * o.S(o.rsft, c, is) - 1.0 * o.S(o.rsft, ijkm, is)) * o.indz[k];
+        double rlkx = (b.e * o.S(o.rsfe, c, is) - b.w * o.S(o.rsfe, imjk, is)) * o.indx[i] * o.inr[i];
+        double rlkz = (b.t * o.S(o.rsft, c, is) - b.b * o.S(o.rsft, ijkm, is)) * o.indz[k];
         double rlky = 0.0;
-        double t = o.S(o.rlkn, c, is) - dt * 1.0 * (rlkx + rlky + rlkz);
-        t = t + dt * 1.0 * o.S(o.sink, c, is);
+        double t = o.S(o.rlkn, c, is) - dt * b.ivf * (rlkx + rlky + rlkz);
+        t = t + dt * b.ivf * o.S(o.sink, c, is);
         o.S(o.rlk, c, is) = std::max(0.0, t);
         rls = rls + o.S(o.rlk, c, is) * o.inrl[is];
     }
@@ -1595,15 +1617,16 @@ void ygas_2d(Oracle &o, double dt) {
         int i, j, k;
         o.ijk_of(c, i, j, k);
         int imjk = o.nbraw(W, c), ijkm = o.nbraw(B, c);
+        const CellFaces b = cell_faces(o, c);
         double rgpgc[PDAC_MAX_NGAS + 1], rgpt = 0, yfy = 0;
         for (int ig = 1; ig <= ng; ++ig) {
             double yfw = o.S(o.yfe, imjk, ig), yfb = o.S(o.yft, ijkm, ig);
-            double yfx = 1.0 * o.S(o.yfe, c, ig) - 1.0 * yfw;
-            double yfz = 1.0 * o.S(o.yft, c, ig) - 1.0 * yfb;
+            double yfx = b.e * o.S(o.yfe, c, ig) - b.w * yfw;
+            double yfz = b.t * o.S(o.yft, c, ig) - b.b * yfb;
             rgpgc[ig] = o.S(o.rgpgcn, c, ig);
-            rgpgc[ig] = rgpgc[ig] - 1.0 * dt * o.indx[i] * yfx * o.inr[i];
-            rgpgc[ig] = rgpgc[ig] - 1.0 * dt * 0.0 * yfy;
-            rgpgc[ig] = rgpgc[ig] - 1.0 * dt * o.indz[k] * yfz;
+            rgpgc[ig] = rgpgc[ig] - b.ivf * dt * o.indx[i] * yfx * o.inr[i];
+            rgpgc[ig] = rgpgc[ig] - b.ivf * dt * 0.0 * yfy;
+            rgpgc[ig] = rgpgc[ig] - b.ivf * dt * o.indz[k] * yfz;
             if (rgpgc[ig] < 0.0) rgpgc[ig] = 0.0;
             rgpt = rgpt + rgpgc[ig];
         }
@@ -1688,22 +1711,23 @@ void htilde_2d(Oracle &o, double dt) {
         int i, j, k;
         o.ijk_of(c, i, j, k);
         int imjk = o.nbraw(W, c), ijkm = o.nbraw(B, c);
-        double egfx = 1.0 * o.egfe[c] - 1.0 * o.egfe[imjk];
-        double egfz = 1.0 * o.egft[c] - 1.0 * o.egft[ijkm];
+        const CellFaces b = cell_faces(o, c);
+        double egfx = b.e * o.egfe[c] - b.w * o.egfe[imjk];
+        double egfz = b.t * o.egft[c] - b.b * o.egft[ijkm];
         double egfy = 0.0;
         double flx = dt * o.indx[i] * egfx * o.inr[i] + dt * 0.0 * egfy + dt * o.indz[k] * egfz;
-        flx = flx * 1.0;
+        flx = flx * b.ivf;
         o.rhg[c] = -flx;
         for (int is = 1; is <= ns; ++is) {
             double esfx, esfz;
-            if (o.S(o.rlk, imjk, is) * o.inrl[is] <= 1.0e-9) esfx = 1.0 * o.S(o.esfe, c, is);
-            else esfx = 1.0 * o.S(o.esfe, c, is) - 1.0 * o.S(o.esfe, imjk, is);
-            if (o.S(o.rlk, ijkm, is) * o.inrl[is] <= 1.0e-9) esfz = 1.0 * o.S(o.esft, c, is);
-            else esfz = 1.0 * o.S(o.esft, c, is) - 1.0 * o.S(o.esft, ijkm, is);
+            if (o.S(o.rlk, imjk, is) * o.inrl[is] <= 1.0e-9) esfx = b.e * o.S(o.esfe, c, is);
+            else esfx = b.e * o.S(o.esfe, c, is) - b.w * o.S(o.esfe, imjk, is);
+            if (o.S(o.rlk, ijkm, is) * o.inrl[is] <= 1.0e-9) esfz = b.t * o.S(o.esft, c, is);
+            else esfz = b.t * o.S(o.esft, c, is) - b.b * o.S(o.esft, ijkm, is);
             double esfy = 0.0;
             flx = dt * o.indx[i] * esfx * o.inr[i] + dt * 0.0 * esfy + dt * o.indz[k] * esfz;
-            flx = flx * 1.0;
-            o.S(o.rhs, c, is) = -flx + o.S(o.sink, c, is) * dt * 1.0 * o.S(o.sies, c, is);
+            flx = flx * b.ivf;
+            o.S(o.rhs, c, is) = -flx + o.S(o.sink, c, is) * dt * b.ivf * o.S(o.sies, c, is);
         }
     }
 }
@@ -1723,8 +1747,9 @@ int ftem_2d(Oracle &o, double dt) {
         int ijke = o.nbrem(E, c), ijkw = o.nbrem(W, c), ijkt = o.nbrem(T, c), ijkb = o.nbrem(B, c);
         double indxc = 1.0 / (dx[i] + (dx[i + 1] + dx[i - 1]) * 0.5);
         double indzc = 1.0 / (dz[k] + (dz[k + 1] + dz[k - 1]) * 0.5);
-        double ugc = 0.5 * (1.0 * o.ug[c] + 1.0 * o.ug[imjk]);
-        double wgc = 0.5 * (1.0 * o.wg[c] + 1.0 * o.wg[ijkm]);
+        const CellFaces bf = cell_faces(o, c);
+        double ugc = 0.5 * (bf.e * o.ug[c] + bf.w * o.ug[imjk]);
+        double wgc = 0.5 * (bf.t * o.wg[c] + bf.b * o.wg[ijkm]);
         double dpxyz = 0.0;
         dpxyz = dpxyz + dt * indxc * ugc * (o.p[ijke] - o.p[ijkw]);
         dpxyz = dpxyz + dt * 0.0 * 0.0 * 0.0;
@@ -1921,6 +1946,10 @@ void boundary_2d(Oracle &o, int sweep) {
                     }
                 }
             }
+            continue;
+        }
+        if (ib_cell(o.flag[c])) {  // forcing points, bdry.f:103-204
+            ib_boundary_cell(o, c);
             continue;
         }
         if (!(o.flag[c] == FLUID || o.flag[c] == DOME || o.flag[c] == BL_CELL)) continue;
@@ -2134,6 +2163,15 @@ int pdac_oracle_create(const pdac_cfg *cfg, void **out) {
     int *vl = new int[cfg->nvent > 0 ? cfg->nvent : 1];
     for (int q = 0; q < cfg->nvent; ++q) vl[q] = cfg->vent_ijk[q];
     o->cfg.vent_ijk = vl;
+    o->cfg.ib_faces = nullptr; o->cfg.ib_ivf = nullptr;
+    for (int a = 0; a < 3; ++a) { o->cfg.ib_num[a] = nullptr; o->cfg.ib_fp[a] = nullptr; o->cfg.ib_nsl[a] = nullptr; }
+    o->cfg.x = o->cfg.xb = o->cfg.y = o->cfg.yb = o->cfg.z = o->cfg.zb = nullptr;
+    ib_setup(*o, cfg);
+    if (ib_check(*o) != PDAC_OK) {
+        delete[] vl;
+        delete o;
+        return PDAC_ERR_CONFIG;
+    }
     setc(*o);
     build_tables(*o);
     if (o->d3) build_tables3(*o);

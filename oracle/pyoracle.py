@@ -24,7 +24,7 @@ _lib = None
 
 def build(force=False):
     """Compile the oracle with its Makefile (g++ only; seconds)."""
-    srcs = ("pdac_oracle.cpp", "pdac_oracle3d.inc", "pdac_oracle_rk3.inc", "pdac_oracle_les.inc",
+    srcs = ("pdac_oracle.cpp", "pdac_oracle3d.inc", "pdac_oracle_rk3.inc", "pdac_oracle_les.inc", "pdac_oracle_ib.inc",
             "../pdac_b200/csrc/fpmath.h", "../pdac_b200/csrc/fpmath_tables.h")
     if force or not os.path.exists(LIB_PATH) or \
             os.path.getmtime(LIB_PATH) < max(os.path.getmtime(os.path.join(HERE, f)) for f in srcs):

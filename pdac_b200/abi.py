@@ -65,6 +65,9 @@ class PdacCfg(C.Structure):
         ("dx", _dp), ("dy", _dp), ("dz", _dp), ("flag", _ip),
         ("p_atm", _dp), ("t_atm", _dp),
         ("nvent", C.c_int), ("vent_ijk", _ip),
+        ("immb", C.c_int), ("ib_faces", _ip), ("ib_ivf", _dp),
+        ("ib_num", _ip * 3), ("ib_nfp", C.c_int * 3), ("ib_fp", _ip * 3), ("ib_nsl", _dp * 3),
+        ("x", _dp), ("xb", _dp), ("y", _dp), ("yb", _dp), ("z", _dp), ("zb", _dp),
     ]
 
 

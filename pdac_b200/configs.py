@@ -221,3 +221,110 @@ def small_3d_opt(optimization=2, **kw):
     d = small_3d(**kw)
     d.set("numeric", optimization=optimization)
     return d
+
+
+# ---- topography and immersed boundaries ------------------------------------
+def write_hill_profile(path, x_end, x_hill, height, sigma, dx=5.0):
+    """A 2D topographic profile (topo.f:306-348 layout): one Gaussian hill
+    of the given height and width centred at x_hill on flat ground at 0,
+    sampled every dx from -dx to x_end + dx."""
+    import numpy as np
+
+    from .topography import write_profile
+    xs = np.arange(-dx, x_end + 2 * dx, dx)
+    zs = height * np.exp(-0.5 * ((xs - x_hill) / sigma) ** 2)
+    write_profile(path, xs, zs)
+    return path
+
+
+def write_hills_dem(path, nx, ny, dxy, n_hills=8, seed=0, h_range=(100.0, 600.0), s_range=(300.0, 1200.0),
+                    vent_xy=None, vent_flat=0.0, dem_cell=None, margin=3):
+    """A seeded ASCII DEM (the layout read_dem_ascii reads) that is the sum
+    of n_hills Gaussian hills with heights drawn from h_range and widths
+    from s_range, centred at uniformly drawn points of the nx x ny mesh of
+    spacing dxy (mesh coordinates: cell centres at (i - 1.5) dxy).  With
+    vent_flat > 0 the ground is flat (at 0) within that radius of vent_xy
+    and rises to the full hills at twice the radius (the flattened crater
+    floor the vent sits on).  The DEM covers
+    the mesh with `margin` DEM cells to spare on every side."""
+    import numpy as np
+
+    from .topography import write_dem_ascii
+    rng = np.random.default_rng(seed)
+    dem_cell = dem_cell or dxy
+    lx, ly = nx * dxy, ny * dxy
+    x0, y0 = -dxy - margin * dem_cell, -dxy - margin * dem_cell
+    nxd = int(np.ceil((lx + 2 * dxy + 2 * margin * dem_cell) / dem_cell)) + 1
+    nyd = int(np.ceil((ly + 2 * dxy + 2 * margin * dem_cell) / dem_cell)) + 1
+    xs = x0 + dem_cell * np.arange(nxd)
+    ys = y0 + dem_cell * np.arange(nyd)
+    X, Y = np.meshgrid(xs, ys, indexing="ij")
+    Z = np.zeros_like(X)
+    for _ in range(n_hills):
+        h = rng.uniform(*h_range)
+        s = rng.uniform(*s_range)
+        cx, cy = rng.uniform(0.0, lx), rng.uniform(0.0, ly)
+        Z += h * np.exp(-0.5 * ((X - cx) ** 2 + (Y - cy) ** 2) / s ** 2)
+    if vent_flat > 0.0 and vent_xy is not None:
+        # a crater floor at ground level within vent_flat of the vent, rising
+        # smoothly to the full hills at twice that distance
+        r = np.sqrt((X - vent_xy[0]) ** 2 + (Y - vent_xy[1]) ** 2)
+        t = np.clip((r - vent_flat) / vent_flat, 0.0, 1.0)
+        Z *= t * t * (3.0 - 2.0 * t)
+    write_dem_ascii(path, x0, y0, dem_cell, Z)
+    return path
+
+
+def plume_2d_topo(dem_file, immb=1, nx=128, nz=192, **kw):
+    """The 2D plume over a topographic profile read from dem_file (itp = 1),
+    with immersed boundaries (immb = 1, the default) or the staircase of
+    no-slip cells (immb = 0)."""
+    d = plume_2d(nx=nx, nz=nz, **kw)
+    d.set("topography", itp=1, dem_file=str(dem_file))
+    d.set("boundaries", immb=immb)
+    return d
+
+
+def small_2d_topo(tmpdir, immb=1, nx=24, nz=24, height=60.0, **kw):
+    """A 24 x 24 (10 m) 2D plume with a 60 m Gaussian hill 150 m from the
+    axis, the profile written under tmpdir."""
+    import os
+    kw.setdefault("vent_radius", 20.0)
+    path = write_hill_profile(os.path.join(str(tmpdir), "hill.dat"), x_end=nx * 10.0, x_hill=150.0,
+                              height=height, sigma=40.0)
+    return plume_2d_topo(path, immb=immb, nx=nx, nz=nz, **kw)
+
+
+def plume_3d_topo(dem_file, immb=1, nx=384, ny=384, nz=256, dxyz=15.0, dt=0.01, w_gas=120.0, t_gas=1100.0,
+                  diameters=None, ep_total=0.03, density=2500.0, **kw):
+    """The large 3D workload over synthetic topography: the DEM in dem_file
+    (write_hills_dem), immersed boundaries, five classes from 20 to 2000 um
+    (log-spaced, 2500 kg/m3) sharing a total volume fraction of 0.03, and
+    the vent (5 x 5 cells at the centre) at 1100 K and 120 m/s."""
+    import numpy as np
+    if diameters is None:
+        diameters = tuple(float(v) for v in np.geomspace(20.0, 2000.0, 5))
+    ns = len(diameters)
+    d = plume_3d(nx=nx, ny=ny, nz=nz, dxyz=dxyz, dt=dt, w_gas=w_gas, t_gas=t_gas, diameters=diameters,
+                 density=density, ep_solid=tuple([ep_total / ns] * ns), **kw)
+    d.set("topography", itp=1, dem_file=str(dem_file), cellsize=dxyz, filtersize=2 * dxyz)
+    d.set("boundaries", immb=immb)
+    # the DEM is given in mesh coordinates: the mesh centre cell stays where it is
+    d.set("mesh", center_x=(nx // 2 - 1.5 + 1) * dxyz, center_y=(ny // 2 - 1.5 + 1) * dxyz)
+    return d
+
+
+def small_3d_topo(tmpdir, immb=1, nx=16, ny=14, nz=14, dxyz=20.0, seed=3, **kw):
+    """A 16 x 14 x 14 (20 m) 3D plume over three seeded hills of 40-100 m
+    with a flat crater floor around the 2 x 2 vent."""
+    import os
+    kw.setdefault("vent_cells", 2)
+    cx = (nx // 2 - 0.5) * dxyz
+    cy = (ny // 2 - 0.5) * dxyz
+    path = write_hills_dem(os.path.join(str(tmpdir), "hills.asc"), nx, ny, dxyz, n_hills=3, seed=seed,
+                           h_range=(40.0, 100.0), s_range=(40.0, 90.0), vent_xy=(cx, cy), vent_flat=3 * dxyz)
+    d = plume_3d(nx=nx, ny=ny, nz=nz, dxyz=dxyz, **kw)
+    d.set("topography", itp=1, dem_file=path, cellsize=dxyz / 2, filtersize=dxyz / 4)
+    d.set("boundaries", immb=immb)
+    d.set("mesh", center_x=(nx // 2 - 1.5 + 1) * dxyz, center_y=(ny // 2 - 1.5 + 1) * dxyz)
+    return d

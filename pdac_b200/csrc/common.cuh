@@ -68,7 +68,34 @@ struct Prm {
     unsigned long long mnx, mny;
     const double *p_atm, *t_atm;
     const int *flag;
+    // immersed boundaries (immb.f, ghost.f:2888-3345); immb = 0: none, and
+    // every face factor below reads as 1
+    int immb;
+    const int *ib_faces;     // per cell: the open faces b_e_ .. b_s_ as bits (1 E, 2 W, 4 T, 8 B, 16 N, 32 S)
+    const double *ib_ivf;    // per cell: ivf_, 1 / fluid volume fraction
+    const int *ib_num[3];    // per cell: numx, numy, numz (1-based forcing point, 0 none)
+    const double *ib_vel[3]; // per forcing point: the nph velocities of the last boundary pass
 };
+
+// The face factors of one cell (faces, immb.f:1263-1278); all 1 without
+// immersed boundaries, as face_init sets them (ghost.f:3323-3344).
+struct CellFaces {
+    double e, w, n, s, t, b, ivf;
+};
+__device__ __forceinline__ CellFaces cell_faces(const Prm &P, int c) {
+    CellFaces f = {1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0};
+    if (P.immb) {
+        const int m = __ldg(P.ib_faces + c);
+        f.e = (m & 1) ? 1.0 : 0.0;
+        f.w = (m & 2) ? 1.0 : 0.0;
+        f.t = (m & 4) ? 1.0 : 0.0;
+        f.b = (m & 8) ? 1.0 : 0.0;
+        f.n = (m & 16) ? 1.0 : 0.0;
+        f.s = (m & 32) ? 1.0 : 0.0;
+        f.ivf = __ldg(P.ib_ivf + c);
+    }
+    return f;
+}
 
 // The metric arrays in the arithmetic type of a flux pass.
 template <typename Real> struct Met;

@@ -24,6 +24,7 @@
 #include "les.cuh"
 #include "sink.cuh"
 #include "mixture.cuh"
+#include "ib.cuh"
 
 using namespace pdac;
 
@@ -111,6 +112,19 @@ struct pdac_ctx {
     // ring mask
     pdac::Sink S{};
     double *d_sinkbuf = nullptr;
+    // immersed boundaries: the forcing-point tables and mesh coordinates
+    // (d_ibint, d_ibdbl) and the state they carry from one boundary pass to
+    // the next (d_ibstate: forcing-point velocities, then the filled_cell_2
+    // toggles, ibstate_doubles in all)
+    pdac::IbDev IB{};
+    int *d_ibint = nullptr;
+    double *d_ibdbl = nullptr, *d_ibstate = nullptr;
+    size_t ibstate_doubles = 0;
+    // the ordered boundary pass (ib.cuh): the boundary cells sorted by level
+    // and the start of every level (empty when one thread per cell gives the
+    // reference's result)
+    int *d_bitems = nullptr;
+    std::vector<int> blevel;
     int *d_ring = nullptr;
     pdac::Wave W{};
     // shared-memory tiled 3D stencil passes: tile shape (index into
@@ -149,6 +163,9 @@ cudaError_t launch_mom_tile_t(const pdac::Prm &P, const pdac::Fld &F, int nph, i
 template <typename Real>
 cudaError_t launch_mom_tile(const pdac::Prm &P, const pdac::Fld &F, int nph, int shape, int kchunk, cudaStream_t st,
                             bool set_attr = false) {
+    // the tiled pass reads its stencils from shared memory and does not
+    // apply the immersed-boundary velocity masks: immersed boundaries use form 0
+    if (P.immb && !set_attr) shape = 0;
     switch (shape) {
         case 1: return launch_mom_tile_t<32, 4, Real>(P, F, nph, kchunk, st, set_attr);
         case 2: return launch_mom_tile_t<32, 8, Real>(P, F, nph, kchunk, st, set_attr);
@@ -258,6 +275,67 @@ void set_constants(pdac_ctx *ctx) {
         }
 }
 
+// immersed boundaries (pdac_cfg immb = 1): the checks the kernels rely on
+// (every index the interpolations and fills reach lies in the mesh) and
+// those the reference makes as it runs (bdry.f:111-113: every immersed or
+// filled cell is a forcing point; interp.f:520-560: the external points of
+// types 21 and 22 lie on the side their interpolation assumes)
+int validate_ib(const pdac_cfg *c, std::string &why) {
+    if (!c->immb) return 0;
+    const bool d3 = c->job_type == 3;
+    const int nx = c->nx, ny = d3 ? c->ny : 1, nz = c->nz;
+    const long n = (long)nx * ny * nz;
+    if (c->time_integration != 0) { why = "immersed boundaries with the explicit solver are not supported"; return 1; }
+    if (!c->ib_faces || !c->ib_ivf || !c->x || !c->xb || !c->z || !c->zb || (d3 && (!c->y || !c->yb))) {
+        why = "immb: the face factors, ivf and the mesh coordinates are required"; return 1;
+    }
+    for (int a = 0; a < 3; ++a) {
+        if (a == 1 && !d3) continue;
+        const int nfp = c->ib_nfp[a];
+        if (nfp < 0 || !c->ib_num[a] || (nfp > 0 && (!c->ib_fp[a] || !c->ib_nsl[a]))) {
+            why = "immb: forcing-point tables missing"; return 1;
+        }
+        for (long m = 0; m < n; ++m)
+            if (c->ib_num[a][m] < 0 || c->ib_num[a][m] > nfp) { why = "immb: forcing-point number out of range"; return 1; }
+        for (int f = 0; f < nfp; ++f) {
+            const int *fp = c->ib_fp[a] + (size_t)6 * f;
+            const int i = fp[0], j = fp[1], k = fp[2], kind = fp[3];
+            if (i < 1 || i > nx || k < 1 || k > nz || (d3 && (j < 1 || j > ny))) {
+                why = "immb: forcing point outside the mesh"; return 1;
+            }
+            if (!d3) {
+                const double nsx = c->ib_nsl[a][(size_t)3 * f];
+                const double cxi = (a == 0 ? c->xb : c->x)[i - 1];
+                if ((kind == 22 && !(nsx < cxi)) || (kind == 21 && !(nsx > cxi))) {
+                    why = "immb: control fpoint (interp.f:520-560)"; return 1;
+                }
+            } else {
+                int di = 0, dj = 0, dk = 0;
+                const int DI[9] = {0, -1, -1, 0, 1, 1, 1, 0, -1}, DJ[9] = {0, 0, -1, -1, -1, 0, 1, 1, 1};
+                if (kind == 0 || kind == 20) dk = 1;
+                else if (kind >= 1 && kind <= 8) { di = DI[kind]; dj = DJ[kind]; }
+                else if (kind >= 21 && kind <= 28) { di = DI[kind - 20]; dj = DJ[kind - 20]; }
+                else { why = "immb: 3D forcing-point type out of range"; return 1; }
+                auto flat = [&](int ii, int jj, int kk) -> long {
+                    if (ii < 1 || ii > nx || jj < 1 || jj > ny || kk < 1 || kk > nz) return -1;
+                    return (ii - 1) + (long)nx * ((jj - 1) + (long)ny * (kk - 1));
+                };
+                const long q = flat(i + di, j + dj, k + dk), qq = flat(i + 2 * di, j + 2 * dj, k + 2 * dk);
+                if (q < 0 || fp[4] != q) { why = "immb: index_q of a forcing point"; return 1; }
+                if ((kind % 2 != 0 || kind == 0) && (qq < 0 || fp[5] != qq)) { why = "immb: index_qq of a forcing point"; return 1; }
+            }
+        }
+    }
+    for (long m = 0; m < n; ++m) {
+        const int f = c->flag[m];
+        if ((f == IMMB || f == FILLED1 || f == FILLED2) && !c->ib_num[0][m] && !(d3 && c->ib_num[1][m]) &&
+            !c->ib_num[2][m]) {
+            why = "immb: an immersed or filled cell is not a forcing point (bdry.f:111-113)"; return 1;
+        }
+    }
+    return 0;
+}
+
 int validate(const pdac_cfg *c, std::string &why) {
     if (c->job_type != 2 && c->job_type != 3) { why = "job_type must be 2 (2D) or 3 (3D)"; return 1; }
     if (c->nx < 5 || c->nz < 5) { why = "nx and nz must be >= 5"; return 1; }
@@ -295,7 +373,100 @@ int validate(const pdac_cfg *c, std::string &why) {
         why = "time_integration = 1 needs pmodel 1 or 2 (explicit_solver.f:632-642)";
         return 1;
     }
-    return 0;
+    return validate_ib(c, why);
+}
+
+// The boundary cells of the ordered boundary pass (ib.cuh) in levels.  A
+// fluid cell next to a wall or an open boundary reads itself and, along
+// every such direction, the neighbour there and the first and second
+// neighbours on the opposite side, and writes itself and that neighbour
+// (bdry.f:208-726); a forcing point reads the cells its interpolation uses
+// and writes itself and the neighbour hn may fill (bdry.f:103-204).  Cells
+// are taken in index order; each goes one level after the last earlier cell
+// that writes what it reads or touches what it writes.  Returns the cells
+// sorted by level (index order within a level) and the level starts; no
+// levels at all when every cell falls in the first level and there are no
+// forcing points (one thread per cell then gives the same result).
+void boundary_levels(const pdac_cfg *c, std::vector<int> &items, std::vector<int> &starts) {
+    items.clear();
+    starts.clear();
+    const bool d3 = c->job_type == 3;
+    const int nx = c->nx, ny = d3 ? c->ny : 1, nz = c->nz;
+    const long n = (long)nx * ny * nz;
+    const int *fl = c->flag;
+    auto acts = [](int f) { return f == SLIP || f == NOSLIP || f == FREE_IO || f == ZERO_GRAD; };
+    auto at = [&](int i, int j, int k) -> int {
+        i = std::min(std::max(i, 1), nx); j = std::min(std::max(j, 1), ny); k = std::min(std::max(k, 1), nz);
+        return (i - 1) + nx * ((j - 1) + ny * (k - 1));
+    };
+    std::vector<int> lw(n, 0), lt(n, 0);  // last level writing / touching each cell
+    std::vector<std::pair<int, int>> lev;  // (level, cell)
+    bool any_ib = false;
+    int maxl = 0;
+    std::vector<int> T, W;
+    for (long m = 0; m < n; ++m) {
+        const int f = fl[m];
+        const int i = (int)(m % nx) + 1, j = (int)((m / nx) % ny) + 1, k = (int)(m / ((long)nx * ny)) + 1;
+        T.assign(1, (int)m);
+        W.assign(1, (int)m);
+        if (c->immb && (f == IMMB || f == FILLED1 || f == FILLED2)) {
+            any_ib = true;
+            for (int a = 0; a < 3; ++a) {
+                if (a == 1 && !d3) continue;
+                const int num = c->ib_num[a][m];
+                if (!num) continue;
+                const int *fp = c->ib_fp[a] + (size_t)6 * (num - 1);
+                if (d3) {
+                    T.push_back(fp[4]);
+                    if (fp[5] >= 0) T.push_back(fp[5]);
+                } else {
+                    for (int di : {-2, -1, 1, 2}) T.push_back(at(i + di, 1, k));
+                    for (int dk : {1, 2}) T.push_back(at(i, 1, k + dk));
+                    T.push_back(at(i + 1, 1, k + 1));
+                    T.push_back(at(i - 1, 1, k + 1));
+                }
+                if (fp[3] >= 20) {  // hn on the neighbour along the axis
+                    const int nb = a == 0 ? at(i + 1, j, k) : (a == 1 ? at(i, j + 1, k) : at(i, j, k + 1));
+                    T.push_back(nb);
+                    W.push_back(nb);
+                }
+            }
+        } else if (f == FLUID || f == DOME || f == BL_CELL) {
+            const int dirs[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 0, 1}, {0, 0, -1}, {0, 1, 0}, {0, -1, 0}};
+            bool any = false;
+            for (int d = 0; d < (d3 ? 6 : 4); ++d) {
+                const int di = dirs[d][0], dj = dirs[d][1], dk = dirs[d][2];
+                const int nb = at(i + di, j + dj, k + dk);
+                if (!acts(fl[nb])) continue;
+                any = true;
+                T.push_back(nb);
+                T.push_back(at(i - di, j - dj, k - dk));
+                T.push_back(at(i - 2 * di, j - 2 * dj, k - 2 * dk));
+                W.push_back(nb);
+            }
+            if (!any) continue;
+        } else {
+            continue;
+        }
+        int L = 0;
+        for (int t : T) L = std::max(L, lw[t]);
+        for (int w : W) L = std::max(L, lt[w]);
+        ++L;
+        for (int t : T) lt[t] = std::max(lt[t], L);
+        for (int w : W) { lw[w] = std::max(lw[w], L); lt[w] = std::max(lt[w], L); }
+        lev.push_back({L, (int)m});
+        maxl = std::max(maxl, L);
+    }
+    if (maxl <= 1 && !any_ib) return;
+    std::stable_sort(lev.begin(), lev.end(), [](const std::pair<int, int> &a, const std::pair<int, int> &b) {
+        return a.first < b.first;
+    });
+    int cur = 0;
+    for (size_t q = 0; q < lev.size(); ++q) {
+        while (cur < lev[q].first) { starts.push_back((int)q); ++cur; }
+        items.push_back(lev[q].second);
+    }
+    starts.push_back((int)lev.size());
 }
 
 // The records of the explicit solver's gas-enthalpy wavefront (fixed by the
@@ -574,6 +745,81 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     CK(cudaMalloc(&ctx->d_flag, n * sizeof(int)));
     CK(cudaMemcpy(ctx->d_flag, cfg->flag, n * sizeof(int), cudaMemcpyHostToDevice));
     P.flag = ctx->d_flag;
+    // immersed boundaries: the tables and coordinates (read-only) and the
+    // state the boundary pass hands to tilde and to the next pass
+    P.immb = cfg->immb ? 1 : 0;
+    if (P.immb) {
+        const int nfp[3] = {cfg->ib_nfp[0], ctx->d3 ? cfg->ib_nfp[1] : 0, cfg->ib_nfp[2]};
+        std::vector<int> hint((size_t)4 * n + (size_t)6 * (nfp[0] + nfp[1] + nfp[2]), 0);
+        std::copy(cfg->ib_faces, cfg->ib_faces + n, hint.begin());
+        size_t io = (size_t)n;
+        size_t inum[3], ifp[3];
+        for (int a = 0; a < 3; ++a) {
+            inum[a] = io;
+            if (nfp[a] > 0 || cfg->ib_num[a]) {
+                if (a != 1 || ctx->d3) std::copy(cfg->ib_num[a], cfg->ib_num[a] + n, hint.begin() + io);
+            }
+            io += n;
+        }
+        for (int a = 0; a < 3; ++a) {
+            ifp[a] = io;
+            if (nfp[a] > 0) std::copy(cfg->ib_fp[a], cfg->ib_fp[a] + (size_t)6 * nfp[a], hint.begin() + io);
+            io += (size_t)6 * nfp[a];
+        }
+        const int lens[6] = {ctx->nx, ctx->nx, ctx->ny, ctx->ny, ctx->nz, ctx->nz};
+        const double *srcs[6] = {cfg->x, cfg->xb, ctx->d3 ? cfg->y : nullptr, ctx->d3 ? cfg->yb : nullptr, cfg->z, cfg->zb};
+        size_t nd = (size_t)n + 3 * ((size_t)nfp[0] + nfp[1] + nfp[2]);
+        for (int q = 0; q < 6; ++q) nd += lens[q] + 5;
+        std::vector<double> hdbl(nd, 0.0);
+        std::copy(cfg->ib_ivf, cfg->ib_ivf + n, hdbl.begin());
+        size_t dofs = (size_t)n, dnsl[3], dcrd[6];
+        for (int a = 0; a < 3; ++a) {
+            dnsl[a] = dofs;
+            if (nfp[a] > 0) std::copy(cfg->ib_nsl[a], cfg->ib_nsl[a] + (size_t)3 * nfp[a], hdbl.begin() + dofs);
+            dofs += (size_t)3 * nfp[a];
+        }
+        for (int q = 0; q < 6; ++q) {  // 1-based, two cells of padding: a[q + 1]
+            dcrd[q] = dofs;
+            const int m = lens[q];
+            double *d = hdbl.data() + dofs;
+            if (srcs[q]) {
+                for (int t = 1; t <= m; ++t) d[t + 1] = srcs[q][t - 1];
+                d[0] = d[1] = d[2];
+                d[m + 3] = d[m + 4] = d[m + 2];
+            }
+            dofs += m + 5;
+        }
+        CK(cudaMalloc(&ctx->d_ibint, hint.size() * sizeof(int)));
+        CK(cudaMemcpy(ctx->d_ibint, hint.data(), hint.size() * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMalloc(&ctx->d_ibdbl, hdbl.size() * sizeof(double)));
+        CK(cudaMemcpy(ctx->d_ibdbl, hdbl.data(), hdbl.size() * sizeof(double), cudaMemcpyHostToDevice));
+        ctx->ibstate_doubles = (size_t)ctx->nph * (nfp[0] + nfp[1] + nfp[2]) + (size_t)n;
+        CK(cudaMalloc(&ctx->d_ibstate, ctx->ibstate_doubles * sizeof(double)));
+        CK(cudaMemset(ctx->d_ibstate, 0, ctx->ibstate_doubles * sizeof(double)));
+        P.ib_faces = ctx->d_ibint;
+        P.ib_ivf = ctx->d_ibdbl;
+        size_t vo = 0;
+        for (int a = 0; a < 3; ++a) {
+            P.ib_num[a] = ctx->d_ibint + inum[a];
+            ctx->IB.fp[a] = ctx->d_ibint + ifp[a];
+            ctx->IB.nsl[a] = ctx->d_ibdbl + dnsl[a];
+            ctx->IB.vel[a] = ctx->d_ibstate + vo;
+            P.ib_vel[a] = ctx->IB.vel[a];
+            vo += (size_t)ctx->nph * nfp[a];
+        }
+        ctx->IB.fc2 = ctx->d_ibstate + vo;
+        ctx->IB.x = ctx->d_ibdbl + dcrd[0]; ctx->IB.xb = ctx->d_ibdbl + dcrd[1];
+        ctx->IB.y = ctx->d_ibdbl + dcrd[2]; ctx->IB.yb = ctx->d_ibdbl + dcrd[3];
+        ctx->IB.z = ctx->d_ibdbl + dcrd[4]; ctx->IB.zb = ctx->d_ibdbl + dcrd[5];
+    }
+    {  // the ordered boundary pass, where cells' boundary updates meet
+        std::vector<int> items;
+        boundary_levels(cfg, items, ctx->blevel);
+        if (!items.empty()) {
+            CK(cudaMalloc(&ctx->d_bitems, items.size() * sizeof(int)));
+            CK(cudaMemcpy(ctx->d_bitems, items.data(), items.size() * sizeof(int), cudaMemcpyHostToDevice));
+        }
+    }
     ctx->nvent = cfg->nvent;
     int nv = std::max(1, cfg->nvent);
     CK(cudaMalloc(&ctx->d_vent, nv * sizeof(int)));
@@ -789,6 +1035,10 @@ int pdac_gpu_destroy(pdac_ctx *ctx) {
     cudaFree(ctx->d_ring);
     cudaFree(ctx->d_wave_idx);
     cudaFree(ctx->d_wave_rec);
+    cudaFree(ctx->d_ibint);
+    cudaFree(ctx->d_ibdbl);
+    cudaFree(ctx->d_ibstate);
+    cudaFree(ctx->d_bitems);
     cudaFreeHost(ctx->h_counters);
     for (auto &e : ctx->ev) cudaEventDestroy(e);
     for (auto &e : ctx->cev) cudaEventDestroy(e);
@@ -914,9 +1164,19 @@ int pdac_gpu_download_state(pdac_ctx *ctx, pdac_state_view *s) { return xfer_sta
 static int enqueue_boundary(pdac_ctx *ctx, cudaStream_t st) {
     if (ctx->nvent > 0 && ctx->cfg.irand >= 1)
         pdac::k_vent<<<blocks(ctx->nvent), TPB, 0, st>>>(ctx->P, ctx->F, ctx->d_vent, ctx->nvent, ctx->d_vfact, ctx->d_vfact0), ctx->launches++;
-    if (ctx->d3) pdac::k_boundary3d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F);
-    else pdac::k_boundary2d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F);
-    ctx->launches++;
+    if (!ctx->blevel.empty()) {  // in levels (ib.cuh)
+        for (size_t L = 0; L + 1 < ctx->blevel.size(); ++L) {
+            const int lo = ctx->blevel[L], hi = ctx->blevel[L + 1];
+            if (hi <= lo) continue;
+            if (ctx->d3) pdac::k_boundary_items<3><<<blocks(hi - lo), TPB, 0, st>>>(ctx->P, ctx->F, ctx->IB, ctx->d_bitems, lo, hi);
+            else pdac::k_boundary_items<2><<<blocks(hi - lo), TPB, 0, st>>>(ctx->P, ctx->F, ctx->IB, ctx->d_bitems, lo, hi);
+            ctx->launches++;
+        }
+    } else {
+        if (ctx->d3) pdac::k_boundary3d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F);
+        else pdac::k_boundary2d<<<blocks(ctx->ncell), TPB, 0, st>>>(ctx->P, ctx->F);
+        ctx->launches++;
+    }
     if (ctx->S.ntr > 0) {
         const long nt = (long)ctx->S.ntr * ctx->ns;
         if (ctx->d3) pdac::k_sink<3><<<blocks(nt), TPB, 0, st>>>(ctx->P, ctx->F, ctx->S, ctx->cfg.dt);
@@ -1947,7 +2207,8 @@ int pdac_gpu_autotune(pdac_ctx *ctx, const char *cache_path, int *out, int nout)
     const bool semi = ctx->ti == 0;
     double *snap = nullptr;
     size_t nv = std::max(ctx->nvent, 1), nm = ctx->S.ntr > 0 ? (size_t)2 * ctx->S.ntr * ctx->ns : 0;
-    const size_t snap_doubles = ctx->arena_doubles + 2 * nv + nm;
+    const size_t nib = ctx->ibstate_doubles;
+    const size_t snap_doubles = ctx->arena_doubles + 2 * nv + nm + nib;
     if (status == PDAC_OK && semi && cudaMalloc(&snap, snap_doubles * sizeof(double)) != cudaSuccess) {
         cudaGetLastError();
         snap = nullptr;
@@ -1963,6 +2224,7 @@ int pdac_gpu_autotune(pdac_ctx *ctx, const char *cache_path, int *out, int nout)
             CK(cp(ctx->d_vfact, s1, nv));
             CK(cp(ctx->d_vfact0, s2, nv));
             if (nm) CK(cp(ctx->d_sinkbuf, s3, nm));
+            if (nib) CK(cp(ctx->d_ibstate, s3 + nm, nib));
             return PDAC_OK;
         };
         // statistics and the last iter's count are the caller's, not the tuner's

@@ -278,11 +278,12 @@ __device__ __forceinline__ void inner_team_run(const Prm &P, const Fld &F, doubl
         const double rx = D == 2 ? P.inr[i] : 1.0;
         const double idx_i = P.indx[i], idz_k = P.indz[k], idy_j = D == 3 ? P.indy[j] : 0.0;
         const double rgpn_c = F.rgpn[c];
+        const CellFaces bf = cell_faces(P, c);  // faces, iter.f:259
         auto resid = [&](double fe, double fw, double fn, double fs, double ft, double fb, double rgpc) {
-            double resx = (1.0 * fe - 1.0 * fw) * idx_i * rx;
-            double resz = (1.0 * ft - 1.0 * fb) * idz_k;
-            double resy = D == 3 ? (1.0 * fn - 1.0 * fs) * idy_j : 0.0;
-            return rgpc - rgpn_c + dt * 1.0 * (resx + resy + resz);
+            double resx = (bf.e * fe - bf.w * fw) * idx_i * rx;
+            double resz = (bf.t * ft - bf.b * fb) * idz_k;
+            double resy = D == 3 ? (bf.n * fn - bf.s * fs) * idy_j : 0.0;
+            return rgpc - rgpn_c + dt * bf.ivf * (resx + resy + resz);
         };
         double dg;  // calc_res of the stored state (raw W/S/B neighbours)
         if (D == 3) {
@@ -333,11 +334,11 @@ __device__ __forceinline__ void inner_team_run(const Prm &P, const Fld &F, doubl
                 double fB = __shfl_sync(tmask, flux[is], lB), fT = __shfl_sync(tmask, flux[is], lT);
                 double fS = 0, fN = 0;
                 if (D == 3) { fS = __shfl_sync(tmask, flux[is], lS); fN = __shfl_sync(tmask, flux[is], lN); }
-                double rlkx = (1.0 * fE - 1.0 * fW) * idx_i * rx;
-                double rlkz = (1.0 * fT - 1.0 * fB) * idz_k;
-                double rlky = D == 3 ? (1.0 * fN - 1.0 * fS) * idy_j : 0.0;
-                double t = rlkn[is - 1] - dt * 1.0 * (rlkx + rlky + rlkz);
-                t = t + dt * 1.0 * sink[is - 1];
+                double rlkx = (bf.e * fE - bf.w * fW) * idx_i * rx;
+                double rlkz = (bf.t * fT - bf.b * fB) * idz_k;
+                double rlky = D == 3 ? (bf.n * fN - bf.s * fS) * idy_j : 0.0;
+                double t = rlkn[is - 1] - dt * bf.ivf * (rlkx + rlky + rlkz);
+                t = t + dt * bf.ivf * sink[is - 1];
                 double v = fmax(0.0, t);
                 rlk[is - 1] = v;
                 rls = rls + v * P.inrl[is];

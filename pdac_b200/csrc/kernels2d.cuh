@@ -96,9 +96,7 @@ __device__ void zerograd_d(const Prm &P, const Fld &F, int n2, int n1) {
     F.p[n2] = F.p[n1];
 }
 
-__global__ void k_boundary2d(Prm P, Fld F) {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= P.ncell) return;
+__device__ void boundary_cell2d(const Prm &P, const Fld &F, int c) {
     int f0 = P.flag[c];
     if (!(f0 == FLUID || f0 == DOME || f0 == BL_CELL)) return;
     int i = c % P.nx + 1, k = c / P.nx + 1;
@@ -229,6 +227,13 @@ __global__ void k_boundary2d(Prm P, Fld F) {
     }
 }
 
+// the boundary pass (bdry.f:22-726) with one thread per cell, for meshes on
+// which no two cells' boundary updates touch the same cell
+__global__ void k_boundary2d(Prm P, Fld F) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < P.ncell) boundary_cell2d(P, F, c);
+}
+
 // ---------------------------------------------------------------------------
 // fieldn, tilde.f:125-274 (2D), with viscon (visc.f:37-148)
 // ---------------------------------------------------------------------------
@@ -299,6 +304,7 @@ __global__ void k_tilde_flux2d(Prm P, Fld F) {
         St u, w, d, dsx, dsz;
         rnb2(u, U, R);
         rnb2(w, W, R);
+        if (ib_masked(P, c)) { ib_mask2(P, u, R, 1); ib_mask2(P, w, R, 4); }
         nb2(d, D, R, M);
         interp_x2(P, d, i, dsx);
         interp_z2(P, d, k, dsz);
@@ -370,6 +376,43 @@ __device__ __forceinline__ void stress2d_cell(const Prm &P, const Raw2 &R, const
     double gradxy = (rb[i] * epsmu2 * txy2 - rb[i - 1] * epsmu1 * txy1);
     gradxy = gradxy * inr[i] * indx[i];
     visz = gradyy + gradxy;
+}
+
+// The forcing terms of tilde's mesh loop at a forcing point of cell c along
+// `axis` (0 x, 1 y, 2 z), tilde.f:708-801: the momentum that brings the face
+// velocity to the forcing point's value (the interpolated no-slip velocity
+// of the last boundary pass) in one step, less the pressure and drag terms
+// the corrector adds back.  nb is the remapped plus-side neighbour, nm the
+// raw minus-side one (the cell-centre relative velocities dugs, dvgs, dwgs
+// of tilde.f:597-612 are recomputed from it), dm and dp the cell sizes d(i)
+// and d(i+1) of the axis, inv = 1 / (dm + dp).
+__device__ __forceinline__ void ib_force(const Prm &P, const Fld &F, int c, int axis, int nb, int nm, double dm,
+                                         double dp, double inv, double dt, const double *kpgv, double &rg,
+                                         double *rs) {
+    const int f = __ldg(P.ib_num[axis] + c);
+    if (f == 0) return;
+    const double *vel = P.ib_vel[axis] + (size_t)(f - 1) * P.nph;
+    const double *G = axis == 0 ? F.ug : (axis == 1 ? F.vg : F.wg);
+    const double *S = axis == 0 ? F.us : (axis == 1 ? F.vs : F.ws);
+    const int ns = P.ns;
+    auto dgs = [&](int is) { return ((G[c] - SOL(S, c, is)) + (G[nm] - SOL(S, nm, is))) * 0.5; };
+    double pseudo = vel[0];
+    double force = (inv * (dp * F.rgp[c] + dm * F.rgp[nb]) * pseudo - rg) / dt;
+    double ep_e = (dm * F.ep[nb] + dp * F.ep[c]) * inv;
+    double presn = -inv * 2.0 * ep_e * (F.p[nb] - F.p[c]);
+    double dragn = 0.0;
+    for (int is = 1; is <= ns; ++is) dragn = dragn - kpgv[is] * dgs(is);
+    force = force - presn - dragn;
+    rg = rg + dt * force;
+    for (int is = 1; is <= ns; ++is) {
+        pseudo = vel[is];
+        force = (inv * (dp * SOL(F.rlk, c, is) + dm * SOL(F.rlk, nb, is)) * pseudo - rs[is]) / dt;
+        ep_e = (dm * SOL(F.rlk, nb, is) + dp * SOL(F.rlk, c, is)) * inv * P.inrl[is];
+        presn = -inv * 2.0 * ep_e * (F.p[nb] - F.p[c]);
+        dragn = kpgv[is] * dgs(is);
+        force = force - presn - dragn;
+        rs[is] = rs[is] + dt * force;
+    }
 }
 
 // tilde mesh loop, tilde.f:418-806 (2D), with viscg/viscs (visc.f:150-291),
@@ -523,6 +566,10 @@ __global__ void k_tilde2d(Prm P, Fld F, double dt, const double *app0u, const do
             }
         }
     }
+    if (P.immb) {
+        ib_force(P, F, c, 0, ijke, imjk, dx[i], dx[i + 1], 1.0 / (dx[i] + dx[i + 1]), dt, kpgv, rug, rus);
+        ib_force(P, F, c, 2, ijkt, ijkm, dz[k], dz[k + 1], 1.0 / (dz[k] + dz[k + 1]), dt, kpgv, rwg, rws);
+    }
     F.rug[c] = rug;
     F.rwg[c] = rwg;
     for (int is = 1; is <= ns; ++is) { SOL(F.rus, c, is) = rus[is]; SOL(F.rws, c, is) = rws[is]; }
@@ -598,22 +645,24 @@ __global__ void k_mflux_init2d(Prm P, Fld F, double dt) {
 // calc_res, iter.f:743-771
 __device__ __forceinline__ double calc_res_2d(const Prm &P, const Fld &F, const Raw2 &R, int i, int k, double dt) {
     int c = R.c;
-    double resx = (1.0 * F.rgfe[c] - 1.0 * F.rgfe[R.w]) * P.indx[i] * P.inr[i];
-    double resz = (1.0 * F.rgft[c] - 1.0 * F.rgft[R.b]) * P.indz[k];
+    const CellFaces b = cell_faces(P, c);
+    double resx = (b.e * F.rgfe[c] - b.w * F.rgfe[R.w]) * P.indx[i] * P.inr[i];
+    double resz = (b.t * F.rgft[c] - b.b * F.rgft[R.b]) * P.indz[k];
     double resy = 0.0;
-    return F.rgp[c] - F.rgpn[c] + dt * 1.0 * (resx + resy + resz);
+    return F.rgp[c] - F.rgpn[c] + dt * b.ivf * (resx + resy + resz);
 }
 
 // calc_eps, iter.f:927-994
 __device__ __forceinline__ void calc_eps_2d(const Prm &P, const Fld &F, const Raw2 &R, int i, int k, double dt) {
     int c = R.c;
+    const CellFaces b = cell_faces(P, c);
     double rls = 0;
     for (int is = 1; is <= P.ns; ++is) {
-        double rlkx = (1.0 * SOL(F.rsfe, c, is) - 1.0 * SOL(F.rsfe, R.w, is)) * P.indx[i] * P.inr[i];
-        double rlkz = (1.0 * SOL(F.rsft, c, is) - 1.0 * SOL(F.rsft, R.b, is)) * P.indz[k];
+        double rlkx = (b.e * SOL(F.rsfe, c, is) - b.w * SOL(F.rsfe, R.w, is)) * P.indx[i] * P.inr[i];
+        double rlkz = (b.t * SOL(F.rsft, c, is) - b.b * SOL(F.rsft, R.b, is)) * P.indz[k];
         double rlky = 0.0;
-        double t = SOL(F.rlkn, c, is) - dt * 1.0 * (rlkx + rlky + rlkz);
-        t = t + dt * 1.0 * SOL(F.sink, c, is);
+        double t = SOL(F.rlkn, c, is) - dt * b.ivf * (rlkx + rlky + rlkz);
+        t = t + dt * b.ivf * SOL(F.sink, c, is);
         double v = fmax(0.0, t);
         SOL(F.rlk, c, is) = v;
         rls = rls + v * P.inrl[is];
@@ -706,15 +755,16 @@ __global__ void k_ygas2d(Prm P, Fld F, double dt) {
     if (c >= P.ncell || !fluid(P, c)) return;
     int i = c % P.nx + 1, k = c / P.nx + 1;
     int imjk = at2(P, max(i - 1, 1), k), ijkm = at2(P, i, max(k - 1, 1));  // raw W/B neighbours
+    const CellFaces b = cell_faces(P, c);
     double rgpgc[PDAC_MAXG], rgpt = 0, yfy = 0;
     for (int ig = 0; ig < P.ng; ++ig) {
         double yfw = GAS(F.yfe, imjk, ig), yfb = GAS(F.yft, ijkm, ig);
-        double yfx = 1.0 * GAS(F.yfe, c, ig) - 1.0 * yfw;
-        double yfz = 1.0 * GAS(F.yft, c, ig) - 1.0 * yfb;
+        double yfx = b.e * GAS(F.yfe, c, ig) - b.w * yfw;
+        double yfz = b.t * GAS(F.yft, c, ig) - b.b * yfb;
         double v = GAS(F.rgpgcn, c, ig);
-        v = v - 1.0 * dt * P.indx[i] * yfx * P.inr[i];
-        v = v - 1.0 * dt * 0.0 * yfy;
-        v = v - 1.0 * dt * P.indz[k] * yfz;
+        v = v - b.ivf * dt * P.indx[i] * yfx * P.inr[i];
+        v = v - b.ivf * dt * 0.0 * yfy;
+        v = v - b.ivf * dt * P.indz[k] * yfz;
         if (v < 0.0) v = 0.0;
         rgpgc[ig] = v;
         rgpt = rgpt + v;
@@ -802,22 +852,23 @@ __global__ void k_htilde2d(Prm P, Fld F, double dt) {
     if (c >= P.ncell || !fluid(P, c)) return;
     int i = c % P.nx + 1, k = c / P.nx + 1;
     int imjk = at2(P, max(i - 1, 1), k), ijkm = at2(P, i, max(k - 1, 1));  // raw W/B neighbours
-    double egfx = 1.0 * F.egfe[c] - 1.0 * F.egfe[imjk];
-    double egfz = 1.0 * F.egft[c] - 1.0 * F.egft[ijkm];
+    const CellFaces b = cell_faces(P, c);
+    double egfx = b.e * F.egfe[c] - b.w * F.egfe[imjk];
+    double egfz = b.t * F.egft[c] - b.b * F.egft[ijkm];
     double egfy = 0.0;
     double flx = dt * P.indx[i] * egfx * P.inr[i] + dt * 0.0 * egfy + dt * P.indz[k] * egfz;
-    flx = flx * 1.0;
+    flx = flx * b.ivf;
     F.rhg[c] = -flx;
     for (int is = 1; is <= P.ns; ++is) {
         double esfx, esfz;
-        if (SOL(F.rlk, imjk, is) * P.inrl[is] <= 1.0e-9) esfx = 1.0 * SOL(F.esfe, c, is);
-        else esfx = 1.0 * SOL(F.esfe, c, is) - 1.0 * SOL(F.esfe, imjk, is);
-        if (SOL(F.rlk, ijkm, is) * P.inrl[is] <= 1.0e-9) esfz = 1.0 * SOL(F.esft, c, is);
-        else esfz = 1.0 * SOL(F.esft, c, is) - 1.0 * SOL(F.esft, ijkm, is);
+        if (SOL(F.rlk, imjk, is) * P.inrl[is] <= 1.0e-9) esfx = b.e * SOL(F.esfe, c, is);
+        else esfx = b.e * SOL(F.esfe, c, is) - b.w * SOL(F.esfe, imjk, is);
+        if (SOL(F.rlk, ijkm, is) * P.inrl[is] <= 1.0e-9) esfz = b.t * SOL(F.esft, c, is);
+        else esfz = b.t * SOL(F.esft, c, is) - b.b * SOL(F.esft, ijkm, is);
         double esfy = 0.0;
         flx = dt * P.indx[i] * esfx * P.inr[i] + dt * 0.0 * esfy + dt * P.indz[k] * esfz;
-        flx = flx * 1.0;
-        SOL(F.rhs, c, is) = -flx + SOL(F.sink, c, is) * dt * 1.0 * SOL(F.sies, c, is);
+        flx = flx * b.ivf;
+        SOL(F.rhs, c, is) = -flx + SOL(F.sink, c, is) * dt * b.ivf * SOL(F.sies, c, is);
     }
 }
 
@@ -838,8 +889,9 @@ __global__ void k_ftem2d(Prm P, Fld F, double dt) {
     int imjk = R.w, ijkm = R.b;
     double indxc = 1.0 / (dx[i] + (dx[i + 1] + dx[i - 1]) * 0.5);
     double indzc = 1.0 / (dz[k] + (dz[k + 1] + dz[k - 1]) * 0.5);
-    double ugc = 0.5 * (1.0 * F.ug[c] + 1.0 * F.ug[imjk]);
-    double wgc = 0.5 * (1.0 * F.wg[c] + 1.0 * F.wg[ijkm]);
+    const CellFaces bf = cell_faces(P, c);
+    double ugc = 0.5 * (bf.e * F.ug[c] + bf.w * F.ug[imjk]);
+    double wgc = 0.5 * (bf.t * F.wg[c] + bf.b * F.wg[ijkm]);
     double dpxyz = 0.0;
     dpxyz = dpxyz + dt * indxc * ugc * (F.p[M.e] - F.p[M.w]);
     dpxyz = dpxyz + dt * 0.0 * 0.0 * 0.0;

@@ -27,9 +27,7 @@ __device__ __forceinline__ void ijk_of(const Prm &P, int c, int &i, int &j, int 
 // ---------------------------------------------------------------------------
 // boundary, bdry.f:22-726 + inoutflow.f:1-126 (3D)
 // ---------------------------------------------------------------------------
-__global__ void k_boundary3d(Prm P, Fld F) {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= P.ncell) return;
+__device__ void boundary_cell3d(const Prm &P, const Fld &F, int c) {
     int f0 = P.flag[c];
     if (!(f0 == FLUID || f0 == DOME || f0 == BL_CELL)) return;
     int i, j, k;
@@ -186,6 +184,12 @@ __global__ void k_boundary3d(Prm P, Fld F) {
     }
 }
 
+// the 3D boundary pass with one thread per cell (see k_boundary2d)
+__global__ void k_boundary3d(Prm P, Fld F) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < P.ncell) boundary_cell3d(P, F, c);
+}
+
 // ---------------------------------------------------------------------------
 // fieldn, tilde.f:125-274 (3D)
 // ---------------------------------------------------------------------------
@@ -270,6 +274,7 @@ __global__ void __launch_bounds__(128, PDAC_FLUX_MINB) k_tilde_flux3d(Prm P, Fld
     rnb3(u, U, R);
     rnb3(v, V, R);
     rnb3(w, W, R);
+    if (ib_masked(P, c)) { ib_mask3(P, u, R, 1); ib_mask3(P, v, R, 16); ib_mask3(P, w, R, 4); }
     nb3(d, D, R, M);
     F6T<Real> f = {0, 0, 0, 0, 0, 0};
     if (COMP == 0) {  // x momentum
@@ -513,6 +518,18 @@ __global__ void __launch_bounds__(128, PDAC_FLUX_MINB) k_tilde3d(Prm P, Fld F, d
             }
         }
     }
+    if (P.immb) {
+        double rs[MP];
+        const int nb3[3] = {M.e, M.n, M.t}, nm3[3] = {R.w, R.s, R.b};
+        const double *d3[3] = {P.dx, P.dy, P.dz};
+        const int q3[3] = {i, j, k};
+        for (int ax = 0; ax < 3; ++ax) {
+            for (int is = 1; is <= ns; ++is) rs[is] = rr[is][ax];
+            const double dm = d3[ax][q3[ax]], dp = d3[ax][q3[ax] + 1];
+            ib_force(P, F, c, ax, nb3[ax], nm3[ax], dm, dp, 1.0 / (dm + dp), dt, kpgv, rr[0][ax], rs);
+            for (int is = 1; is <= ns; ++is) rr[is][ax] = rs[is];
+        }
+    }
     F.rug[c] = rr[0][0]; F.rvg[c] = rr[0][1]; F.rwg[c] = rr[0][2];
 #pragma unroll
     for (int is = 1; is <= ns; ++is) { SOL(F.rus, c, is) = rr[is][0]; SOL(F.rvs, c, is) = rr[is][1]; SOL(F.rws, c, is) = rr[is][2]; }
@@ -599,24 +616,26 @@ __global__ void k_mflux_init3d(Prm P, Fld F, double dt) {
 // calc_res, iter.f:743-771 (3D)
 __device__ __forceinline__ double calc_res_3d(const Prm &P, const Fld &F, const Raw3 &R, int i, int j, int k, double dt) {
     int c = R.c;
-    double resx = (1.0 * F.rgfe[c] - 1.0 * F.rgfe[R.w]) * P.indx[i] * 1.0;
-    double resz = (1.0 * F.rgft[c] - 1.0 * F.rgft[R.b]) * P.indz[k];
-    double resy = (1.0 * F.rgfn[c] - 1.0 * F.rgfn[R.s]) * P.indy[j];
-    return F.rgp[c] - F.rgpn[c] + dt * 1.0 * (resx + resy + resz);
+    const CellFaces b = cell_faces(P, c);
+    double resx = (b.e * F.rgfe[c] - b.w * F.rgfe[R.w]) * P.indx[i] * 1.0;
+    double resz = (b.t * F.rgft[c] - b.b * F.rgft[R.b]) * P.indz[k];
+    double resy = (b.n * F.rgfn[c] - b.s * F.rgfn[R.s]) * P.indy[j];
+    return F.rgp[c] - F.rgpn[c] + dt * b.ivf * (resx + resy + resz);
 }
 
 // calc_eps, iter.f:927-994 (3D)
 template <int NP>
 __device__ __forceinline__ void calc_eps_3d(const Prm &P, const Fld &F, const Raw3 &R, int i, int j, int k, double dt) {
     int c = R.c;
+    const CellFaces b = cell_faces(P, c);
     double rls = 0;
 #pragma unroll
     for (int is = 1; is <= nphases<NP>(P) - 1; ++is) {
-        double rlkx = (1.0 * SOL(F.rsfe, c, is) - 1.0 * SOL(F.rsfe, R.w, is)) * P.indx[i] * 1.0;
-        double rlkz = (1.0 * SOL(F.rsft, c, is) - 1.0 * SOL(F.rsft, R.b, is)) * P.indz[k];
-        double rlky = (1.0 * SOL(F.rsfn, c, is) - 1.0 * SOL(F.rsfn, R.s, is)) * P.indy[j];
-        double t = SOL(F.rlkn, c, is) - dt * 1.0 * (rlkx + rlky + rlkz);
-        t = t + dt * 1.0 * SOL(F.sink, c, is);
+        double rlkx = (b.e * SOL(F.rsfe, c, is) - b.w * SOL(F.rsfe, R.w, is)) * P.indx[i] * 1.0;
+        double rlkz = (b.t * SOL(F.rsft, c, is) - b.b * SOL(F.rsft, R.b, is)) * P.indz[k];
+        double rlky = (b.n * SOL(F.rsfn, c, is) - b.s * SOL(F.rsfn, R.s, is)) * P.indy[j];
+        double t = SOL(F.rlkn, c, is) - dt * b.ivf * (rlkx + rlky + rlkz);
+        t = t + dt * b.ivf * SOL(F.sink, c, is);
         double v = fmax(0.0, t);
         SOL(F.rlk, c, is) = v;
         rls = rls + v * P.inrl[is];
@@ -670,15 +689,16 @@ __global__ void k_ygas3d(Prm P, Fld F, double dt) {
     int i, j, k;
     ijk_of(P, c, i, j, k);
     int imjk = at3(P, max(i - 1, 1), j, k), ijmk = at3(P, i, max(j - 1, 1), k), ijkm = at3(P, i, j, max(k - 1, 1));
+    const CellFaces b = cell_faces(P, c);
     double rgpgc[PDAC_MAXG], rgpt = 0;
     for (int ig = 0; ig < P.ng; ++ig) {
-        double yfx = 1.0 * GAS(F.yfe, c, ig) - 1.0 * GAS(F.yfe, imjk, ig);
-        double yfz = 1.0 * GAS(F.yft, c, ig) - 1.0 * GAS(F.yft, ijkm, ig);
-        double yfy = 1.0 * GAS(F.yfn, c, ig) - 1.0 * GAS(F.yfn, ijmk, ig);
+        double yfx = b.e * GAS(F.yfe, c, ig) - b.w * GAS(F.yfe, imjk, ig);
+        double yfz = b.t * GAS(F.yft, c, ig) - b.b * GAS(F.yft, ijkm, ig);
+        double yfy = b.n * GAS(F.yfn, c, ig) - b.s * GAS(F.yfn, ijmk, ig);
         double v = GAS(F.rgpgcn, c, ig);
-        v = v - 1.0 * dt * P.indx[i] * yfx * 1.0;
-        v = v - 1.0 * dt * P.indy[j] * yfy;
-        v = v - 1.0 * dt * P.indz[k] * yfz;
+        v = v - b.ivf * dt * P.indx[i] * yfx * 1.0;
+        v = v - b.ivf * dt * P.indy[j] * yfy;
+        v = v - b.ivf * dt * P.indz[k] * yfz;
         if (v < 0.0) v = 0.0;
         rgpgc[ig] = v;
         rgpt = rgpt + v;
@@ -772,23 +792,24 @@ __global__ void k_htilde3d(Prm P, Fld F, double dt) {
     int i, j, k;
     ijk_of(P, c, i, j, k);
     int imjk = at3(P, max(i - 1, 1), j, k), ijmk = at3(P, i, max(j - 1, 1), k), ijkm = at3(P, i, j, max(k - 1, 1));
-    double egfx = 1.0 * F.egfe[c] - 1.0 * F.egfe[imjk];
-    double egfz = 1.0 * F.egft[c] - 1.0 * F.egft[ijkm];
-    double egfy = 1.0 * F.egfn[c] - 1.0 * F.egfn[ijmk];
+    const CellFaces b = cell_faces(P, c);
+    double egfx = b.e * F.egfe[c] - b.w * F.egfe[imjk];
+    double egfz = b.t * F.egft[c] - b.b * F.egft[ijkm];
+    double egfy = b.n * F.egfn[c] - b.s * F.egfn[ijmk];
     double flx = dt * P.indx[i] * egfx * 1.0 + dt * P.indy[j] * egfy + dt * P.indz[k] * egfz;
-    flx = flx * 1.0;
+    flx = flx * b.ivf;
     F.rhg[c] = -flx;
     for (int is = 1; is <= P.ns; ++is) {
         double ex, ez, ey;
-        if (SOL(F.rlk, imjk, is) * P.inrl[is] <= 1.0e-9) ex = 1.0 * SOL(F.esfe, c, is);
-        else ex = 1.0 * SOL(F.esfe, c, is) - 1.0 * SOL(F.esfe, imjk, is);
-        if (SOL(F.rlk, ijkm, is) * P.inrl[is] <= 1.0e-9) ez = 1.0 * SOL(F.esft, c, is);
-        else ez = 1.0 * SOL(F.esft, c, is) - 1.0 * SOL(F.esft, ijkm, is);
-        if (SOL(F.rlk, ijmk, is) * P.inrl[is] <= 1.0e-9) ey = 1.0 * SOL(F.esfn, c, is);
-        else ey = 1.0 * SOL(F.esfn, c, is) - 1.0 * SOL(F.esfn, ijmk, is);
+        if (SOL(F.rlk, imjk, is) * P.inrl[is] <= 1.0e-9) ex = b.e * SOL(F.esfe, c, is);
+        else ex = b.e * SOL(F.esfe, c, is) - b.w * SOL(F.esfe, imjk, is);
+        if (SOL(F.rlk, ijkm, is) * P.inrl[is] <= 1.0e-9) ez = b.t * SOL(F.esft, c, is);
+        else ez = b.t * SOL(F.esft, c, is) - b.b * SOL(F.esft, ijkm, is);
+        if (SOL(F.rlk, ijmk, is) * P.inrl[is] <= 1.0e-9) ey = b.n * SOL(F.esfn, c, is);
+        else ey = b.n * SOL(F.esfn, c, is) - b.s * SOL(F.esfn, ijmk, is);
         flx = dt * P.indx[i] * ex * 1.0 + dt * P.indy[j] * ey + dt * P.indz[k] * ez;
-        flx = flx * 1.0;
-        SOL(F.rhs, c, is) = -flx + SOL(F.sink, c, is) * dt * 1.0 * SOL(F.sies, c, is);
+        flx = flx * b.ivf;
+        SOL(F.rhs, c, is) = -flx + SOL(F.sink, c, is) * dt * b.ivf * SOL(F.sies, c, is);
     }
 }
 
@@ -810,10 +831,11 @@ __global__ void k_ftem3d(Prm P, Fld F, double dt) {
     int imjk = R.w, ijmk = R.s, ijkm = R.b;
     double indxc = 1.0 / (dx[i] + (dx[i + 1] + dx[i - 1]) * 0.5);
     double indzc = 1.0 / (dz[k] + (dz[k + 1] + dz[k - 1]) * 0.5);
-    double ugc = 0.5 * (1.0 * F.ug[c] + 1.0 * F.ug[imjk]);
-    double wgc = 0.5 * (1.0 * F.wg[c] + 1.0 * F.wg[ijkm]);
+    const CellFaces bf = cell_faces(P, c);
+    double ugc = 0.5 * (bf.e * F.ug[c] + bf.w * F.ug[imjk]);
+    double wgc = 0.5 * (bf.t * F.wg[c] + bf.b * F.wg[ijkm]);
     double indyc = 1.0 / (dy[j] + (dy[j + 1] + dy[j - 1]) * 0.5);
-    double vgc = 0.5 * (1.0 * F.vg[c] + 1.0 * F.vg[ijmk]);
+    double vgc = 0.5 * (bf.n * F.vg[c] + bf.s * F.vg[ijmk]);
     double dpxyz = 0.0;
     dpxyz = dpxyz + dt * indxc * ugc * (F.p[M.e] - F.p[M.w]);
     dpxyz = dpxyz + dt * indyc * vgc * (F.p[M.n] - F.p[M.s]);

@@ -91,6 +91,24 @@ __device__ __forceinline__ void rnb2(St &s, const T *a, const Raw2 &R) {  // sub
     s.eet = a[R.eet]; s.ett = a[R.ett]; s.eee = a[R.eee]; s.ttt = a[R.ttt];
     s.ww = 0; s.bb = 0;
 }
+
+// Velocity masks of tilde's flux stencils in boundary-layer and immersed
+// cells with immersed boundaries (tilde.f:896-945, subscr.f:1548-1582): each
+// raw stencil velocity times the open-face factor of its own cell (bit 1 =
+// b_e_ for u, 4 = b_t_ for w).  The members the reference leaves undefined
+// are not read by the first-order fluxes such cells take.
+__device__ __forceinline__ double ib_open(const Prm &P, int cell, int bit) {
+    return (__ldg(P.ib_faces + cell) & bit) ? 1.0 : 0.0;
+}
+__device__ __forceinline__ bool ib_masked(const Prm &P, int c) {
+    return P.immb && (P.flag[c] == BL_CELL || P.flag[c] == IMMB);
+}
+__device__ __forceinline__ void ib_mask2(const Prm &P, St &s, const Raw2 &R, int bit) {
+    s.c = s.c * ib_open(P, R.c, bit); s.e = s.e * ib_open(P, R.e, bit); s.w = s.w * ib_open(P, R.w, bit);
+    s.t = s.t * ib_open(P, R.t, bit); s.b = s.b * ib_open(P, R.b, bit);
+    s.ee = s.ee * ib_open(P, R.ee, bit); s.tt = s.tt * ib_open(P, R.tt, bit);
+    s.et = s.et * ib_open(P, R.et, bit); s.eb = s.eb * ib_open(P, R.eb, bit); s.wt = s.wt * ib_open(P, R.wt, bit);
+}
 template <typename T>
 __device__ __forceinline__ void first_nb2(St &s, const T *a, const Raw2 &R, const Rem2 &M) {
     s.c = a[R.c]; s.e = a[M.e]; s.t = a[M.t]; s.w = a[M.w]; s.b = a[M.b];

@@ -113,6 +113,18 @@ __device__ __forceinline__ void rnb3(S3T<Real> &s, const T *a, const Raw3 &R) {
     s.een = a[R.een]; s.eet = a[R.eet]; s.enn = a[R.enn]; s.nnt = a[R.nnt]; s.ett = a[R.ett]; s.ntt = a[R.ntt];
     s.ww = s.ss = s.bb = 0;
 }
+
+// the 3D velocity masks of tilde.f:1072-1124 (bit 1 = b_e_ for u, 16 = b_n_
+// for v, 4 = b_t_ for w); see ib_mask2
+template <typename Real>
+__device__ __forceinline__ void ib_mask3(const Prm &P, S3T<Real> &s, const Raw3 &R, int bit) {
+    auto m = [&](int cell) { return Real(ib_open(P, cell, bit)); };
+    s.c = s.c * m(R.c); s.e = s.e * m(R.e); s.w = s.w * m(R.w); s.n = s.n * m(R.n); s.s = s.s * m(R.s);
+    s.t = s.t * m(R.t); s.b = s.b * m(R.b); s.ee = s.ee * m(R.ee); s.nn = s.nn * m(R.nn); s.tt = s.tt * m(R.tt);
+    s.en = s.en * m(R.en); s.es = s.es * m(R.es); s.wn = s.wn * m(R.wn); s.et = s.et * m(R.et);
+    s.wt = s.wt * m(R.wt); s.nt = s.nt * m(R.nt); s.st = s.st * m(R.st); s.eb = s.eb * m(R.eb);
+    s.nb = s.nb * m(R.nb);
+}
 template <typename T, typename Real>
 __device__ __forceinline__ void first_nb3(S3T<Real> &s, const T *a, const Raw3 &R, const Rem3 &M) {
     s.c = a[R.c]; s.e = a[M.e]; s.w = a[M.w]; s.n = a[M.n]; s.s = a[M.s]; s.t = a[M.t]; s.b = a[M.b];

@@ -417,8 +417,19 @@ class Deck:
             bad.append("time_integration=1 with pmodel other than 1 or 2")
         if self["irex"] > 1:
             bad.append("irex>1 (reactions)")
-        if self["immb"] != 0 or self["itp"] != 0:
-            bad.append("immersed boundaries / topography")
+        if self["itp"] not in (0, 1):
+            bad.append("itp other than 0 or 1")
+        elif self["itp"] == 1:
+            if self["grigen"] != 0:
+                bad.append("topography (itp=1) on a generated mesh (grigen>0)")
+            if self.is3d and self["iavv"] != 0:
+                bad.append("iavv>0 (average_dem)")
+            if self.is3d and self["ismt"] != 1 and self["filtersize"] >= self["cellsize"]:
+                bad.append("ismt=2, 3 (gaussian and barnes DEM filters)")
+            if self["immb"] not in (0, 1):
+                bad.append("immb other than 0 or 1")
+            elif self["immb"] == 1 and self["time_integration"] == 1:
+                bad.append("immersed boundaries with the explicit solver (time_integration=1)")
         if self["isink"] < 0:
             bad.append("isink<0")
         if self["idome"] != 0:

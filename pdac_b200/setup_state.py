@@ -24,6 +24,12 @@ from .deck import Deck, MAX_NGAS
 
 # cell flags, grid.f:45-58
 FLUID, SLIP, NOSLIP, FREE_IO, INLET, ZERO_GRAD, VENT = 1, 2, 4, 8, 16, 32, 64
+BL_CELL = 5  # boundary-layer cell, grid.f:48 (no-slip bit + fluid bit)
+
+
+def _nint(x):
+    """Fortran NINT of a non-negative value (half away from zero)."""
+    return int(math.floor(x + 0.5))
 
 # setup.f:563-571 (g/mol) and 608
 GMW = np.array([32.0, 28.0, 44.0, 2.0, 18.0, 28.96442, 64.0]) * 1.0e-3
@@ -266,8 +272,22 @@ class Case:
         self.gas_type = deck.gas_types()
         self._grid()
         self._flags()
-        self.p_atm, self.t_atm = atmosphere_profile(deck, self.z)
+        # pdac.f:138-191: import_topography, locate_vent, export_topography,
+        # set_forcing; the atmosphere (setup, pdac.f:267) sees the mesh as
+        # the topography left it
+        self.topography = None
+        self.ib = None
+        if int(deck["itp"]) >= 1:
+            from .topography import Topography
+            self.topography = Topography(self)
+            self.topography.set_profile()
         self._vent()
+        self._export_topography()
+        if int(deck["itp"]) >= 1 and int(deck["immb"]) == 1:
+            from .topography import ImmersedBoundaries
+            self.ib = ImmersedBoundaries(self.topography)
+            self.flag = self.flag3.reshape(-1).copy()
+        self.p_atm, self.t_atm = atmosphere_profile(deck, self.z)
         self.state = self._initial_state()
 
     # grid.f:206-345
@@ -316,6 +336,13 @@ class Case:
             self.zb[k] = self.zb[k - 1] + self.dz[k]
             self.z[k] = self.zb[k] - 0.5 * self.dz[k]
         self.itc = int(d["itc"]) if not self.is3d else 0
+        # mesh centre cell and domain extent of a prescribed mesh without
+        # added cells (grid.f:229-239); the topography needs them
+        self.iv = _nint(nx / 2.0)
+        self.jv = _nint(ny / 2.0) if self.is3d else 1
+        self.domain_x, self.dxmax = float(np.sum(self.dx)), float(np.max(self.dx))
+        self.domain_y = float(np.sum(self.dy)) if self.is3d else 0.0
+        self.dymax = float(np.max(self.dy)) if self.is3d else 0.0
 
     def idx(self, i, j, k):
         """1-based (i, j, k) -> flat 0-based index."""
@@ -357,9 +384,10 @@ class Case:
         nx, nz = self.nx, self.nz
         fl = self.flag3[:, 0, :]
         xvent = d["xvent"]
-        iv = int(round(nx / 2.0))
+        iv = _nint(nx / 2.0)
+        in_center = bool(d["vent_in_center"]) and self.topography is None  # vent.f:79
         if xvent == -99999.0:
-            xvent = self.x[iv - 1] if d["vent_in_center"] else self.xb[iv - 1]
+            xvent = self.x[iv - 1] if in_center else self.xb[iv - 1]
         iiv = 1
         for i in range(1, nx + 1):
             if self.x[i - 1] <= xvent:
@@ -367,11 +395,18 @@ class Case:
         if iiv == 1 or self.itc == 1:
             iiv = 2
         xvent = self.xb[iiv - 2]
-        kkv = 1
-        for k in range(1, nz):
-            if fl[k - 1, iiv - 1] in (SLIP, NOSLIP):
-                kkv = k
-        quota = kkv
+        if self.topography is None:
+            kkv = 1
+            for k in range(1, nz):
+                if fl[k - 1, iiv - 1] in (SLIP, NOSLIP):
+                    kkv = k
+            quota = kkv
+        else:
+            # the vent sits on the topography, which is flattened around it
+            # (vent.f:165-178, flatten_dem_vent_2D topo.f:828-854)
+            quota = int(self.topography.ord[iiv - 1])
+            self.topography.flatten_vent_2d(xvent, d["vent_radius"], quota)
+            fl = self.flag3[:, 0, :]
         vr = d["vent_radius"]
         iwest, ieast = 2, 2
         for i in range(2, nx + 1):
@@ -396,6 +431,40 @@ class Case:
                 fl[kk - 1, i - 1] = FLUID
         self.flag3[:, 0, :] = fl
         self.flag = self.flag3.reshape(-1).copy()
+
+    # export_topography, topo.f:1114-1181, which pdac.f:180 calls for every
+    # run: a fluid cell up to three rows above the last no-slip cell below it
+    # in its column becomes a boundary-layer cell (flag 5).  Such cells take
+    # first-order fluxes, because the MUSCL corrections and the limiters test
+    # flag == fluid (flux_*.f, iter.f:634-897, tilde.f:955-1248).  The
+    # reference carries the row of the last no-slip cell from one column to
+    # the next (j, then i, then k, i fastest among the columns), so a column
+    # with no no-slip cell (a vent column) uses the previous column's; before
+    # the first no-slip cell the reference leaves it undefined, and it is 0
+    # here.  The level of the last no-slip cell's bottom face is kept per
+    # column as topo_c (the discrete topography the immersed boundaries
+    # start from).
+    def _export_topography(self):
+        nx, ny, nz = self.nx, self.ny, self.nz
+        fl = self.flag3.reshape(nz, ny * nx)
+        ncol = ny * nx
+        kk = np.arange(1, nz + 1, dtype=np.int64)[:, None]
+        noslip = fl == NOSLIP
+        # row (1-based) of the last no-slip cell at or below each cell, 0 if none
+        below = np.maximum.accumulate(np.where(noslip, kk, 0), axis=0)
+        last = below[-1]
+        has = last > 0
+        # the value carried into each column from the columns before it
+        src = np.maximum.accumulate(np.where(has, np.arange(ncol), -1))
+        carried_out = np.where(src >= 0, last[np.maximum(src, 0)], 0)
+        carried_in = np.concatenate(([0], carried_out[:-1]))
+        q = np.where(below > 0, below, carried_in[None, :])
+        bl = (fl == FLUID) & (kk <= q + 3)
+        fl[bl] = BL_CELL
+        self.flag3 = fl.reshape(nz, ny, nx)
+        self.flag = self.flag3.reshape(-1).copy()
+        zb = np.asarray(self.zb, dtype=np.float64)
+        self.topo_c = np.where(has, zb[np.maximum(last - 1, 0)], 0.0).reshape(ny, nx)
 
     def _initial_state(self):
         d = self.deck
@@ -575,6 +644,26 @@ class Case:
         c.p_atm, c.t_atm = abi.dptr(keep["p_atm"]), abi.dptr(keep["t_atm"])
         c.nvent = len(self.vent)
         c.vent_ijk = abi.iptr(keep["vent"])
+        for name in ("x", "xb", "y", "yb", "z", "zb"):
+            keep[name] = np.ascontiguousarray(getattr(self, name), dtype=np.float64)
+            setattr(c, name, abi.dptr(keep[name]))
+        c.immb = 0
+        if self.ib is not None:
+            ib = self.ib
+            c.immb = 1
+            keep["ib_faces"] = np.ascontiguousarray(ib.faces, dtype=np.int32)
+            keep["ib_ivf"] = np.ascontiguousarray(ib.ivf, dtype=np.float64)
+            c.ib_faces, c.ib_ivf = abi.iptr(keep["ib_faces"]), abi.dptr(keep["ib_ivf"])
+            for a, lst in enumerate((ib.fptx, ib.fpty, ib.fptz)):
+                keep[f"ib_num{a}"] = np.ascontiguousarray(ib.num[a], dtype=np.int32)
+                fp = np.array([[p.i, p.j, p.k, p.int, p.q - 1, p.qq - 1] for p in lst] or [[0, 0, 0, 0, -1, -1]],
+                              dtype=np.int32)
+                nsl = np.array([[p.nx_, p.ny_, p.nz_] for p in lst] or [[0.0, 0.0, 0.0]], dtype=np.float64)
+                keep[f"ib_fp{a}"], keep[f"ib_nsl{a}"] = np.ascontiguousarray(fp), np.ascontiguousarray(nsl)
+                c.ib_num[a] = abi.iptr(keep[f"ib_num{a}"])
+                c.ib_nfp[a] = len(lst)
+                c.ib_fp[a] = abi.iptr(keep[f"ib_fp{a}"])
+                c.ib_nsl[a] = abi.dptr(keep[f"ib_nsl{a}"])
         c._keep = keep
         return c
 

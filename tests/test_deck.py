@@ -70,7 +70,10 @@ def test_parse_hand_written_deck_and_set_up_a_closed_box():
     case = Case(d)
     f = case.flag.reshape(case.nz, case.nx)
     assert (f[0, 1:-1] == NOSLIP).all() and (f[-1, 1:-1] == NOSLIP).all()
-    assert (f[:, 0] == NOSLIP).all() and (f[1:-1, 1:-1] == FLUID).all()
+    assert (f[:, 0] == NOSLIP).all()
+    # export_topography (topo.f:1114-1181): the three rows above the no-slip
+    # ground are boundary-layer cells
+    assert (f[1:4, 1:-1] == 5).all() and (f[4:-1, 1:-1] == FLUID).all()
     assert case.gas_type == [6]
 
 
@@ -82,6 +85,11 @@ def test_plume_vent_and_flags():
     vent_i = [v["i"] for v in case.vent]
     assert vent_i == [2, 3, 4, 5, 6]                   # r in [0, 50] m with 10 m cells
     assert all(f[0, i - 1] == VENT for i in vent_i)
+    # boundary-layer rows (topo.f:1114-1181): three above the no-slip ground,
+    # two above the vent, whose columns hold no no-slip cell and keep the
+    # starting row 0
+    assert (f[1:4, 6:-1] == 5).all() and (f[4:-1, 6:-1] == FLUID).all()
+    assert (f[1:3, 1:6] == 5).all() and (f[3:-1, 1:6] == FLUID).all()
     assert case.gas_type == [5, 6]                     # H2O, Air (gas_check order)
     st = case.state
     c = case.vent[0]["ijk"]
