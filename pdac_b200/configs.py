@@ -307,11 +307,22 @@ def plume_3d_topo(dem_file, immb=1, nx=384, ny=384, nz=256, dxyz=15.0, dt=0.01, 
     ns = len(diameters)
     d = plume_3d(nx=nx, ny=ny, nz=nz, dxyz=dxyz, dt=dt, w_gas=w_gas, t_gas=t_gas, diameters=diameters,
                  density=density, ep_solid=tuple([ep_total / ns] * ns), **kw)
-    d.set("topography", itp=1, dem_file=str(dem_file), cellsize=dxyz, filtersize=2 * dxyz)
+    # the DEM is resampled at the mesh spacing; the hills are smooth, so the
+    # low-pass filter of resize_dem is off (filtersize < cellsize): it would
+    # also raise the crater floor around the vent
+    d.set("topography", itp=1, dem_file=str(dem_file), cellsize=dxyz, filtersize=0.5 * dxyz)
     d.set("boundaries", immb=immb)
-    # the DEM is given in mesh coordinates: the mesh centre cell stays where it is
-    d.set("mesh", center_x=(nx // 2 - 1.5 + 1) * dxyz, center_y=(ny // 2 - 1.5 + 1) * dxyz)
+    # the DEM is given in mesh coordinates (cell centres at (i - 1.5) dxyz):
+    # compute_UTM_coords (topo.f:731-751) then leaves the mesh where it is
+    d.set("mesh", center_x=(nx // 2 - 1.5) * dxyz, center_y=(ny // 2 - 1.5) * dxyz)
     return d
+
+
+def _vent_centre(n, cells, d):
+    """Mesh coordinate of the centre of the vent block of plume_3d (cells
+    nx // 2 - cells // 2 + 1 .. + cells - 1 along an axis of n cells)."""
+    lo = n // 2 - cells // 2 + 1
+    return (lo + 0.5 * (cells - 1) - 1.5) * d
 
 
 def small_3d_topo(tmpdir, immb=1, nx=16, ny=14, nz=14, dxyz=20.0, seed=3, **kw):
@@ -319,12 +330,34 @@ def small_3d_topo(tmpdir, immb=1, nx=16, ny=14, nz=14, dxyz=20.0, seed=3, **kw):
     with a flat crater floor around the 2 x 2 vent."""
     import os
     kw.setdefault("vent_cells", 2)
-    cx = (nx // 2 - 0.5) * dxyz
-    cy = (ny // 2 - 0.5) * dxyz
+    cx = _vent_centre(nx, kw["vent_cells"], dxyz)
+    cy = _vent_centre(ny, kw["vent_cells"], dxyz)
     path = write_hills_dem(os.path.join(str(tmpdir), "hills.asc"), nx, ny, dxyz, n_hills=3, seed=seed,
                            h_range=(40.0, 100.0), s_range=(40.0, 90.0), vent_xy=(cx, cy), vent_flat=3 * dxyz)
     d = plume_3d(nx=nx, ny=ny, nz=nz, dxyz=dxyz, **kw)
     d.set("topography", itp=1, dem_file=path, cellsize=dxyz / 2, filtersize=dxyz / 4)
     d.set("boundaries", immb=immb)
-    d.set("mesh", center_x=(nx // 2 - 1.5 + 1) * dxyz, center_y=(ny // 2 - 1.5 + 1) * dxyz)
+    d.set("mesh", center_x=(nx // 2 - 1.5) * dxyz, center_y=(ny // 2 - 1.5) * dxyz)
     return d
+
+
+def plume_3d_hills(nx=384, ny=384, nz=256, dxyz=15.0, seed=0, immb=1, dem_dir=None, **kw):
+    """The large 3D workload with its synthetic topography written out: the
+    sum of 8 seeded Gaussian hills (heights 100-600 m, widths 300-1200 m on
+    the 384-cell mesh, both scaled with nx / 384 on smaller meshes so that a
+    reduced case keeps the shape of the terrain) with a flat crater floor of
+    four cells' radius around the vent, as an ASCII DEM under dem_dir
+    (default: the system temporary directory), read back through the
+    topography path (itp = 1) with immersed boundaries."""
+    import os
+    import tempfile
+    dem_dir = dem_dir or os.path.join(tempfile.gettempdir(), "pdac_b200_dem")
+    os.makedirs(dem_dir, exist_ok=True)
+    cx = _vent_centre(nx, 5, dxyz)
+    cy = _vent_centre(ny, 5, dxyz)
+    path = os.path.join(dem_dir, f"hills_{nx}x{ny}_{dxyz:g}m_seed{seed}_v2.asc")
+    sc = nx / 384.0
+    if not os.path.exists(path):
+        write_hills_dem(path, nx, ny, dxyz, n_hills=8, seed=seed, h_range=(100.0 * sc, 600.0 * sc),
+                        s_range=(300.0 * sc, 1200.0 * sc), vent_xy=(cx, cy), vent_flat=4 * dxyz)
+    return plume_3d_topo(path, immb=immb, nx=nx, ny=ny, nz=nz, dxyz=dxyz, **kw)

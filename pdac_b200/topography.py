@@ -749,6 +749,14 @@ class ImmersedBoundaries:
                         fp.ny_ = gg * cy[j - 1] + (1.0 - gg) * cy[j - 1 + _DJ[gint]]
                         fp.nz_ = cz[k - 1]
                         out.append(fp)
+                if o < 1:
+                    # a column whose topography lies below the first face
+                    # (interpolate_dem does not round to the centimetre as
+                    # set_profile does, so the translated mesh can leave one
+                    # there): the reference writes this point past the end of
+                    # its table (the count of topo.f:1021-1022 skips it) and
+                    # never reads it back
+                    continue
                 fp = ForcingPoint(i, j, o, 0, 0, 0, 1, (cx[i - 1], cy[j - 1], topo2d[i - 1, j - 1]))
                 out.append(fp)
         return out
