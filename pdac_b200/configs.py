@@ -210,16 +210,23 @@ def small_3d_mixture(formatted=False, **kw):
 
 def small_2d_opt(optimization=2, **kw):
     """small_2d with the reference's optimized inner loop (optimization = 2,
-    opt_inner_loop, iter.f:1255-1547)."""
+    opt_inner_loop, iter.f:1255-1547) and a no-slip east wall.  The loop's
+    density stencils keep the loop-entry value in slots remapped to the cell
+    itself, which only the MUSCL corrections of fluid cells next to a wall
+    read; the rows above the ground are boundary-layer cells with
+    first-order fluxes, so the side wall is where the variant shows."""
     d = small_2d(**kw)
     d.set("numeric", optimization=optimization)
+    d.set("boundaries", east=3)
     return d
 
 
 def small_3d_opt(optimization=2, **kw):
-    """small_3d with the optimized inner loop of small_2d_opt."""
+    """small_3d with the optimized inner loop of small_2d_opt and no-slip
+    walls on the x sides."""
     d = small_3d(**kw)
     d.set("numeric", optimization=optimization)
+    d.set("boundaries", west=3, east=3)
     return d
 
 

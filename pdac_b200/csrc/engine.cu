@@ -1321,8 +1321,8 @@ static int enqueue_sweep(pdac_ctx *ctx, double dt, cudaStream_t st, bool prof) {
         if (prof) CK(cudaEventRecord(ctx->cev[3 * col], st));
         pdac::k_resid_collect<<<blocks((long)nwords, TPB_RESID), TPB_RESID, 0, st>>>(ctx->P, col, dirty, ctx->d_cand, ncand);
         int *wl = ctx->d_work + col * ctx->work_stride;
-        if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_resid_test, 3, test_grid, TPB_RESID, st, ctx->P, F, dt, ctx->d_cand, ncand, wl, cnt);
-        else PHASE_LAUNCH_D(nph, pdac::k_resid_test, 2, test_grid, TPB_RESID, st, ctx->P, F, dt, ctx->d_cand, ncand, wl, cnt);
+        if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_resid_test, 3, test_grid, TPB_RESID, st, ctx->P, F, dt, ctx->d_cand, ncand, wl, cnt, dirty);
+        else PHASE_LAUNCH_D(nph, pdac::k_resid_test, 2, test_grid, TPB_RESID, st, ctx->P, F, dt, ctx->d_cand, ncand, wl, cnt, dirty);
         if (prof) CK(cudaEventRecord(ctx->cev[3 * col + 1], st));
         if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_inner_team, 3, g, TPB_TEAM, st, ctx->P, F, dt, ctx->d_nit, wl, cnt, dirty);
         else PHASE_LAUNCH_D(nph, pdac::k_inner_team, 2, g, TPB_TEAM, st, ctx->P, F, dt, ctx->d_nit, wl, cnt, dirty);
@@ -1619,8 +1619,8 @@ int pdac_gpu_iter_static(pdac_ctx *ctx, double dt, int *nit_out) {
         for (int col = 0; col < 3; ++col) {
             int *cnt = wcount + col, *ncand = wcount + 6 + col;
             pdac::k_resid_collect<<<blocks((long)nwords, TPB_RESID), TPB_RESID, 0, st>>>(ctx->P, col, dirty, cand, ncand);
-            if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_resid_test, 3, test_grid, TPB_RESID, st, ctx->P, F, dt, cand, ncand, work, cnt);
-            else PHASE_LAUNCH_D(nph, pdac::k_resid_test, 2, test_grid, TPB_RESID, st, ctx->P, F, dt, cand, ncand, work, cnt);
+            if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_resid_test, 3, test_grid, TPB_RESID, st, ctx->P, F, dt, cand, ncand, work, cnt, dirty);
+            else PHASE_LAUNCH_D(nph, pdac::k_resid_test, 2, test_grid, TPB_RESID, st, ctx->P, F, dt, cand, ncand, work, cnt, dirty);
             ctx->launches++;
             long team_threads = (nthr + (ctx->d3 ? 4 : 7)) / (ctx->d3 ? 5 : 8) * 32;
             int g = std::min(ctx->inner_grid, blocks(team_threads, TPB_TEAM));

@@ -398,12 +398,15 @@ __global__ void __launch_bounds__(128, PDAC_INNER_MINB(NP)) k_inner_team(Prm P, 
 // The active set is one bit per cell: the test of a cell reads only its own
 // p/rog/rgp and the mass fluxes of its faces, which change only when the
 // cell or a face neighbour runs the inner loop; such a run sets the bits of
-// those cells (mark_dirty), and a clean cell would recompute exactly the
-// values it holds, so it is not tested.  k_resid_collect turns the set bits
-// of one colour's fluid cells into a candidate list (clearing them, and the
+// those cells (mark_dirty).  A converged test rewrites the cell's volume
+// fractions (calc_eps, from the same fluxes) and rgp = ep rog: if that
+// changes rgp, the next test computes a different residual, so the cell
+// keeps its bit; otherwise a clean cell would recompute exactly the values
+// it holds, and it is not tested.  k_resid_collect turns the set bits of
+// one colour's fluid cells into a candidate list (clearing them, and the
 // bits of non-fluid cells, which are never tested); k_resid_test tests each
-// candidate: a converged cell updates its volume fractions (calc_eps) and
-// rgp, an unconverged one goes to the worklist of k_inner_team.
+// candidate: a converged cell updates its volume fractions and rgp, an
+// unconverged one goes to the worklist of k_inner_team.
 // candidates of one colour: the block's threads take consecutive words of
 // the bitmask, block-uniform rounds over the grid (one round when the grid
 // covers the words)
@@ -440,7 +443,7 @@ __global__ void __launch_bounds__(TPB_RESID) k_resid_collect(Prm P, int colour, 
 // the residual test of the len candidates, block-uniform rounds
 template <int TPBK, int NP, int D>
 __device__ __forceinline__ void test_phase(const Prm &P, const Fld &F, double dt, const int *cand, int len, int *work,
-                                           int *count) {
+                                           int *count, unsigned *dirty) {
     for (int base = blockIdx.x * TPBK; base < len; base += gridDim.x * TPBK) {
         int idx = base + threadIdx.x, c = -1, nmine = 0;
         if (idx < len) {
@@ -460,8 +463,13 @@ __device__ __forceinline__ void test_phase(const Prm &P, const Fld &F, double dt
                 dg = calc_res_2d(P, F, R, i, k, dt);
                 if (fabs(dg) <= F.conv[c]) calc_eps_2d(P, F, R, i, k, dt);
             }
-            if (fabs(dg) <= F.conv[c]) F.rgp[c] = F.ep[c] * F.rog[c];
-            else nmine = 1;
+            if (fabs(dg) <= F.conv[c]) {
+                const double old = F.rgp[c];
+                F.rgp[c] = F.ep[c] * F.rog[c];
+                if (__double_as_longlong(F.rgp[c]) != __double_as_longlong(old)) mark_dirty(dirty, c);
+            } else {
+                nmine = 1;
+            }
         }
         block_append_n<TPBK, 1>(work, count, &c, nmine, count + 3, idx < len ? 1 : 0);
     }
@@ -469,8 +477,8 @@ __device__ __forceinline__ void test_phase(const Prm &P, const Fld &F, double dt
 
 template <int NP, int D>
 __global__ void __launch_bounds__(TPB_RESID) k_resid_test(Prm P, Fld F, double dt, const int *cand, const int *ncand,
-                                                          int *work, int *count) {
-    test_phase<TPB_RESID, NP, D>(P, F, dt, cand, *ncand, work, count);
+                                                          int *work, int *count, unsigned *dirty) {
+    test_phase<TPB_RESID, NP, D>(P, F, dt, cand, *ncand, work, count, dirty);
 }
 
 // The whole outer sweep loop of iter (iter.f:204-410) in one cooperative
@@ -499,7 +507,7 @@ __global__ void __launch_bounds__(128, PDAC_INNER_MINB(NP)) k_iter_coop(Prm P, F
             collect_phase<128>(P, col, W.dirty, W.cand, W.wcount + 6 + col);
             g.sync();
             int *wl = W.work + col * W.wstride;
-            test_phase<128, NP, D>(P, F, dt, W.cand, __ldcg(W.wcount + 6 + col), wl, W.wcount + col);
+            test_phase<128, NP, D>(P, F, dt, W.cand, __ldcg(W.wcount + 6 + col), wl, W.wcount + col, W.dirty);
             g.sync();
             inner_team_run<NP, D, false>(P, F, dt, nit, wl, __ldcg(W.wcount + col), W.dirty, warp, nwarps);
             g.sync();

