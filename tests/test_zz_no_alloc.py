@@ -56,6 +56,35 @@ def test_static_scratch_iter_matches_iter(which):
     new.close()
 
 
+def _scratch_bytes(nx, ny, nz):
+    """The static variant's scratch for a mesh (the header's formula)."""
+    wl = 4 * ((nx + 2) // 3) * ny * nz
+    wl = (wl + 255) // 256 * 256
+    return 256 + 2 * wl + 4 * ((nx * ny * nz + 31) // 32)
+
+
+def test_static_scratch_near_its_bound():
+    """A 2D plume of 1600 x 1850 cells (2.96 M) needs 98.6 % of the 8 MiB
+    array: one step through pdac_gpu_iter_static equals one through
+    pdac_gpu_iter."""
+    from pdac_b200 import configs
+    from pdac_b200.engine import Engine
+    from pdac_b200.setup_state import Case
+    nx, nz = 1600, 1850
+    need = _scratch_bytes(nx, 1, nz)
+    assert 0.98 * 8 * 1024 * 1024 < need <= 8 * 1024 * 1024
+    case = Case(configs.plume_2d(nx=nx, nz=nz))
+    ref, new = Engine(case), Engine(case)
+    _bind(new.L)
+    n_ref = _step(ref, 1, static=False)
+    n_new = _step(new, 1, static=True)
+    assert n_new == n_ref
+    errs, bad = compare_state(new.download(), ref.download(), STEP_FIELDS, TOL, case.nsolid, case.ncell)
+    assert not bad, bad
+    ref.close()
+    new.close()
+
+
 def test_static_scratch_rejects_a_mesh_that_does_not_fit():
     from pdac_b200 import configs
     from pdac_b200.engine import Engine
