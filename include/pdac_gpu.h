@@ -399,10 +399,13 @@ int pdac_gpu_set_tuning(pdac_ctx *ctx, const int *in, int nin);
  * by one time step each, pdac_gpu_step(member, sweep, ...) on every member,
  * with the members' kernels running concurrently on the device.  A member on
  * the semi-implicit path (time_integration = 0, rungekut = 1, no implicit-
- * flux modes, cstop unset, more than one gas) takes its whole step as one
- * CUDA graph -- boundary to ftem, the outer sweep loop as a conditional
- * node, its outcome copied back once -- launched on its stream by the
- * calling thread; the other members are driven by a pool of nthreads host
+ * flux modes, cstop unset, more than one gas) takes its whole step as
+ * graph nodes -- boundary to ftem, the outer sweep loop as a conditional
+ * node, its outcome copied back once -- and all such members' nodes form
+ * ONE CUDA graph (independent branches), launched once per batch step by
+ * the calling thread (rebuilt after a member's launch shapes change; one
+ * graph per member if that graph cannot be instantiated); the other
+ * members are driven by a pool of nthreads host
  * threads (<= 0: one per such member).  Both give the member's results of
  * pdac_gpu_step, bit for bit; pdac_gpu_phase_times is not updated by a
  * graph step.  While in a batch, members run without cooperative launches

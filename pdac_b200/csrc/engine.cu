@@ -62,6 +62,7 @@ struct pdac_ctx {
     // failures of ftem, non-finite flag] read back once per step
     cudaGraph_t step_graph = nullptr;
     cudaGraphExec_t step_exec = nullptr;
+    long graph_gen = 0;  // bumped whenever captured launch shapes go stale (put_tuning)
     long long step_launches = 0;
     int *d_status = nullptr, *h_status = nullptr;
     unsigned *d_dirty = nullptr;                 // corrector active set, one bit per cell
@@ -2090,6 +2091,7 @@ void put_tuning(pdac_ctx *ctx, const Tuning &t) {
     if (ctx->ex_graph) { cudaGraphDestroy(ctx->ex_graph); ctx->ex_graph = nullptr; }
     if (ctx->step_exec) { cudaGraphExecDestroy(ctx->step_exec); ctx->step_exec = nullptr; }
     if (ctx->step_graph) { cudaGraphDestroy(ctx->step_graph); ctx->step_graph = nullptr; }
+    ctx->graph_gen++;
 }
 
 bool tuning_valid(const pdac_ctx *ctx, const Tuning &t) {
@@ -2810,13 +2812,14 @@ static int enqueue_step_post(pdac_ctx *ctx, double dt, cudaStream_t st) {
     return PDAC_OK;
 }
 
-static int build_step_graph(pdac_ctx *ctx) {
-    if (ctx->step_exec) { cudaGraphExecDestroy(ctx->step_exec); ctx->step_exec = nullptr; }
-    if (ctx->step_graph) { cudaGraphDestroy(ctx->step_graph); ctx->step_graph = nullptr; }
+// the nodes of one whole semi-implicit step of ctx in graph g: the kernels
+// before the sweep loop (a child graph), the loop as a conditional WHILE
+// node, the kernels after it (a child graph, ending with the step's status
+// copied to pinned host memory); the kernels are captured on ctx's stream
+static int add_step_nodes(pdac_ctx *ctx, cudaGraph_t g) {
     const double dt = ctx->cfg.dt;
     cudaStream_t st = ctx->stream;
     const long long before = ctx->launches;
-    CK(cudaGraphCreate(&ctx->step_graph, 0));
     cudaGraph_t part = nullptr;
     // the kernels before the sweep loop
     CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
@@ -2825,19 +2828,19 @@ static int build_step_graph(pdac_ctx *ctx) {
     if (s) { ctx->launches = before; return s; }
     CK(e);
     cudaGraphNode_t pre, loop_node, post;
-    e = cudaGraphAddChildGraphNode(&pre, ctx->step_graph, nullptr, 0, part);
+    e = cudaGraphAddChildGraphNode(&pre, g, nullptr, 0, part);
     cudaGraphDestroy(part);
     CK(e);
     // the sweep loop
     cudaGraphConditionalHandle loop;
-    CK(cudaGraphConditionalHandleCreate(&loop, ctx->step_graph, 1, cudaGraphCondAssignDefault));
+    CK(cudaGraphConditionalHandleCreate(&loop, g, 1, cudaGraphCondAssignDefault));
     alignas(cudaGraphNodeParams) unsigned char cp_storage[sizeof(cudaGraphNodeParams)] = {};
     cudaGraphNodeParams &cp = *reinterpret_cast<cudaGraphNodeParams *>(cp_storage);
     cp.type = cudaGraphNodeTypeConditional;
     cp.conditional.handle = loop;
     cp.conditional.type = cudaGraphCondTypeWhile;
     cp.conditional.size = 1;
-    CK(cudaGraphAddNode(&loop_node, ctx->step_graph, &pre, 1, &cp));
+    CK(cudaGraphAddNode(&loop_node, g, &pre, 1, &cp));
     CK(cudaStreamBeginCaptureToGraph(st, cp.conditional.phGraph_out[0], nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
     const long long mid = ctx->launches;
     s = enqueue_sweep(ctx, dt, st, false);
@@ -2856,9 +2859,18 @@ static int build_step_graph(pdac_ctx *ctx) {
     ctx->launches = before;
     if (s) return s;
     CK(e);
-    e = cudaGraphAddChildGraphNode(&post, ctx->step_graph, &loop_node, 1, part);
+    e = cudaGraphAddChildGraphNode(&post, g, &loop_node, 1, part);
     cudaGraphDestroy(part);
     CK(e);
+    return PDAC_OK;
+}
+
+static int build_step_graph(pdac_ctx *ctx) {
+    if (ctx->step_exec) { cudaGraphExecDestroy(ctx->step_exec); ctx->step_exec = nullptr; }
+    if (ctx->step_graph) { cudaGraphDestroy(ctx->step_graph); ctx->step_graph = nullptr; }
+    CK(cudaGraphCreate(&ctx->step_graph, 0));
+    int s = add_step_nodes(ctx, ctx->step_graph);
+    if (s) return s;
     CK(cudaGraphInstantiate(&ctx->step_exec, ctx->step_graph, 0));
     return PDAC_OK;
 }
@@ -2892,6 +2904,13 @@ struct pdac_batch {
     std::vector<cudaEvent_t> fin;
     double last_ms = 0.0;
     std::string err;
+    // every graph member's whole step in one graph, launched once per batch
+    // step on the lead stream (the members' branches are independent); the
+    // members' graph generations it was built at
+    cudaGraph_t bgraph = nullptr;
+    cudaGraphExec_t bexec = nullptr;
+    std::vector<long> bgen;
+    bool one_graph = true;
 };
 
 static void batch_worker(pdac_batch *b, int w) {
@@ -2932,6 +2951,8 @@ static void batch_free(pdac_batch *b) {
         c->ex_dt = -1.0;
     }
     for (auto e : b->fin) if (e) cudaEventDestroy(e);
+    if (b->bexec) cudaGraphExecDestroy(b->bexec);
+    if (b->bgraph) cudaGraphDestroy(b->bgraph);
     if (b->t0) cudaEventDestroy(b->t0);
     if (b->t1) cudaEventDestroy(b->t1);
     if (b->lead) cudaStreamDestroy(b->lead);
@@ -2997,23 +3018,73 @@ int pdac_gpu_batch_create(pdac_ctx *const *members, int nmember, int nthreads, p
     return PDAC_OK;
 }
 
-int pdac_gpu_batch_step(pdac_batch *b, int sweep, int *nit, int *status) {
-    if (!b) return PDAC_ERR_ARG;
-    if (cudaEventRecord(b->t0, b->lead) != cudaSuccess) return PDAC_ERR_CUDA;
-    // the graph members: one launch each from this thread (a member's graph
-    // is built at its first batch step, with its streams idle)
-    std::vector<char> launched(b->m.size(), 0);
+// (re)build the batch graph: every graph member's step nodes in one graph
+static int build_batch_graph(pdac_batch *b) {
+    if (b->bexec) { cudaGraphExecDestroy(b->bexec); b->bexec = nullptr; }
+    if (b->bgraph) { cudaGraphDestroy(b->bgraph); b->bgraph = nullptr; }
+    if (cudaGraphCreate(&b->bgraph, 0) != cudaSuccess) return PDAC_ERR_CUDA;
+    b->bgen.assign(b->m.size(), -1);
     for (size_t i = 0; i < b->m.size(); ++i) {
         if (!b->graph[i]) continue;
-        pdac_ctx *c = b->m[i];
-        int s = c->step_exec ? PDAC_OK : build_step_graph(c);
-        if (!s && (cudaStreamWaitEvent(c->stream, b->t0, 0) != cudaSuccess ||
-                   cudaGraphLaunch(c->step_exec, c->stream) != cudaSuccess))
-            s = fail(c, PDAC_ERR_CUDA, "batch: step graph launch failed");
-        cudaEventRecord(b->fin[i], c->stream);
-        b->status[i] = s;
-        b->nit[i] = 0;
-        launched[i] = s == PDAC_OK;
+        int s = add_step_nodes(b->m[i], b->bgraph);
+        if (s) return s;
+        b->bgen[i] = b->m[i]->graph_gen;
+    }
+    if (cudaGraphInstantiate(&b->bexec, b->bgraph, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return PDAC_ERR_CUDA;
+    }
+    return PDAC_OK;
+}
+
+int pdac_gpu_batch_step(pdac_batch *b, int sweep, int *nit, int *status) {
+    if (!b) return PDAC_ERR_ARG;
+    std::vector<char> launched(b->m.size(), 0);
+    bool any_graph = false;
+    for (size_t i = 0; i < b->m.size(); ++i) any_graph = any_graph || b->graph[i];
+    // the batch graph runs on the lead stream: it first waits for what the
+    // graph members' own streams hold (uploads, set-up)
+    if (any_graph && b->one_graph)
+        for (size_t i = 0; i < b->m.size(); ++i) {
+            if (!b->graph[i]) continue;
+            if (cudaEventRecord(b->fin[i], b->m[i]->stream) != cudaSuccess ||
+                cudaStreamWaitEvent(b->lead, b->fin[i], 0) != cudaSuccess)
+                return PDAC_ERR_CUDA;
+        }
+    if (cudaEventRecord(b->t0, b->lead) != cudaSuccess) return PDAC_ERR_CUDA;
+    // the graph members: all in one graph launched on the lead stream, built
+    // at the first batch step with the members' streams idle (and again when
+    // a member's launch shapes change); if that graph cannot be built, one
+    // graph launch per member from this thread
+    bool stale = !b->bexec;
+    for (size_t i = 0; i < b->m.size() && !stale; ++i) stale = b->graph[i] && b->bgen[i] != b->m[i]->graph_gen;
+    if (any_graph && b->one_graph && stale && build_batch_graph(b) != PDAC_OK) {
+        b->one_graph = false;
+        if (b->bexec) { cudaGraphExecDestroy(b->bexec); b->bexec = nullptr; }
+        if (b->bgraph) { cudaGraphDestroy(b->bgraph); b->bgraph = nullptr; }
+        for (pdac_ctx *c : b->m) c->err.clear();
+    }
+    if (any_graph && b->one_graph) {
+        const bool ok = cudaGraphLaunch(b->bexec, b->lead) == cudaSuccess;
+        for (size_t i = 0; i < b->m.size(); ++i) {
+            if (!b->graph[i]) continue;
+            b->status[i] = ok ? PDAC_OK : fail(b->m[i], PDAC_ERR_CUDA, "batch: batch graph launch failed");
+            b->nit[i] = 0;
+            launched[i] = ok;
+        }
+    } else {
+        for (size_t i = 0; i < b->m.size(); ++i) {
+            if (!b->graph[i]) continue;
+            pdac_ctx *c = b->m[i];
+            int s = c->step_exec ? PDAC_OK : build_step_graph(c);
+            if (!s && (cudaStreamWaitEvent(c->stream, b->t0, 0) != cudaSuccess ||
+                       cudaGraphLaunch(c->step_exec, c->stream) != cudaSuccess))
+                s = fail(c, PDAC_ERR_CUDA, "batch: step graph launch failed");
+            cudaEventRecord(b->fin[i], c->stream);
+            b->status[i] = s;
+            b->nit[i] = 0;
+            launched[i] = s == PDAC_OK;
+        }
     }
     {
         std::lock_guard<std::mutex> lk(b->mu);
@@ -3026,8 +3097,10 @@ int pdac_gpu_batch_step(pdac_batch *b, int sweep, int *nit, int *status) {
         std::unique_lock<std::mutex> lk(b->mu);
         b->done.wait(lk, [&] { return b->pending == 0; });
     }
-    for (auto e : b->fin)
-        if (cudaStreamWaitEvent(b->lead, e, 0) != cudaSuccess) return PDAC_ERR_CUDA;
+    for (size_t i = 0; i < b->m.size(); ++i) {
+        if (b->graph[i] && b->one_graph) continue;  // ran on the lead stream
+        if (cudaStreamWaitEvent(b->lead, b->fin[i], 0) != cudaSuccess) return PDAC_ERR_CUDA;
+    }
     if (cudaEventRecord(b->t1, b->lead) != cudaSuccess || cudaEventSynchronize(b->t1) != cudaSuccess) return PDAC_ERR_CUDA;
     float ms = 0;
     if (cudaEventElapsedTime(&ms, b->t0, b->t1) != cudaSuccess) return PDAC_ERR_CUDA;

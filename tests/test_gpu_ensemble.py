@@ -50,6 +50,35 @@ def test_batch_matches_members_run_alone(nthreads):
             np.testing.assert_array_equal(got[m][name], v, err_msg=f"member {m} field {name}")
 
 
+def test_batch_graph_rebuilt_after_new_launch_shapes():
+    """The semi-implicit members run as one graph built at the first batch
+    step; a member's new launch shapes (pdac_gpu_set_tuning between batch
+    steps) rebuild it, and the results stay those of the decks run alone."""
+    from pdac_b200 import configs
+    from pdac_b200.engine import Engine
+    from pdac_b200.ensemble import Batch
+    from pdac_b200.setup_state import Case
+    decks = [configs.plume_3d(nx=40, ny=21, nz=30, vent_cells=4), configs.small_2d(nx=14, nz=19)]
+    steps = 4
+    engines = [Engine(Case(d)) for d in decks]
+    b = Batch(engines)
+    got_nit = []
+    for s in range(1, steps + 1):
+        if s == 3:
+            engines[0].set_tuning(dict(tile_shape=2, tile_kchunk=7, inner_grid=148 * 4, test_grid=148 * 2,
+                                       coop_cells_per_block=1024))
+        got_nit.append(b.step(s))
+    got = [e.download() for e in engines]
+    b.close()
+    for e in engines:
+        e.close()
+    for m, d in enumerate(decks):
+        nits, ref = _run_alone(d, steps)
+        assert [row[m] for row in got_nit] == nits, m
+        for name, v in ref.items():
+            np.testing.assert_array_equal(got[m][name], v, err_msg=f"member {m} field {name}")
+
+
 def test_batch_rejects_a_member_given_twice():
     from pdac_b200 import configs
     from pdac_b200.engine import Engine, PdacError
