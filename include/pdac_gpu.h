@@ -48,8 +48,8 @@ extern "C" {
 #define PDAC_MAX_NSOLID   8
 #define PDAC_MAX_NGAS     7
 
-/* precision modes.  PDAC_PREC_MIXED (3D runs only; 2D is rejected at
- * create): the face-flux passes -- momentum (flux_u/v/w.f), mass (flux_m.f),
+/* precision modes.  PDAC_PREC_MIXED (2D and 3D runs, both time
+ * integrations): the face-flux passes -- momentum (flux_u/v/w.f), mass (flux_m.f),
  * species and enthalpy (flux_sc.f, hotc.f) -- compute in FP32 from the FP64
  * state and store their fluxes in FP64; the state, every conservative update,
  * the pressure correction and the equations of state stay in FP64.  A face

@@ -61,8 +61,8 @@ struct Prm {
     // reciprocal face spacings of interp.f and flux_*.f, divided once on the host
     // (an IEEE division, so the same bits as dividing in the kernel)
     const double *hx, *hy, *hz;
-    const float *dxf, *dyf, *dzf, *indxf, *indyf, *indzf, *hxf, *hyf, *hzf;  // FP32 copies (mixed precision), else null
-    int mixed;  // 1: the 3D flux passes compute in FP32 (PDAC_PREC_MIXED)
+    const float *dxf, *dyf, *dzf, *indxf, *indyf, *indzf, *hxf, *hyf, *hzf, *rf, *rbf;  // FP32 copies (mixed precision), else null
+    int mixed;  // 1: the face-flux passes compute in FP32 (PDAC_PREC_MIXED)
     // c / nx and c / (nx ny) as a 64-bit multiply-high: mnx = ceil(2^64 / nx)
     // (mny likewise for ny), exact for every c < 2^32; 0 = divide instead
     unsigned long long mnx, mny;
@@ -109,6 +109,8 @@ template <> struct Met<double> {
     static __device__ __forceinline__ const double *hx(const Prm &P) { return P.hx; }
     static __device__ __forceinline__ const double *hy(const Prm &P) { return P.hy; }
     static __device__ __forceinline__ const double *hz(const Prm &P) { return P.hz; }
+    static __device__ __forceinline__ const double *r(const Prm &P) { return P.r; }
+    static __device__ __forceinline__ const double *rb(const Prm &P) { return P.rb; }
 };
 template <> struct Met<float> {
     static __device__ __forceinline__ const float *dx(const Prm &P) { return P.dxf; }
@@ -120,6 +122,8 @@ template <> struct Met<float> {
     static __device__ __forceinline__ const float *hx(const Prm &P) { return P.hxf; }
     static __device__ __forceinline__ const float *hy(const Prm &P) { return P.hyf; }
     static __device__ __forceinline__ const float *hz(const Prm &P) { return P.hzf; }
+    static __device__ __forceinline__ const float *r(const Prm &P) { return P.rf; }
+    static __device__ __forceinline__ const float *rb(const Prm &P) { return P.rbf; }
 };
 
 // Device pointers of every field (state, n-level, tilde, fluxes, solver).

@@ -356,7 +356,6 @@ int validate(const pdac_cfg *c, std::string &why) {
         why = "precision must be PDAC_PREC_FP64 or PDAC_PREC_MIXED";
         return 1;
     }
-    if (c->precision == PDAC_PREC_MIXED && c->job_type != 3) { why = "PDAC_PREC_MIXED is built for 3D runs only"; return 1; }
     if (c->time_integration != 0 && c->time_integration != 1) { why = "time_integration must be 0 or 1"; return 1; }
     if (c->iturb != 0 && c->iturb != 1) { why = "iturb must be 0 or 1 (iturb = 2 needs the topography's roughness)"; return 1; }
     if (c->iturb == 1 && c->modturbo != 1 && c->modturbo != 2) {
@@ -728,7 +727,7 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     P.hx = mp[12]; P.hy = mp[13]; P.hz = mp[14];
     P.mixed = cfg->precision == PDAC_PREC_MIXED;
     if (P.mixed) {  // the metric of the FP32 flux passes: each FP64 value rounded to nearest
-        const int qs[9] = {0, 1, 2, 3, 4, 5, 12, 13, 14};
+        const int qs[11] = {0, 1, 2, 3, 4, 5, 12, 13, 14, 6, 7};
         size_t ftot = 0;
         for (int q : qs) ftot += mets[q]->size();
         std::vector<float> hf;
@@ -737,11 +736,11 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
             for (double v : *mets[q]) hf.push_back((float)v);
         CK(cudaMalloc(&ctx->metric_f, ftot * sizeof(float)));
         CK(cudaMemcpy(ctx->metric_f, hf.data(), ftot * sizeof(float), cudaMemcpyHostToDevice));
-        const float *fp[9];
+        const float *fp[11];
         size_t fo = 0;
-        for (int q = 0; q < 9; ++q) { fp[q] = ctx->metric_f + fo; fo += mets[qs[q]]->size(); }
+        for (int q = 0; q < 11; ++q) { fp[q] = ctx->metric_f + fo; fo += mets[qs[q]]->size(); }
         P.dxf = fp[0]; P.dyf = fp[1]; P.dzf = fp[2]; P.indxf = fp[3]; P.indyf = fp[4]; P.indzf = fp[5];
-        P.hxf = fp[6]; P.hyf = fp[7]; P.hzf = fp[8];
+        P.hxf = fp[6]; P.hyf = fp[7]; P.hzf = fp[8]; P.rf = fp[9]; P.rbf = fp[10];
     }
     CK(cudaMalloc(&ctx->d_flag, n * sizeof(int)));
     CK(cudaMemcpy(ctx->d_flag, cfg->flag, n * sizeof(int), cudaMemcpyHostToDevice));
@@ -1270,7 +1269,8 @@ static int enqueue_tilde(pdac_ctx *ctx, double dt, cudaStream_t st) {
     } else {
         for (double *a : {F.ugfe, F.ugft, F.wgfe, F.wgft}) CK(cudaMemsetAsync(a, 0, n * sizeof(double), st));
         for (double *a : {F.usfe, F.usft, F.wsfe, F.wsft}) CK(cudaMemsetAsync(a, 0, n * ns * sizeof(double), st));
-        pdac::k_tilde_flux2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F), ctx->launches++;
+        (ctx->P.mixed ? pdac::k_tilde_flux2d<float> : pdac::k_tilde_flux2d<double>)<<<blocks(n), TPB, 0, st>>>(ctx->P, F),
+            ctx->launches++;
         pdac::k_tilde2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt, ctx->d_app0u, ctx->d_app0w), ctx->launches++;
     }
     if (ctx->P.alpha != 1.0 && ctx->cfg.rungekut > 1) {
@@ -1655,7 +1655,8 @@ static int enqueue_ygas(pdac_ctx *ctx, double dt, cudaStream_t st) {
             ctx->launches++;
         pdac::k_ygas3d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F, dt), ctx->launches++;
     } else {
-        pdac::k_ygas_flux2d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F), ctx->launches++;
+        (ctx->P.mixed ? pdac::k_ygas_flux2d<float> : pdac::k_ygas_flux2d<double>)<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F),
+            ctx->launches++;
         pdac::k_ygas2d<<<blocks(n), TPB, 0, st>>>(ctx->P, ctx->F, dt), ctx->launches++;
     }
     CK(cudaGetLastError());
@@ -1695,7 +1696,9 @@ static int enqueue_htilde(pdac_ctx *ctx, double dt, cudaStream_t st) {
             ctx->launches++;
         pdac::k_htilde3d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt), ctx->launches++;
     } else {
-        pdac::k_htilde_flux2d<true><<<blocks(n), TPB, 0, st>>>(ctx->P, F), ctx->launches++;
+        (ctx->P.mixed ? pdac::k_htilde_flux2d<true, float> : pdac::k_htilde_flux2d<true, double>)<<<blocks(n), TPB, 0, st>>>(
+            ctx->P, F),
+            ctx->launches++;
         pdac::k_htilde2d<<<blocks(n), TPB, 0, st>>>(ctx->P, F, dt), ctx->launches++;
     }
     CK(cudaGetLastError());
@@ -1838,9 +1841,15 @@ static long long enqueue_explicit(pdac_ctx *ctx, double dt, cudaStream_t st, boo
             }
             L += 2 + mom_launches(ctx->tile_shape);
         } else {
-            pdac::k_rk3_mflux<2><<<blocks(n), TPB, 0, st>>>(P, F);
-            pdac::k_tilde_flux2d<<<blocks(n), TPB, 0, st>>>(P, F);
-            pdac::k_htilde_flux2d<false><<<blocks(n), TPB, 0, st>>>(P, F);
+            if (P.mixed) {
+                pdac::k_rk3_mflux<2, float><<<blocks(n), TPB, 0, st>>>(P, F);
+                pdac::k_tilde_flux2d<float><<<blocks(n), TPB, 0, st>>>(P, F);
+                pdac::k_htilde_flux2d<false, float><<<blocks(n), TPB, 0, st>>>(P, F);
+            } else {
+                pdac::k_rk3_mflux<2><<<blocks(n), TPB, 0, st>>>(P, F);
+                pdac::k_tilde_flux2d<<<blocks(n), TPB, 0, st>>>(P, F);
+                pdac::k_htilde_flux2d<false><<<blocks(n), TPB, 0, st>>>(P, F);
+            }
             L += 3;
         }
     };

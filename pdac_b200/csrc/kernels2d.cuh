@@ -283,6 +283,9 @@ __global__ void k_fieldn2d(Prm P, Fld F) {
 // ---------------------------------------------------------------------------
 // tilde fluxes, compute_all_fluxes_tilde tilde.f:850-1326 (2D)
 // ---------------------------------------------------------------------------
+// Real: the arithmetic of the face fluxes (float in PDAC_PREC_MIXED; the
+// stencil values are the FP64 state rounded once, the fluxes stored in FP64)
+template <typename Real = double>
 __global__ void k_tilde_flux2d(Prm P, Fld F) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.ncell || !fluid(P, c)) return;
@@ -301,14 +304,14 @@ __global__ void k_tilde_flux2d(Prm P, Fld F) {
         double *fut = ph == 0 ? F.ugft : F.usft + (size_t)(ph - 1) * P.ncell;
         double *fwe = ph == 0 ? F.wgfe : F.wsfe + (size_t)(ph - 1) * P.ncell;
         double *fwt = ph == 0 ? F.wgft : F.wsft + (size_t)(ph - 1) * P.ncell;
-        St u, w, d, dsx, dsz;
+        St2T<Real> u, w, d, dsx, dsz;
         rnb2(u, U, R);
         rnb2(w, W, R);
         if (ib_masked(P, c)) { ib_mask2(P, u, R, 1); ib_mask2(P, w, R, 4); }
         nb2(d, D, R, M);
         interp_x2(P, d, i, dsx);
         interp_z2(P, d, k, dsz);
-        double ue = 0, ut = 0, uw = 0, ub = 0, we = 0, wt = 0, ww = 0, wb = 0;
+        Real ue = 0, ut = 0, uw = 0, ub = 0, we = 0, wt = 0, ww = 0, wb = 0;
         flu_2d(P, ue, ut, uw, ub, dow, dob, dsx, u, w, i);
         flw_2d(P, we, wt, ww, wb, dow, dob, dsz, u, w, i, k);
         if (mus) {
@@ -720,6 +723,7 @@ __device__ __forceinline__ void padjust(PAdj &s, double &p, int &kros, double d3
 // ---------------------------------------------------------------------------
 // ygas, ygas.f:27-325 (2D)
 // ---------------------------------------------------------------------------
+template <typename Real = double>
 __global__ void k_ygas_flux2d(Prm P, Fld F) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.ncell || !fluid(P, c)) return;
@@ -729,15 +733,15 @@ __global__ void k_ygas_flux2d(Prm P, Fld F) {
     raw2(P, i, k, R);
     rem2(P, i, k, R, M);
     bool dow = !fluid(P, R.w), dob = !fluid(P, R.b), mus = P.muscl > 0 && P.flag[c] == FLUID;
-    St d;
+    St2T<Real> d;
     first_nb2(d, F.rgp, R, M);
     if (mus) third_nb2(d, F.rgp, M);
-    double uw = F.ug[R.w], uc = F.ug[c], wb = F.wg[R.b], wc = F.wg[c];
+    Real uw = F.ug[R.w], uc = F.ug[c], wb = F.wg[R.b], wc = F.wg[c];
     for (int ig = 0; ig < P.ng; ++ig) {
         const double *Y = F.ygc + (size_t)ig * P.ncell;
-        St y;
+        St2T<Real> y;
         first_nb2(y, Y, R, M);
-        double fe = 0, ft = 0, fw = 0, fb = 0;
+        Real fe = 0, ft = 0, fw = 0, fb = 0;
         fsc_2d(P, fe, ft, fw, fb, dow, dob, d, y, uw, uc, wb, wc, i);
         if (mus) {
             third_nb2(y, Y, M);
@@ -784,7 +788,7 @@ __global__ void k_ygas2d(Prm P, Fld F, double dt) {
 // ---------------------------------------------------------------------------
 // GRAV adds the work of gravity to the convective flux (htilde); the
 // explicit solver's calc_all_fluxes (explicit_solver.f:2165-2885) has none
-template <bool GRAV>
+template <bool GRAV, typename Real = double>
 __global__ void k_htilde_flux2d(Prm P, Fld F) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.ncell || !fluid(P, c)) return;
@@ -804,27 +808,27 @@ __global__ void k_htilde_flux2d(Prm P, Fld F) {
         const double *W = ph == 0 ? F.wg : F.ws + off;
         double *fE = ph == 0 ? F.egfe : F.esfe + off;
         double *fT = ph == 0 ? F.egft : F.esft + off;
-        St en, de;
+        St2T<Real> en, de;
         first_nb2(en, EN, R, M);
         first_nb2(de, DE, R, M);
-        double uw = U[R.w], uc = U[c], wb = W[R.b], wc = W[c];
-        double fe = 0, ft = 0, fw = 0, fb = 0;
+        Real uw = U[R.w], uc = U[c], wb = W[R.b], wc = W[c];
+        Real fe = 0, ft = 0, fw = 0, fb = 0;
         fsc_2d(P, fe, ft, fw, fb, dow, dob, en, de, uw, uc, wb, wc, i);
         if (mus) {
             third_nb2(en, EN, M);
             third_nb2(de, DE, M);
             muscl_fsc_2d(P, fe, ft, en, de, uc, wc, i, k);
         }
-        double he = 0, ht = 0, hwv = 0, hbv = 0;
+        Real he = 0, ht = 0, hwv = 0, hbv = 0;
         bool visc = ph == 0 ? P.gas_viscosity : P.part_viscosity;
         if (visc) {
-            St ka, ep, te;
+            St2T<Real> ka, ep, te;
             if (ph == 0) {
                 first_nb2(ka, P.iturb ? F.kapgt : F.kapg, R, M);
                 first_nb2(ep, F.ep, R, M);
                 first_nb2(te, F.tg, R, M);
             } else {
-                double kk = P.kap[ph], ir = P.inrl[ph];
+                Real kk = P.kap[ph], ir = P.inrl[ph];
                 ka.c = ka.e = ka.w = ka.t = ka.b = kk;
                 ep.c = ir * de.c; ep.e = ir * de.e; ep.w = ir * de.w; ep.t = ir * de.t; ep.b = ir * de.b;
                 first_nb2(te, F.ts + off, R, M);
@@ -842,8 +846,8 @@ __global__ void k_htilde_flux2d(Prm P, Fld F) {
         // W/B faces towards non-fluid cells; when the neighbour's flag is not
         // exactly 1 but still fluid (dome/immb), hotc writes hgfw yet htilde
         // does not subtract it (htilde.f:338-339) -- only non-fluid matter here.
-        if (dow) fE[R.w] = fw - (hw ? hwv : 0.0);
-        if (dob) fT[R.b] = fb - (hb ? hbv : 0.0);
+        if (dow) fE[R.w] = fw - (hw ? hwv : Real(0));
+        if (dob) fT[R.b] = fb - (hb ? hbv : Real(0));
     }
 }
 

@@ -74,18 +74,20 @@ __device__ __forceinline__ void rem2(const Prm &P, int i, int k, const Raw2 &R, 
 }
 
 // ---- stencils (subscr.f TYPE(stencil)) -------------------------------------
-struct St {
-    double c, e, w, t, b, ee, ww, tt, bb, et, wt, eb, eet, ett, eee, ttt;
+template <typename Real>
+struct St2T {
+    Real c, e, w, t, b, ee, ww, tt, bb, et, wt, eb, eet, ett, eee, ttt;
 };
-template <typename T>
-__device__ __forceinline__ void nb2(St &s, const T *a, const Raw2 &R, const Rem2 &M) {  // subscr.f nb
+using St = St2T<double>;
+template <typename T, typename Real>
+__device__ __forceinline__ void nb2(St2T<Real> &s, const T *a, const Raw2 &R, const Rem2 &M) {  // subscr.f nb
     s.c = a[R.c]; s.e = a[M.e]; s.t = a[M.t]; s.w = a[M.w]; s.b = a[M.b];
     s.et = a[M.et]; s.wt = a[M.wt]; s.eb = a[M.eb]; s.ee = a[M.ee]; s.tt = a[M.tt];
     s.eet = a[M.eet]; s.ett = a[M.ett]; s.eee = a[M.eee]; s.ttt = a[M.ttt];
     s.ww = 0; s.bb = 0;
 }
-template <typename T>
-__device__ __forceinline__ void rnb2(St &s, const T *a, const Raw2 &R) {  // subscr.f rnb_r
+template <typename T, typename Real>
+__device__ __forceinline__ void rnb2(St2T<Real> &s, const T *a, const Raw2 &R) {  // subscr.f rnb_r
     s.c = a[R.c]; s.e = a[R.e]; s.t = a[R.t]; s.w = a[R.w]; s.b = a[R.b];
     s.wt = a[R.wt]; s.et = a[R.et]; s.eb = a[R.eb]; s.ee = a[R.ee]; s.tt = a[R.tt];
     s.eet = a[R.eet]; s.ett = a[R.ett]; s.eee = a[R.eee]; s.ttt = a[R.ttt];
@@ -103,22 +105,23 @@ __device__ __forceinline__ double ib_open(const Prm &P, int cell, int bit) {
 __device__ __forceinline__ bool ib_masked(const Prm &P, int c) {
     return P.immb && (P.flag[c] == BL_CELL || P.flag[c] == IMMB);
 }
-__device__ __forceinline__ void ib_mask2(const Prm &P, St &s, const Raw2 &R, int bit) {
-    s.c = s.c * ib_open(P, R.c, bit); s.e = s.e * ib_open(P, R.e, bit); s.w = s.w * ib_open(P, R.w, bit);
-    s.t = s.t * ib_open(P, R.t, bit); s.b = s.b * ib_open(P, R.b, bit);
-    s.ee = s.ee * ib_open(P, R.ee, bit); s.tt = s.tt * ib_open(P, R.tt, bit);
-    s.et = s.et * ib_open(P, R.et, bit); s.eb = s.eb * ib_open(P, R.eb, bit); s.wt = s.wt * ib_open(P, R.wt, bit);
+template <typename Real>
+__device__ __forceinline__ void ib_mask2(const Prm &P, St2T<Real> &s, const Raw2 &R, int bit) {
+    s.c = s.c * Real(ib_open(P, R.c, bit)); s.e = s.e * Real(ib_open(P, R.e, bit)); s.w = s.w * Real(ib_open(P, R.w, bit));
+    s.t = s.t * Real(ib_open(P, R.t, bit)); s.b = s.b * Real(ib_open(P, R.b, bit));
+    s.ee = s.ee * Real(ib_open(P, R.ee, bit)); s.tt = s.tt * Real(ib_open(P, R.tt, bit));
+    s.et = s.et * Real(ib_open(P, R.et, bit)); s.eb = s.eb * Real(ib_open(P, R.eb, bit)); s.wt = s.wt * Real(ib_open(P, R.wt, bit));
 }
-template <typename T>
-__device__ __forceinline__ void first_nb2(St &s, const T *a, const Raw2 &R, const Rem2 &M) {
+template <typename T, typename Real>
+__device__ __forceinline__ void first_nb2(St2T<Real> &s, const T *a, const Raw2 &R, const Rem2 &M) {
     s.c = a[R.c]; s.e = a[M.e]; s.t = a[M.t]; s.w = a[M.w]; s.b = a[M.b];
 }
-template <typename T>
-__device__ __forceinline__ void first_rnb2(St &s, const T *a, const Raw2 &R) {
+template <typename T, typename Real>
+__device__ __forceinline__ void first_rnb2(St2T<Real> &s, const T *a, const Raw2 &R) {
     s.c = a[R.c]; s.e = a[R.e]; s.t = a[R.t]; s.w = a[R.w]; s.b = a[R.b];
 }
-template <typename T>
-__device__ __forceinline__ void third_nb2(St &s, const T *a, const Rem2 &M) {
+template <typename T, typename Real>
+__device__ __forceinline__ void third_nb2(St2T<Real> &s, const T *a, const Rem2 &M) {
     s.ee = a[M.ee]; s.tt = a[M.tt]; s.ww = a[M.ww]; s.bb = a[M.bb];
 }
 
@@ -139,11 +142,12 @@ __device__ __forceinline__ Real limiter(int t, Real erre, double beta_) {
 }
 
 // ---- interp.f:14-320, members used in 2D -------------------------------------
-__device__ __forceinline__ void interp_x2(const Prm &P, const St &f, int i, St &s) {
-    const double *dx = P.dx;
+template <typename Real>
+__device__ __forceinline__ void interp_x2(const Prm &P, const St2T<Real> &f, int i, St2T<Real> &s) {
+    const Real *dx = Met<Real>::dx(P);
     int ip2 = min(P.nx, i + 2), ip3 = min(P.nx, i + 3);
-    double indxm = P.hx[i - 1], indxp = P.hx[i];
-    double indxpp = P.hx[i + 1], indxppp = P.hx[ip2];
+    Real indxm = Met<Real>::hx(P)[i - 1], indxp = Met<Real>::hx(P)[i];
+    Real indxpp = Met<Real>::hx(P)[i + 1], indxppp = Met<Real>::hx(P)[ip2];
     s.c = (dx[i + 1] * f.c + dx[i] * f.e) * indxp;
     s.e = (dx[ip2] * f.e + dx[i + 1] * f.ee) * indxpp;
     s.t = (dx[i + 1] * f.t + dx[i] * f.et) * indxp;
@@ -152,11 +156,12 @@ __device__ __forceinline__ void interp_x2(const Prm &P, const St &f, int i, St &
     s.ee = (dx[ip2] * f.eee + dx[ip3] * f.ee) * indxppp;
     s.tt = (dx[i] * f.ett + dx[i + 1] * f.tt) * indxp;
 }
-__device__ __forceinline__ void interp_z2(const Prm &P, const St &f, int k, St &s) {
-    const double *dz = P.dz;
+template <typename Real>
+__device__ __forceinline__ void interp_z2(const Prm &P, const St2T<Real> &f, int k, St2T<Real> &s) {
+    const Real *dz = Met<Real>::dz(P);
     int kp2 = min(P.nz, k + 2), kp3 = min(P.nz, k + 3);
-    double indzm = P.hz[k - 1], indzp = P.hz[k];
-    double indzpp = P.hz[k + 1], indzppp = P.hz[kp2];
+    Real indzm = Met<Real>::hz(P)[k - 1], indzp = Met<Real>::hz(P)[k];
+    Real indzpp = Met<Real>::hz(P)[k + 1], indzppp = Met<Real>::hz(P)[kp2];
     s.c = (dz[k + 1] * f.c + dz[k] * f.t) * indzp;
     s.e = (dz[k + 1] * f.e + dz[k] * f.et) * indzp;
     s.t = (dz[kp2] * f.t + dz[k + 1] * f.tt) * indzpp;
@@ -168,98 +173,102 @@ __device__ __forceinline__ void interp_z2(const Prm &P, const St &f, int k, St &
 
 // ---- momentum fluxes, flux_u.f:230-340 and flux_w.f:220-356 -------------------
 // W/B fluxes are produced only when that neighbour is not a fluid cell.
-__device__ __forceinline__ void flu_2d(const Prm &P, double &fe, double &ft, double &fw, double &fb, bool dow, bool dob,
-                                       const St &d, const St &u, const St &w, int i) {
-    const double *dx = P.dx;
-    double indxp = P.hx[i], cs;
+template <typename Real>
+__device__ __forceinline__ void flu_2d(const Prm &P, Real &fe, Real &ft, Real &fw, Real &fb, bool dow, bool dob,
+                                       const St2T<Real> &d, const St2T<Real> &u, const St2T<Real> &w, int i) {
+    const Real *dx = Met<Real>::dx(P);
+    Real indxp = Met<Real>::hx(P)[i], cs;
     if (dow) {
-        cs = 0.5 * (u.c + u.w);
-        fw = 0.5 * (cs - fabs(cs)) * d.c * u.c * P.r[i] + 0.5 * (cs + fabs(cs)) * d.w * u.w * P.r[i];
+        cs = Real(0.5) * (u.c + u.w);
+        fw = Real(0.5) * (cs - fabs(cs)) * d.c * u.c * Met<Real>::r(P)[i] + Real(0.5) * (cs + fabs(cs)) * d.w * u.w * Met<Real>::r(P)[i];
     }
     if (dob) {
         cs = (dx[i + 1] * w.b + dx[i] * w.eb) * indxp;
-        fb = 0.5 * (cs - fabs(cs)) * d.c * u.c + 0.5 * (cs + fabs(cs)) * d.b * u.b;
+        fb = Real(0.5) * (cs - fabs(cs)) * d.c * u.c + Real(0.5) * (cs + fabs(cs)) * d.b * u.b;
     }
-    cs = 0.5 * (u.c + u.e);
-    fe = 0.5 * (cs - fabs(cs)) * d.e * u.e * P.r[i + 1] + 0.5 * (cs + fabs(cs)) * d.c * u.c * P.r[i + 1];
+    cs = Real(0.5) * (u.c + u.e);
+    fe = Real(0.5) * (cs - fabs(cs)) * d.e * u.e * Met<Real>::r(P)[i + 1] + Real(0.5) * (cs + fabs(cs)) * d.c * u.c * Met<Real>::r(P)[i + 1];
     cs = (dx[i + 1] * w.c + dx[i] * w.e) * indxp;
-    ft = 0.5 * (cs - fabs(cs)) * d.t * u.t + 0.5 * (cs + fabs(cs)) * d.c * u.c;
+    ft = Real(0.5) * (cs - fabs(cs)) * d.t * u.t + Real(0.5) * (cs + fabs(cs)) * d.c * u.c;
 }
 
-__device__ __forceinline__ void muscl_flu_2d(const Prm &P, double &fe, double &ft, const St &d, const St &u, const St &w,
+template <typename Real>
+__device__ __forceinline__ void muscl_flu_2d(const Prm &P, Real &fe, Real &ft, const St2T<Real> &d, const St2T<Real> &u, const St2T<Real> &w,
                                              int i, int k, bool doe, bool dot) {
-    const double *dx = P.dx, *dz = P.dz, *indx = P.indx;
+    const Real *dx = Met<Real>::dx(P), *dz = Met<Real>::dz(P), *indx = Met<Real>::indx(P);
     int ip2 = min(P.nx, i + 2), kp2 = min(P.nz, k + 2);
-    double indxp = P.hx[i], indzm = P.hz[k - 1];
-    double indzp = P.hz[k], indzpp = P.hz[k + 1];
-    double erre, incr = 0, cs, lim, upwnd, gradc;
+    Real indxp = Met<Real>::hx(P)[i], indzm = Met<Real>::hz(P)[k - 1];
+    Real indzp = Met<Real>::hz(P)[k], indzpp = Met<Real>::hz(P)[k + 1];
+    Real erre, incr = 0, cs, lim, upwnd, gradc;
     if (doe) {
         gradc = indx[i + 1] * (d.e * u.e - d.c * u.c);
-        double gradw = indx[i] * (d.c * u.c - d.w * u.w);
-        double grade = indx[ip2] * (d.ee * u.ee - d.e * u.e);
-        erre = 0; cs = 0.5 * (u.c + u.e);
-        if (cs >= 0) { if (gradc != 0) erre = gradw / gradc; incr = 0.5 * dx[i + 1]; }
-        else if (cs < 0) { if (gradc != 0) erre = grade / gradc; incr = -0.5 * dx[i + 1]; }
+        Real gradw = indx[i] * (d.c * u.c - d.w * u.w);
+        Real grade = indx[ip2] * (d.ee * u.ee - d.e * u.e);
+        erre = 0; cs = Real(0.5) * (u.c + u.e);
+        if (cs >= 0) { if (gradc != 0) erre = gradw / gradc; incr = Real(0.5) * dx[i + 1]; }
+        else if (cs < 0) { if (gradc != 0) erre = grade / gradc; incr = -Real(0.5) * dx[i + 1]; }
         lim = limiter(P.lv, erre, P.beta);
         upwnd = lim * gradc * incr;
-        fe = fe + upwnd * cs * P.r[i + 1];
+        fe = fe + upwnd * cs * Met<Real>::r(P)[i + 1];
     }
     if (dot) {
-        gradc = (d.t * u.t - d.c * u.c) * 2.0 * indzp;
-        double gradb = (d.c * u.c - d.b * u.b) * 2.0 * indzm;
-        double gradt = (d.tt * u.tt - d.t * u.t) * 2.0 * indzpp;
+        gradc = (d.t * u.t - d.c * u.c) * Real(2.0) * indzp;
+        Real gradb = (d.c * u.c - d.b * u.b) * Real(2.0) * indzm;
+        Real gradt = (d.tt * u.tt - d.t * u.t) * Real(2.0) * indzpp;
         erre = 0; cs = (dx[i + 1] * w.c + dx[i] * w.e) * indxp;
-        if (cs >= 0) { if (gradc != 0) erre = gradb / gradc; incr = 0.5 * dz[k]; }
-        else if (cs < 0) { if (gradc != 0) erre = gradt / gradc; incr = -0.5 * dz[k + 1]; }
+        if (cs >= 0) { if (gradc != 0) erre = gradb / gradc; incr = Real(0.5) * dz[k]; }
+        else if (cs < 0) { if (gradc != 0) erre = gradt / gradc; incr = -Real(0.5) * dz[k + 1]; }
         lim = limiter(P.lv, erre, P.beta);
         upwnd = lim * gradc * incr;
         ft = ft + upwnd * cs;
     }
 }
 
-__device__ __forceinline__ void flw_2d(const Prm &P, double &fe, double &ft, double &fw, double &fb, bool dow, bool dob,
-                                       const St &d, const St &u, const St &w, int i, int k) {
-    const double *dz = P.dz;
-    double indzp = P.hz[k], cs;
+template <typename Real>
+__device__ __forceinline__ void flw_2d(const Prm &P, Real &fe, Real &ft, Real &fw, Real &fb, bool dow, bool dob,
+                                       const St2T<Real> &d, const St2T<Real> &u, const St2T<Real> &w, int i, int k) {
+    const Real *dz = Met<Real>::dz(P);
+    Real indzp = Met<Real>::hz(P)[k], cs;
     if (dow) {
         cs = (u.wt * dz[k] + u.w * dz[k + 1]) * indzp;
-        fw = 0.5 * d.w * w.w * (cs + fabs(cs)) * P.rb[i - 1] + 0.5 * d.c * w.c * (cs - fabs(cs)) * P.rb[i - 1];
+        fw = Real(0.5) * d.w * w.w * (cs + fabs(cs)) * Met<Real>::rb(P)[i - 1] + Real(0.5) * d.c * w.c * (cs - fabs(cs)) * Met<Real>::rb(P)[i - 1];
     }
     if (dob) {
-        cs = 0.5 * (w.c + w.b);
-        fb = 0.5 * d.b * w.b * (cs + fabs(cs)) + 0.5 * d.c * w.c * (cs - fabs(cs));
+        cs = Real(0.5) * (w.c + w.b);
+        fb = Real(0.5) * d.b * w.b * (cs + fabs(cs)) + Real(0.5) * d.c * w.c * (cs - fabs(cs));
     }
     cs = indzp * (u.c * dz[k + 1] + u.t * dz[k]);
-    fe = 0.5 * d.c * w.c * (cs + fabs(cs)) * P.rb[i] + 0.5 * d.e * w.e * (cs - fabs(cs)) * P.rb[i];
-    cs = 0.5 * (w.t + w.c);
-    ft = 0.5 * d.c * w.c * (cs + fabs(cs)) + 0.5 * d.t * w.t * (cs - fabs(cs));
+    fe = Real(0.5) * d.c * w.c * (cs + fabs(cs)) * Met<Real>::rb(P)[i] + Real(0.5) * d.e * w.e * (cs - fabs(cs)) * Met<Real>::rb(P)[i];
+    cs = Real(0.5) * (w.t + w.c);
+    ft = Real(0.5) * d.c * w.c * (cs + fabs(cs)) + Real(0.5) * d.t * w.t * (cs - fabs(cs));
 }
 
-__device__ __forceinline__ void muscl_flw_2d(const Prm &P, double &fe, double &ft, const St &d, const St &u, const St &w,
+template <typename Real>
+__device__ __forceinline__ void muscl_flw_2d(const Prm &P, Real &fe, Real &ft, const St2T<Real> &d, const St2T<Real> &u, const St2T<Real> &w,
                                              int i, int k, bool doe, bool dot) {
-    const double *dx = P.dx, *dz = P.dz, *indz = P.indz;
+    const Real *dx = Met<Real>::dx(P), *dz = Met<Real>::dz(P), *indz = Met<Real>::indz(P);
     int ip2 = min(P.nx, i + 2), kp2 = min(P.nz, k + 2);
-    double indxm = P.hx[i - 1], indxp = P.hx[i];
-    double indxpp = P.hx[i + 1], indzp = P.hz[k];
-    double erre, incr = 0, cs, lim, upwnd, gradc;
+    Real indxm = Met<Real>::hx(P)[i - 1], indxp = Met<Real>::hx(P)[i];
+    Real indxpp = Met<Real>::hx(P)[i + 1], indzp = Met<Real>::hz(P)[k];
+    Real erre, incr = 0, cs, lim, upwnd, gradc;
     if (doe) {
-        gradc = 2.0 * indxp * (d.e * w.e - d.c * w.c);
-        double gradw = 2.0 * indxm * (d.c * w.c - d.w * w.w);
-        double grade = 2.0 * indxpp * (d.ee * w.ee - d.e * w.e);
+        gradc = Real(2.0) * indxp * (d.e * w.e - d.c * w.c);
+        Real gradw = Real(2.0) * indxm * (d.c * w.c - d.w * w.w);
+        Real grade = Real(2.0) * indxpp * (d.ee * w.ee - d.e * w.e);
         erre = 0; cs = indzp * (u.c * dz[k + 1] + u.t * dz[k]);
-        if (cs >= 0) { if (gradc != 0) erre = gradw / gradc; incr = 0.5 * dx[i]; }
-        else if (cs < 0) { if (gradc != 0) erre = grade / gradc; incr = -0.5 * dx[i + 1]; }
+        if (cs >= 0) { if (gradc != 0) erre = gradw / gradc; incr = Real(0.5) * dx[i]; }
+        else if (cs < 0) { if (gradc != 0) erre = grade / gradc; incr = -Real(0.5) * dx[i + 1]; }
         lim = limiter(P.lv, erre, P.beta);
         upwnd = lim * gradc * incr;
-        fe = fe + upwnd * cs * P.rb[i];
+        fe = fe + upwnd * cs * Met<Real>::rb(P)[i];
     }
     if (dot) {
         gradc = (d.t * w.t - d.c * w.c) * indz[k + 1];
-        double gradb = (d.c * w.c - d.b * w.b) * indz[k];
-        double gradt = (d.tt * w.tt - d.t * w.t) * indz[kp2];
-        erre = 0; cs = 0.5 * (w.t + w.c);
-        if (cs >= 0) { if (gradc != 0) erre = gradb / gradc; incr = 0.5 * dz[k + 1]; }
-        else if (cs < 0) { if (gradc != 0) erre = gradt / gradc; incr = -0.5 * dz[k + 1]; }
+        Real gradb = (d.c * w.c - d.b * w.b) * indz[k];
+        Real gradt = (d.tt * w.tt - d.t * w.t) * indz[kp2];
+        erre = 0; cs = Real(0.5) * (w.t + w.c);
+        if (cs >= 0) { if (gradc != 0) erre = gradb / gradc; incr = Real(0.5) * dz[k + 1]; }
+        else if (cs < 0) { if (gradc != 0) erre = gradt / gradc; incr = -Real(0.5) * dz[k + 1]; }
         lim = limiter(P.lv, erre, P.beta);
         upwnd = lim * gradc * incr;
         ft = ft + upwnd * cs;
@@ -270,123 +279,129 @@ __device__ __forceinline__ void muscl_flw_2d(const Prm &P, double &fe, double &f
 // Each helper returns one face of the cell (i, k) as the reference computes it
 // in that cell's call: first-order donor cell plus the MUSCL correction when
 // `muscl_on` (cell flag == fluid) and the neighbour test of fmas holds.
-struct MF2 { double w, e, b, t; };
+template <typename Real>
+struct MF2T { Real w, e, b, t; };
+using MF2 = MF2T<double>;
 
-__device__ __forceinline__ void massflux_2d(const Prm &P, const St &d, double uw, double uc, double wb, double wc,
-                                            int i, int k, bool muscl_on, int flw, int fle, int flb, int flt, MF2 &f) {
-    const double *dx = P.dx, *dz = P.dz, *rb = P.rb;
-    double cs;
-    cs = uw; f.w = 0.5 * (cs - fabs(cs)) * d.c * rb[i - 1] + 0.5 * (cs + fabs(cs)) * d.w * rb[i - 1];
-    cs = wb; f.b = 0.5 * (cs - fabs(cs)) * d.c + 0.5 * (cs + fabs(cs)) * d.b;
-    cs = uc; f.e = 0.5 * (cs - fabs(cs)) * d.e * rb[i] + 0.5 * (cs + fabs(cs)) * d.c * rb[i];
-    cs = wc; f.t = 0.5 * (cs - fabs(cs)) * d.t + 0.5 * (cs + fabs(cs)) * d.c;
+template <typename Real>
+__device__ __forceinline__ void massflux_2d(const Prm &P, const St2T<Real> &d, Real uw, Real uc, Real wb, Real wc,
+                                            int i, int k, bool muscl_on, int flw, int fle, int flb, int flt, MF2T<Real> &f) {
+    const Real *dx = Met<Real>::dx(P), *dz = Met<Real>::dz(P), *rb = Met<Real>::rb(P);
+    Real cs;
+    cs = uw; f.w = Real(0.5) * (cs - fabs(cs)) * d.c * rb[i - 1] + Real(0.5) * (cs + fabs(cs)) * d.w * rb[i - 1];
+    cs = wb; f.b = Real(0.5) * (cs - fabs(cs)) * d.c + Real(0.5) * (cs + fabs(cs)) * d.b;
+    cs = uc; f.e = Real(0.5) * (cs - fabs(cs)) * d.e * rb[i] + Real(0.5) * (cs + fabs(cs)) * d.c * rb[i];
+    cs = wc; f.t = Real(0.5) * (cs - fabs(cs)) * d.t + Real(0.5) * (cs + fabs(cs)) * d.c;
     if (!muscl_on) return;
     int im2 = max(1, i - 2), ip2 = min(P.nx, i + 2), km2 = max(1, k - 2), kp2 = min(P.nz, k + 2);
-    double indxmm = P.hx[max(i - 2, 0)], indxm = P.hx[i - 1];
-    double indxp = P.hx[i], indxpp = P.hx[i + 1];
-    double indzmm = P.hz[max(k - 2, 0)], indzm = P.hz[k - 1];
-    double indzp = P.hz[k], indzpp = P.hz[k + 1];
-    double gradc, gradw, grade, gradb, gradt, erre, incr = 0, lim, upwnd;
+    Real indxmm = Met<Real>::hx(P)[max(i - 2, 0)], indxm = Met<Real>::hx(P)[i - 1];
+    Real indxp = Met<Real>::hx(P)[i], indxpp = Met<Real>::hx(P)[i + 1];
+    Real indzmm = Met<Real>::hz(P)[max(k - 2, 0)], indzm = Met<Real>::hz(P)[k - 1];
+    Real indzp = Met<Real>::hz(P)[k], indzpp = Met<Real>::hz(P)[k + 1];
+    Real gradc, gradw, grade, gradb, gradt, erre, incr = 0, lim, upwnd;
     // West
-    gradc = 2.0 * indxm * (d.c - d.w);
-    gradw = 2.0 * indxmm * (d.w - d.ww);
-    grade = 2.0 * indxp * (d.e - d.c);
+    gradc = Real(2.0) * indxm * (d.c - d.w);
+    gradw = Real(2.0) * indxmm * (d.w - d.ww);
+    grade = Real(2.0) * indxp * (d.e - d.c);
     lim = 0; erre = 0; cs = uw;
-    if (cs >= 0) { if (gradc != 0) erre = gradw / gradc; incr = 0.5 * dx[i - 1]; }
-    else if (cs < 0) { if (gradc != 0) erre = grade / gradc; incr = -0.5 * dx[i]; }
+    if (cs >= 0) { if (gradc != 0) erre = gradw / gradc; incr = Real(0.5) * dx[i - 1]; }
+    else if (cs < 0) { if (gradc != 0) erre = grade / gradc; incr = -Real(0.5) * dx[i]; }
     if (i != 2 && flw == FLUID) lim = limiter(P.lm, erre, P.beta);
     upwnd = lim * gradc * incr;
     f.w = f.w + upwnd * cs * rb[i - 1];
     // East
     gradw = gradc; gradc = grade;
-    grade = 2.0 * indxpp * (d.ee - d.e);
+    grade = Real(2.0) * indxpp * (d.ee - d.e);
     lim = 0; erre = 0; cs = uc;
-    if (cs >= 0) { if (gradc != 0) erre = gradw / gradc; incr = 0.5 * dx[i]; }
-    else if (cs < 0) { if (gradc != 0) erre = grade / gradc; incr = -0.5 * dx[i + 1]; }
+    if (cs >= 0) { if (gradc != 0) erre = gradw / gradc; incr = Real(0.5) * dx[i]; }
+    else if (cs < 0) { if (gradc != 0) erre = grade / gradc; incr = -Real(0.5) * dx[i + 1]; }
     if (i != P.nx - 1 && fle == FLUID) lim = limiter(P.lm, erre, P.beta);
     upwnd = lim * gradc * incr;
     f.e = f.e + upwnd * cs * rb[i];
     // Bottom
-    gradc = 2.0 * indzm * (d.c - d.b);
-    gradb = 2.0 * indzmm * (d.b - d.bb);
-    gradt = 2.0 * indzp * (d.t - d.c);
+    gradc = Real(2.0) * indzm * (d.c - d.b);
+    gradb = Real(2.0) * indzmm * (d.b - d.bb);
+    gradt = Real(2.0) * indzp * (d.t - d.c);
     lim = 0; erre = 0; cs = wb;
-    if (cs >= 0) { if (gradc != 0) erre = gradb / gradc; incr = 0.5 * dz[k - 1]; }
-    else if (cs < 0) { if (gradc != 0) erre = gradt / gradc; incr = -0.5 * dz[k]; }
+    if (cs >= 0) { if (gradc != 0) erre = gradb / gradc; incr = Real(0.5) * dz[k - 1]; }
+    else if (cs < 0) { if (gradc != 0) erre = gradt / gradc; incr = -Real(0.5) * dz[k]; }
     if (k != 2 && flb == FLUID) lim = limiter(P.lm, erre, P.beta);
     upwnd = lim * gradc * incr;
     f.b = f.b + upwnd * cs;
     // Top
     gradb = gradc; gradc = gradt;
-    gradt = 2.0 * indzpp * (d.tt - d.t);
+    gradt = Real(2.0) * indzpp * (d.tt - d.t);
     lim = 0; erre = 0; cs = wc;
-    if (cs >= 0) { if (gradc != 0) erre = gradb / gradc; incr = 0.5 * dz[k]; }
-    else if (cs < 0) { if (gradc != 0) erre = gradt / gradc; incr = -0.5 * dz[k + 1]; }
+    if (cs >= 0) { if (gradc != 0) erre = gradb / gradc; incr = Real(0.5) * dz[k]; }
+    else if (cs < 0) { if (gradc != 0) erre = gradt / gradc; incr = -Real(0.5) * dz[k + 1]; }
     if (k != P.nz - 1 && flt == FLUID) lim = limiter(P.lm, erre, P.beta);
     upwnd = lim * gradc * incr;
     f.t = f.t + upwnd * cs;
 }
 
 // ---- scalar fluxes, flux_sc.f:236-390 -------------------------------------------
-__device__ __forceinline__ void fsc_2d(const Prm &P, double &fe, double &ft, double &fw, double &fb, bool dow, bool dob,
-                                       const St &d, const St &f, double uw, double uc, double wb, double wc, int i) {
-    const double *rb = P.rb;
-    double cs;
-    if (dow) { cs = uw; fw = 0.5 * (cs - fabs(cs)) * d.c * f.c * rb[i - 1] + 0.5 * (cs + fabs(cs)) * d.w * f.w * rb[i - 1]; }
-    if (dob) { cs = wb; fb = 0.5 * (cs - fabs(cs)) * d.c * f.c + 0.5 * (cs + fabs(cs)) * d.b * f.b; }
-    cs = uc; fe = 0.5 * (cs - fabs(cs)) * d.e * f.e * rb[i] + 0.5 * (cs + fabs(cs)) * d.c * f.c * rb[i];
-    cs = wc; ft = 0.5 * (cs - fabs(cs)) * d.t * f.t + 0.5 * (cs + fabs(cs)) * d.c * f.c;
+template <typename Real>
+__device__ __forceinline__ void fsc_2d(const Prm &P, Real &fe, Real &ft, Real &fw, Real &fb, bool dow, bool dob,
+                                       const St2T<Real> &d, const St2T<Real> &f, Real uw, Real uc, Real wb, Real wc, int i) {
+    const Real *rb = Met<Real>::rb(P);
+    Real cs;
+    if (dow) { cs = uw; fw = Real(0.5) * (cs - fabs(cs)) * d.c * f.c * rb[i - 1] + Real(0.5) * (cs + fabs(cs)) * d.w * f.w * rb[i - 1]; }
+    if (dob) { cs = wb; fb = Real(0.5) * (cs - fabs(cs)) * d.c * f.c + Real(0.5) * (cs + fabs(cs)) * d.b * f.b; }
+    cs = uc; fe = Real(0.5) * (cs - fabs(cs)) * d.e * f.e * rb[i] + Real(0.5) * (cs + fabs(cs)) * d.c * f.c * rb[i];
+    cs = wc; ft = Real(0.5) * (cs - fabs(cs)) * d.t * f.t + Real(0.5) * (cs + fabs(cs)) * d.c * f.c;
 }
-__device__ __forceinline__ void muscl_fsc_2d(const Prm &P, double &fe, double &ft, const St &d, const St &f, double uc,
-                                             double wc, int i, int k) {
-    const double *dx = P.dx, *dz = P.dz;
+template <typename Real>
+__device__ __forceinline__ void muscl_fsc_2d(const Prm &P, Real &fe, Real &ft, const St2T<Real> &d, const St2T<Real> &f, Real uc,
+                                             Real wc, int i, int k) {
+    const Real *dx = Met<Real>::dx(P), *dz = Met<Real>::dz(P);
     int ip2 = min(P.nx, i + 2), kp2 = min(P.nz, k + 2);
-    double indxm = P.hx[i - 1], indxp = P.hx[i], indxpp = P.hx[i + 1];
-    double indzm = P.hz[k - 1], indzp = P.hz[k], indzpp = P.hz[k + 1];
-    double gradc = 2.0 * indxp * (d.e * f.e - d.c * f.c);
-    double gradw = 2.0 * indxm * (d.c * f.c - d.w * f.w);
-    double grade = 2.0 * indxpp * (d.ee * f.ee - d.e * f.e);
-    double lim = 0, erre = 0, incr = 0, cs = uc, upwnd;
-    if (cs >= 0) { if (gradc != 0) erre = gradw / gradc; incr = 0.5 * dx[i]; }
-    else if (cs < 0) { if (gradc != 0) erre = grade / gradc; incr = -0.5 * dx[i + 1]; }
+    Real indxm = Met<Real>::hx(P)[i - 1], indxp = Met<Real>::hx(P)[i], indxpp = Met<Real>::hx(P)[i + 1];
+    Real indzm = Met<Real>::hz(P)[k - 1], indzp = Met<Real>::hz(P)[k], indzpp = Met<Real>::hz(P)[k + 1];
+    Real gradc = Real(2.0) * indxp * (d.e * f.e - d.c * f.c);
+    Real gradw = Real(2.0) * indxm * (d.c * f.c - d.w * f.w);
+    Real grade = Real(2.0) * indxpp * (d.ee * f.ee - d.e * f.e);
+    Real lim = 0, erre = 0, incr = 0, cs = uc, upwnd;
+    if (cs >= 0) { if (gradc != 0) erre = gradw / gradc; incr = Real(0.5) * dx[i]; }
+    else if (cs < 0) { if (gradc != 0) erre = grade / gradc; incr = -Real(0.5) * dx[i + 1]; }
     if (i != P.nx - 1) lim = limiter(P.lm, erre, P.beta);
     upwnd = lim * gradc * incr;
-    fe = fe + upwnd * cs * P.rb[i];
-    gradc = 2.0 * indzp * (d.t * f.t - d.c * f.c);
-    double gradb = 2.0 * indzm * (d.c * f.c - d.b * f.b);
-    double gradt = 2.0 * indzpp * (d.tt * f.tt - d.t * f.t);
+    fe = fe + upwnd * cs * Met<Real>::rb(P)[i];
+    gradc = Real(2.0) * indzp * (d.t * f.t - d.c * f.c);
+    Real gradb = Real(2.0) * indzm * (d.c * f.c - d.b * f.b);
+    Real gradt = Real(2.0) * indzpp * (d.tt * f.tt - d.t * f.t);
     lim = 0; erre = 0; cs = wc;
-    if (cs >= 0) { if (gradc != 0) erre = gradb / gradc; incr = 0.5 * dz[k]; }
-    else if (cs < 0) { if (gradc != 0) erre = gradt / gradc; incr = -0.5 * dz[k + 1]; }
+    if (cs >= 0) { if (gradc != 0) erre = gradb / gradc; incr = Real(0.5) * dz[k]; }
+    else if (cs < 0) { if (gradc != 0) erre = gradt / gradc; incr = -Real(0.5) * dz[k + 1]; }
     if (k != P.nz - 1) lim = limiter(P.lm, erre, P.beta);
     upwnd = lim * gradc * incr;
     ft = ft + upwnd * cs;
 }
 
 // ---- hotc.f:12-82 (2D members) ---------------------------------------------------
-__device__ __forceinline__ void hotc_2d(const Prm &P, double &hfe, double &hft, double &hfw, double &hfb, bool dow, bool dob,
-                                        const St &ep, const St &tg, const St &ka, int i, int k) {
-    const double *dx = P.dx, *dz = P.dz;
+template <typename Real>
+__device__ __forceinline__ void hotc_2d(const Prm &P, Real &hfe, Real &hft, Real &hfw, Real &hfb, bool dow, bool dob,
+                                        const St2T<Real> &ep, const St2T<Real> &tg, const St2T<Real> &ka, int i, int k) {
+    const Real *dx = Met<Real>::dx(P), *dz = Met<Real>::dz(P);
     if (dow) {
-        double indxm = P.hx[i - 1];
-        double kmw = (dx[i - 1] * ka.c + dx[i] * ka.w) * indxm;
-        double epmw = (dx[i - 1] * ep.c + dx[i] * ep.w) * indxm;
-        hfw = kmw * epmw * (tg.c - tg.w) * indxm * 2.0 * P.rb[i - 1];
+        Real indxm = Met<Real>::hx(P)[i - 1];
+        Real kmw = (dx[i - 1] * ka.c + dx[i] * ka.w) * indxm;
+        Real epmw = (dx[i - 1] * ep.c + dx[i] * ep.w) * indxm;
+        hfw = kmw * epmw * (tg.c - tg.w) * indxm * Real(2.0) * Met<Real>::rb(P)[i - 1];
     }
     if (dob) {
-        double indzm = P.hz[k - 1];
-        double kmb = (dz[k - 1] * ka.c + dz[k] * ka.b) * indzm;
-        double epmb = (dz[k - 1] * ep.c + dz[k] * ep.b) * indzm;
-        hfb = kmb * epmb * (tg.c - tg.b) * indzm * 2.0;
+        Real indzm = Met<Real>::hz(P)[k - 1];
+        Real kmb = (dz[k - 1] * ka.c + dz[k] * ka.b) * indzm;
+        Real epmb = (dz[k - 1] * ep.c + dz[k] * ep.b) * indzm;
+        hfb = kmb * epmb * (tg.c - tg.b) * indzm * Real(2.0);
     }
-    double indxp = P.hx[i];
-    double kme = (dx[i + 1] * ka.c + dx[i] * ka.e) * indxp;
-    double epme = (dx[i + 1] * ep.c + dx[i] * ep.e) * indxp;
-    hfe = kme * epme * (tg.e - tg.c) * indxp * 2.0 * P.rb[i];
-    double indzp = P.hz[k];
-    double kmt = (dz[k + 1] * ka.c + dz[k] * ka.t) * indzp;
-    double epmt = (dz[k + 1] * ep.c + dz[k] * ep.t) * indzp;
-    hft = kmt * epmt * (tg.t - tg.c) * indzp * 2.0;
+    Real indxp = Met<Real>::hx(P)[i];
+    Real kme = (dx[i + 1] * ka.c + dx[i] * ka.e) * indxp;
+    Real epme = (dx[i + 1] * ep.c + dx[i] * ep.e) * indxp;
+    hfe = kme * epme * (tg.e - tg.c) * indxp * Real(2.0) * Met<Real>::rb(P)[i];
+    Real indzp = Met<Real>::hz(P)[k];
+    Real kmt = (dz[k + 1] * ka.c + dz[k] * ka.t) * indzp;
+    Real epmt = (dz[k + 1] * ep.c + dz[k] * ep.t) * indzp;
+    hft = kmt * epmt * (tg.t - tg.c) * indzp * Real(2.0);
 }
 
 // ---- closures ----------------------------------------------------------------

@@ -456,14 +456,15 @@ __global__ void __launch_bounds__(128, PDAC_FLUX_MINB) k_rk3_mflux(Prm P, Fld F)
             const double *W = ph == 0 ? F.wg : F.ws + off;
             double *fe = ph == 0 ? F.rgfe : F.rsfe + off;
             double *ft = ph == 0 ? F.rgft : F.rsft + off;
-            St d;
+            St2T<Real> d;
             first_nb2(d, Dn, R, M);
             if (mus) {
                 third_nb2(d, Dn, M);
                 d.ww = 0.0; d.bb = 0.0;
             }
-            MF2 f;
-            massflux_2d(P, d, U[R.w], U[c], W[R.b], W[c], i, k, mus, fl[R.w], fl[R.e], fl[R.b], fl[R.t], f);
+            MF2T<Real> f;
+            massflux_2d(P, d, Real(U[R.w]), Real(U[c]), Real(W[R.b]), Real(W[c]), i, k, mus, fl[R.w], fl[R.e], fl[R.b],
+                        fl[R.t], f);
             fe[R.w] = f.w;
             ft[R.b] = f.b;
             if (!fluid(P, R.e)) fe[c] = f.e;
