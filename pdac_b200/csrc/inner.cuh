@@ -103,6 +103,33 @@ struct FaceK<NP, true> {
 // the six scalars of FaceK
 enum { FK_PNB = 0, FK_D0EPNB, FK_K1, FK_K2, FK_D1, FK_INV };
 
+// The loop-invariant density stencil of one face's mass fluxes by phase:
+// the near (cm, cp) and far (cf) neighbour values and the cell's own values
+// at loop entry (o, read by opt_inner_loop's stale slots).  SH = true keeps
+// them in this lane's column of a shared [4 NC][KS] array, as FaceK does.
+template <int NC, bool SH>
+struct DensK;
+
+template <int NC>
+struct DensK<NC, false> {
+    double cm_[NC], cp_[NC], cf_[NC], o_[NC];
+    __device__ __forceinline__ explicit DensK(double *) {}
+    __device__ __forceinline__ double &cm(int l) { return cm_[l]; }
+    __device__ __forceinline__ double &cp(int l) { return cp_[l]; }
+    __device__ __forceinline__ double &cf(int l) { return cf_[l]; }
+    __device__ __forceinline__ double &o(int l) { return o_[l]; }
+};
+
+template <int NC>
+struct DensK<NC, true> {
+    double *s;  // this lane's column: element q at s[q * KS]
+    __device__ __forceinline__ explicit DensK(double *col) : s(col) {}
+    __device__ __forceinline__ double &cm(int l) { return s[l * KS]; }
+    __device__ __forceinline__ double &cp(int l) { return s[(NC + l) * KS]; }
+    __device__ __forceinline__ double &cf(int l) { return s[(2 * NC + l) * KS]; }
+    __device__ __forceinline__ double &o(int l) { return s[(3 * NC + l) * KS]; }
+};
+
 template <int NP, bool RO, class KT>
 __device__ __forceinline__ void face_prepare(const Prm &P, const Fld &F, int c, int nb, int raw, int ii, int dir,
                                              int side, double dt, KT &K) {
@@ -178,6 +205,9 @@ __device__ __forceinline__ void face_assemble(const Prm &P, KT &K, int side, dou
 #define PDAC_INNER_MINB_SMALL 3
 #endif
 #define PDAC_INNER_MINB(NP) ((NP) > 0 && (NP) <= 4 ? PDAC_INNER_MINB_SMALL : 2)
+#ifndef PDAC_INNER_SHD_MAXP
+#define PDAC_INNER_SHD_MAXP 4
+#endif
 
 // the inner loop of the worklist's nwork cells (outer sweep nit, 1-based)
 // by the warps warp, warp + nwarps, ... of the launch; RO as in ldro
@@ -195,6 +225,10 @@ __device__ __forceinline__ void inner_team_run(const Prm &P, const Fld &F, doubl
     const unsigned tmask = ((1u << T) - 1u) << tb;
     constexpr bool SH = NP > 0 && NP <= 6;  // FaceK in shared memory (40 KB per block at NP = 6)
     __shared__ double kcols[SH ? FaceK<NP, true>::N : 1][SH ? KS : 1];
+    // DensK in shared memory up to four phases (16 KB per block at NP = 4;
+    // with FaceK within the 48 KB of static shared memory a block may hold)
+    constexpr bool SHD = NP > 0 && NP <= PDAC_INNER_SHD_MAXP;
+    __shared__ double dcols[SHD ? 4 * NC : 1][SHD ? KS : 1];
     for (int w = warp * TPW + tw; w < nwork; w += nwarps * TPW) {
         const int c = list[w];
         int i, j, k;
@@ -253,24 +287,24 @@ __device__ __forceinline__ void inner_team_run(const Prm &P, const Fld &F, doubl
         // values, or the cell's own current value where the slot is the cell
         const int rfar = minus ? rmm : rpp;
         const bool sm = rm == c, sp = rp == c, sfar = rfar == c;
-        double cm[NC], cp[NC], cfar[NC];
-        cm[0] = ldro<RO>(F.rgp + rm); cp[0] = ldro<RO>(F.rgp + rp); cfar[0] = mus ? ldro<RO>(F.rgp + rfar) : 0.0;
+        DensK<NC, SHD> Dk(&dcols[0][SHD ? threadIdx.x : 0]);
+        Dk.cm(0) = ldro<RO>(F.rgp + rm); Dk.cp(0) = ldro<RO>(F.rgp + rp); Dk.cf(0) = mus ? ldro<RO>(F.rgp + rfar) : 0.0;
 #pragma unroll
         for (int l = 2; l <= nph; ++l) {
             const double *D_ = F.rlk + (size_t)(l - 2) * n;
-            cm[l - 1] = ldro<RO>(D_ + rm); cp[l - 1] = ldro<RO>(D_ + rp); cfar[l - 1] = mus ? ldro<RO>(D_ + rfar) : 0.0;
+            Dk.cm(l - 1) = ldro<RO>(D_ + rm); Dk.cp(l - 1) = ldro<RO>(D_ + rp);
+            Dk.cf(l - 1) = mus ? ldro<RO>(D_ + rfar) : 0.0;
         }
         // opt_inner_loop (iter.f:1255-1547) builds the density stencils once
         // and updates only their centre: a neighbour slot remapped to the
         // cell keeps the loop-entry value there
-        double own0[NC];
-        own0[0] = F.rgp[c];
+        Dk.o(0) = F.rgp[c];
 #pragma unroll
-        for (int l = 2; l <= nph; ++l) own0[l - 1] = F.rlk[(size_t)(l - 2) * n + c];
+        for (int l = 2; l <= nph; ++l) Dk.o(l - 1) = F.rlk[(size_t)(l - 2) * n + c];
         const bool stale = P.opt == 2;
         auto mflux = [&](int ph, double own) {
-            const double slot = stale ? own0[ph] : own;
-            double dm = sm ? slot : cm[ph], dp = sp ? slot : cp[ph], df = sfar ? slot : cfar[ph];
+            const double slot = stale ? Dk.o(ph) : own;
+            double dm = sm ? slot : Dk.cm(ph), dp = sp ? slot : Dk.cp(ph), df = sfar ? slot : Dk.cf(ph);
             return minus ? face_mflux(P, g, true, vel[ph], own, dm, df, dp, 0.0, mus)
                          : face_mflux(P, g, false, vel[ph], own, dm, 0.0, dp, df, mus);
         };
