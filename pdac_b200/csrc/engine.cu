@@ -238,6 +238,38 @@ inline int blocks(long n, int tpb = TPB) { return (int)((n + tpb - 1) / tpb); }
         }                                                                          \
     } while (0)
 
+// the inner-loop kernels (k_inner_team) with their dynamic shared memory
+#define INNER_LAUNCH_D(nph, KERNEL, D, grid, tpb, st, ...)                                                   \
+    do {                                                                                                     \
+        switch (nph) {                                                                                       \
+            case 2: KERNEL<2, D><<<grid, tpb, pdac::inner_smem_bytes<2>(), st>>>(__VA_ARGS__); break;      \
+            case 3: KERNEL<3, D><<<grid, tpb, pdac::inner_smem_bytes<3>(), st>>>(__VA_ARGS__); break;      \
+            case 4: KERNEL<4, D><<<grid, tpb, pdac::inner_smem_bytes<4>(), st>>>(__VA_ARGS__); break;      \
+            case 6: KERNEL<6, D><<<grid, tpb, pdac::inner_smem_bytes<6>(), st>>>(__VA_ARGS__); break;      \
+            default: KERNEL<0, D><<<grid, tpb, pdac::inner_smem_bytes<0>(), st>>>(__VA_ARGS__); break;     \
+        }                                                                                                    \
+    } while (0)
+
+// raise the dynamic shared-memory limit of the inner-loop kernels (once per
+// context at create, outside any stream capture)
+template <int NP>
+static cudaError_t set_inner_attrs_np() {
+    const int sm = (int)pdac::inner_smem_bytes<NP>();
+    cudaError_t e = cudaFuncSetAttribute(pdac::k_inner_team<NP, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(pdac::k_inner_team<NP, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(pdac::k_iter_coop<NP, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(pdac::k_iter_coop<NP, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    return e;
+}
+static cudaError_t set_inner_attrs() {
+    cudaError_t e = set_inner_attrs_np<2>();
+    if (e == cudaSuccess) e = set_inner_attrs_np<3>();
+    if (e == cudaSuccess) e = set_inner_attrs_np<4>();
+    if (e == cudaSuccess) e = set_inner_attrs_np<6>();
+    if (e == cudaSuccess) e = set_inner_attrs_np<0>();
+    return e;
+}
+
 // setup.f:551-616 and particles.f:35-79: gas and particle constants
 void set_constants(pdac_ctx *ctx) {
     Prm &P = ctx->P;
@@ -578,6 +610,7 @@ static cudaError_t launch_iter_coop_np(pdac_ctx *ctx, double dt, cudaStream_t st
     at[0].val.cooperative = 1;
     lc.gridDim = dim3(ctx->coop_blocks);
     lc.blockDim = dim3(TPB_TEAM);
+    lc.dynamicSmemBytes = pdac::inner_smem_bytes<NP>();
     lc.stream = st;
     lc.attrs = at;
     lc.numAttrs = 1;
@@ -607,14 +640,21 @@ static int setup_iter_coop(pdac_ctx *ctx) {
     CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     if (!coop) return PDAC_OK;
-    auto occ_of = [&](auto kernel) { return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, TPB_TEAM, 0); };
+    auto occ_of = [&](auto kernel, size_t smem) {
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, TPB_TEAM, smem);
+    };
     cudaError_t e;
     switch (ctx->nph) {
-        case 2: e = ctx->d3 ? occ_of(pdac::k_iter_coop<2, 3>) : occ_of(pdac::k_iter_coop<2, 2>); break;
-        case 3: e = ctx->d3 ? occ_of(pdac::k_iter_coop<3, 3>) : occ_of(pdac::k_iter_coop<3, 2>); break;
-        case 4: e = ctx->d3 ? occ_of(pdac::k_iter_coop<4, 3>) : occ_of(pdac::k_iter_coop<4, 2>); break;
-        case 6: e = ctx->d3 ? occ_of(pdac::k_iter_coop<6, 3>) : occ_of(pdac::k_iter_coop<6, 2>); break;
-        default: e = ctx->d3 ? occ_of(pdac::k_iter_coop<0, 3>) : occ_of(pdac::k_iter_coop<0, 2>); break;
+        case 2: e = ctx->d3 ? occ_of(pdac::k_iter_coop<2, 3>, pdac::inner_smem_bytes<2>())
+                            : occ_of(pdac::k_iter_coop<2, 2>, pdac::inner_smem_bytes<2>()); break;
+        case 3: e = ctx->d3 ? occ_of(pdac::k_iter_coop<3, 3>, pdac::inner_smem_bytes<3>())
+                            : occ_of(pdac::k_iter_coop<3, 2>, pdac::inner_smem_bytes<3>()); break;
+        case 4: e = ctx->d3 ? occ_of(pdac::k_iter_coop<4, 3>, pdac::inner_smem_bytes<4>())
+                            : occ_of(pdac::k_iter_coop<4, 2>, pdac::inner_smem_bytes<4>()); break;
+        case 6: e = ctx->d3 ? occ_of(pdac::k_iter_coop<6, 3>, pdac::inner_smem_bytes<6>())
+                            : occ_of(pdac::k_iter_coop<6, 2>, pdac::inner_smem_bytes<6>()); break;
+        default: e = ctx->d3 ? occ_of(pdac::k_iter_coop<0, 3>, pdac::inner_smem_bytes<0>())
+                             : occ_of(pdac::k_iter_coop<0, 2>, pdac::inner_smem_bytes<0>()); break;
     }
     CK(e);
     ctx->coop_cpb = PDAC_COOP_CELLS_PER_BLOCK;
@@ -958,6 +998,7 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     int nq = 1 + ns + ng;
     CK(cudaMalloc(&ctx->d_partial, (size_t)nq * 1024 * sizeof(double)));
     if (ctx->d3) CK(set_tile_attrs(ctx->P, ctx->F));
+    CK(set_inner_attrs());
     if (t1) {
         int st = setup_wave(ctx, cfg->flag);
         if (st) return st;
@@ -1325,8 +1366,8 @@ static int enqueue_sweep(pdac_ctx *ctx, double dt, cudaStream_t st, bool prof) {
         if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_resid_test, 3, test_grid, TPB_RESID, st, ctx->P, F, dt, ctx->d_cand, ncand, wl, cnt, dirty);
         else PHASE_LAUNCH_D(nph, pdac::k_resid_test, 2, test_grid, TPB_RESID, st, ctx->P, F, dt, ctx->d_cand, ncand, wl, cnt, dirty);
         if (prof) CK(cudaEventRecord(ctx->cev[3 * col + 1], st));
-        if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_inner_team, 3, g, TPB_TEAM, st, ctx->P, F, dt, ctx->d_nit, wl, cnt, dirty);
-        else PHASE_LAUNCH_D(nph, pdac::k_inner_team, 2, g, TPB_TEAM, st, ctx->P, F, dt, ctx->d_nit, wl, cnt, dirty);
+        if (ctx->d3) INNER_LAUNCH_D(nph, pdac::k_inner_team, 3, g, TPB_TEAM, st, ctx->P, F, dt, ctx->d_nit, wl, cnt, dirty);
+        else INNER_LAUNCH_D(nph, pdac::k_inner_team, 2, g, TPB_TEAM, st, ctx->P, F, dt, ctx->d_nit, wl, cnt, dirty);
         if (prof) CK(cudaEventRecord(ctx->cev[3 * col + 2], st));
     }
     // implicit_enthalpy: the enthalpy fluxes (with implicit_fluxes) and the
@@ -1625,8 +1666,8 @@ int pdac_gpu_iter_static(pdac_ctx *ctx, double dt, int *nit_out) {
             ctx->launches++;
             long team_threads = (nthr + (ctx->d3 ? 4 : 7)) / (ctx->d3 ? 5 : 8) * 32;
             int g = std::min(ctx->inner_grid, blocks(team_threads, TPB_TEAM));
-            if (ctx->d3) PHASE_LAUNCH_D(nph, pdac::k_inner_team, 3, g, TPB_TEAM, st, ctx->P, F, dt, dnit, work, cnt, dirty);
-            else PHASE_LAUNCH_D(nph, pdac::k_inner_team, 2, g, TPB_TEAM, st, ctx->P, F, dt, dnit, work, cnt, dirty);
+            if (ctx->d3) INNER_LAUNCH_D(nph, pdac::k_inner_team, 3, g, TPB_TEAM, st, ctx->P, F, dt, dnit, work, cnt, dirty);
+            else INNER_LAUNCH_D(nph, pdac::k_inner_team, 2, g, TPB_TEAM, st, ctx->P, F, dt, dnit, work, cnt, dirty);
             ctx->launches += 2;
         }
         CK(cudaMemcpyAsync(ctx->h_counters, wcount, 6 * sizeof(int), cudaMemcpyDeviceToHost, st));

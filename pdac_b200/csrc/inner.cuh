@@ -204,10 +204,27 @@ __device__ __forceinline__ void face_assemble(const Prm &P, KT &K, int side, dou
 #ifndef PDAC_INNER_MINB_SMALL
 #define PDAC_INNER_MINB_SMALL 3
 #endif
-#define PDAC_INNER_MINB(NP) ((NP) > 0 && (NP) <= 4 ? PDAC_INNER_MINB_SMALL : 2)
-#ifndef PDAC_INNER_SHD_MAXP
-#define PDAC_INNER_SHD_MAXP 4
+#ifndef PDAC_INNER_MINB_LARGE
+#define PDAC_INNER_MINB_LARGE 2
 #endif
+#define PDAC_INNER_MINB(NP) ((NP) > 0 && (NP) <= 4 ? PDAC_INNER_MINB_SMALL : PDAC_INNER_MINB_LARGE)
+#ifndef PDAC_INNER_SHD_MAXP
+#define PDAC_INNER_SHD_MAXP 6
+#endif
+
+// the inner loop's shared memory, allocated at launch (dynamic): FaceK
+// columns for up to six phases, then DensK columns up to
+// PDAC_INNER_SHD_MAXP phases (64.5 KB per block at six phases)
+template <int NP>
+__host__ __device__ constexpr int inner_face_rows() { return (NP > 0 && NP <= 6) ? FaceK<NP, true>::N : 0; }
+template <int NP>
+__host__ __device__ constexpr int inner_dens_rows() {
+    return (NP > 0 && NP <= PDAC_INNER_SHD_MAXP) ? 4 * (Sys<NP>::M - 1) : 0;
+}
+template <int NP>
+__host__ __device__ constexpr size_t inner_smem_bytes() {
+    return (size_t)(inner_face_rows<NP>() + inner_dens_rows<NP>()) * KS * sizeof(double);
+}
 
 // the inner loop of the worklist's nwork cells (outer sweep nit, 1-based)
 // by the warps warp, warp + nwarps, ... of the launch; RO as in ldro
@@ -223,12 +240,11 @@ __device__ __forceinline__ void inner_team_run(const Prm &P, const Fld &F, doubl
     if (tw >= TPW) return;  // idle lanes take no part in any team
     const int q = lane - tw * T, tb = tw * T;
     const unsigned tmask = ((1u << T) - 1u) << tb;
-    constexpr bool SH = NP > 0 && NP <= 6;  // FaceK in shared memory (40 KB per block at NP = 6)
-    __shared__ double kcols[SH ? FaceK<NP, true>::N : 1][SH ? KS : 1];
-    // DensK in shared memory up to four phases (16 KB per block at NP = 4;
-    // with FaceK within the 48 KB of static shared memory a block may hold)
-    constexpr bool SHD = NP > 0 && NP <= PDAC_INNER_SHD_MAXP;
-    __shared__ double dcols[SHD ? 4 * NC : 1][SHD ? KS : 1];
+    constexpr bool SH = inner_face_rows<NP>() > 0;   // FaceK in shared memory (40 KB per block at NP = 6)
+    constexpr bool SHD = inner_dens_rows<NP>() > 0;  // DensK too (16 KB at NP = 4, 24 KB at NP = 6)
+    extern __shared__ __align__(16) double inner_smem[];
+    double *const kcols = inner_smem;                              // [FaceK rows][KS]
+    double *const dcols = inner_smem + inner_face_rows<NP>() * KS;  // [4 NC][KS]
     for (int w = warp * TPW + tw; w < nwork; w += nwarps * TPW) {
         const int c = list[w];
         int i, j, k;
@@ -281,13 +297,13 @@ __device__ __forceinline__ void inner_team_run(const Prm &P, const Fld &F, doubl
         vel[0] = gvel[fcell];
 #pragma unroll
         for (int l = 2; l <= nph; ++l) vel[l - 1] = svel[(l - 2) * n + fcell];
-        FaceK<NP, SH> K(&kcols[0][SH ? threadIdx.x : 0]);
+        FaceK<NP, SH> K(kcols + threadIdx.x);
         if (solved) face_prepare<NP, RO>(P, F, c, minus ? rm : rp, rawnb, ii, dir, minus ? -1 : +1, dt, K);
         // mass-flux stencil of this face by phase (gas first): neighbour
         // values, or the cell's own current value where the slot is the cell
         const int rfar = minus ? rmm : rpp;
         const bool sm = rm == c, sp = rp == c, sfar = rfar == c;
-        DensK<NC, SHD> Dk(&dcols[0][SHD ? threadIdx.x : 0]);
+        DensK<NC, SHD> Dk(dcols + threadIdx.x);
         Dk.cm(0) = ldro<RO>(F.rgp + rm); Dk.cp(0) = ldro<RO>(F.rgp + rp); Dk.cf(0) = mus ? ldro<RO>(F.rgp + rfar) : 0.0;
 #pragma unroll
         for (int l = 2; l <= nph; ++l) {

@@ -99,6 +99,31 @@ def test_steps(tmp_path, builder, immb, steps):
     eng.close()
 
 
+def test_hills_five_classes(tmp_path):
+    """The large workload's deck (seeded Gaussian hills, immersed boundaries,
+    five particle classes: the six-phase inner loop) on a 40 x 40 x 32 mesh:
+    whole steps with equal outer sweeps and fields within 1e-9, the oracle
+    restarted from the engine's state every step."""
+    import pyoracle
+    from pdac_b200 import configs
+    from pdac_b200.engine import Engine
+    from pdac_b200.setup_state import Case
+    case = Case(configs.plume_3d_hills(nx=40, ny=40, nz=32, dem_dir=str(tmp_path)))
+    assert case.nsolid == 5 and case.ib is not None
+    eng = Engine(case)
+    ora = pyoracle.Oracle(case, order=pyoracle.ORDER_COLORED)
+    fluid = (case.flag & 1) == 1
+    fields3 = STEP_FIELDS + ("vg", "vs")
+    for s in range(1, 7):
+        ora.set_state(eng.download())
+        n1, n2 = eng.step(s), ora.step(s)
+        assert n1 == n2, f"step {s}: outer sweeps {n1} vs {n2}"
+        errs, bad = compare_state(eng.download(), ora.get_state(), fields3, TOL_STEP, case.nsolid, case.ncell,
+                                  cells=fluid)
+        assert not bad, f"step {s}: {bad}"
+    eng.close()
+
+
 def test_forcing_point_checks_reject_bad_tables(tmp_path):
     """An immersed cell without a forcing point (the reference stops there,
     bdry.f:111-113) is rejected at create with PDAC_ERR_CONFIG, by the
