@@ -1339,6 +1339,9 @@ static int enqueue_ftem(pdac_ctx *ctx, double dt, cudaStream_t st, bool in_sweep
 // one outer sweep of the corrector (iter.f:241-410): three colour phases of
 // candidate collection, residual test and inner loop; the sweep number is
 // read on the device from d_nit
+// kernels of the corrector in one graph sweep, k_sweep_check included
+static long long sweep_kernels(const pdac_ctx *) { return 10; }
+
 static int enqueue_sweep(pdac_ctx *ctx, double dt, cudaStream_t st, bool prof) {
     Fld &F = ctx->F;
     // implicit_fluxes: momentum fluxes, stresses and drag of the current
@@ -1410,7 +1413,7 @@ static int build_iter_graph(pdac_ctx *ctx, double dt) {
     // which run here only to record them)
     const long long before = ctx->launches;
     int s = enqueue_sweep(ctx, dt, st, false);
-    ctx->it_per_sweep = 10 + (ctx->launches - before);
+    ctx->it_per_sweep = sweep_kernels(ctx) + (ctx->launches - before);
     ctx->launches = before;
     if (!s) pdac::k_sweep_check<<<1, 1, 0, st>>>(ctx->d_wcount, ctx->d_nit, ctx->cfg.maxout, loop);
     cudaGraph_t captured = nullptr;
@@ -2894,7 +2897,7 @@ static int add_step_nodes(pdac_ctx *ctx, cudaGraph_t g) {
     CK(cudaStreamBeginCaptureToGraph(st, cp.conditional.phGraph_out[0], nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
     const long long mid = ctx->launches;
     s = enqueue_sweep(ctx, dt, st, false);
-    ctx->it_per_sweep = 10 + (ctx->launches - mid);
+    ctx->it_per_sweep = sweep_kernels(ctx) + (ctx->launches - mid);
     ctx->launches = mid;
     if (!s) pdac::k_sweep_check<<<1, 1, 0, st>>>(ctx->d_wcount, ctx->d_nit, ctx->cfg.maxout, loop);
     cudaGraph_t body = nullptr;

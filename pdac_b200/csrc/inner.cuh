@@ -490,6 +490,35 @@ __global__ void __launch_bounds__(TPB_RESID) k_resid_collect(Prm P, int colour, 
     collect_phase<TPB_RESID>(P, colour, dirty, cand, ncand);
 }
 
+// the residual test of cell c (iter.f:241-319): a converged cell updates its
+// volume fractions and rgp (keeping its active-set bit if rgp changed);
+// returns true for an unconverged cell, which goes to the inner loop
+template <int NP, int D>
+__device__ __forceinline__ bool test_cell(const Prm &P, const Fld &F, double dt, int c, unsigned *dirty) {
+    double dg;
+    if (D == 3) {
+        int i, j, k;
+        ijk_of(P, c, i, j, k);
+        Raw3 R;
+        raw3(P, i, j, k, R);
+        dg = calc_res_3d(P, F, R, i, j, k, dt);
+        if (fabs(dg) <= F.conv[c]) calc_eps_3d<NP>(P, F, R, i, j, k, dt);
+    } else {
+        int i = c % P.nx + 1, k = c / P.nx + 1;
+        Raw2 R;
+        raw2(P, i, k, R);
+        dg = calc_res_2d(P, F, R, i, k, dt);
+        if (fabs(dg) <= F.conv[c]) calc_eps_2d(P, F, R, i, k, dt);
+    }
+    if (fabs(dg) <= F.conv[c]) {
+        const double old = F.rgp[c];
+        F.rgp[c] = F.ep[c] * F.rog[c];
+        if (__double_as_longlong(F.rgp[c]) != __double_as_longlong(old)) mark_dirty(dirty, c);
+        return false;
+    }
+    return true;
+}
+
 // the residual test of the len candidates, block-uniform rounds
 template <int TPBK, int NP, int D>
 __device__ __forceinline__ void test_phase(const Prm &P, const Fld &F, double dt, const int *cand, int len, int *work,
@@ -498,28 +527,7 @@ __device__ __forceinline__ void test_phase(const Prm &P, const Fld &F, double dt
         int idx = base + threadIdx.x, c = -1, nmine = 0;
         if (idx < len) {
             c = cand[idx];
-            double dg;
-            if (D == 3) {
-                int i, j, k;
-                ijk_of(P, c, i, j, k);
-                Raw3 R;
-                raw3(P, i, j, k, R);
-                dg = calc_res_3d(P, F, R, i, j, k, dt);
-                if (fabs(dg) <= F.conv[c]) calc_eps_3d<NP>(P, F, R, i, j, k, dt);
-            } else {
-                int i = c % P.nx + 1, k = c / P.nx + 1;
-                Raw2 R;
-                raw2(P, i, k, R);
-                dg = calc_res_2d(P, F, R, i, k, dt);
-                if (fabs(dg) <= F.conv[c]) calc_eps_2d(P, F, R, i, k, dt);
-            }
-            if (fabs(dg) <= F.conv[c]) {
-                const double old = F.rgp[c];
-                F.rgp[c] = F.ep[c] * F.rog[c];
-                if (__double_as_longlong(F.rgp[c]) != __double_as_longlong(old)) mark_dirty(dirty, c);
-            } else {
-                nmine = 1;
-            }
+            nmine = test_cell<NP, D>(P, F, dt, c, dirty) ? 1 : 0;
         }
         block_append_n<TPBK, 1>(work, count, &c, nmine, count + 3, idx < len ? 1 : 0);
     }
@@ -531,9 +539,62 @@ __global__ void __launch_bounds__(TPB_RESID) k_resid_test(Prm P, Fld F, double d
     test_phase<TPB_RESID, NP, D>(P, F, dt, cand, *ncand, work, count, dirty);
 }
 
+// One colour phase of the cooperative sweep loop in one pass: collect, test
+// and inner loop fused, with one grid barrier after it instead of three.
+// Each warp takes one word of the active set (32 consecutive cells) at a time:
+// lane b tests the cell of bit b when that bit is set and the cell is a
+// fluid cell of the colour, the unconverged cells (at most 11 of the 32 are
+// of one colour) go to a warp-local list in shared memory, and the warp's
+// teams run their inner loops.  Cells of one colour share no stencil data,
+// so testing and iterating them in this order gives the bits of the
+// three-launch form.  The colour's set bits of a word are cleared
+// atomically before its cells are tested: other warps set bits of the
+// neighbouring cells meanwhile.  Adds the unconverged cells to wcount[col]
+// and the tested ones to wcount[3 + col].  RO as in ldro.
+template <int NP, int D, bool RO>
+__device__ __forceinline__ void fused_phase(const Prm &P, const Fld &F, double dt, int nit, int colour,
+                                            unsigned *dirty, int *wcount, unsigned warp, unsigned nwarps) {
+    const int lane = threadIdx.x & 31;
+    __shared__ int wlist[KS / 32][32];
+    int *const mylist = wlist[threadIdx.x >> 5];
+    const unsigned nwords = ((unsigned)P.ncell + 31u) / 32u;
+    int nwork_sum = 0, ntest_sum = 0;
+    for (unsigned t = warp; t < nwords; t += nwarps) {  // uniform across the warp
+        const unsigned w = __ldcg(dirty + t);
+        const int c = (int)(32u * t) + lane;
+        bool cand = false, clear = false;
+        if (((w >> lane) & 1u) && c < P.ncell) {
+            if (!(P.flag[c] & 1)) {
+                clear = true;  // a non-fluid cell is never tested
+            } else {
+                int i = c % P.nx + 1, r = c / P.nx, j = r % P.ny + 1, k = r / P.ny + 1;
+                cand = (i + j + k) % 3 == colour;
+                clear = cand;
+            }
+        }
+        const unsigned cm = __ballot_sync(0xffffffffu, clear);
+        if (lane == 0 && cm) atomicAnd(dirty + t, ~cm);
+        __syncwarp();
+        const bool unconv = cand && test_cell<NP, D>(P, F, dt, c, dirty);
+        const unsigned um = __ballot_sync(0xffffffffu, unconv);
+        if (unconv) mylist[__popc(um & ((1u << lane) - 1u))] = c;
+        ntest_sum += __popc(__ballot_sync(0xffffffffu, cand));
+        __syncwarp();
+        const int nwork = __popc(um);
+        nwork_sum += nwork;
+        if (nwork) inner_team_run<NP, D, RO>(P, F, dt, nit, mylist, nwork, dirty, 0, 1);
+        __syncwarp();  // the list is read before the next word overwrites it
+    }
+    if (lane == 0) {
+        if (nwork_sum) atomicAdd(wcount + colour, nwork_sum);
+        if (ntest_sum) atomicAdd(wcount + 3 + colour, ntest_sum);
+    }
+}
+
 // The whole outer sweep loop of iter (iter.f:204-410) in one cooperative
-// launch, for small domains: the colour phases' collect, test and inner
-// loop follow each other across grid-wide barriers instead of launches.
+// launch, for small domains: the colour phases (fused_phase: collect, test
+// and inner loop in one pass) follow each other across grid-wide barriers
+// instead of launches.
 // Every thread of the grid takes every barrier the same number of times:
 // the loop ends on counters that all threads read after the same barrier.
 struct SweepWork {
@@ -554,12 +615,7 @@ __global__ void __launch_bounds__(128, PDAC_INNER_MINB(NP)) k_iter_coop(Prm P, F
         if (blockIdx.x == 0 && threadIdx.x < 9) W.wcount[threadIdx.x] = 0;
         g.sync();
         for (int col = 0; col < 3; ++col) {
-            collect_phase<128>(P, col, W.dirty, W.cand, W.wcount + 6 + col);
-            g.sync();
-            int *wl = W.work + col * W.wstride;
-            test_phase<128, NP, D>(P, F, dt, W.cand, __ldcg(W.wcount + 6 + col), wl, W.wcount + col, W.dirty);
-            g.sync();
-            inner_team_run<NP, D, false>(P, F, dt, nit, wl, __ldcg(W.wcount + col), W.dirty, warp, nwarps);
+            fused_phase<NP, D, false>(P, F, dt, nit, col, W.dirty, W.wcount, warp, nwarps);
             g.sync();
         }
         const long unconverged = (long)__ldcg(W.wcount) + __ldcg(W.wcount + 1) + __ldcg(W.wcount + 2);
