@@ -226,6 +226,206 @@ __host__ __device__ constexpr size_t inner_smem_bytes() {
     return (size_t)(inner_face_rows<NP>() + inner_dens_rows<NP>()) * KS * sizeof(double);
 }
 
+// The inner loop of cell c (outer sweep nit, 1-based) by the team of lanes
+// tb .. tb + T - 1 of this warp (lane q of the team owns face q); kcols and
+// dcols are the shared FaceK and DensK arrays.  RO as in ldro.
+template <int NP, int D, bool RO>
+__device__ __forceinline__ void inner_team_cell(const Prm &P, const Fld &F, double dt, int nit, int c, unsigned *dirty,
+                                                int q, int tb, unsigned tmask, double *kcols, double *dcols) {
+    constexpr int NC = Sys<NP>::M - 1;   // phase capacity
+    constexpr bool SH = inner_face_rows<NP>() > 0;   // FaceK in shared memory (40 KB per block at NP = 6)
+    constexpr bool SHD = inner_dens_rows<NP>() > 0;  // DensK too (16 KB at NP = 4, 24 KB at NP = 6)
+    const int nph = nphases<NP>(P), ns = nph - 1;
+    const size_t n = P.ncell;
+    int i, j, k;
+    if (D == 3) ijk_of(P, c, i, j, k);
+    else { i = c % P.nx + 1; j = 1; k = c / P.nx + 1; }
+    const int *fl = P.flag;
+    // ---- this lane's face: axis, side, raw and remapped neighbours -------
+    const int a = D == 3 ? q % 3 : q % 2;
+    const bool minus = D == 3 ? q < 3 : q < 2;
+    const int dir = D == 3 ? a : (a == 0 ? 0 : 2);
+    const int ii = dir == 0 ? i : (dir == 1 ? j : k);
+    const int nax = dir == 0 ? P.nx : (dir == 1 ? P.ny : P.nz);
+    int raw_m, raw_p, rm, rmm, rp, rpp;
+    if (D == 3) {
+        Raw3 R;
+        Rem3 M;
+        raw3(P, i, j, k, R);
+        rem3(P, i, j, k, R, M);
+        if (dir == 0) { raw_m = R.w; raw_p = R.e; rm = M.w; rmm = M.ww; rp = M.e; rpp = M.ee; }
+        else if (dir == 1) { raw_m = R.s; raw_p = R.n; rm = M.s; rmm = M.ss; rp = M.n; rpp = M.nn; }
+        else { raw_m = R.b; raw_p = R.t; rm = M.b; rmm = M.bb; rp = M.t; rpp = M.tt; }
+    } else {
+        Raw2 R;
+        Rem2 M;
+        raw2(P, i, k, R);
+        rem2(P, i, k, R, M);
+        if (dir == 0) { raw_m = R.w; raw_p = R.e; rm = M.w; rmm = M.ww; rp = M.e; rpp = M.ee; }
+        else { raw_m = R.b; raw_p = R.t; rm = M.b; rmm = M.bb; rp = M.t; rpp = M.tt; }
+    }
+    const int rawnb = minus ? raw_m : raw_p;
+    const bool solved = (fl[rawnb] & 1) != 0;
+    const int fcell = minus ? rawnb : c;  // where this face's velocity and fluxes live
+    const bool mus = P.muscl > 0 && fl[c] == FLUID;
+    FaceGeo g;
+    {
+        const double *dd = dir == 0 ? P.dx : (dir == 1 ? P.dy : P.dz);
+        int im2 = max(1, ii - 2), ip2 = min(nax, ii + 2);
+        g.inmm = 1.0 / (dd[ii - 1] + dd[im2]);
+        g.inm = 1.0 / (dd[ii] + dd[ii - 1]);
+        g.inp = 1.0 / (dd[ii] + dd[ii + 1]);
+        g.inpp = 1.0 / (dd[ii + 1] + dd[ip2]);
+        g.incr_p = minus ? 0.5 * dd[ii - 1] : 0.5 * dd[ii];
+        g.incr_m = minus ? -0.5 * dd[ii] : -0.5 * dd[ii + 1];
+        g.r = (D == 2 && dir == 0) ? (minus ? P.rb[i - 1] : P.rb[i]) : 1.0;
+        g.lim_on = minus ? (ii != 2 && fl[raw_m] == FLUID) : (ii != nax - 1 && fl[raw_p] == FLUID);
+    }
+    double *const gvel = dir == 0 ? F.ug : (dir == 1 ? F.vg : F.wg);
+    double *const svel = dir == 0 ? F.us : (dir == 1 ? F.vs : F.ws);
+    double vel[NC];
+    vel[0] = gvel[fcell];
+#pragma unroll
+    for (int l = 2; l <= nph; ++l) vel[l - 1] = svel[(l - 2) * n + fcell];
+    FaceK<NP, SH> K(kcols + threadIdx.x);
+    if (solved) face_prepare<NP, RO>(P, F, c, minus ? rm : rp, rawnb, ii, dir, minus ? -1 : +1, dt, K);
+    // mass-flux stencil of this face by phase (gas first): neighbour
+    // values, or the cell's own current value where the slot is the cell
+    const int rfar = minus ? rmm : rpp;
+    const bool sm = rm == c, sp = rp == c, sfar = rfar == c;
+    DensK<NC, SHD> Dk(dcols + threadIdx.x);
+    Dk.cm(0) = ldro<RO>(F.rgp + rm); Dk.cp(0) = ldro<RO>(F.rgp + rp); Dk.cf(0) = mus ? ldro<RO>(F.rgp + rfar) : 0.0;
+#pragma unroll
+    for (int l = 2; l <= nph; ++l) {
+        const double *D_ = F.rlk + (size_t)(l - 2) * n;
+        Dk.cm(l - 1) = ldro<RO>(D_ + rm); Dk.cp(l - 1) = ldro<RO>(D_ + rp);
+        Dk.cf(l - 1) = mus ? ldro<RO>(D_ + rfar) : 0.0;
+    }
+    // opt_inner_loop (iter.f:1255-1547) builds the density stencils once
+    // and updates only their centre: a neighbour slot remapped to the
+    // cell keeps the loop-entry value there
+    Dk.o(0) = F.rgp[c];
+#pragma unroll
+    for (int l = 2; l <= nph; ++l) Dk.o(l - 1) = F.rlk[(size_t)(l - 2) * n + c];
+    const bool stale = P.opt == 2;
+    auto mflux = [&](int ph, double own) {
+        const double slot = stale ? Dk.o(ph) : own;
+        double dm = sm ? slot : Dk.cm(ph), dp = sp ? slot : Dk.cp(ph), df = sfar ? slot : Dk.cf(ph);
+        return minus ? face_mflux(P, g, true, vel[ph], own, dm, df, dp, 0.0, mus)
+                     : face_mflux(P, g, false, vel[ph], own, dm, 0.0, dp, df, mus);
+    };
+    // ---- cell state (identical in every lane) ------------------------------
+    const double rx = D == 2 ? P.inr[i] : 1.0;
+    const double idx_i = P.indx[i], idz_k = P.indz[k], idy_j = D == 3 ? P.indy[j] : 0.0;
+    const double rgpn_c = F.rgpn[c];
+    const CellFaces bf = cell_faces(P, c);  // faces, iter.f:259
+    auto resid = [&](double fe, double fw, double fn, double fs, double ft, double fb, double rgpc) {
+        double resx = (bf.e * fe - bf.w * fw) * idx_i * rx;
+        double resz = (bf.t * ft - bf.b * fb) * idz_k;
+        double resy = D == 3 ? (bf.n * fn - bf.s * fs) * idy_j : 0.0;
+        return rgpc - rgpn_c + dt * bf.ivf * (resx + resy + resz);
+    };
+    double dg;  // calc_res of the stored state (raw W/S/B neighbours)
+    if (D == 3) {
+        int cw = at3(P, max(i - 1, 1), j, k), cs = at3(P, i, max(j - 1, 1), k), cb = at3(P, i, j, max(k - 1, 1));
+        dg = resid(F.rgfe[c], F.rgfe[cw], F.rgfn[c], F.rgfn[cs], F.rgft[c], F.rgft[cb], F.rgp[c]);
+    } else {
+        int cw = at2(P, max(i - 1, 1), k), cb = at2(P, i, max(k - 1, 1));
+        dg = resid(F.rgfe[c], F.rgfe[cw], 0.0, 0.0, F.rgft[c], F.rgft[cb], F.rgp[c]);
+    }
+    double dgorig = dg;
+    const double conv = F.conv[c];
+    double d3 = dg, p3 = F.p[c], abeta = F.abeta[c];
+    // the mixture molecular weight of thermal_eosg (eosg.f:114-137), which
+    // does not change within the loop: summed once, in thermal_eosg's order
+    double mg = 0;
+    for (int ig = 0; ig < P.ng; ++ig) mg = mg + GAS(F.xgc, c, ig) * P.gmw[P.gas_type[ig]];
+    const double tgc = F.tg[c];
+    const double rgas_tg = P.rgas * tgc;
+    int kros = -1;
+    PAdj s = {0, 0, 0, 0, 0, 0};
+    double p = F.p[c], ep = F.ep[c], rog = F.rog[c], rgp = F.rgp[c];
+    double rlk[NC], rlkn[NC], sink[NC];
+#pragma unroll
+    for (int is = 1; is <= ns; ++is) {
+        rlk[is - 1] = F.rlk[(is - 1) * n + c];
+        rlkn[is - 1] = F.rlkn[(is - 1) * n + c];
+        sink[is - 1] = F.sink[(is - 1) * n + c];
+    }
+    double flux[NC];  // this lane's face mass flux by phase (gas first)
+#pragma unroll
+    for (int l = 0; l < NC; ++l) flux[l] = 0.0;
+    // source lanes of the faces (3D: W S B E N T = 0..5; 2D: W B E T = 0..3)
+    const int lW = tb + 0, lE = tb + (D == 3 ? 3 : 2), lB = tb + (D == 3 ? 2 : 1), lT = tb + (D == 3 ? 5 : 3);
+    const int lS = tb + 1, lN = tb + 4;
+    for (int loop = 1; loop <= P.inmax; ++loop) {
+        if (loop > 1 || nit > 1) padjust(s, p, kros, d3, p3, P.omega, abeta);
+        rog = p / rgas_tg * mg;  // thermal_eosg
+        rgp = ep * rog;
+        // this lane's face system (matrix.f:351-630)
+        if (solved) face_assemble<NP>(P, K, minus ? -1 : +1, p, ep, rgp, rlk, vel);
+        // particle mass fluxes and volume fractions (iter.f:778-994)
+#pragma unroll
+        for (int is = 1; is <= ns; ++is) flux[is] = mflux(is, rlk[is - 1]);
+        double rls = 0;
+#pragma unroll
+        for (int is = 1; is <= ns; ++is) {
+            double fW = __shfl_sync(tmask, flux[is], lW), fE = __shfl_sync(tmask, flux[is], lE);
+            double fB = __shfl_sync(tmask, flux[is], lB), fT = __shfl_sync(tmask, flux[is], lT);
+            double fS = 0, fN = 0;
+            if (D == 3) { fS = __shfl_sync(tmask, flux[is], lS); fN = __shfl_sync(tmask, flux[is], lN); }
+            double rlkx = (bf.e * fE - bf.w * fW) * idx_i * rx;
+            double rlkz = (bf.t * fT - bf.b * fB) * idz_k;
+            double rlky = D == 3 ? (bf.n * fN - bf.s * fS) * idy_j : 0.0;
+            double t = rlkn[is - 1] - dt * bf.ivf * (rlkx + rlky + rlkz);
+            t = t + dt * bf.ivf * sink[is - 1];
+            double v = fmax(0.0, t);
+            rlk[is - 1] = v;
+            rls = rls + v * P.inrl[is];
+        }
+        ep = 1.0 - rls;
+        if (rls > 1.0 && q == 0) atomicAdd(&F.counters[2], 1);
+        rgp = ep * rog;
+        // gas mass flux and continuity residual (iter.f:597-771)
+        flux[0] = mflux(0, rgp);
+        {
+            double fW = __shfl_sync(tmask, flux[0], lW), fE = __shfl_sync(tmask, flux[0], lE);
+            double fB = __shfl_sync(tmask, flux[0], lB), fT = __shfl_sync(tmask, flux[0], lT);
+            double fS = 0, fN = 0;
+            if (D == 3) { fS = __shfl_sync(tmask, flux[0], lS); fN = __shfl_sync(tmask, flux[0], lN); }
+            dg = resid(fE, fW, fN, fS, fT, fB, rgp);
+        }
+        if (fabs(dg) > conv || fabs(dg) >= fabs(dgorig)) {
+            if (nit == 1 && loop == 1) dgorig = dg;
+            d3 = dg;
+        } else if (fabs(dg) <= conv) {
+            break;
+        }
+    }
+    // ---- final values -----------------------------------------------------
+    {
+        // face mass fluxes (every face, as calc_*_mass_flux writes them)
+        double *gfa = dir == 0 ? F.rgfe : (dir == 1 ? F.rgfn : F.rgft);
+        double *sfa = dir == 0 ? F.rsfe : (dir == 1 ? F.rsfn : F.rsft);
+        gfa[fcell] = flux[0];
+#pragma unroll
+        for (int is = 1; is <= ns; ++is) sfa[(size_t)(is - 1) * n + fcell] = flux[is];
+        if (solved) {
+            gvel[fcell] = vel[0];
+#pragma unroll
+            for (int l = 2; l <= nph; ++l) svel[(l - 2) * n + fcell] = vel[l - 1];
+        }
+        mark_dirty(dirty, rawnb);
+    }
+    if (q == 0) {
+        F.p[c] = p; F.rog[c] = rog; F.rgp[c] = rgp; F.ep[c] = ep;
+#pragma unroll
+        for (int is = 1; is <= ns; ++is) F.rlk[(is - 1) * n + c] = rlk[is - 1];
+        F.abeta[c] = abeta;
+        mark_dirty(dirty, c);
+    }
+}
+
 // the inner loop of the worklist's nwork cells (outer sweep nit, 1-based)
 // by the warps warp, warp + nwarps, ... of the launch; RO as in ldro
 template <int NP, int D, bool RO>
@@ -233,208 +433,15 @@ __device__ __forceinline__ void inner_team_run(const Prm &P, const Fld &F, doubl
                                                int nwork, unsigned *dirty, int warp, int nwarps) {
     constexpr int T = D == 3 ? 6 : 4;    // lanes per cell
     constexpr int TPW = 32 / T;          // teams per warp (3D: 5, lanes 30 and 31 idle)
-    constexpr int NC = Sys<NP>::M - 1;   // phase capacity
-    const int nph = nphases<NP>(P), ns = nph - 1;
-    const size_t n = P.ncell;
     const int lane = threadIdx.x & 31, tw = lane / T;
     if (tw >= TPW) return;  // idle lanes take no part in any team
     const int q = lane - tw * T, tb = tw * T;
     const unsigned tmask = ((1u << T) - 1u) << tb;
-    constexpr bool SH = inner_face_rows<NP>() > 0;   // FaceK in shared memory (40 KB per block at NP = 6)
-    constexpr bool SHD = inner_dens_rows<NP>() > 0;  // DensK too (16 KB at NP = 4, 24 KB at NP = 6)
     extern __shared__ __align__(16) double inner_smem[];
     double *const kcols = inner_smem;                              // [FaceK rows][KS]
     double *const dcols = inner_smem + inner_face_rows<NP>() * KS;  // [4 NC][KS]
-    for (int w = warp * TPW + tw; w < nwork; w += nwarps * TPW) {
-        const int c = list[w];
-        int i, j, k;
-        if (D == 3) ijk_of(P, c, i, j, k);
-        else { i = c % P.nx + 1; j = 1; k = c / P.nx + 1; }
-        const int *fl = P.flag;
-        // ---- this lane's face: axis, side, raw and remapped neighbours -------
-        const int a = D == 3 ? q % 3 : q % 2;
-        const bool minus = D == 3 ? q < 3 : q < 2;
-        const int dir = D == 3 ? a : (a == 0 ? 0 : 2);
-        const int ii = dir == 0 ? i : (dir == 1 ? j : k);
-        const int nax = dir == 0 ? P.nx : (dir == 1 ? P.ny : P.nz);
-        int raw_m, raw_p, rm, rmm, rp, rpp;
-        if (D == 3) {
-            Raw3 R;
-            Rem3 M;
-            raw3(P, i, j, k, R);
-            rem3(P, i, j, k, R, M);
-            if (dir == 0) { raw_m = R.w; raw_p = R.e; rm = M.w; rmm = M.ww; rp = M.e; rpp = M.ee; }
-            else if (dir == 1) { raw_m = R.s; raw_p = R.n; rm = M.s; rmm = M.ss; rp = M.n; rpp = M.nn; }
-            else { raw_m = R.b; raw_p = R.t; rm = M.b; rmm = M.bb; rp = M.t; rpp = M.tt; }
-        } else {
-            Raw2 R;
-            Rem2 M;
-            raw2(P, i, k, R);
-            rem2(P, i, k, R, M);
-            if (dir == 0) { raw_m = R.w; raw_p = R.e; rm = M.w; rmm = M.ww; rp = M.e; rpp = M.ee; }
-            else { raw_m = R.b; raw_p = R.t; rm = M.b; rmm = M.bb; rp = M.t; rpp = M.tt; }
-        }
-        const int rawnb = minus ? raw_m : raw_p;
-        const bool solved = (fl[rawnb] & 1) != 0;
-        const int fcell = minus ? rawnb : c;  // where this face's velocity and fluxes live
-        const bool mus = P.muscl > 0 && fl[c] == FLUID;
-        FaceGeo g;
-        {
-            const double *dd = dir == 0 ? P.dx : (dir == 1 ? P.dy : P.dz);
-            int im2 = max(1, ii - 2), ip2 = min(nax, ii + 2);
-            g.inmm = 1.0 / (dd[ii - 1] + dd[im2]);
-            g.inm = 1.0 / (dd[ii] + dd[ii - 1]);
-            g.inp = 1.0 / (dd[ii] + dd[ii + 1]);
-            g.inpp = 1.0 / (dd[ii + 1] + dd[ip2]);
-            g.incr_p = minus ? 0.5 * dd[ii - 1] : 0.5 * dd[ii];
-            g.incr_m = minus ? -0.5 * dd[ii] : -0.5 * dd[ii + 1];
-            g.r = (D == 2 && dir == 0) ? (minus ? P.rb[i - 1] : P.rb[i]) : 1.0;
-            g.lim_on = minus ? (ii != 2 && fl[raw_m] == FLUID) : (ii != nax - 1 && fl[raw_p] == FLUID);
-        }
-        double *const gvel = dir == 0 ? F.ug : (dir == 1 ? F.vg : F.wg);
-        double *const svel = dir == 0 ? F.us : (dir == 1 ? F.vs : F.ws);
-        double vel[NC];
-        vel[0] = gvel[fcell];
-#pragma unroll
-        for (int l = 2; l <= nph; ++l) vel[l - 1] = svel[(l - 2) * n + fcell];
-        FaceK<NP, SH> K(kcols + threadIdx.x);
-        if (solved) face_prepare<NP, RO>(P, F, c, minus ? rm : rp, rawnb, ii, dir, minus ? -1 : +1, dt, K);
-        // mass-flux stencil of this face by phase (gas first): neighbour
-        // values, or the cell's own current value where the slot is the cell
-        const int rfar = minus ? rmm : rpp;
-        const bool sm = rm == c, sp = rp == c, sfar = rfar == c;
-        DensK<NC, SHD> Dk(dcols + threadIdx.x);
-        Dk.cm(0) = ldro<RO>(F.rgp + rm); Dk.cp(0) = ldro<RO>(F.rgp + rp); Dk.cf(0) = mus ? ldro<RO>(F.rgp + rfar) : 0.0;
-#pragma unroll
-        for (int l = 2; l <= nph; ++l) {
-            const double *D_ = F.rlk + (size_t)(l - 2) * n;
-            Dk.cm(l - 1) = ldro<RO>(D_ + rm); Dk.cp(l - 1) = ldro<RO>(D_ + rp);
-            Dk.cf(l - 1) = mus ? ldro<RO>(D_ + rfar) : 0.0;
-        }
-        // opt_inner_loop (iter.f:1255-1547) builds the density stencils once
-        // and updates only their centre: a neighbour slot remapped to the
-        // cell keeps the loop-entry value there
-        Dk.o(0) = F.rgp[c];
-#pragma unroll
-        for (int l = 2; l <= nph; ++l) Dk.o(l - 1) = F.rlk[(size_t)(l - 2) * n + c];
-        const bool stale = P.opt == 2;
-        auto mflux = [&](int ph, double own) {
-            const double slot = stale ? Dk.o(ph) : own;
-            double dm = sm ? slot : Dk.cm(ph), dp = sp ? slot : Dk.cp(ph), df = sfar ? slot : Dk.cf(ph);
-            return minus ? face_mflux(P, g, true, vel[ph], own, dm, df, dp, 0.0, mus)
-                         : face_mflux(P, g, false, vel[ph], own, dm, 0.0, dp, df, mus);
-        };
-        // ---- cell state (identical in every lane) ------------------------------
-        const double rx = D == 2 ? P.inr[i] : 1.0;
-        const double idx_i = P.indx[i], idz_k = P.indz[k], idy_j = D == 3 ? P.indy[j] : 0.0;
-        const double rgpn_c = F.rgpn[c];
-        const CellFaces bf = cell_faces(P, c);  // faces, iter.f:259
-        auto resid = [&](double fe, double fw, double fn, double fs, double ft, double fb, double rgpc) {
-            double resx = (bf.e * fe - bf.w * fw) * idx_i * rx;
-            double resz = (bf.t * ft - bf.b * fb) * idz_k;
-            double resy = D == 3 ? (bf.n * fn - bf.s * fs) * idy_j : 0.0;
-            return rgpc - rgpn_c + dt * bf.ivf * (resx + resy + resz);
-        };
-        double dg;  // calc_res of the stored state (raw W/S/B neighbours)
-        if (D == 3) {
-            int cw = at3(P, max(i - 1, 1), j, k), cs = at3(P, i, max(j - 1, 1), k), cb = at3(P, i, j, max(k - 1, 1));
-            dg = resid(F.rgfe[c], F.rgfe[cw], F.rgfn[c], F.rgfn[cs], F.rgft[c], F.rgft[cb], F.rgp[c]);
-        } else {
-            int cw = at2(P, max(i - 1, 1), k), cb = at2(P, i, max(k - 1, 1));
-            dg = resid(F.rgfe[c], F.rgfe[cw], 0.0, 0.0, F.rgft[c], F.rgft[cb], F.rgp[c]);
-        }
-        double dgorig = dg;
-        const double conv = F.conv[c];
-        double d3 = dg, p3 = F.p[c], abeta = F.abeta[c];
-        // the mixture molecular weight of thermal_eosg (eosg.f:114-137), which
-        // does not change within the loop: summed once, in thermal_eosg's order
-        double mg = 0;
-        for (int ig = 0; ig < P.ng; ++ig) mg = mg + GAS(F.xgc, c, ig) * P.gmw[P.gas_type[ig]];
-        const double tgc = F.tg[c];
-        const double rgas_tg = P.rgas * tgc;
-        int kros = -1;
-        PAdj s = {0, 0, 0, 0, 0, 0};
-        double p = F.p[c], ep = F.ep[c], rog = F.rog[c], rgp = F.rgp[c];
-        double rlk[NC], rlkn[NC], sink[NC];
-#pragma unroll
-        for (int is = 1; is <= ns; ++is) {
-            rlk[is - 1] = F.rlk[(is - 1) * n + c];
-            rlkn[is - 1] = F.rlkn[(is - 1) * n + c];
-            sink[is - 1] = F.sink[(is - 1) * n + c];
-        }
-        double flux[NC];  // this lane's face mass flux by phase (gas first)
-#pragma unroll
-        for (int l = 0; l < NC; ++l) flux[l] = 0.0;
-        // source lanes of the faces (3D: W S B E N T = 0..5; 2D: W B E T = 0..3)
-        const int lW = tb + 0, lE = tb + (D == 3 ? 3 : 2), lB = tb + (D == 3 ? 2 : 1), lT = tb + (D == 3 ? 5 : 3);
-        const int lS = tb + 1, lN = tb + 4;
-        for (int loop = 1; loop <= P.inmax; ++loop) {
-            if (loop > 1 || nit > 1) padjust(s, p, kros, d3, p3, P.omega, abeta);
-            rog = p / rgas_tg * mg;  // thermal_eosg
-            rgp = ep * rog;
-            // this lane's face system (matrix.f:351-630)
-            if (solved) face_assemble<NP>(P, K, minus ? -1 : +1, p, ep, rgp, rlk, vel);
-            // particle mass fluxes and volume fractions (iter.f:778-994)
-#pragma unroll
-            for (int is = 1; is <= ns; ++is) flux[is] = mflux(is, rlk[is - 1]);
-            double rls = 0;
-#pragma unroll
-            for (int is = 1; is <= ns; ++is) {
-                double fW = __shfl_sync(tmask, flux[is], lW), fE = __shfl_sync(tmask, flux[is], lE);
-                double fB = __shfl_sync(tmask, flux[is], lB), fT = __shfl_sync(tmask, flux[is], lT);
-                double fS = 0, fN = 0;
-                if (D == 3) { fS = __shfl_sync(tmask, flux[is], lS); fN = __shfl_sync(tmask, flux[is], lN); }
-                double rlkx = (bf.e * fE - bf.w * fW) * idx_i * rx;
-                double rlkz = (bf.t * fT - bf.b * fB) * idz_k;
-                double rlky = D == 3 ? (bf.n * fN - bf.s * fS) * idy_j : 0.0;
-                double t = rlkn[is - 1] - dt * bf.ivf * (rlkx + rlky + rlkz);
-                t = t + dt * bf.ivf * sink[is - 1];
-                double v = fmax(0.0, t);
-                rlk[is - 1] = v;
-                rls = rls + v * P.inrl[is];
-            }
-            ep = 1.0 - rls;
-            if (rls > 1.0 && q == 0) atomicAdd(&F.counters[2], 1);
-            rgp = ep * rog;
-            // gas mass flux and continuity residual (iter.f:597-771)
-            flux[0] = mflux(0, rgp);
-            {
-                double fW = __shfl_sync(tmask, flux[0], lW), fE = __shfl_sync(tmask, flux[0], lE);
-                double fB = __shfl_sync(tmask, flux[0], lB), fT = __shfl_sync(tmask, flux[0], lT);
-                double fS = 0, fN = 0;
-                if (D == 3) { fS = __shfl_sync(tmask, flux[0], lS); fN = __shfl_sync(tmask, flux[0], lN); }
-                dg = resid(fE, fW, fN, fS, fT, fB, rgp);
-            }
-            if (fabs(dg) > conv || fabs(dg) >= fabs(dgorig)) {
-                if (nit == 1 && loop == 1) dgorig = dg;
-                d3 = dg;
-            } else if (fabs(dg) <= conv) {
-                break;
-            }
-        }
-        // ---- final values -----------------------------------------------------
-        {
-            // face mass fluxes (every face, as calc_*_mass_flux writes them)
-            double *gfa = dir == 0 ? F.rgfe : (dir == 1 ? F.rgfn : F.rgft);
-            double *sfa = dir == 0 ? F.rsfe : (dir == 1 ? F.rsfn : F.rsft);
-            gfa[fcell] = flux[0];
-#pragma unroll
-            for (int is = 1; is <= ns; ++is) sfa[(size_t)(is - 1) * n + fcell] = flux[is];
-            if (solved) {
-                gvel[fcell] = vel[0];
-#pragma unroll
-                for (int l = 2; l <= nph; ++l) svel[(l - 2) * n + fcell] = vel[l - 1];
-            }
-            mark_dirty(dirty, rawnb);
-        }
-        if (q == 0) {
-            F.p[c] = p; F.rog[c] = rog; F.rgp[c] = rgp; F.ep[c] = ep;
-#pragma unroll
-            for (int is = 1; is <= ns; ++is) F.rlk[(is - 1) * n + c] = rlk[is - 1];
-            F.abeta[c] = abeta;
-            mark_dirty(dirty, c);
-        }
-    }
+    for (int w = warp * TPW + tw; w < nwork; w += nwarps * TPW)
+        inner_team_cell<NP, D, RO>(P, F, dt, nit, list[w], dirty, q, tb, tmask, kcols, dcols);
 }
 
 template <int NP, int D>
