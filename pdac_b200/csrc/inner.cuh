@@ -556,16 +556,18 @@ __global__ void __launch_bounds__(TPB_RESID) k_resid_test(Prm P, Fld F, double d
 // so testing and iterating them in this order gives the bits of the
 // three-launch form.  The colour's set bits of a word are cleared
 // atomically before its cells are tested: other warps set bits of the
-// neighbouring cells meanwhile.  Adds the unconverged cells to wcount[col]
-// and the tested ones to wcount[3 + col].  RO as in ldro.
+// neighbouring cells meanwhile.  Appends the unconverged cells to the
+// colour's worklist (work, wcount[col] long; the cells the last sweep left
+// unconverged, as pdac_gpu_unconverged_cells reports them) and adds the
+// tested ones to wcount[3 + col].  RO as in ldro.
 template <int NP, int D, bool RO>
 __device__ __forceinline__ void fused_phase(const Prm &P, const Fld &F, double dt, int nit, int colour,
-                                            unsigned *dirty, int *wcount, unsigned warp, unsigned nwarps) {
+                                            unsigned *dirty, int *wcount, int *work, unsigned warp, unsigned nwarps) {
     const int lane = threadIdx.x & 31;
     __shared__ int wlist[KS / 32][32];
     int *const mylist = wlist[threadIdx.x >> 5];
     const unsigned nwords = ((unsigned)P.ncell + 31u) / 32u;
-    int nwork_sum = 0, ntest_sum = 0;
+    int ntest_sum = 0;
     for (unsigned t = warp; t < nwords; t += nwarps) {  // uniform across the warp
         const unsigned w = __ldcg(dirty + t);
         const int c = (int)(32u * t) + lane;
@@ -588,14 +590,16 @@ __device__ __forceinline__ void fused_phase(const Prm &P, const Fld &F, double d
         ntest_sum += __popc(__ballot_sync(0xffffffffu, cand));
         __syncwarp();
         const int nwork = __popc(um);
-        nwork_sum += nwork;
-        if (nwork) inner_team_run<NP, D, RO>(P, F, dt, nit, mylist, nwork, dirty, 0, 1);
+        if (nwork) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(wcount + colour, nwork);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (unconv) work[base + __popc(um & ((1u << lane) - 1u))] = c;
+            inner_team_run<NP, D, RO>(P, F, dt, nit, mylist, nwork, dirty, 0, 1);
+        }
         __syncwarp();  // the list is read before the next word overwrites it
     }
-    if (lane == 0) {
-        if (nwork_sum) atomicAdd(wcount + colour, nwork_sum);
-        if (ntest_sum) atomicAdd(wcount + 3 + colour, ntest_sum);
-    }
+    if (lane == 0 && ntest_sum) atomicAdd(wcount + 3 + colour, ntest_sum);
 }
 
 // The whole outer sweep loop of iter (iter.f:204-410) in one cooperative
@@ -622,7 +626,7 @@ __global__ void __launch_bounds__(128, PDAC_INNER_MINB(NP)) k_iter_coop(Prm P, F
         if (blockIdx.x == 0 && threadIdx.x < 9) W.wcount[threadIdx.x] = 0;
         g.sync();
         for (int col = 0; col < 3; ++col) {
-            fused_phase<NP, D, false>(P, F, dt, nit, col, W.dirty, W.wcount, warp, nwarps);
+            fused_phase<NP, D, false>(P, F, dt, nit, col, W.dirty, W.wcount, W.work + col * W.wstride, warp, nwarps);
             g.sync();
         }
         const long unconverged = (long)__ldcg(W.wcount) + __ldcg(W.wcount + 1) + __ldcg(W.wcount + 2);
