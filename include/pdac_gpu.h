@@ -206,6 +206,19 @@ const char *pdac_gpu_last_error(const pdac_ctx *ctx);
 /* ---- state transfer ---------------------------------------------------- */
 int pdac_gpu_upload_state(pdac_ctx *ctx, const pdac_state_view *s);
 int pdac_gpu_download_state(pdac_ctx *ctx, pdac_state_view *s);
+/* pdac_gpu_download_state into out followed by pdac_gpu_upload_state from
+ * in, as one call whose two copy directions overlap: field by field, each
+ * field's upload starts once that field's download is done, so out and in
+ * may be the same view (a host that keeps the module arrays of
+ * press.f/velocity.f/dens.f/temp.f in step with the device hands back what
+ * it read, or what it changed field by field), and the download of the next
+ * field runs beside it.  Fields of out may be NULL (not read back); in
+ * needs the fields pdac_gpu_upload_state needs.  Returns with both
+ * directions complete and the uploaded fields checked (PDAC_ERR_NONFINITE
+ * as for an upload).  No counterpart in the reference, whose host arrays
+ * are the state; it is the hand-off of those arrays between two time
+ * steps (prog.f:162-331) when the host keeps its own copy.                */
+int pdac_gpu_exchange_state(pdac_ctx *ctx, pdac_state_view *out, const pdac_state_view *in);
 
 /* ---- per-call mirrors of the time loop (prog.f:143-417) --------------- */
 /* boundary (bdry.f:22-726) at time-step number 'sweep' (1-based)          */

@@ -103,6 +103,11 @@ struct pdac_ctx {
     // accumulated device ms of the groups [flux passes, stage kernels,
     // gas-enthalpy wavefronts, final rhs + coefficients + solve]
     cudaEvent_t xev[9];
+    // pdac_gpu_exchange_state: its upload stream and one event per field,
+    // created at its first call
+    cudaStream_t up_stream = nullptr;
+    cudaEvent_t fev[20] = {};
+    cudaEvent_t up_done = nullptr;
     double ex_ms[4] = {0, 0, 0, 0};
     long long ex_calls = 0;
     // gas-enthalpy wavefront on hyperplane-ordered records: the cooperative
@@ -1085,6 +1090,9 @@ int pdac_gpu_destroy(pdac_ctx *ctx) {
     for (auto &e : ctx->cev) cudaEventDestroy(e);
     for (auto &e : ctx->user_ev) cudaEventDestroy(e);
     for (auto &e : ctx->xev) cudaEventDestroy(e);
+    for (auto &e : ctx->fev) if (e) cudaEventDestroy(e);
+    if (ctx->up_done) cudaEventDestroy(ctx->up_done);
+    if (ctx->up_stream) cudaStreamDestroy(ctx->up_stream);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return PDAC_OK;
@@ -1154,18 +1162,28 @@ static int check_finite(pdac_ctx *ctx, const std::vector<std::pair<const double 
     return fail(ctx, PDAC_ERR_NONFINITE, std::string(where) + ": non-finite value in " + which);
 }
 
-static int xfer_state(pdac_ctx *ctx, pdac_state_view *s, bool up) {
-    if (!ctx || !s) return PDAC_ERR_ARG;
+// the state fields of a view with their device arrays, element counts and
+// whether an upload needs them
+struct XField { double *h; double *d; size_t cnt; bool need; const char *name; };
+static constexpr int kStateFields = 18;
+static void state_fields(pdac_ctx *ctx, const pdac_state_view *s, XField (&xs)[kStateFields]) {
     size_t n = ctx->ncell, ns = ctx->ns, ng = ctx->ng;
     Fld &F = ctx->F;
-    struct X { double *h; double *d; size_t cnt; bool need; const char *name; };
-    X xs[] = {{s->p, F.p, n, true, "p"}, {s->ep, F.ep, n, true, "ep"}, {s->rog, F.rog, n, true, "rog"},
-              {s->rgp, F.rgp, n, true, "rgp"}, {s->tg, F.tg, n, true, "tg"}, {s->sieg, F.sieg, n, true, "sieg"},
-              {s->cg, F.cg, n, true, "cg"}, {s->ug, F.ug, n, true, "ug"}, {s->vg, F.vg, n, ctx->d3, "vg"},
-              {s->wg, F.wg, n, true, "wg"}, {s->rlk, F.rlk, n * ns, true, "rlk"}, {s->ts, F.ts, n * ns, true, "ts"},
-              {s->sies, F.sies, n * ns, true, "sies"}, {s->us, F.us, n * ns, true, "us"},
-              {s->vs, F.vs, n * ns, ctx->d3, "vs"}, {s->ws, F.ws, n * ns, true, "ws"},
-              {s->ygc, F.ygc, n * ng, true, "ygc"}, {s->xgc, F.xgc, n * ng, true, "xgc"}};
+    XField v[kStateFields] = {
+        {s->p, F.p, n, true, "p"}, {s->ep, F.ep, n, true, "ep"}, {s->rog, F.rog, n, true, "rog"},
+        {s->rgp, F.rgp, n, true, "rgp"}, {s->tg, F.tg, n, true, "tg"}, {s->sieg, F.sieg, n, true, "sieg"},
+        {s->cg, F.cg, n, true, "cg"}, {s->ug, F.ug, n, true, "ug"}, {s->vg, F.vg, n, ctx->d3, "vg"},
+        {s->wg, F.wg, n, true, "wg"}, {s->rlk, F.rlk, n * ns, true, "rlk"}, {s->ts, F.ts, n * ns, true, "ts"},
+        {s->sies, F.sies, n * ns, true, "sies"}, {s->us, F.us, n * ns, true, "us"},
+        {s->vs, F.vs, n * ns, ctx->d3, "vs"}, {s->ws, F.ws, n * ns, true, "ws"},
+        {s->ygc, F.ygc, n * ng, true, "ygc"}, {s->xgc, F.xgc, n * ng, true, "xgc"}};
+    for (int q = 0; q < kStateFields; ++q) xs[q] = v[q];
+}
+
+static int xfer_state(pdac_ctx *ctx, pdac_state_view *s, bool up) {
+    if (!ctx || !s) return PDAC_ERR_ARG;
+    XField xs[kStateFields];
+    state_fields(ctx, s, xs);
     std::vector<std::pair<const double *, size_t>> sent;
     std::vector<std::string> names;
     for (auto &x : xs) {
@@ -1200,6 +1218,45 @@ static int check_step_state(pdac_ctx *ctx) {
 
 int pdac_gpu_upload_state(pdac_ctx *ctx, const pdac_state_view *s) { return xfer_state(ctx, const_cast<pdac_state_view *>(s), true); }
 int pdac_gpu_download_state(pdac_ctx *ctx, pdac_state_view *s) { return xfer_state(ctx, s, false); }
+
+// pdac_gpu_exchange_state: pdac_gpu_download_state into `out`, then
+// pdac_gpu_upload_state from `in`, with the two directions overlapped.
+// Field f is copied device -> host on the context's stream (after every
+// earlier call's kernels) and host -> device on a second stream that first
+// waits for that download, so the upload of field f may read the buffer its
+// download has just filled (out == in) and overwrites nothing the device or
+// the download still needs, while the download of field f + 1 runs beside
+// it on the other copy engine.  The context's stream waits for the last
+// upload; the uploaded fields are checked as pdac_gpu_upload_state checks
+// them, and the call returns with both directions complete.
+int pdac_gpu_exchange_state(pdac_ctx *ctx, pdac_state_view *out, const pdac_state_view *in) {
+    if (!ctx || !out || !in) return PDAC_ERR_ARG;
+    XField xo[kStateFields], xi[kStateFields];
+    state_fields(ctx, out, xo);
+    state_fields(ctx, in, xi);
+    for (int q = 0; q < kStateFields; ++q)
+        if (!xi[q].h && xi[q].need) return fail(ctx, PDAC_ERR_ARG, "exchange: a required state field of in is NULL");
+    if (!ctx->up_stream) {
+        CK(cudaStreamCreateWithFlags(&ctx->up_stream, cudaStreamNonBlocking));
+        for (auto &e : ctx->fev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ctx->up_done, cudaEventDisableTiming));
+    }
+    cudaStream_t a = ctx->stream, b = ctx->up_stream;
+    std::vector<std::pair<const double *, size_t>> sent;
+    std::vector<std::string> names;
+    for (int q = 0; q < kStateFields; ++q) {
+        const size_t bytes = xi[q].cnt * sizeof(double);
+        if (xo[q].h) CK(cudaMemcpyAsync(xo[q].h, xo[q].d, bytes, cudaMemcpyDeviceToHost, a));
+        CK(cudaEventRecord(ctx->fev[q], a));
+        if (!xi[q].h) continue;
+        CK(cudaStreamWaitEvent(b, ctx->fev[q], 0));
+        CK(cudaMemcpyAsync(xi[q].d, xi[q].h, bytes, cudaMemcpyHostToDevice, b));
+        if (xi[q].cnt) { sent.push_back({xi[q].d, xi[q].cnt}); names.push_back(xi[q].name); }
+    }
+    CK(cudaEventRecord(ctx->up_done, b));
+    CK(cudaStreamWaitEvent(a, ctx->up_done, 0));
+    return check_finite(ctx, sent, names, "exchange");
+}
 
 // the kernels of boundary on stream st (also inside a whole-step graph)
 static int enqueue_boundary(pdac_ctx *ctx, cudaStream_t st) {

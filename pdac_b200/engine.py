@@ -45,6 +45,8 @@ def lib():
         L.pdac_gpu_upload_state.restype = C.c_int
         L.pdac_gpu_download_state.argtypes = [P, C.POINTER(abi.PdacStateView)]
         L.pdac_gpu_download_state.restype = C.c_int
+        L.pdac_gpu_exchange_state.argtypes = [P, C.POINTER(abi.PdacStateView), C.POINTER(abi.PdacStateView)]
+        L.pdac_gpu_exchange_state.restype = C.c_int
         L.pdac_gpu_phase_times.argtypes = [P, C.POINTER(C.c_double)]
         L.pdac_gpu_phase_times.restype = C.c_int
         L.pdac_gpu_set_vent_factors.argtypes = [P, C.POINTER(C.c_double), C.c_int]
@@ -64,7 +66,7 @@ def lib():
 
 EXPORTED = (
     "pdac_gpu_create", "pdac_gpu_destroy", "pdac_gpu_last_error", "pdac_gpu_upload_state",
-    "pdac_gpu_download_state", "pdac_gpu_boundary", "pdac_gpu_fieldn", "pdac_gpu_tilde", "pdac_gpu_iter",
+    "pdac_gpu_download_state", "pdac_gpu_exchange_state", "pdac_gpu_boundary", "pdac_gpu_fieldn", "pdac_gpu_tilde", "pdac_gpu_iter",
     "pdac_gpu_initialize_fieldn", "pdac_gpu_explicit_iter", "pdac_gpu_sgsg", "pdac_gpu_sgss",
     "pdac_gpu_ygas", "pdac_gpu_htilde", "pdac_gpu_ftem", "pdac_gpu_step", "pdac_gpu_set_vent_factors",
     "pdac_gpu_get_array", "pdac_gpu_mass_totals", "pdac_gpu_phase_times", "pdac_gpu_stats",
