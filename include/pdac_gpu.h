@@ -109,7 +109,9 @@ typedef struct pdac_cfg {
     int    pmodel, drag_model, icpc;
     double tref;
     int    gas_viscosity, part_viscosity, repulsive_model;
-    int    iturb;               /* 0 none, 1 Smagorinsky sub-grid model      */
+    int    iturb;               /* 0 none, 1 Smagorinsky sub-grid model, 2
+                                   the same with ground roughness (zrough,
+                                   topo_c below)                             */
     int    modturbo;            /* 1 static Smagorinsky, 2 dynamic (Germano,
                                    turbo.f:180-349; 2D falls back to 1)      */
     int    iss;                 /* 1 particle sub-grid stress (turbo.f:437)  */
@@ -179,6 +181,16 @@ typedef struct pdac_cfg {
     const double *x, *xb, *y, *yb, *z, *zb; /* cell-centre and face coordinates
                                        (nx, nx, ny, ny, nz, nz), as the
                                        topography translated them            */
+
+    /* ground roughness of the sub-grid model (iturb = 2; turbo.f:72-101,
+     * roughness.f:12-36): the &topography namelist's zrough (m) and the
+     * level of the ground under each column, topo_c(i) / topo2d_c(i, j) as
+     * set-up leaves them (export_topography, topo.f:1114-1160, overwritten by
+     * the immersed boundaries' interpolation, immb.f:117-119, 227-230): nx
+     * values in 2D, nx * ny in 3D (i fastest).  Read at create; topo_c may
+     * be NULL unless iturb = 2.                                              */
+    double        zrough;
+    const double *topo_c;
 } pdac_cfg;
 
 /*

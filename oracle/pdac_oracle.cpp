@@ -2166,6 +2166,7 @@ int pdac_oracle_create(const pdac_cfg *cfg, void **out) {
     o->cfg.ib_faces = nullptr; o->cfg.ib_ivf = nullptr;
     for (int a = 0; a < 3; ++a) { o->cfg.ib_num[a] = nullptr; o->cfg.ib_fp[a] = nullptr; o->cfg.ib_nsl[a] = nullptr; }
     o->cfg.x = o->cfg.xb = o->cfg.y = o->cfg.yb = o->cfg.z = o->cfg.zb = nullptr;
+    o->cfg.topo_c = nullptr;
     ib_setup(*o, cfg);
     if (ib_check(*o) != PDAC_OK) {
         delete[] vl;
@@ -2176,7 +2177,7 @@ int pdac_oracle_create(const pdac_cfg *cfg, void **out) {
     build_tables(*o);
     if (o->d3) build_tables3(*o);
     alloc(*o);
-    les_setup(*o);
+    les_setup(*o, cfg);
     sink_setup(*o);
     *out = o;
     return PDAC_OK;

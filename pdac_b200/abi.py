@@ -68,6 +68,7 @@ class PdacCfg(C.Structure):
         ("immb", C.c_int), ("ib_faces", _ip), ("ib_ivf", _dp),
         ("ib_num", _ip * 3), ("ib_nfp", C.c_int * 3), ("ib_fp", _ip * 3), ("ib_nsl", _dp * 3),
         ("x", _dp), ("xb", _dp), ("y", _dp), ("yb", _dp), ("z", _dp), ("zb", _dp),
+        ("zrough", C.c_double), ("topo_c", _dp),
     ]
 
 

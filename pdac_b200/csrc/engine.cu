@@ -394,8 +394,9 @@ int validate(const pdac_cfg *c, std::string &why) {
         return 1;
     }
     if (c->time_integration != 0 && c->time_integration != 1) { why = "time_integration must be 0 or 1"; return 1; }
-    if (c->iturb != 0 && c->iturb != 1) { why = "iturb must be 0 or 1 (iturb = 2 needs the topography's roughness)"; return 1; }
-    if (c->iturb == 1 && c->modturbo != 1 && c->modturbo != 2) {
+    if (c->iturb < 0 || c->iturb > 2) { why = "iturb must be 0, 1 or 2"; return 1; }
+    if (c->iturb == 2 && !c->topo_c) { why = "iturb = 2 needs topo_c, the ground level of every column"; return 1; }
+    if (c->iturb >= 1 && c->modturbo != 1 && c->modturbo != 2) {
         why = "modturbo must be 1 (static Smagorinsky) or 2 (dynamic; static in 2D, as turbo.f:180-185)";
         return 1;
     }
@@ -965,19 +966,36 @@ int pdac_gpu_create(const pdac_cfg *cfg, pdac_ctx **out) {
     // reference's (ncell, n) column-major arrays; the stride pads slot ends
     F.counters = ctx->d_counters;
     if (lt) {
-        // turbulence_setup (turbo.f:42-108), iturb = 1: smag = (cmut delta)^2,
-        // delta = sqrt(dz dx) in 2D, (dz dy dx)^(1/3) times anis in 3D
+        // turbulence_setup (turbo.f:42-108): smag = lm^2 with the
+        // Smagorinsky length lm = cmut delta, delta = sqrt(dz dx) in 2D and
+        // (dz dy dx)^(1/3) in 3D (times anis in 3D).  With iturb = 2 a cell
+        // whose centre is zsgs = z(k) - topo_c above the ground matches it
+        // with the roughness length lb = 0.4 (zsgs + zrough):
+        // lm = sqrt(1 / (1 / ls^2 + 1 / lb^2)); a cell at or below the ground
+        // keeps the lm of the cell before it in the loop, as the reference's
+        // loop variable does (0 before the first assigned cell, which the
+        // reference leaves undefined; only fluid cells, all above the
+        // ground, use smag)
         std::vector<double> smag(n);
+        double lm = 0.0;
+        auto rough = [&](double ls, double zsgs) {
+            if (cfg->iturb == 1) { lm = ls; return; }
+            if (zsgs > 0.0) {
+                double lb = 0.4 * (zsgs + cfg->zrough);
+                lm = std::sqrt(1.0 / (1.0 / (ls * ls) + 1.0 / (lb * lb)));
+            }
+        };
         for (int c = 0; c < n; ++c) {
             int i = c % nx + 1, j = (c / nx) % ny + 1, k = c / (nx * ny) + 1;
-            double lm;
             if (!ctx->d3) {
                 double delt = std::sqrt(dz[k] * dx[i]);
-                lm = cfg->cmut * delt;
+                double ls = cfg->cmut * delt;
+                rough(ls, cfg->iturb == 2 ? cfg->z[k - 1] - cfg->topo_c[i - 1] : 0.0);
                 smag[c] = lm * lm;
             } else {
                 double delt = std::pow(dz[k] * dy[j] * dx[i], 1.0 / 3.0);
-                lm = cfg->cmut * delt;
+                double ls = cfg->cmut * delt;
+                rough(ls, cfg->iturb == 2 ? cfg->z[k - 1] - cfg->topo_c[(size_t)(j - 1) * nx + (i - 1)] : 0.0);
                 smag[c] = lm * lm;
                 // anis, turbo.f:670-700
                 double deltamax = std::max(dx[i], std::max(dy[j], dz[k]));

@@ -1,9 +1,11 @@
 // les.cuh -- the sub-grid turbulence model of turbo.f on the device
 // (iturb = 1: static Smagorinsky, modturbo = 1, or the dynamic model in 3D,
-// modturbo = 2; iss = 1 particle sub-grid stress).
+// modturbo = 2; iturb = 2 the same with the ground-roughness mixing length;
+// iss = 1 particle sub-grid stress).
 //
-// smag = (cmut delta)^2 (x anis in 3D) is fixed per cell at set-up on the
-// host (turbulence_setup, turbo.f:42-108).  Each step k_sgsg sets the
+// smag = lm^2 (x anis in 3D), lm = cmut delta or, with iturb = 2, matched
+// with the roughness length, is fixed per cell at set-up on the host
+// (turbulence_setup, turbo.f:42-108).  Each step k_sgsg sets the
 // turbulent viscosity and conductivity of the fluid cells from the strain
 // rate (sgsg, turbo.f:145-349) and k_sgss the particle sub-grid viscosity
 // (sgss, turbo.f:437-475).  The consumers add the molecular values in place

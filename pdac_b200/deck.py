@@ -397,9 +397,9 @@ class Deck:
     def check(self):
         """Options of the reference that this engine does not implement."""
         bad = []
-        if self["iturb"] not in (0, 1):
-            bad.append("iturb=2 (sub-grid model with ground roughness, needs topography)")
-        if self["iturb"] == 1 and self["modturbo"] not in (1, 2):
+        if self["iturb"] not in (0, 1, 2):
+            bad.append("iturb other than 0, 1 or 2")
+        if self["iturb"] >= 1 and self["modturbo"] not in (1, 2):
             bad.append("modturbo other than 1 or 2")
         if self["iss"] not in (0, 1):
             bad.append("iss>1")

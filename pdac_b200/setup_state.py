@@ -647,6 +647,18 @@ class Case:
         for name in ("x", "xb", "y", "yb", "z", "zb"):
             keep[name] = np.ascontiguousarray(getattr(self, name), dtype=np.float64)
             setattr(c, name, abi.dptr(keep[name]))
+        # the ground level under each column for the roughness length of the
+        # sub-grid model (turbo.f:72-101): export_topography's, or the
+        # immersed boundaries' interpolated profile / DEM when they replaced it
+        # (immb.f:117-119, 227-230); i fastest
+        if self.ib is not None:
+            tc = np.asarray(self.ib.topo_c, dtype=np.float64)
+            tc = tc.T.reshape(-1) if tc.ndim == 2 else tc.reshape(-1)
+        else:
+            tc = np.asarray(self.topo_c, dtype=np.float64).reshape(-1)
+        keep["topo_c"] = np.ascontiguousarray(tc)
+        c.topo_c = abi.dptr(keep["topo_c"])
+        c.zrough = float(d["zrough"])
         c.immb = 0
         if self.ib is not None:
             ib = self.ib

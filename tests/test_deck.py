@@ -98,7 +98,7 @@ def test_plume_vent_and_flags():
 
 def test_unsupported_options_are_rejected():
     d = configs.plume_2d()
-    d.set("model", iturb=2)
+    d.set("model", iturb=3)
     with pytest.raises(ValueError, match="iturb"):
         Case(d)
     d = configs.plume_3d(nx=8, ny=8, nz=8)
@@ -115,6 +115,17 @@ def test_sub_grid_model_reaches_the_configuration():
     d = configs.plume_3d(nx=8, ny=8, nz=8)
     d.set("model", iturb=1, modturbo=2)
     assert Case(d).cfg().modturbo == 2
+
+
+def test_ground_roughness_reaches_the_configuration():
+    d = configs.plume_2d()
+    d.set("model", iturb=2)
+    d.set("topography", zrough=0.5)
+    case = Case(d)
+    cfg = case.cfg()
+    assert cfg.iturb == 2 and cfg.zrough == 0.5
+    # flat ground: the top of the no-slip bottom row under every column
+    assert [cfg.topo_c[i] for i in range(case.nx)] == [case.zb[0]] * case.nx
 
 
 def test_explicit_solver_selection():

@@ -141,3 +141,35 @@ def test_forcing_point_checks_reject_bad_tables(tmp_path):
     assert e.value.status == abi.PDAC_ERR_CONFIG
     with pytest.raises(RuntimeError, match="config"):
         pyoracle.Oracle(case)
+
+
+@pytest.mark.parametrize("builder,immb", [("small_2d_topo", 1), ("small_3d_topo", 1), ("small_3d_topo", 0)])
+def test_sub_grid_model_with_ground_roughness(tmp_path, builder, immb):
+    """iturb = 2 (turbo.f:72-101): the mixing length of every cell equals the
+    oracle's bit for bit, and four steps with the static model and the
+    particle sub-grid stress agree over the fluid cells to 1e-9, the
+    model's viscosities included, with the same sweep counts."""
+    import pyoracle
+    from pdac_b200 import configs
+    from pdac_b200.engine import Engine
+    from pdac_b200.setup_state import Case
+    d = getattr(configs, builder)(tmp_path, immb=immb)
+    d.set("model", iturb=2, modturbo=1, iss=1)
+    d.set("topography", zrough=2.0)
+    case = Case(d)
+    eng = Engine(case)
+    ora = pyoracle.Oracle(case, order=pyoracle.ORDER_COLORED)
+    assert np.array_equal(eng.get("smag"), ora.get("smag"))
+    fields = STEP_FIELDS + (("vg", "vs") if case.is3d else ())
+    fluid = (case.flag & 1) == 1
+    for s in range(1, 5):
+        n1, n2 = eng.step(s), ora.step(s)
+        assert n1 == n2, f"step {s}: outer sweeps gpu {n1} oracle {n2}"
+        got, ref = eng.download(), ora.get_state()
+        errs, bad = compare_state(got, ref, fields, TOL_STEP, case.nsolid, case.ncell, cells=fluid)
+        assert not bad, f"step {s}: {bad}"
+        for name in ("mugt", "kapgt", "must"):
+            e = rel_linf(eng.get(name), ora.get(name))
+            assert e <= TOL_STEP, f"step {s}: {name} {e}"
+    eng.close()
+
