@@ -39,6 +39,9 @@ def write(case, path):
     d = case.deck
     cfg = case.cfg()
     mode = str(d["restart_mode"]).strip()
+    if mode == "outp_recover":
+        # the case file carries no start time or output counter
+        raise ValueError("restart_mode 'outp_recover' runs through the Python driver (pdac_b200.files.run)")
     with open(path, "wb") as f:
         f.write(MAGIC)
         f.write(bytes(cfg))

@@ -66,6 +66,16 @@ def mole(ygc, gas_type):
     return np.stack([ygc[ig] / g[ig] * molinv for ig in range(ygc.shape[0])])
 
 
+def mas(xgc, gas_type):
+    """Molar to mass fractions, eosg.f:70-99; xgc has shape (ngas, ...)."""
+    g = GMW[np.asarray(gas_type) - 1].reshape((-1,) + (1,) * (xgc.ndim - 1))
+    mass = np.zeros(xgc.shape[1:])
+    for ig in range(xgc.shape[0]):
+        mass = mass + xgc[ig] * g[ig]
+    massinv = np.where(np.abs(mass) < 1e-10, 0.0, 1.0 / np.where(mass == 0, 1.0, mass))
+    return np.stack([xgc[ig] * g[ig] * massinv for ig in range(xgc.shape[0])])
+
+
 def _powi(x, n):
     """x**n for an integer n by repeated squaring, as Fortran evaluates an
     integer power."""

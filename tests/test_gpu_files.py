@@ -319,3 +319,41 @@ def test_unformatted_output_with_mixture_fields(tmp_path):
     for r, a in zip(recs[-len(tail):], tail):
         np.testing.assert_array_equal(np.frombuffer(r, dtype="<f4"), a.astype(np.float32))
     eng.close()
+
+
+@pytest.mark.parametrize("formatted", [False, True])
+def test_outp_recover_continues_a_run(tmp_path, formatted):
+    """restart_mode = 'outp_recover' (setup.f:151-155): files.run writes
+    output.0000 .. output.0002; a second run with nfil = 1 starts from the
+    fields of output.0001 (outp_recover, cnvert with itd > 2) at that file's
+    time, writes output.0002 next, and its steps agree with the oracle's
+    from the same recovered state (same sweeps, 1e-9)."""
+    import pyoracle
+    from pdac_b200 import configs, files
+    from pdac_b200.engine import Engine
+    from pdac_b200.setup_state import Case
+    d = configs.small_2d()
+    dt = d["dt"]
+    d.set("control", tpr=2 * dt, tdump=100 * dt, tstop=1.0, formatted_output=formatted, formatted_input=formatted)
+    eng = Engine(Case(d))
+    files.run(eng, str(tmp_path), max_steps=4)
+    eng.close()
+    d.set("control", restart_mode="outp_recover", nfil=1)
+    case = Case(d)
+    t_file, st = files.recover_output(case, str(tmp_path / "output.0001"))
+    assert t_file == pytest.approx(2 * dt, rel=1e-6)
+    eng2 = Engine(case)
+    t, nfil, sweep = files.run(eng2, str(tmp_path), max_steps=2)
+    assert sweep == 4 and nfil == 3
+    # the same recovered state through both, two steps
+    eng3 = Engine(case, upload=False)
+    eng3.upload(st)
+    ora = pyoracle.Oracle(case, order=pyoracle.ORDER_COLORED)
+    ora.set_state(st)
+    for s in (3, 4):
+        assert eng3.step(s) == ora.step(s)
+        errs, bad = compare_state(eng3.download(), ora.get_state(), STEP_FIELDS, 1e-9, case.nsolid, case.ncell,
+                                  cells=(case.flag & 1) == 1)
+        assert not bad, f"step {s}: {bad}"
+    eng2.close()
+    eng3.close()
